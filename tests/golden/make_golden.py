@@ -1,0 +1,195 @@
+"""Generate golden fixtures by running the reference solver itself.
+
+Run in the build container, where the reference source tree is available:
+
+    python tests/golden/make_golden.py /root/reference/src
+
+It imports the reference package from the given source directory, runs every
+case of ``cases.py`` on the reference NumPy float64 backend (plus the float32
+pin of the reference's own FP32 test), and writes compressed ``.npz``
+fixtures next to this script.  The fixtures travel with the repository; no
+test reads the reference at run time.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+
+import cases as C  # noqa: E402
+
+
+def _import_reference(src: str):
+    sys.path.insert(0, src)
+    import ionosphere_fdtd  # noqa: F401
+    from ionosphere_fdtd import mesh as rmesh
+    from ionosphere_fdtd import solver as rsolver
+    from ionosphere_fdtd import sources as rsources
+    from ionosphere_fdtd import surface_impedance as rsi
+    from ionosphere_fdtd import plasma as rplasma
+    from ionosphere_fdtd import materials as rmat
+    from ionosphere_fdtd import data_artifacts as rdata
+    from ionosphere_fdtd.backends import numpy_backend as rnb
+
+    return rmesh, rsolver, rsources, rsi, rplasma, rmat, rdata, rnb
+
+
+def _sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _provenance(rdata):
+    return rdata.DatasetProvenance(
+        dataset_id="golden.synthetic-plasma.v1",
+        title="Synthetic plasma for parity fixtures",
+        version="1",
+        source_url="https://example.invalid/golden-plasma",
+        citation="Synthetic fixture.",
+        license="CC0-1.0",
+        retrieved_at="2026-12-01T00:00:00Z",
+        source_sha256="0" * 64,
+        coordinate_reference_system="geocentric Cartesian",
+        variables=(
+            rdata.VariableProvenance("B", "T", "T", "identity"),
+            rdata.VariableProvenance("number_density", "m^-3", "m^-3", "identity"),
+            rdata.VariableProvenance("collision_frequency", "Hz", "Hz", "identity"),
+        ),
+    )
+
+
+def build_reference(case: dict, mods, dtype: str = "float64"):
+    rmesh, rsolver, rsources, rsi, rplasma, rmat, rdata, _ = mods
+    cfg = rsolver.SimulationConfig(**case["config"])
+    mesh = rmesh.build_geodesic_mesh(cfg.subdivision)
+    mat = case.get("material", "default")
+    if mat == "default":
+        material = None
+    elif mat == "profile":
+        material = C.ProfileMaterial()
+    elif mat == "patchy":
+        material = C.PatchyMaterial()
+    else:
+        material = rmat.EarthIonosphereMaterial(**mat[1])
+    source = None
+    spec = case.get("source")
+    if spec is not None:
+        spec = dict(spec)
+        kind = spec.pop("kind")
+        if "seed_vertex" in spec:
+            lat, lon = C.vertex_lat_lon(mesh.vertices, C.source_vertex(mesh.n_vertices, spec.pop("seed_vertex")))
+            spec.update(latitude_deg=lat, longitude_deg=lon)
+        source = (rsources.TangentialGaussianCurrent if kind == "tangential" else rsources.GaussianCurrent)(**spec)
+    surface = None
+    sspec = case.get("surface")
+    if sspec is not None:
+        if sspec["conductivity"] == "scalar":
+            surface = rsi.ConductiveHalfSpaceSurface(sspec["value"])
+        else:
+            surface = rsi.ConductiveHalfSpaceSurface(C.smooth_log_normal(mesh.edge_midpoints(), sspec["seed"]))
+    plasma = None
+    pspec = case.get("plasma")
+    if pspec is not None:
+        alt = np.linspace(cfg.minimum_altitude_m, cfg.maximum_altitude_m, cfg.radial_cells + 1)
+        mids = 0.5 * (alt[:-1] + alt[1:])
+        shape = (mesh.n_faces, len(mids))
+        if pspec["kind"] == "profile":
+            magnetic, density, collision = C.profile_plasma_arrays(mesh.n_faces, mids, pspec["magnetic_t"])
+        else:
+            magnetic = np.zeros((*shape, 3))
+            magnetic[..., 2] = pspec["magnetic_t"]
+            density = np.full(shape, pspec["density_m3"])
+            collision = np.full(shape, pspec["collision_hz"])
+        species = [rplasma.ColdPlasmaSpecies("electron", -rplasma.ELEMENTARY_CHARGE_C, rplasma.ELECTRON_MASS_KG, density, collision)]
+        if pspec.get("two_species"):
+            species.append(rplasma.ColdPlasmaSpecies("O+", rplasma.ELEMENTARY_CHARGE_C, 16 * 1.672_621_925_95e-27, 0.5 * density, 0.1 * collision))
+        plasma = rplasma.MeshPlasmaModel.from_mesh(
+            mesh, mids, magnetic, tuple(species), provenance=(_provenance(rdata),), interpolation="synthetic"
+        )
+    sim = rsolver.GeodesicFDTD(
+        cfg, material=material, source=source, surface_impedance=surface, plasma=plasma, mesh=mesh, backend="numpy", dtype=dtype
+    )
+    init = case.get("init")
+    if init is not None:
+        shapes = {name: getattr(sim, name).shape for name in ("er", "et", "hr", "ht")}
+        for name, values in C.initial_fields(shapes, *init).items():
+            getattr(sim, name)[:] = values
+    return sim
+
+
+def run_case(name: str, case: dict, mods, dtype: str = "float64") -> dict:
+    sim = build_reference(case, mods, dtype)
+    out: dict[str, np.ndarray] = {"time_step_s": np.asarray(sim.time_step_s), "cfl_limit_s": np.asarray(sim.cfl_time_step_limit_s)}
+    rspec = case.get("receivers")
+    if rspec is not None:
+        v, k, w = C.receiver_rows(sim.mesh.n_vertices, sim.altitudes_m, rspec["seed"], rspec["count"])
+        out["traces"] = sim.record_er_observations(v, k, w, case["steps"])
+    else:
+        sim.step(case["steps"])
+    for field in ("er", "et", "hr", "ht"):
+        out[field] = np.asarray(getattr(sim, field))
+    if sim._surface_impedance_ade is not None:
+        out["si_memory"] = np.asarray(sim._surface_impedance_ade.memory)
+    if sim._plasma_coupler is not None:
+        for i, j in enumerate(sim._plasma_coupler.ade.current_density):
+            out[f"plasma_current_{i}"] = np.asarray(j)
+    out["max_abs"] = np.asarray([float(np.max(np.abs(out[f]))) for f in ("er", "et", "hr", "ht")])
+    return out
+
+
+def mesh_fixtures(mods) -> None:
+    rmesh = mods[0]
+    rnb = mods[7]
+    digests = {}
+    tables = ("edges", "faces", "face_edges", "face_edge_signs", "edge_left_faces", "edge_right_faces", "vertex_degree")
+    floats = ("vertices", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles", "dual_cell_solid_angles")
+    for level in range(0, 7):
+        mesh = rmesh.build_geodesic_mesh(level)
+        backend = rnb.NumPyBackend(mesh)
+        entry = {t: _sha(np.asarray(getattr(mesh, t), dtype=np.int64)) for t in tables}
+        entry["vertex_edges"] = _sha(np.asarray(backend.vertex_edges, dtype=np.int64))
+        entry["vertex_edge_signs"] = _sha(np.asarray(backend.vertex_edge_signs, dtype=np.float64))
+        entry.update({f: _sha(np.asarray(getattr(mesh, f), dtype=np.float64)) for f in floats})
+        digests[str(level)] = entry
+        if level <= 3:
+            arrays = {t: np.asarray(getattr(mesh, t)) for t in tables + floats}
+            arrays["vertex_edges"] = backend.vertex_edges
+            arrays["vertex_edge_signs"] = backend.vertex_edge_signs
+            np.savez_compressed(HERE / f"mesh_s{level}.npz", **arrays)
+    (HERE / "mesh_digests.json").write_text(json.dumps(digests, indent=1, sort_keys=True) + "\n")
+
+
+def main(src: str) -> None:
+    mods = _import_reference(src)
+    mesh_fixtures(mods)
+    for name, case in C.CASES.items():
+        np.savez_compressed(HERE / f"case_{name}.npz", **run_case(name, case, mods))
+        print("wrote", name)
+    # the reference's float32 pin: 80 steps of source_s1 in float32
+    pin = dict(C.CASES["source_s1"], steps=80)
+    np.savez_compressed(HERE / "case_source_s1_f32x80.npz", **run_case("source_s1_f32", pin, mods, dtype="float32"))
+    np.savez_compressed(HERE / "case_source_s1_f64x80.npz", **run_case("source_s1_f64", pin, mods, dtype="float64"))
+    # H observations with decimation (solver.py:1138-1229)
+    sim = build_reference(C.CASES["source_s1"], mods)
+    hr, ht = sim.record_h_observations(
+        np.asarray(((0,), (5,)), dtype=np.int64),
+        np.asarray(((2,), (4,)), dtype=np.int64),
+        np.asarray(((1.0,), (1.0,))),
+        np.asarray(((0, 1, 2), (7, 8, 9)), dtype=np.int64),
+        np.asarray(((2, 2, 2), (0, 3, 6)), dtype=np.int64),
+        np.asarray(((0.2, -0.3, 0.5), (1.0, 0.5, -0.5))),
+        11,
+        sample_every=3,
+    )
+    np.savez_compressed(HERE / "obs_h_source_s1.npz", hr=hr, ht=ht)
+    print("done")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
