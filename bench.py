@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 geodesic FDTD time step (prints one JSON line).
+
+Workload (default ``config2``): icosahedral subdivision 7 (163,842 dual
+cells) x 40 radial cells, FP32 fields, exponential conductive integrator,
+Drude electron plasma ADE, one 50 Hz Gaussian source and 64 barycentric
+receivers; seeded synthetic inputs, random 1e-6 initial fields.  One bench
+"step" is ``--time-steps`` leapfrog steps (default 1000) of that simulation,
+launched as CUDA-graph chunks on one GPU.  ``value`` is whole-job
+Gcell-updates/s (cells = vertices x radial cells) with the state resident in
+HBM; ``e2e`` is the same metric through the public API
+(``GeodesicFDTD.record_er_observations``) with host-computed source currents
+copied in and receiver traces copied out every bench step.
+
+``--impl reference`` times the CPU oracle (a NumPy restatement of the
+reference's own NumPy path, the reference being pure Python) on a bounded
+sample of the same workload.  Under torchrun every rank runs an independent
+replica (the plain solver does not shard), timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "Gcell-updates/s"
+UNIT = "Gcell/s"
+
+
+def parse() -> argparse.Namespace:
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("engine", "reference"), default="engine")
+    p.add_argument("--workload", choices=("config2", "config4"), default="config2")
+    p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def measured_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profile(workload: str) -> float | None:
+    """DRAM bytes per leapfrog step from the committed ncu summary, if any."""
+
+    path = ROOT / "profiles" / f"fdtd_step_{workload}_traffic.txt"
+    try:
+        for line in path.read_text().splitlines():
+            if line.startswith("dram_bytes_per_step:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU while the timed region runs."""
+
+    QUERY = (
+        "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+        "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, uuid: str | None):
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"bench_clocks_{os.getpid()}.csv"
+        if uuid is None:
+            return
+        try:
+            self.handle = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", uuid, f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.handle,
+                stderr=subprocess.DEVNULL,
+            )
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.handle.close()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build(workload: str, device: str):
+    from ionosphere_fdtd_b200 import workloads as W
+
+    if workload == "config4":
+        wl = W.config4(device=device)
+    else:
+        wl = W.config2(device=device)
+    W.seed_fields(wl.simulation)
+    return wl
+
+
+def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
+    """Time the CPU oracle on ``steps`` leapfrog steps of the same workload (float32)."""
+
+    import oracle.fdtd as O
+    from ionosphere_fdtd_b200 import workloads as W
+    from ionosphere_fdtd_b200.mesh import build_geodesic_mesh
+
+    sub, L = (9, 80) if workload == "config4" else (7, 40)
+    lo = 0.0 if workload == "config4" else -100_000.0
+    mesh = build_geodesic_mesh(sub)
+    alt = np.linspace(lo, 100_000.0, L + 1)
+    mids = 0.5 * (alt[:-1] + alt[1:])
+    shape = (mesh.n_faces, L)
+    plasma = O.OraclePlasma(
+        np.zeros((*shape, 3)),
+        [O.OracleSpecies(-1.602_176_634e-19, 9.109_383_713_9e-31,
+                         np.broadcast_to(1.0e6 * np.exp((mids - 85_000.0) / 3_000.0), shape),
+                         np.broadcast_to(1.0e7 * np.exp(-(mids - 70_000.0) / 6_000.0), shape))],
+    )
+    surface = O.OracleSurface(W.smooth_log_normal(mesh.edge_midpoints(), 20260814)) if workload == "config4" else None
+    sim = O.OracleFDTD(
+        subdivision=sub, radial_cells=L, minimum_altitude_m=lo, material=W.ProfileMaterial(), plasma=plasma,
+        surface=surface, mesh=mesh, dtype=np.float32,
+        source=O.OracleSource(peak_current_a=1.0, carrier_frequency_hz=50.0 if workload == "config2" else 20.0),
+    )
+    rng = np.random.default_rng(20260814)
+    for f in ("er", "et", "hr", "ht"):
+        getattr(sim, f)[:] = (1.0e-6 * rng.standard_normal(getattr(sim, f).shape)).astype(np.float32)
+    sim.step(warm)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    cells = mesh.n_vertices * L
+    return {"gcells": cells * steps / dt / 1e9, "seconds": dt, "steps": steps, "cells": cells, "sub": sub, "L": L}
+
+
+def reference_arm(args, world: int, rank: int) -> None:
+    if rank != 0:
+        return
+    per_step = 1
+    for _ in range(args.warmup):
+        oracle_sample(args.workload, per_step, warm=0)
+    rates, secs = [], 0.0
+    for _ in range(args.steps):
+        r = oracle_sample(args.workload, per_step, warm=0)
+        rates.append(r["gcells"])
+        secs += r["seconds"]
+    value = statistics.median(rates)
+    sample = f"{per_step} leapfrog step(s) of s{r['sub']}/L{r['L']} float32 per bench step, NumPy oracle restating the reference NumPy backend, single-threaded gathers"
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "cells": r["cells"], "time_steps_per_step": per_step, "device": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
+    device = f"cuda:{local}"
+    wl = build(args.workload, device)
+    sim = wl.simulation
+    T = args.time_steps or (1000 if args.workload == "config2" else 100)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(max(args.warmup, 3)):
+        sim.step(T)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    uuid = getattr(torch.cuda.get_device_properties(local), "uuid", None)
+    sampler = ClockSampler(f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None))
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    torch.cuda.synchronize()
+    start.record(stream)
+    marks[0].record(stream)
+    for i in range(args.steps):
+        sim.step(T)
+        marks[i + 1].record(stream)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed_ms = start.elapsed_time(stop)
+    per_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
+    if dist:
+        t = torch.tensor([elapsed_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+        dist.barrier()
+    total_cells = wl.cells * T * args.steps * world
+    value = total_cells / (elapsed_ms / 1e3) / 1e9
+
+    # end to end through the public API: host currents in, receiver traces out
+    e2e = None
+    if not args.no_e2e:
+        v, k, w = wl.receivers
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            traces = sim.record_er_observations(v, k, w, T)
+        t1 = time.perf_counter()
+        wall = t1 - t0
+        if dist:
+            t = torch.tensor([wall], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {
+            "value": wl.cells * T * args.steps * world / wall / 1e9,
+            "unit": UNIT,
+            "h2d_bytes_per_step": 8 * T,
+            "d2h_bytes_per_step": int(traces.nbytes),
+            "api": "GeodesicFDTD.record_er_observations",
+        }
+
+    peak, peak_kind = measured_peak()
+    step_ms = statistics.median(per_step_ms) / T
+    achieved = wl.bytes_per_step / (step_ms / 1e3) / 1e9
+    traffic = traffic_from_profile(args.workload)
+    roofline = {
+        "bound": "hbm",
+        "kernel": "one leapfrog step (kh_kernel + ke_kernel, CUDA graph)",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_source": f"{peak_kind} hbm_gbs",
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "algorithmic_bytes_per_step": wl.bytes_per_step,
+        "traffic": traffic,
+    }
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = oracle_sample(args.workload, 3)
+        cpu = {
+            "value": r["gcells"],
+            "unit": UNIT,
+            "cores": 1,
+            "kind": "port",
+            "sample": f"{r['steps']} leapfrog steps of the same s{r['sub']}/L{r['L']} float32 workload after 1 warm-up step ({r['seconds']:.1f} s), NumPy oracle",
+        }
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": args.workload,
+                "subdivision": sim.config.subdivision,
+                "radial_cells": sim.config.radial_cells,
+                "cells": wl.cells,
+                "time_steps_per_step": T,
+                "plasma": "drude (1 species)",
+                "surface_impedance": sim._surface_impedance_ade is not None,
+                "receivers": int(wl.receivers[0].shape[0]),
+                "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
+                "parallelism": f"replicas x{world}",
+            },
+            "hbm_gbs": achieved,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 2 * T * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,181 @@
+/*
+ * ifdtd.h - C ABI of the B200 geodesic FDTD time-step engine.
+ *
+ * The reference (ruddyscent/ionosphere-fdtd v0.2.0) is pure Python: its
+ * time-step path is GeodesicFDTD.step (src/ionosphere_fdtd/solver.py:789-816)
+ * running on the ArrayBackend seam (src/ionosphere_fdtd/backends/base.py:19-89,
+ * selected by create_backend in backends/__init__.py:12-33).  There is no FFI
+ * in the reference; each entry point below names the reference interface it
+ * replaces.  All pointers are plain host or device pointers, all sizes are
+ * plain integers, and no torch type appears.  Every function returns an
+ * ifdtd_status; ifdtd_last_error() gives the message of the last failure on
+ * the calling thread.
+ *
+ * Layout contract: every field is a row-major (entity, radial) array with the
+ * radial index contiguous, exactly the reference's er (V, L+1), et (E, L),
+ * hr (F, L), ht (E, L+1) arrays (solver.py:315-322); surface-impedance memory
+ * is (E, T) (surface_impedance.py:203); plasma current densities are
+ * (F, L, 3) per species (plasma.py:411).  Element type is float (dtype 4) or
+ * double (dtype 8) for a whole plan.
+ */
+#ifndef IFDTD_H
+#define IFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFDTD_MAX_SPECIES 4
+#define IFDTD_MAX_SOURCES 16
+
+typedef enum ifdtd_status {
+  IFDTD_OK = 0,
+  IFDTD_ERR_ARGUMENT = 1,   /* invalid argument (maps to ValueError) */
+  IFDTD_ERR_CUDA = 2,       /* CUDA runtime failure (maps to RuntimeError) */
+  IFDTD_ERR_NONFINITE = 3,  /* a field holds NaN/Inf (diagnostics) */
+  IFDTD_ERR_UNSUPPORTED = 4 /* feature or device not supported (BackendUnavailableError) */
+} ifdtd_status;
+
+typedef struct ifdtd_plan ifdtd_plan;
+typedef struct ifdtd_probe ifdtd_probe;
+
+/* Mesh tables as GeodesicMesh holds them (src/ionosphere_fdtd/mesh.py:21-41). */
+typedef struct ifdtd_mesh_desc {
+  int32_t n_vertices, n_edges, n_faces;
+  const int64_t* edges;            /* (E,2) tail, head            mesh.py:27  */
+  const int64_t* faces;            /* (F,3) outward-oriented      mesh.py:26  */
+  const int64_t* face_edges;       /* (F,3)                       mesh.py:28  */
+  const int64_t* face_edge_signs;  /* (F,3) +1 / -1               mesh.py:29  */
+  const int64_t* edge_left_faces;  /* (E)                         mesh.py:30  */
+  const int64_t* edge_right_faces; /* (E)                         mesh.py:31  */
+  const double* primal_edge_angles;     /* (E) theta              mesh.py:33 */
+  const double* dual_edge_angles;       /* (E) phi                mesh.py:34 */
+  const double* face_solid_angles;      /* (F) A_f                mesh.py:35 */
+  const double* dual_cell_solid_angles; /* (V) A*_v               mesh.py:36 */
+} ifdtd_mesh_desc;
+
+/* Radial grid and integration controls (solver.py:260-283, 296-300). */
+typedef struct ifdtd_grid_desc {
+  int32_t radial_cells;   /* L; nodes 0..L, midpoints 0..L-1 */
+  int32_t full_spherical; /* geometry_mode == "full-spherical" */
+  const double* radii_m;  /* (L+1) node radii */
+  double time_step_s;
+} ifdtd_grid_desc;
+
+/* Physics coefficients built by the host exactly as the reference builds them:
+ * loss coefficients (solver.py:706-761), source supports (solver.py:936-987,
+ * sources.py:220-235, 290-335), surface-impedance ADE (surface_impedance.py:
+ * 176-203), plasma ADE and coupler tables (plasma.py:374-411, 458-487). */
+typedef struct ifdtd_physics_desc {
+  /* loss coefficients; rows = 1 (altitude-only profile) or V / E */
+  int32_t coef_rows_er, coef_rows_et;
+  const double *ca_er, *cb_er; /* (rows, L+1) */
+  const double *ca_et, *cb_et; /* (rows, L)   */
+  /* vertical source: er[v,k] -= coef * I(step); tangential: et[e,j] -= coef * I */
+  int32_t n_src_er;
+  const int64_t *src_er_vertex, *src_er_layer;
+  const double* src_er_coef;
+  int32_t n_src_et;
+  const int64_t *src_et_edge, *src_et_layer;
+  const double* src_et_coef;
+  /* lower surface-impedance ADE (terms = 0 disables) */
+  int32_t si_terms;
+  const double* si_scale;    /* (E) sqrt(mu / sigma_e) */
+  const double* si_decay;    /* (T) (1-a)/(1+a) */
+  const double* si_drive;    /* (T) a/(1+a)     */
+  const double* si_history;  /* (T) w/(1+a)     */
+  double si_metric;          /* m_0 / r_0 (full-spherical) or 1 */
+  /* cold-plasma ADE (species = 0 disables) */
+  int32_t plasma_species;
+  int32_t plasma_rows;       /* 1 (altitude-only) or F */
+  int32_t plasma_magnetized; /* 0: b = 0 everywhere */
+  const double* plasma_coef; /* (S, 6, rows, L): decay, cos, sin, d_par, d_re, d_im */
+  const double* plasma_bdir; /* (rows, L, 3) unit B (magnetized only) */
+  const double* plasma_reconstruction; /* (F,3,3) pinv(tangents).T per face */
+  const double* face_centers;          /* (F,3) */
+  const double* plasma_tangent_left;   /* (E,3) */
+  const double* plasma_tangent_right;  /* (E,3) */
+  int32_t vertex_face_width;           /* W */
+  const int64_t* vertex_faces;         /* (V,W) padded with weight 0 */
+  const double* vertex_face_weights;   /* (V,W) */
+} ifdtd_physics_desc;
+
+/* Tuning of the launch geometry (0 = defaults). */
+typedef struct ifdtd_tuning {
+  int32_t faces_per_patch; /* faces owned by one CTA (default 32) */
+  int32_t threads;         /* threads per CTA (default 256) */
+  int32_t graph_chunk;     /* steps captured per CUDA graph (default 32; 0 disables) */
+} ifdtd_tuning;
+
+/* Mutable state of one simulation: device pointers owned by the caller. */
+typedef struct ifdtd_state {
+  void *er, *et, *hr, *ht;
+  void* si_memory;                          /* (E,T) or NULL */
+  void* plasma_current[IFDTD_MAX_SPECIES];  /* (F,L,3) each */
+} ifdtd_state;
+
+int32_t ifdtd_version(void);
+int32_t ifdtd_last_error(char* buffer, size_t size);
+int32_t ifdtd_device_count(int32_t* count);
+
+/* Build a plan for one simulation: uploads derived device tables
+ * (replaces GeodesicFDTD.__init__'s backend setup, solver.py:238-375). */
+int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* grid,
+                          const ifdtd_physics_desc* physics, const ifdtd_tuning* tuning,
+                          int32_t dtype_bytes, int32_t device, ifdtd_plan** out);
+int32_t ifdtd_plan_destroy(ifdtd_plan* plan);
+/* Bytes of device memory held by the plan (tables, staging, scratch). */
+int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);
+
+/* Advance n_steps leapfrog steps in place; currents (device, float64,
+ * n_steps) are the source waveform I((n+1/2)dt) per step.  Replaces
+ * GeodesicFDTD.step / _advance_fields / _advance_field_chunk
+ * (solver.py:789-816, 867-875) and the backend compile_step hook
+ * (backends/base.py:27-34, torch_backend.py:91-96). */
+int32_t ifdtd_step(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
+                   int32_t n_steps, void* stream);
+
+/* The two half steps of one leapfrog step, for callers that drive them
+ * separately: the magnetic update (solver.py:877-921) and the electric update
+ * with source current I (solver.py:923-989).  ifdtd_step is the pair. */
+int32_t ifdtd_update_magnetic(ifdtd_plan* plan, const ifdtd_state* state, void* stream);
+int32_t ifdtd_update_electric(ifdtd_plan* plan, const ifdtd_state* state, double current, void* stream);
+
+/* Weighted observation probe: out[r] = sum_k w[r,k] * field[index[r,k], layer[r,k]]
+ * accumulated in float64.  field_kind: 0 er, 1 et, 2 hr, 3 ht.  Replaces the
+ * sampling closures of record_er_observations / record_h_observations
+ * (solver.py:1122-1124, 1212-1220). */
+int32_t ifdtd_probe_create(ifdtd_plan* plan, int32_t field_kind, int32_t rows, int32_t width,
+                           const int64_t* index, const int64_t* layer, const double* weight,
+                           ifdtd_probe** out);
+int32_t ifdtd_probe_destroy(ifdtd_probe* probe);
+int32_t ifdtd_sample(ifdtd_plan* plan, const ifdtd_state* state, const ifdtd_probe* probe,
+                     double* out_row, void* stream);
+/* Step n_steps times, sampling after every step into out_rows (n_steps, rows)
+ * (record_er_observations' inner loop, solver.py:1126-1135). */
+int32_t ifdtd_step_sampled(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
+                           int32_t n_steps, const ifdtd_probe* probe, double* out_rows, void* stream);
+
+/* max |field| of er, et, hr, ht into out4 (device, float64); the four
+ * reductions of diagnostics() (solver.py:1027-1030, torch_backend.py:218-219). */
+int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, void* stream);
+
+/* The four topology primitives of the ArrayBackend contract on (N, cols)
+ * row-major arrays (backends/base.py:59-73, torch_backend.py:172-198). */
+int32_t ifdtd_edge_difference(ifdtd_plan* plan, const void* vertex_values, int32_t cols,
+                              void* out, void* stream);
+int32_t ifdtd_dual_edge_difference(ifdtd_plan* plan, const void* face_values, int32_t cols,
+                                   void* out, void* stream);
+int32_t ifdtd_face_circulation(ifdtd_plan* plan, const void* edge_values, int32_t cols,
+                               void* out, void* stream);
+int32_t ifdtd_dual_cell_circulation(ifdtd_plan* plan, const void* edge_values, int32_t cols,
+                                    void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IFDTD_H */

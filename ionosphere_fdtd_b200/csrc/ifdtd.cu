@@ -1,0 +1,814 @@
+// C ABI of the geodesic FDTD engine: plan construction, the step loop (direct
+// launches or CUDA-graph chunks), observation probes, reductions and the
+// ArrayBackend primitives.  Declarations and reference citations: include/ifdtd.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/ifdtd.h"
+#include "step_kernels.cuh"
+
+using namespace ifdtd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+  do {                                                                                          \
+    cudaError_t _e = (expr);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      return fail(IFDTD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));          \
+  } while (0)
+
+struct DeviceArena {
+  std::vector<void*> blocks;
+  size_t bytes = 0;
+  ~DeviceArena() {
+    for (void* p : blocks) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t upload(const std::vector<T>& host, const T** out) {
+    *out = nullptr;
+    if (host.empty()) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, host.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    blocks.push_back(p);
+    bytes += host.size() * sizeof(T);
+    e = cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice);
+    *out = static_cast<const T*>(p);
+    return e;
+  }
+  cudaError_t alloc(size_t n, void** out) {
+    *out = nullptr;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(out, n);
+    if (e != cudaSuccess) return e;
+    blocks.push_back(*out);
+    bytes += n;
+    return cudaSuccess;
+  }
+};
+
+}  // namespace
+
+struct ifdtd_probe {
+  ifdtd_plan* plan;
+  int kind, rows, width;
+  int* index = nullptr;
+  int* layer = nullptr;
+  double* weight = nullptr;
+  double* staging = nullptr;  // (graph_chunk, rows)
+  DeviceArena arena;          // the probe's own device buffers
+};
+
+struct GraphEntry {
+  int chunk;
+  const ifdtd_probe* probe;
+  cudaGraphExec_t exec;
+};
+
+struct ifdtd_plan {
+  int dtype = 4;
+  int device = 0;
+  int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
+  int n_patches = 0, threads = 256, chunk = 32;
+  bool plasma = false;
+  DeviceArena arena;
+  void* d_rec = nullptr;               // Rec<real> in device memory
+  std::vector<unsigned char> h_rec;    // host image of the record
+  double* d_cur = nullptr;             // staging currents (chunk)
+  void* d_jtot = nullptr;              // summed species current (S > 1)
+  // primitive tables
+  const int2* edge_th = nullptr;
+  const int2* edge_lr = nullptr;
+  const int4* face_e = nullptr;
+  const int* face_sign = nullptr;
+  const int* v_off = nullptr;
+  const int* v_edge = nullptr;
+  const int* v_sign = nullptr;
+  ifdtd_state last_state;
+  bool have_state = false;
+  cudaStream_t capture_stream = nullptr;
+  std::vector<GraphEntry> graphs;
+  std::vector<ifdtd_probe*> probes;
+  ~ifdtd_plan() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+  }
+};
+
+namespace {
+
+template <typename real>
+std::vector<real> cast(const double* p, size_t n) {
+  std::vector<real> out(n);
+  for (size_t i = 0; i < n; ++i) out[i] = (real)p[i];
+  return out;
+}
+
+bool in_range(const int64_t* p, size_t n, int64_t hi) {
+  for (size_t i = 0; i < n; ++i)
+    if (p[i] < 0 || p[i] >= hi) return false;
+  return true;
+}
+
+template <typename real>
+int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G, const ifdtd_physics_desc* X,
+               const ifdtd_tuning* tune) {
+  Rec<real> R;
+  std::memset(&R, 0, sizeof(R));
+  const int nV = M->n_vertices, nE = M->n_edges, nF = M->n_faces, L = G->radial_cells;
+  if (nV < 4 || nE < 6 || nF < 4 || L < 2) return fail(IFDTD_ERR_ARGUMENT, "mesh or radial grid too small");
+  if ((int64_t)nE * (L + 1) >= (int64_t)1 << 31 || (int64_t)nF * L * 3 >= (int64_t)1 << 31)
+    return fail(IFDTD_ERR_ARGUMENT, "problem exceeds 2^31 samples per array");
+  if (!in_range(M->edges, 2 * (size_t)nE, nV) || !in_range(M->faces, 3 * (size_t)nF, nV) ||
+      !in_range(M->face_edges, 3 * (size_t)nF, nE) || !in_range(M->edge_left_faces, nE, nF) ||
+      !in_range(M->edge_right_faces, nE, nF))
+    return fail(IFDTD_ERR_ARGUMENT, "mesh index table out of range");
+  const int fpp = (tune && tune->faces_per_patch > 0) ? tune->faces_per_patch : 32;
+  const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
+  if (threads % 32 || threads > 256) return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 <= 256");
+  if ((int64_t)fpp * 3 * (L + 1) >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
+  P->threads = threads;
+  // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
+  P->chunk = (tune && tune->graph_chunk >= 0) ? tune->graph_chunk : 32;
+  P->nV = nV;
+  P->nE = nE;
+  P->nF = nF;
+  P->L = L;
+  DeviceArena& A = P->arena;
+
+  // ---- edges ----
+  std::vector<int2> th(nE), lr(nE);
+  std::vector<real> inv_theta(nE), inv_phi(nE);
+  std::vector<int> owner_e(nE);
+  for (int e = 0; e < nE; ++e) {
+    th[e] = make_int2((int)M->edges[2 * e], (int)M->edges[2 * e + 1]);
+    lr[e] = make_int2((int)M->edge_left_faces[e], (int)M->edge_right_faces[e]);
+    inv_theta[e] = (real)(1.0 / M->primal_edge_angles[e]);
+    inv_phi[e] = (real)(1.0 / M->dual_edge_angles[e]);
+    owner_e[e] = std::min(lr[e].x, lr[e].y);
+    if (e > 0 && owner_e[e] < owner_e[e - 1])
+      return fail(IFDTD_ERR_ARGUMENT, "edges are not numbered in face-scan order");
+  }
+  // ---- faces ----
+  std::vector<int4> fe(nF), fv(nF);
+  std::vector<int> fsign(3 * (size_t)nF);
+  std::vector<real> fw(3 * (size_t)nF);
+  for (int f = 0; f < nF; ++f) {
+    fe[f] = make_int4((int)M->face_edges[3 * f], (int)M->face_edges[3 * f + 1], (int)M->face_edges[3 * f + 2], 0);
+    fv[f] = make_int4((int)M->faces[3 * f], (int)M->faces[3 * f + 1], (int)M->faces[3 * f + 2], 0);
+    const double inv_a = 1.0 / M->face_solid_angles[f];
+    for (int i = 0; i < 3; ++i) {
+      const int64_t s = M->face_edge_signs[3 * f + i];
+      if (s != 1 && s != -1) return fail(IFDTD_ERR_ARGUMENT, "face edge signs must be +1 or -1");
+      fsign[3 * f + i] = (int)s;
+      fw[3 * f + i] = (real)((double)s * M->primal_edge_angles[M->face_edges[3 * f + i]] * inv_a);
+    }
+  }
+  // ---- vertex incidence in reference slot order: tail uses, then head uses ----
+  std::vector<int> deg(nV, 0);
+  for (int e = 0; e < nE; ++e) {
+    deg[th[e].x]++;
+    deg[th[e].y]++;
+  }
+  std::vector<int> v_off(nV + 1, 0);
+  for (int v = 0; v < nV; ++v) v_off[v + 1] = v_off[v] + deg[v];
+  std::vector<int> fill(v_off.begin(), v_off.end() - 1);
+  std::vector<int> v_edge(2 * (size_t)nE), v_sign(2 * (size_t)nE);
+  std::vector<real> v_coef(2 * (size_t)nE);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int e = 0; e < nE; ++e) {
+      const int v = pass == 0 ? th[e].x : th[e].y;
+      const int q = fill[v]++;
+      v_edge[q] = e;
+      v_sign[q] = pass == 0 ? 1 : -1;
+      v_coef[q] = (real)((pass == 0 ? 1.0 : -1.0) * M->dual_edge_angles[e] / M->dual_cell_solid_angles[v]);
+    }
+  // ---- patches: faces [p*fpp, (p+1)*fpp), edges by lowest adjacent face, vertices by lowest incident face ----
+  const int n_patches = (nF + fpp - 1) / fpp;
+  P->n_patches = n_patches;
+  std::vector<int> eptr(n_patches + 1);
+  {
+    int e = 0;
+    for (int p = 0; p <= n_patches; ++p) {
+      const int bound = std::min(p * fpp, nF);
+      while (e < nE && owner_e[e] < bound) ++e;
+      eptr[p] = (p == n_patches) ? nE : e;
+    }
+  }
+  std::vector<int> owner_v(nV, nF);
+  for (int f = 0; f < nF; ++f) {
+    owner_v[fv[f].x] = std::min(owner_v[fv[f].x], f);
+    owner_v[fv[f].y] = std::min(owner_v[fv[f].y], f);
+    owner_v[fv[f].z] = std::min(owner_v[fv[f].z], f);
+  }
+  std::vector<int> vptr(n_patches + 1, 0), vlist(nV);
+  for (int v = 0; v < nV; ++v) {
+    if (owner_v[v] >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex without incident face");
+    vptr[owner_v[v] / fpp + 1]++;
+  }
+  for (int p = 0; p < n_patches; ++p) vptr[p + 1] += vptr[p];
+  {
+    std::vector<int> cursor(vptr.begin(), vptr.end() - 1);
+    for (int v = 0; v < nV; ++v) vlist[cursor[owner_v[v] / fpp]++] = v;
+  }
+  // ---- radial metric ----
+  const double* r = G->radii_m;
+  std::vector<real> invr(L + 1), rr(L + 1), mid(L), invm(L), invdr(L), invcd(L + 1);
+  std::vector<double> m(L);
+  for (int k = 0; k <= L; ++k) {
+    if (!(r[k] > 0.0) || (k > 0 && !(r[k] > r[k - 1]))) return fail(IFDTD_ERR_ARGUMENT, "radii must increase");
+    invr[k] = (real)(1.0 / r[k]);
+    rr[k] = (real)r[k];
+  }
+  for (int j = 0; j < L; ++j) {
+    m[j] = 0.5 * (r[j] + r[j + 1]);
+    mid[j] = (real)m[j];
+    invm[j] = (real)(1.0 / m[j]);
+    invdr[j] = (real)(1.0 / (r[j + 1] - r[j]));
+  }
+  invcd[0] = (real)(2.0 / (r[1] - r[0]));
+  invcd[L] = (real)(2.0 / (r[L] - r[L - 1]));
+  for (int k = 1; k < L; ++k) invcd[k] = (real)(1.0 / (m[k] - m[k - 1]));
+
+  // ---- coefficients ----
+  if (!(X->coef_rows_er == 1 || X->coef_rows_er == nV) || !(X->coef_rows_et == 1 || X->coef_rows_et == nE))
+    return fail(IFDTD_ERR_ARGUMENT, "coefficient rows must be 1 or the entity count");
+  if ((X->coef_rows_er == 1) != (X->coef_rows_et == 1))
+    return fail(IFDTD_ERR_ARGUMENT, "er and et coefficients must both be compressed or both full");
+  const size_t ner = (size_t)X->coef_rows_er * (L + 1), net = (size_t)X->coef_rows_et * L;
+
+  // ---- sources ----
+  if (X->n_src_er < 0 || X->n_src_er > IFDTD_MAX_SOURCES || X->n_src_et < 0 || X->n_src_et > IFDTD_MAX_SOURCES)
+    return fail(IFDTD_ERR_ARGUMENT, "too many source supports");
+  std::vector<int> sv(X->n_src_er), sk(X->n_src_er), se(X->n_src_et), sj(X->n_src_et);
+  int vmin = 1 << 30, vmax = -1, emin = 1 << 30, emax = -1;
+  for (int s = 0; s < X->n_src_er; ++s) {
+    if (X->src_er_vertex[s] < 0 || X->src_er_vertex[s] >= nV || X->src_er_layer[s] < 0 || X->src_er_layer[s] > L)
+      return fail(IFDTD_ERR_ARGUMENT, "vertical source support out of range");
+    sv[s] = (int)X->src_er_vertex[s];
+    sk[s] = (int)X->src_er_layer[s];
+    vmin = std::min(vmin, sv[s]);
+    vmax = std::max(vmax, sv[s]);
+  }
+  for (int s = 0; s < X->n_src_et; ++s) {
+    if (X->src_et_edge[s] < 0 || X->src_et_edge[s] >= nE || X->src_et_layer[s] < 0 || X->src_et_layer[s] >= L)
+      return fail(IFDTD_ERR_ARGUMENT, "tangential source support out of range");
+    se[s] = (int)X->src_et_edge[s];
+    sj[s] = (int)X->src_et_layer[s];
+    emin = std::min(emin, se[s]);
+    emax = std::max(emax, se[s]);
+  }
+
+  // ---- upload ----
+#define UP(vec, field)                                                   \
+  do {                                                                   \
+    cudaError_t _e = A.upload(vec, &R.field);                            \
+    if (_e != cudaSuccess)                                               \
+      return fail(IFDTD_ERR_CUDA, std::string("upload ") + #field + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+  UP(eptr, eptr);
+  UP(vptr, vptr);
+  UP(vlist, vlist);
+  UP(th, edge_th);
+  UP(lr, edge_lr);
+  UP(inv_theta, inv_theta);
+  UP(inv_phi, inv_phi);
+  UP(fe, face_e);
+  UP(fv, face_v);
+  UP(fw, face_w);
+  UP(v_off, v_off);
+  UP(v_edge, v_edge);
+  UP(v_coef, v_coef);
+  UP(invr, invr);
+  UP(rr, rr);
+  UP(mid, mid);
+  UP(invm, invm);
+  UP(invdr, invdr);
+  UP(invcd, invcd);
+  {
+    auto ca = cast<real>(X->ca_er, ner), cb = cast<real>(X->cb_er, ner);
+    auto ct = cast<real>(X->ca_et, net), cu = cast<real>(X->cb_et, net);
+    UP(ca, ca_er);
+    UP(cb, cb_er);
+    UP(ct, ca_et);
+    UP(cu, cb_et);
+  }
+  if (X->n_src_er) {
+    auto c = cast<real>(X->src_er_coef, X->n_src_er);
+    UP(sv, src_er_v);
+    UP(sk, src_er_k);
+    UP(c, src_er_c);
+  }
+  if (X->n_src_et) {
+    auto c = cast<real>(X->src_et_coef, X->n_src_et);
+    UP(se, src_et_e);
+    UP(sj, src_et_j);
+    UP(c, src_et_c);
+  }
+  {
+    cudaError_t e1 = A.upload(fsign, &P->face_sign);
+    cudaError_t e2 = A.upload(v_sign, &P->v_sign);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(IFDTD_ERR_CUDA, "upload of primitive tables failed");
+  }
+  P->edge_th = R.edge_th;
+  P->edge_lr = R.edge_lr;
+  P->face_e = R.face_e;
+  P->v_off = R.v_off;
+  P->v_edge = R.v_edge;
+
+  // ---- surface impedance ----
+  P->T = X->si_terms;
+  if (X->si_terms < 0 || X->si_terms > 256) return fail(IFDTD_ERR_ARGUMENT, "surface impedance terms out of range");
+  if (X->si_terms > 0) {
+    const int T = X->si_terms;
+    auto sc = cast<real>(X->si_scale, nE), dc = cast<real>(X->si_decay, T), dr = cast<real>(X->si_drive, T),
+         hw = cast<real>(X->si_history, T);
+    double hsum = 0.0;
+    for (int p = 0; p < T; ++p) hsum += X->si_history[p];
+    UP(sc, si_scale);
+    UP(dc, si_decay);
+    UP(dr, si_drive);
+    UP(hw, si_hist);
+    R.si_metric = (real)X->si_metric;
+    R.si_kappa = (real)(2.0 * G->time_step_s / (1.256637062120e-6 * (r[1] - r[0])));
+    R.si_hist_sum = (real)hsum;
+  }
+
+  // ---- plasma ----
+  P->S = X->plasma_species;
+  if (X->plasma_species < 0 || X->plasma_species > IFDTD_MAX_SPECIES)
+    return fail(IFDTD_ERR_ARGUMENT, "plasma species count out of range");
+  if (X->plasma_species > 0) {
+    const int S = X->plasma_species;
+    if (!(X->plasma_rows == 1 || X->plasma_rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
+    P->plasma = true;
+    auto rc = cast<real>(X->plasma_reconstruction, 9 * (size_t)nF);
+    auto ce = cast<real>(X->face_centers, 3 * (size_t)nF);
+    auto tl = cast<real>(X->plasma_tangent_left, 3 * (size_t)nE);
+    auto tr = cast<real>(X->plasma_tangent_right, 3 * (size_t)nE);
+    auto pc = cast<real>(X->plasma_coef, (size_t)S * 6 * X->plasma_rows * L);
+    UP(rc, recon);
+    UP(ce, centre);
+    UP(tl, tan_l);
+    UP(tr, tan_r);
+    UP(pc, pcoef);
+    if (X->plasma_magnetized) {
+      auto bd = cast<real>(X->plasma_bdir, (size_t)X->plasma_rows * L * 3);
+      UP(bd, bdir);
+    }
+    const int W = X->vertex_face_width;
+    std::vector<int> vf_off(nV + 1, 0), vf_face;
+    std::vector<real> vf_wc;
+    for (int v = 0; v < nV; ++v) {
+      for (int q = 0; q < W; ++q) {
+        const double w = X->vertex_face_weights[(size_t)v * W + q];
+        if (w == 0.0) continue;
+        const int64_t f = X->vertex_faces[(size_t)v * W + q];
+        if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
+        vf_face.push_back((int)f);
+        for (int c = 0; c < 3; ++c) vf_wc.push_back((real)(w * X->face_centers[3 * f + c]));
+      }
+      vf_off[v + 1] = (int)vf_face.size();
+    }
+    UP(vf_off, vf_off);
+    UP(vf_face, vf_face);
+    UP(vf_wc, vf_wc);
+    if (S > 1) {
+      cudaError_t e = A.alloc((size_t)nF * L * 3 * sizeof(real), &P->d_jtot);
+      if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of summed plasma current failed");
+      R.Jtot = (real*)P->d_jtot;
+    }
+  }
+#undef UP
+
+  // ---- record ----
+  R.nV = nV;
+  R.nE = nE;
+  R.nF = nF;
+  R.L = L;
+  R.n_patches = n_patches;
+  R.fpp = fpp;
+  R.full = G->full_spherical ? 1 : 0;
+  R.si_terms = X->si_terms;
+  R.n_species = X->plasma_species;
+  R.plasma_full = X->plasma_rows == nF && nF != 1 ? 1 : 0;
+  R.magnetized = X->plasma_magnetized ? 1 : 0;
+  R.coef_full = X->coef_rows_er != 1 ? 1 : 0;
+  R.n_src_er = X->n_src_er;
+  R.n_src_et = X->n_src_et;
+  R.src_er_vmin = vmin;
+  R.src_er_vmax = vmax;
+  R.src_et_emin = emin;
+  R.src_et_emax = emax;
+  R.dtmu = (real)(G->time_step_s / 1.256637062120e-6);
+  {
+    void* cur = nullptr;
+    cudaError_t e = A.alloc(std::max(P->chunk, 1) * sizeof(double), &cur);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of current staging failed");
+    P->d_cur = (double*)cur;
+    R.cur = P->d_cur;
+  }
+  P->h_rec.resize(sizeof(Rec<real>));
+  std::memcpy(P->h_rec.data(), &R, sizeof(R));
+  {
+    cudaError_t e = A.alloc(sizeof(Rec<real>), &P->d_rec);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of launch record failed");
+    CUDA_TRY(cudaMemcpy(P->d_rec, &R, sizeof(R), cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&P->capture_stream, cudaStreamNonBlocking));
+  return IFDTD_OK;
+}
+
+// Refresh the state pointers in the device record when they changed.
+template <typename real>
+int bind_state(ifdtd_plan* P, const ifdtd_state* st, cudaStream_t stream) {
+  if (!st || !st->er || !st->et || !st->hr || !st->ht) return fail(IFDTD_ERR_ARGUMENT, "state pointers missing");
+  if (P->T > 0 && !st->si_memory) return fail(IFDTD_ERR_ARGUMENT, "surface impedance memory missing");
+  for (int s = 0; s < P->S; ++s)
+    if (!st->plasma_current[s]) return fail(IFDTD_ERR_ARGUMENT, "plasma current missing");
+  if (P->have_state && std::memcmp(&P->last_state, st, sizeof(*st)) == 0) return IFDTD_OK;
+  Rec<real>* R = reinterpret_cast<Rec<real>*>(P->h_rec.data());
+  R->er = (real*)st->er;
+  R->et = (real*)st->et;
+  R->hr = (real*)st->hr;
+  R->ht = (real*)st->ht;
+  R->si_mem = (real*)st->si_memory;
+  for (int s = 0; s < kMaxSpecies; ++s) R->J[s] = (real*)st->plasma_current[s];
+  // pageable source: the runtime stages it before returning, so h_rec may change afterwards
+  CUDA_TRY(cudaMemcpyAsync(P->d_rec, P->h_rec.data(), sizeof(Rec<real>), cudaMemcpyHostToDevice, stream));
+  P->last_state = *st;
+  P->have_state = true;
+  return IFDTD_OK;
+}
+
+template <typename real>
+cudaError_t launch_step(ifdtd_plan* P, int istep, const ifdtd_probe* probe, int row, cudaStream_t st) {
+  const Rec<real>* rec = (const Rec<real>*)P->d_rec;
+  if (P->plasma) {
+    kh_kernel<real, true><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1);
+    ke_kernel<real, true><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1, istep);
+  } else {
+    kh_kernel<real, false><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1);
+    ke_kernel<real, false><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1, istep);
+  }
+  if (probe) {
+    const int blocks = (probe->rows * 32 + 255) / 256;
+    sample_rec_kernel<real><<<blocks, 256, 0, st>>>(rec, probe->kind, probe->rows, probe->width, probe->index,
+                                                     probe->layer, probe->weight,
+                                                     probe->staging + (size_t)row * probe->rows);
+  }
+  return cudaGetLastError();
+}
+
+template <typename real>
+int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int n, const ifdtd_probe* probe,
+              double* out_rows, cudaStream_t stream) {
+  int rc = bind_state<real>(P, st, stream);
+  if (rc) return rc;
+  if (n <= 0) return IFDTD_OK;
+  const int cap = std::max(P->chunk, 1);
+  for (int s0 = 0; s0 < n; s0 += cap) {
+    const int c = std::min(cap, n - s0);
+    if (currents)
+      CUDA_TRY(cudaMemcpyAsync(P->d_cur, currents + s0, c * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    else
+      CUDA_TRY(cudaMemsetAsync(P->d_cur, 0, c * sizeof(double), stream));
+    if (P->chunk > 0 && c == P->chunk) {
+      cudaGraphExec_t exec = nullptr;
+      for (auto& g : P->graphs)
+        if (g.chunk == c && g.probe == probe) exec = g.exec;
+      if (!exec) {
+        cudaGraph_t graph;
+        CUDA_TRY(cudaStreamBeginCapture(P->capture_stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (int i = 0; i < c && le == cudaSuccess; ++i) le = launch_step<real>(P, i, probe, i, P->capture_stream);
+        cudaError_t ce = cudaStreamEndCapture(P->capture_stream, &graph);
+        if (le != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le));
+        if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        P->graphs.push_back({c, probe, exec});
+      }
+      CUDA_TRY(cudaGraphLaunch(exec, stream));
+    } else {
+      for (int i = 0; i < c; ++i) {
+        cudaError_t e = launch_step<real>(P, i, probe, i, stream);
+        if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+      }
+    }
+    if (probe && out_rows)
+      CUDA_TRY(cudaMemcpyAsync(out_rows + (size_t)s0 * probe->rows, probe->staging,
+                               (size_t)c * probe->rows * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  }
+  return IFDTD_OK;
+}
+
+struct DeviceGuard {
+  int previous = -1;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&previous) == cudaSuccess && previous != device) cudaSetDevice(device);
+    else previous = -1;
+  }
+  ~DeviceGuard() {
+    if (previous >= 0) cudaSetDevice(previous);
+  }
+};
+
+int grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)std::min<size_t>(std::max<size_t>(b, 1), 148 * 16);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ifdtd_version(void) { return 10000; }
+
+int32_t ifdtd_last_error(char* buffer, size_t size) {
+  if (!buffer || size == 0) return IFDTD_ERR_ARGUMENT;
+  std::snprintf(buffer, size, "%s", g_last_error.c_str());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_device_count(int32_t* count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (count) *count = (e == cudaSuccess) ? n : 0;
+  if (e != cudaSuccess) return fail(IFDTD_ERR_UNSUPPORTED, cudaGetErrorString(e));
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* grid, const ifdtd_physics_desc* physics,
+                          const ifdtd_tuning* tuning, int32_t dtype_bytes, int32_t device, ifdtd_plan** out) {
+  if (!out || !mesh || !grid || !physics) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (dtype_bytes != 4 && dtype_bytes != 8) return fail(IFDTD_ERR_ARGUMENT, "dtype must be 4 or 8 bytes");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(IFDTD_ERR_UNSUPPORTED, "no CUDA device");
+  if (device < 0 || device >= n) return fail(IFDTD_ERR_UNSUPPORTED, "CUDA device index out of range");
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return fail(IFDTD_ERR_UNSUPPORTED, "this build targets sm_100a (B200)");
+  DeviceGuard guard(device);
+  ifdtd_plan* P = new ifdtd_plan();
+  P->dtype = dtype_bytes;
+  P->device = device;
+  const int rc = dtype_bytes == 4 ? build_plan<float>(P, mesh, grid, physics, tuning)
+                                  : build_plan<double>(P, mesh, grid, physics, tuning);
+  if (rc != IFDTD_OK) {
+    delete P;
+    return rc;
+  }
+  *out = P;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_plan_destroy(ifdtd_plan* plan) {
+  if (!plan) return IFDTD_OK;
+  DeviceGuard guard(plan->device);
+  cudaDeviceSynchronize();
+  for (ifdtd_probe* p : plan->probes) p->plan = nullptr;
+  delete plan;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes) {
+  if (!plan || !bytes) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  *bytes = (int64_t)plan->arena.bytes;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_step(ifdtd_plan* plan, const ifdtd_state* state, const double* currents, int32_t n_steps, void* stream) {
+  if (!plan) return fail(IFDTD_ERR_ARGUMENT, "null plan");
+  if (n_steps < 0) return fail(IFDTD_ERR_ARGUMENT, "negative step count");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->dtype == 4 ? run_steps<float>(plan, state, currents, n_steps, nullptr, nullptr, st)
+                          : run_steps<double>(plan, state, currents, n_steps, nullptr, nullptr, st);
+}
+
+int32_t ifdtd_update_magnetic(ifdtd_plan* plan, const ifdtd_state* state, void* stream) {
+  if (!plan) return fail(IFDTD_ERR_ARGUMENT, "null plan");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
+  if (rc) return rc;
+  if (plan->dtype == 4) {
+    const Rec<float>* rec = (const Rec<float>*)plan->d_rec;
+    if (plan->plasma) kh_kernel<float, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
+    else kh_kernel<float, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
+  } else {
+    const Rec<double>* rec = (const Rec<double>*)plan->d_rec;
+    if (plan->plasma) kh_kernel<double, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
+    else kh_kernel<double, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_update_electric(ifdtd_plan* plan, const ifdtd_state* state, double current, void* stream) {
+  if (!plan) return fail(IFDTD_ERR_ARGUMENT, "null plan");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
+  if (rc) return rc;
+  // pageable source: staged by the runtime before the call returns
+  CUDA_TRY(cudaMemcpyAsync(plan->d_cur, &current, sizeof(double), cudaMemcpyHostToDevice, st));
+  if (plan->dtype == 4) {
+    const Rec<float>* rec = (const Rec<float>*)plan->d_rec;
+    if (plan->plasma) ke_kernel<float, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
+    else ke_kernel<float, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
+  } else {
+    const Rec<double>* rec = (const Rec<double>*)plan->d_rec;
+    if (plan->plasma) ke_kernel<double, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
+    else ke_kernel<double, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_probe_create(ifdtd_plan* plan, int32_t field_kind, int32_t rows, int32_t width, const int64_t* index,
+                           const int64_t* layer, const double* weight, ifdtd_probe** out) {
+  if (!plan || !out || !index || !layer || !weight) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  if (field_kind < 0 || field_kind > 3 || rows <= 0 || width <= 0) return fail(IFDTD_ERR_ARGUMENT, "bad probe shape");
+  const int64_t n_ent = field_kind == 0 ? plan->nV : field_kind == 2 ? plan->nF : plan->nE;
+  const int64_t n_lay = (field_kind == 0 || field_kind == 3) ? plan->L + 1 : plan->L;
+  const size_t n = (size_t)rows * width;
+  std::vector<int> idx(n), lay(n);
+  std::vector<double> w(weight, weight + n);
+  for (size_t i = 0; i < n; ++i) {
+    if (index[i] < 0 || index[i] >= n_ent || layer[i] < 0 || layer[i] >= n_lay)
+      return fail(IFDTD_ERR_ARGUMENT, "probe index out of range");
+    idx[i] = (int)index[i];
+    lay[i] = (int)layer[i];
+  }
+  DeviceGuard guard(plan->device);
+  ifdtd_probe* p = new ifdtd_probe();
+  p->plan = plan;
+  p->kind = field_kind;
+  p->rows = rows;
+  p->width = width;
+  const int* di = nullptr;
+  const int* dl = nullptr;
+  const double* dw = nullptr;
+  void* stg = nullptr;
+  if (p->arena.upload(idx, &di) != cudaSuccess || p->arena.upload(lay, &dl) != cudaSuccess ||
+      p->arena.upload(w, &dw) != cudaSuccess ||
+      p->arena.alloc((size_t)std::max(plan->chunk, 1) * rows * sizeof(double), &stg) != cudaSuccess) {
+    delete p;
+    return fail(IFDTD_ERR_CUDA, "probe upload failed");
+  }
+  p->index = (int*)di;
+  p->layer = (int*)dl;
+  p->weight = (double*)dw;
+  p->staging = (double*)stg;
+  plan->probes.push_back(p);
+  *out = p;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_probe_destroy(ifdtd_probe* probe) {
+  // the probe's buffers are released with it; graphs that sample it are dropped
+  if (!probe) return IFDTD_OK;
+  if (probe->plan) {
+    DeviceGuard guard(probe->plan->device);
+    cudaDeviceSynchronize();
+    auto& v = probe->plan->probes;
+    v.erase(std::remove(v.begin(), v.end(), probe), v.end());
+    auto& g = probe->plan->graphs;
+    for (auto it = g.begin(); it != g.end();) {
+      if (it->probe == probe) {
+        cudaGraphExecDestroy(it->exec);
+        it = g.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  delete probe;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_sample(ifdtd_plan* plan, const ifdtd_state* state, const ifdtd_probe* probe, double* out_row,
+                     void* stream) {
+  if (!plan || !probe || !out_row || probe->plan != plan) return fail(IFDTD_ERR_ARGUMENT, "bad sample arguments");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
+  if (rc) return rc;
+  const void* field = probe->kind == 0 ? state->er : probe->kind == 1 ? state->et : probe->kind == 2 ? state->hr : state->ht;
+  const int pitch = (probe->kind == 0 || probe->kind == 3) ? plan->L + 1 : plan->L;
+  const int blocks = (probe->rows * 32 + 255) / 256;
+  if (plan->dtype == 4)
+    sample_kernel<float><<<blocks, 256, 0, st>>>((const float*)field, pitch, probe->rows, probe->width, probe->index,
+                                                 probe->layer, probe->weight, out_row);
+  else
+    sample_kernel<double><<<blocks, 256, 0, st>>>((const double*)field, pitch, probe->rows, probe->width,
+                                                  probe->index, probe->layer, probe->weight, out_row);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_step_sampled(ifdtd_plan* plan, const ifdtd_state* state, const double* currents, int32_t n_steps,
+                           const ifdtd_probe* probe, double* out_rows, void* stream) {
+  if (!plan || !probe || !out_rows || probe->plan != plan) return fail(IFDTD_ERR_ARGUMENT, "bad sampled-step arguments");
+  if (n_steps < 0) return fail(IFDTD_ERR_ARGUMENT, "negative step count");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->dtype == 4 ? run_steps<float>(plan, state, currents, n_steps, probe, out_rows, st)
+                          : run_steps<double>(plan, state, currents, n_steps, probe, out_rows, st);
+}
+
+int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, void* stream) {
+  if (!plan || !state || !out4) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemsetAsync(out4, 0, 4 * sizeof(double), st));
+  const size_t n0 = (size_t)plan->nV * (plan->L + 1), n1 = (size_t)plan->nE * plan->L;
+  const size_t n2 = (size_t)plan->nF * plan->L, n3 = (size_t)plan->nE * (plan->L + 1);
+  dim3 grid(grid_for(std::max(std::max(n0, n1), std::max(n2, n3))), 4);
+  if (plan->dtype == 4)
+    max_abs_kernel<float><<<grid, 256, 0, st>>>((const float*)state->er, n0, (const float*)state->et, n1,
+                                                (const float*)state->hr, n2, (const float*)state->ht, n3,
+                                                (unsigned long long*)out4);
+  else
+    max_abs_kernel<double><<<grid, 256, 0, st>>>((const double*)state->er, n0, (const double*)state->et, n1,
+                                                 (const double*)state->hr, n2, (const double*)state->ht, n3,
+                                                 (unsigned long long*)out4);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+#define PRIM_PROLOGUE                                                        \
+  if (!plan || !in || !out || cols <= 0) return fail(IFDTD_ERR_ARGUMENT, "bad primitive arguments"); \
+  DeviceGuard guard(plan->device);                                           \
+  cudaStream_t st = (cudaStream_t)stream;
+
+int32_t ifdtd_edge_difference(ifdtd_plan* plan, const void* in, int32_t cols, void* out, void* stream) {
+  PRIM_PROLOGUE
+  const int g = grid_for((size_t)plan->nE * cols);
+  if (plan->dtype == 4)
+    pair_difference_kernel<float><<<g, 256, 0, st>>>((const float*)in, cols, plan->nE, plan->edge_th, false, (float*)out);
+  else
+    pair_difference_kernel<double><<<g, 256, 0, st>>>((const double*)in, cols, plan->nE, plan->edge_th, false,
+                                                      (double*)out);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_dual_edge_difference(ifdtd_plan* plan, const void* in, int32_t cols, void* out, void* stream) {
+  PRIM_PROLOGUE
+  const int g = grid_for((size_t)plan->nE * cols);
+  if (plan->dtype == 4)
+    pair_difference_kernel<float><<<g, 256, 0, st>>>((const float*)in, cols, plan->nE, plan->edge_lr, true, (float*)out);
+  else
+    pair_difference_kernel<double><<<g, 256, 0, st>>>((const double*)in, cols, plan->nE, plan->edge_lr, true,
+                                                      (double*)out);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_face_circulation(ifdtd_plan* plan, const void* in, int32_t cols, void* out, void* stream) {
+  PRIM_PROLOGUE
+  const int g = grid_for((size_t)plan->nF * cols);
+  if (plan->dtype == 4)
+    face_circulation_kernel<float><<<g, 256, 0, st>>>((const float*)in, cols, plan->nF, plan->face_e, plan->face_sign,
+                                                      (float*)out);
+  else
+    face_circulation_kernel<double><<<g, 256, 0, st>>>((const double*)in, cols, plan->nF, plan->face_e,
+                                                       plan->face_sign, (double*)out);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_dual_cell_circulation(ifdtd_plan* plan, const void* in, int32_t cols, void* out, void* stream) {
+  PRIM_PROLOGUE
+  const int g = grid_for((size_t)plan->nV * cols);
+  if (plan->dtype == 4)
+    dual_cell_circulation_kernel<float><<<g, 256, 0, st>>>((const float*)in, cols, plan->nV, plan->v_off, plan->v_edge,
+                                                           plan->v_sign, (float*)out);
+  else
+    dual_cell_circulation_kernel<double><<<g, 256, 0, st>>>((const double*)in, cols, plan->nV, plan->v_off,
+                                                            plan->v_edge, plan->v_sign, (double*)out);
+  CUDA_TRY(cudaGetLastError());
+  return IFDTD_OK;
+}
+
+}  // extern "C"

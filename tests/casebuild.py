@@ -135,3 +135,99 @@ def grouped_rel_l2(actual: dict, expected: dict) -> dict[str, float]:
         e = np.concatenate([np.asarray(expected[f], dtype=np.float64).ravel() for f in group])
         out["".join(group)] = rel_l2(a, e)
     return out
+
+
+def product_provenance():
+    from ionosphere_fdtd_b200 import DatasetProvenance, VariableProvenance
+
+    return DatasetProvenance(
+        dataset_id="golden.synthetic-plasma.v1",
+        title="Synthetic plasma for parity fixtures",
+        version="1",
+        source_url="https://example.invalid/golden-plasma",
+        citation="Synthetic fixture.",
+        license="CC0-1.0",
+        retrieved_at="2026-12-01T00:00:00Z",
+        source_sha256="0" * 64,
+        coordinate_reference_system="geocentric Cartesian",
+        variables=(
+            VariableProvenance("B", "T", "T", "identity"),
+            VariableProvenance("number_density", "m^-3", "m^-3", "identity"),
+            VariableProvenance("collision_frequency", "Hz", "Hz", "identity"),
+        ),
+    )
+
+
+def build_product(case: dict, dtype: str = "float64", **kwargs):
+    """The CUDA engine (GeodesicFDTD of ionosphere_fdtd_b200) for a parity case."""
+
+    import ionosphere_fdtd_b200 as P
+
+    cfg = P.SimulationConfig(**case["config"])
+    mesh = P.build_geodesic_mesh(cfg.subdivision)
+    mat = case.get("material", "default")
+    if mat == "default":
+        material = None
+    elif mat == "profile":
+        material = C.ProfileMaterial()
+    elif mat == "patchy":
+        material = C.PatchyMaterial()
+    else:
+        material = P.EarthIonosphereMaterial(**mat[1])
+    source = None
+    spec = case.get("source")
+    if spec is not None:
+        spec = dict(spec)
+        kind = spec.pop("kind")
+        if "seed_vertex" in spec:
+            lat, lon = C.vertex_lat_lon(mesh.vertices, C.source_vertex(mesh.n_vertices, spec.pop("seed_vertex")))
+            spec.update(latitude_deg=lat, longitude_deg=lon)
+        source = (P.TangentialGaussianCurrent if kind == "tangential" else P.GaussianCurrent)(**spec)
+    surface = None
+    sspec = case.get("surface")
+    if sspec is not None:
+        sigma = sspec["value"] if sspec["conductivity"] == "scalar" else C.smooth_log_normal(mesh.edge_midpoints(), sspec["seed"])
+        surface = P.ConductiveHalfSpaceSurface(sigma)
+    plasma = None
+    pspec = case.get("plasma")
+    if pspec is not None:
+        mids, magnetic, species = plasma_arrays(pspec, mesh.n_faces, case["config"])
+        names = ["electron", "O+"]
+        plasma = P.MeshPlasmaModel.from_mesh(
+            mesh,
+            mids,
+            magnetic,
+            tuple(P.ColdPlasmaSpecies(names[i], q, m, n, nu) for i, (q, m, n, nu) in enumerate(species)),
+            provenance=(product_provenance(),),
+            interpolation="synthetic",
+        )
+    sim = P.GeodesicFDTD(
+        cfg, material=material, source=source, surface_impedance=surface, plasma=plasma, mesh=mesh,
+        backend="torch", device="cuda", dtype=dtype, **kwargs,
+    )
+    init = case.get("init")
+    if init is not None:
+        shapes = {n: tuple(getattr(sim, n).shape) for n in ("er", "et", "hr", "ht")}
+        for n, v in C.initial_fields(shapes, *init).items():
+            getattr(sim, n).copy_(sim.backend.asarray(v))
+    return sim
+
+
+def run_product(case: dict, dtype: str = "float64", **kwargs) -> dict[str, np.ndarray]:
+    sim = build_product(case, dtype, **kwargs)
+    out = {"time_step_s": np.asarray(sim.time_step_s), "cfl_limit_s": np.asarray(sim.cfl_time_step_limit_s)}
+    rspec = case.get("receivers")
+    if rspec is not None:
+        v, k, w = C.receiver_rows(sim.mesh.n_vertices, sim.altitudes_m, rspec["seed"], rspec["count"])
+        out["traces"] = sim.record_er_observations(v, k, w, case["steps"])
+    else:
+        sim.step(case["steps"])
+    for f in ("er", "et", "hr", "ht"):
+        out[f] = sim.to_numpy(getattr(sim, f))
+    if sim._surface_impedance_ade is not None:
+        out["si_memory"] = sim.to_numpy(sim._surface_impedance_ade.memory)
+    if sim._plasma_coupler is not None:
+        for i, j in enumerate(sim._plasma_coupler.ade.current_density):
+            out[f"plasma_current_{i}"] = sim.to_numpy(j)
+    out["_sim"] = sim
+    return out

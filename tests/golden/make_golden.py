@@ -165,8 +165,37 @@ def mesh_fixtures(mods) -> None:
     (HERE / "mesh_digests.json").write_text(json.dumps(digests, indent=1, sort_keys=True) + "\n")
 
 
+def checkpoint_fixture(mods) -> None:
+    """A reference-written v4 checkpoint (surface impedance + source, float64)
+    and the reference's continuation after 7 more steps."""
+
+    _, rsolver, rsources, rsi, _, rmat, _, _ = mods
+    cfg = rsolver.SimulationConfig(
+        subdivision=1, radial_cells=4, minimum_altitude_m=0.0, maximum_altitude_m=100_000.0,
+        courant_factor=0.25, radial_boundary_condition="surface-impedance",
+    )
+    source = rsources.GaussianCurrent(peak_current_a=2.0e6, center_time_s=1.0e-4, one_over_e_half_width_s=5.0e-5, carrier_frequency_hz=5.0)
+    sim = rsolver.GeodesicFDTD(cfg, material=rmat.EarthIonosphereMaterial(), source=source,
+                               surface_impedance=rsi.ConductiveHalfSpaceSurface(1.0 / 30.0), backend="numpy", dtype="float64")
+    shapes = {n: getattr(sim, n).shape for n in ("er", "et", "hr", "ht")}
+    for n, v in C.initial_fields(shapes, 99, 1.0e-9).items():
+        getattr(sim, n)[:] = v
+    sim.step(5)
+    sim.save_checkpoint(HERE / "reference_checkpoint_v4.npz")
+    sim.step(7)
+    np.savez_compressed(
+        HERE / "reference_checkpoint_continuation.npz",
+        steps_before=np.asarray(5), steps_after=np.asarray(7),
+        er=sim.er, et=sim.et, hr=sim.hr, ht=sim.ht, si_memory=sim._surface_impedance_ade.memory,
+    )
+
+
 def main(src: str) -> None:
     mods = _import_reference(src)
+    if "--checkpoint-only" in sys.argv:
+        checkpoint_fixture(mods)
+        return
+    checkpoint_fixture(mods)
     mesh_fixtures(mods)
     for name, case in C.CASES.items():
         np.savez_compressed(HERE / f"case_{name}.npz", **run_case(name, case, mods))
@@ -192,4 +221,5 @@ def main(src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else "/root/reference/src")

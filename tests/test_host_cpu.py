@@ -1,0 +1,214 @@
+"""Host-side parts of the engine that need no GPU: mesh tables (bit-exact with
+the reference), setup coefficients (against the oracle), validation, and the
+C ABI library's exports."""
+
+import hashlib
+import json
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import cases as C
+from casebuild import GOLDEN, golden
+
+import ionosphere_fdtd_b200 as P
+from ionosphere_fdtd_b200 import plasma as PL
+
+ROOT = Path(__file__).resolve().parent.parent
+INT_TABLES = ("edges", "faces", "face_edges", "face_edge_signs", "edge_left_faces", "edge_right_faces", "vertex_degree")
+FLOAT_TABLES = ("vertices", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles", "dual_cell_solid_angles")
+
+
+@pytest.mark.parametrize("level", [0, 1, 2, 3])
+def test_mesh_tables_are_bit_exact_with_reference(level):
+    ref = golden(f"mesh_s{level}")
+    mesh = P.build_geodesic_mesh(level)
+    for name in INT_TABLES + FLOAT_TABLES:
+        np.testing.assert_array_equal(getattr(mesh, name), ref[name], err_msg=name)
+
+
+@pytest.mark.parametrize("level", [4, 5, 6])
+def test_mesh_digests_match_reference(level):
+    digests = json.loads((GOLDEN / "mesh_digests.json").read_text())[str(level)]
+    mesh = P.build_geodesic_mesh(level)
+    for name in INT_TABLES:
+        got = hashlib.sha256(np.ascontiguousarray(getattr(mesh, name), dtype=np.int64).tobytes()).hexdigest()
+        assert got == digests[name], name
+    for name in FLOAT_TABLES:
+        got = hashlib.sha256(np.ascontiguousarray(getattr(mesh, name), dtype=np.float64).tobytes()).hexdigest()
+        assert got == digests[name], name
+
+
+def test_mesh_counts_and_topology():
+    for level in range(5):
+        m = P.build_geodesic_mesh(level)
+        assert (m.n_vertices, m.n_edges, m.n_faces) == (10 * 4**level + 2, 30 * 4**level, 20 * 4**level)
+        assert np.count_nonzero(m.vertex_degree == 5) == 12
+        assert not m.vertices.flags.writeable
+        # boundary of boundary: grad then curl vanishes
+        x = np.random.default_rng(level).standard_normal(m.n_vertices)
+        np.testing.assert_allclose(m.face_circulation(m.edge_difference(x)), 0.0, atol=1e-12)
+
+
+def test_custom_topology_renumbering_is_accepted():
+    uniform = P.build_geodesic_mesh(1)
+    custom = P.build_geodesic_mesh_from_topology(uniform.vertices, np.roll(uniform.faces, 1, axis=0))
+    assert custom.topology_kind == "custom" and custom.n_edges == uniform.n_edges
+
+
+def test_plasma_tables_match_oracle():
+    import oracle.fdtd as O
+    from casebuild import build_oracle
+
+    case = C.CASES["plasma_magnetized_s1"]
+    ora = build_oracle(case)
+    mesh = P.build_geodesic_mesh(1)
+    recon, _ = PL.face_reconstruction(mesh)
+    np.testing.assert_array_equal(recon, ora.p_recon)
+    faces, weights = PL.vertex_face_average(mesh)
+    np.testing.assert_array_equal(faces, ora.p_vfaces)
+    np.testing.assert_array_equal(weights, ora.p_vweights)
+    assert O.OracleFDTD is type(ora)
+
+
+def test_plasma_coefficients_compress_exactly_for_altitude_profiles():
+    from casebuild import plasma_arrays, product_provenance
+
+    case = C.CASES["plasma_drude_s2"]
+    mesh = P.build_geodesic_mesh(2)
+    mids, magnetic, species = plasma_arrays(case["plasma"], mesh.n_faces, case["config"])
+    model = P.MeshPlasmaModel.from_mesh(
+        mesh, mids, magnetic, tuple(P.ColdPlasmaSpecies(f"s{i}", *s) for i, s in enumerate(species)),
+        provenance=(product_provenance(),), interpolation="synthetic",
+    )
+    coef, bdir, magnetized, rows = PL.ade_coefficients(model, 1.0e-6)
+    assert rows == 1 and not magnetized
+    # the same coefficients computed on the full grid, row by row
+    full = []
+    nu = species[0][3]
+    full_decay = np.exp(-nu * 1.0e-6)
+    np.testing.assert_array_equal(np.broadcast_to(coef[0, 0], full_decay.shape), full_decay)
+    assert coef.shape == (1, 6, 1, len(mids)) and not full
+
+
+def test_simulation_config_validation_messages():
+    with pytest.raises(ValueError, match="mesh_relaxations"):
+        P.SimulationConfig(mesh_relaxations=-1)
+    with pytest.raises(ValueError, match="finite"):
+        P.SimulationConfig(time_step_s=np.nan)
+    with pytest.raises(ValueError, match="radial_cells"):
+        P.SimulationConfig(subdivision=1, radial_cells=6, radial_altitudes_m=(-100_000.0, 0.0, 100_000.0))
+    with pytest.raises(ValueError, match="minimum_altitude_m=0"):
+        P.SimulationConfig(radial_boundary_condition="surface-impedance")
+    with pytest.raises(ValueError, match="geometry_mode"):
+        P.SimulationConfig(geometry_mode="flat")
+    with pytest.raises(ValueError, match="smoothly graded"):
+        P.SimulationConfig(subdivision=0, radial_cells=5, minimum_altitude_m=-10_000.0, maximum_altitude_m=4_000.0,
+                           radial_altitudes_m=(-10_000.0, -6_000.0, -2_000.0, -1_000.0, 0.0, 4_000.0))
+
+
+def test_sources_match_oracle_supports_and_waveform():
+    import oracle.fdtd as O
+
+    src = P.GaussianCurrent(peak_current_a=2.0, carrier_frequency_hz=20.0)
+    osrc = O.OracleSource(peak_current_a=2.0, carrier_frequency_hz=20.0)
+    times = np.linspace(0.0, 0.2, 101)
+    np.testing.assert_array_equal(src.current_series(times, 1e-5), [src.current_a(t, 1e-5) for t in times])
+    np.testing.assert_allclose([src.current_a(t, 1e-5) for t in times], [osrc.current_a(t, 1e-5) for t in times], rtol=0, atol=0)
+
+
+def test_surface_impedance_fit_and_coefficients():
+    model = P.ConductiveHalfSpaceSurface(1.0e-2)
+    import oracle.fdtd as O
+
+    ref = O.OracleSurface(1.0e-2)
+    np.testing.assert_array_equal(model.pole_rates_s_inv, ref.poles())
+    np.testing.assert_array_equal(model.diffusive_weights_sqrt_s_inv, ref.weights())
+    f = np.linspace(5.0, 45.0, 9)
+    rel = np.abs(model.impedance_ohm(f) - model.exact_impedance_ohm(f)) / np.abs(model.exact_impedance_ohm(f))
+    assert np.max(rel) < 0.05
+
+
+def test_geodesic_fdtd_refuses_cpu_backends():
+    with pytest.raises(P.BackendUnavailableError):
+        P.GeodesicFDTD(P.SimulationConfig(subdivision=0, radial_cells=2), backend="numpy")
+    try:
+        import torch
+
+        cuda = torch.cuda.is_available()
+    except ImportError:  # pragma: no cover
+        cuda = False
+    if not cuda:
+        with pytest.raises(P.BackendUnavailableError):
+            P.GeodesicFDTD(P.SimulationConfig(subdivision=0, radial_cells=2), backend="torch", device="cuda")
+    with pytest.raises(P.BackendUnavailableError):
+        P.GeodesicFDTD(P.SimulationConfig(subdivision=0, radial_cells=2), backend="torch", device="cpu")
+
+
+def test_checkpoint_metadata_rejects_foreign_files(tmp_path):
+    path = tmp_path / "bad.npz"
+    np.savez_compressed(path, metadata=np.asarray(json.dumps({"format": "other", "version": 4})))
+    with pytest.raises(P.CheckpointError, match="not an ionosphere-fdtd checkpoint"):
+        P.load_checkpoint(path)
+    np.savez_compressed(path, metadata=np.asarray(json.dumps({"format": "ionosphere-fdtd-checkpoint", "version": 9})))
+    with pytest.raises(P.CheckpointError, match="unsupported checkpoint version"):
+        P.load_checkpoint(path)
+    (tmp_path / "trunc.npz").write_bytes(b"PK\x03\x04 truncated")
+    with pytest.raises(P.CheckpointError):
+        P.load_checkpoint(tmp_path / "trunc.npz")
+
+
+def test_plasma_artifact_round_trip_and_corruption(tmp_path):
+    from casebuild import product_provenance
+
+    mesh = P.build_geodesic_mesh(0)
+    shape = (mesh.n_faces, 2)
+    magnetic = np.zeros((*shape, 3))
+    magnetic[..., 2] = 5e-5
+    sp = P.ColdPlasmaSpecies("electron", -P.ELEMENTARY_CHARGE_C, P.ELECTRON_MASS_KG, np.full(shape, 1e3), np.full(shape, 200.0))
+    model = P.MeshPlasmaModel.from_mesh(mesh, np.asarray((25e3, 75e3)), magnetic, (sp,), provenance=(product_provenance(),), interpolation="x")
+    restored = P.MeshPlasmaModel.load(model.save(tmp_path / "p.npz"))
+    assert restored.content_sha256 == model.content_sha256
+    with np.load(tmp_path / "p.npz") as a:
+        arrays = {n: np.array(a[n]) for n in a.files}
+    arrays["magnetic_field_t"][0, 0, 0] += 1e-9
+    np.savez_compressed(tmp_path / "c.npz", **arrays)
+    with pytest.raises(ValueError, match="checksum mismatch"):
+        P.MeshPlasmaModel.load(tmp_path / "c.npz")
+
+
+def _declared_symbols() -> set[str]:
+    text = (ROOT / "include" / "ifdtd.h").read_text()
+    return set(re.findall(r"^\s*int32_t\s+(ifdtd_\w+)\s*\(", text, flags=re.M))
+
+
+def test_c_abi_library_exports_every_declared_symbol():
+    import ctypes
+
+    from ionosphere_fdtd_b200 import _native as N
+    from ionosphere_fdtd_b200.build import build
+
+    build()
+    lib = ctypes.CDLL(str(N.LIBRARY))
+    declared = _declared_symbols()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(N.exported_symbols())
+    assert N.load().ifdtd_version() >= 10000
+
+
+def test_c_abi_reports_missing_device_or_bad_arguments():
+    import ctypes
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    lib = N.load()
+    plan = ctypes.c_void_p()
+    status = lib.ifdtd_plan_create(None, None, None, None, 4, 0, ctypes.byref(plan))
+    assert status == N.ERR_ARGUMENT and "null" in N.last_error()
+    count = ctypes.c_int32(-1)
+    lib.ifdtd_device_count(ctypes.byref(count))
+    assert count.value >= 0

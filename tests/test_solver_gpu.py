@@ -1,0 +1,206 @@
+"""Reference-style behaviour tests of the CUDA engine (mirrors of the reference's
+tests/test_backends.py, test_solver.py, test_surface_impedance.py,
+test_checkpoint.py on the public API)."""
+
+import numpy as np
+import pytest
+
+import ionosphere_fdtd_b200 as P
+from ionosphere_fdtd_b200 import GeodesicFDTD, SimulationConfig
+from ionosphere_fdtd_b200.constants import MU_0
+
+pytestmark = pytest.mark.gpu
+
+
+def small_config(**changes):
+    values = dict(subdivision=1, radial_cells=6, courant_factor=0.25)
+    values.update(changes)
+    return SimulationConfig(**values)
+
+
+def sim(config=None, **kw):
+    kw.setdefault("device", "cuda")
+    kw.setdefault("dtype", "float64")
+    return GeodesicFDTD(config or small_config(), **kw)
+
+
+@pytest.mark.parametrize("trailing", [(), (7,), (3, 4)])
+def test_primitives_match_mesh_operators(trailing):
+    s = sim()
+    mesh = s.mesh
+    rng = np.random.default_rng(42)
+    b = s.backend
+    ev = rng.standard_normal((mesh.n_edges,) + trailing)
+    vv = rng.standard_normal((mesh.n_vertices,) + trailing)
+    fv = rng.standard_normal((mesh.n_faces,) + trailing)
+    np.testing.assert_allclose(b.to_numpy(b.face_circulation(b.asarray(ev))), mesh.face_circulation(ev), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(b.to_numpy(b.dual_cell_circulation(b.asarray(ev))), mesh.dual_cell_circulation(ev), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(b.to_numpy(b.edge_difference(b.asarray(vv))), mesh.edge_difference(vv), rtol=0, atol=0)
+    np.testing.assert_allclose(b.to_numpy(b.dual_edge_difference(b.asarray(fv))), mesh.dual_edge_difference(fv), rtol=0, atol=0)
+
+
+def test_dual_cell_circulation_is_bitwise_repeatable():
+    s = sim(SimulationConfig(subdivision=3, radial_cells=6, courant_factor=0.2))
+    values = s.backend.asarray(np.random.default_rng(20260805).standard_normal((s.mesh.n_edges, 7)))
+    first = s.backend.dual_cell_circulation(values)
+    for _ in range(10):
+        assert s.backend.torch.equal(first, s.backend.dual_cell_circulation(values))
+
+
+def test_float32_face_circulation_keeps_precision_semantics():
+    s = sim(dtype="float32")
+    mesh = s.mesh
+    values = np.zeros(mesh.n_edges, dtype=np.float32)
+    values[mesh.face_edges[0]] = np.asarray((1.0e8, 1.0, -1.0e8), dtype=np.float32) * mesh.face_edge_signs[0]
+    out = s.backend.to_numpy(s.backend.face_circulation(s.backend.asarray(values)))
+    assert out.dtype == np.float32
+    np.testing.assert_array_equal(out, mesh.face_circulation(values))
+
+
+def test_zero_fields_are_stationary():
+    s = sim()
+    s.step(3)
+    for f in ("er", "et", "hr", "ht"):
+        assert not np.any(s.to_numpy(getattr(s, f)))
+
+
+def test_loss_coefficient_damps_uncoupled_radial_field():
+    s = sim(material=P.EarthIonosphereMaterial(lithosphere_conductivity_s_m=1.0e-2))
+    s.er[:, 0] = 1.0
+    expected = s.to_numpy(s._ca_er)[:, 0].copy()
+    s.step()
+    assert np.allclose(s.to_numpy(s.er)[:, 0], expected)
+
+
+def test_radial_pec_ghosts_give_the_one_sided_curl():
+    s = sim(small_config(geometry_mode="thin-shell"))
+    profile = np.arange(1, s.et.shape[1] + 1, dtype=np.float64)
+    s.et[0] = s.backend.asarray(profile)
+    expected = np.empty(s.ht.shape[1])
+    expected[0] = 2.0 * profile[0] / s.radial_steps_m[0]
+    expected[-1] = -2.0 * profile[-1] / s.radial_steps_m[-1]
+    expected[1:-1] = np.diff(profile) / np.diff(s.radial_midpoints_m)
+    s._update_magnetic_fields()
+    np.testing.assert_allclose(s.to_numpy(s.ht)[0], -s.time_step_s / MU_0 * expected, rtol=1e-14, atol=0.0)
+
+
+def test_high_conductivity_surface_converges_to_lower_pec_curl():
+    base = dict(subdivision=0, radial_cells=4, minimum_altitude_m=0.0, maximum_altitude_m=100_000.0, courant_factor=0.2)
+    pec = sim(SimulationConfig(**base))
+    imp = sim(SimulationConfig(radial_boundary_condition="surface-impedance", **base), surface_impedance=P.ConductiveHalfSpaceSurface(1.0e30))
+    rng = np.random.default_rng(20260820)
+    er = rng.standard_normal(tuple(pec.er.shape))
+    et = rng.standard_normal(tuple(pec.et.shape))
+    ht = rng.standard_normal(tuple(pec.ht.shape))
+    for s in (pec, imp):
+        s.er.copy_(s.backend.asarray(er))
+        s.et.copy_(s.backend.asarray(et))
+        s.ht.copy_(s.backend.asarray(ht))
+        s._update_magnetic_fields()
+    np.testing.assert_allclose(imp.to_numpy(imp.ht), pec.to_numpy(pec.ht), rtol=2e-13, atol=2e-14)
+
+
+def test_plasma_current_changes_et_and_limits_time_step():
+    from casebuild import product_provenance
+
+    mesh = P.build_geodesic_mesh(0)
+    shape = (mesh.n_faces, 2)
+    magnetic = np.zeros((*shape, 3))
+    magnetic[..., 2] = 50e-6
+    species = P.ColdPlasmaSpecies("electron", -P.ELEMENTARY_CHARGE_C, P.ELECTRON_MASS_KG, np.full(shape, 1e8), np.full(shape, 200.0))
+    model = P.MeshPlasmaModel.from_mesh(mesh, np.asarray((25_000.0, 75_000.0)), magnetic, (species,), provenance=(product_provenance(),), interpolation="synthetic")
+    cfg = SimulationConfig(subdivision=0, radial_cells=2, minimum_altitude_m=0.0, maximum_altitude_m=100_000.0, courant_factor=0.2)
+    plasma = sim(cfg, mesh=mesh, plasma=model)
+    vacuum = sim(cfg, mesh=mesh)
+    values = np.random.default_rng(20260820).standard_normal(tuple(plasma.et.shape)) * 1e-6
+    plasma.et.copy_(plasma.backend.asarray(values))
+    vacuum.et.copy_(vacuum.backend.asarray(values))
+    plasma._update_electric_fields()
+    vacuum._update_electric_fields()
+    assert np.max(np.abs(plasma.to_numpy(plasma.et) - vacuum.to_numpy(vacuum.et))) > 0.0
+    assert plasma.cfl_time_step_limit_s < vacuum.cfl_time_step_limit_s
+    assert plasma.diagnostics()["plasma_species"] == 1
+
+
+def test_observation_recording_includes_initial_state():
+    s = sim(source=P.GaussianCurrent(peak_current_a=1.0e6))
+    traces = s.record_er_observations(np.asarray(((0, 1, 2),)), np.asarray((3,)), np.asarray(((0.2, 0.3, 0.5),)), 5, synchronize_every=2)
+    assert traces.shape == (6, 1)
+    assert traces[0, 0] == 0.0
+    assert s.steps == 5
+    assert np.isfinite(traces).all()
+
+
+def test_observation_validation_matches_reference_messages():
+    s = sim()
+    with pytest.raises(ValueError, match="sum to one"):
+        s.record_er_observations(np.asarray(((0, 1),)), np.asarray((0,)), np.asarray(((0.2, 0.3),)), 1)
+    with pytest.raises(ValueError, match="finite"):
+        s.record_er_observations(np.asarray(((0,),)), np.asarray((0,)), np.asarray(((np.nan,),)), 1)
+    with pytest.raises(ValueError, match="integer"):
+        s.step(1.5)
+
+
+def test_leapfrog_clocks_and_diagnostics():
+    s = sim()
+    assert s.magnetic_time_s == pytest.approx(-0.5 * s.time_step_s)
+    s.er.copy_(s.backend.asarray(np.random.default_rng(1).standard_normal(tuple(s.er.shape))))
+    s.step(3)
+    d = s.diagnostics()
+    assert d["electric_time_s"] == pytest.approx(3 * s.time_step_s)
+    assert d["magnetic_time_s"] == pytest.approx(2.5 * s.time_step_s)
+    for f, key in (("er", "max_abs_er_v_m"), ("et", "max_abs_et_v_m"), ("hr", "max_abs_hr_a_m"), ("ht", "max_abs_ht_a_m")):
+        assert d[key] == float(np.max(np.abs(s.to_numpy(getattr(s, f)))))
+    assert d["backend"] == "torch" and d["device"].startswith("cuda")
+
+
+def test_diagnostics_report_nonfinite_fields():
+    s = sim(dtype="float32")
+    s.hr[3, 2] = float("nan")
+    assert np.isnan(s.diagnostics()["max_abs_hr_a_m"])
+
+
+def test_checkpoint_round_trip_and_continuation(tmp_path):
+    material = P.EarthIonosphereMaterial(anomalies=(P.SphericalAnomaly(35.0, 126.0, 500_000.0, -20_000.0, -1_000.0, 0.5),))
+    source = P.GaussianCurrent(peak_current_a=2.0e6, center_time_s=0.01, one_over_e_half_width_s=0.02, carrier_frequency_hz=5.0)
+    whole = sim(material=material, source=source)
+    part = sim(material=material, source=source)
+    whole.step(12)
+    part.step(5)
+    resumed = GeodesicFDTD.load_checkpoint(part.save_checkpoint(tmp_path / "state.npz"), device="cuda")
+    assert resumed.steps == 5
+    resumed.step(7)
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(resumed.to_numpy(getattr(resumed, f)), whole.to_numpy(getattr(whole, f)))
+
+
+def test_reference_checkpoint_loads_and_continues():
+    """A checkpoint written by the reference (NumPy, float64) restores on CUDA and
+    continues to the reference's own continuation."""
+
+    from casebuild import GOLDEN, golden
+
+    resumed = GeodesicFDTD.load_checkpoint(GOLDEN / "reference_checkpoint_v4.npz", device="cuda", dtype="float64")
+    cont = golden("reference_checkpoint_continuation")
+    assert resumed.steps == int(cont["steps_before"])
+    resumed.step(int(cont["steps_after"]))
+    for f in ("er", "et", "hr", "ht", "si_memory"):
+        got = resumed.to_numpy(resumed._surface_impedance_ade.memory) if f == "si_memory" else resumed.to_numpy(getattr(resumed, f))
+        scale = max(np.max(np.abs(cont[g])) for g in (("er", "et") if f in ("er", "et") else ("hr", "ht")))
+        np.testing.assert_allclose(got, cont[f], rtol=1e-9, atol=1e-11 * scale, err_msg=f)
+
+
+def test_surface_impedance_solver_remains_bounded():
+    cfg = SimulationConfig(subdivision=0, radial_cells=4, minimum_altitude_m=0.0, maximum_altitude_m=100_000.0, courant_factor=0.35, radial_boundary_condition="surface-impedance")
+    s = sim(cfg, surface_impedance=P.ConductiveHalfSpaceSurface(1.0 / 50.0))
+    rng = np.random.default_rng(20260820)
+    for name in ("er", "et"):
+        getattr(s, name).copy_(s.backend.asarray(377.0e-9 * rng.standard_normal(tuple(getattr(s, name).shape))))
+    for name in ("hr", "ht"):
+        getattr(s, name).copy_(s.backend.asarray(1.0e-9 * rng.standard_normal(tuple(getattr(s, name).shape))))
+    e0 = max(float(s.er.abs().max()), float(s.et.abs().max()))
+    h0 = max(float(s.hr.abs().max()), float(s.ht.abs().max()))
+    s.step(500)
+    e1 = max(float(s.er.abs().max()), float(s.et.abs().max()))
+    h1 = max(float(s.hr.abs().max()), float(s.ht.abs().max()))
+    assert np.isfinite(e1) and np.isfinite(h1) and e1 < 2 * e0 and h1 < 2 * h0
