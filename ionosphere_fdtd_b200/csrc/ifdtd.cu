@@ -84,7 +84,8 @@ struct ifdtd_plan {
   int dtype = 4;
   int device = 0;
   int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
-  int n_patches = 0, threads = 256, chunk = 32;
+  int n_patches = 0, threads = 256, chunk = 32, maxdeg = 6;
+  size_t smem_bytes = 0;
   bool plasma = false;
   DeviceArena arena;
   void* d_rec = nullptr;               // Rec<real> in device memory
@@ -226,6 +227,23 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     std::vector<int> cursor(vptr.begin(), vptr.end() - 1);
     for (int v = 0; v < nV; ++v) vlist[cursor[owner_v[v] / fpp]++] = v;
   }
+  // ---- fixed-width vertex slots in vlist order (reference slot order, zero-padded) ----
+  int maxdeg = 0;
+  for (int v = 0; v < nV; ++v) maxdeg = std::max(maxdeg, deg[v]);
+  const int MD = maxdeg <= 6 ? 6 : (maxdeg <= 12 ? 12 : 0);
+  if (MD == 0) return fail(IFDTD_ERR_UNSUPPORTED, "vertex degree above 12 is not supported");
+  std::vector<int> ps_edge((size_t)nV * MD);
+  std::vector<real> ps_coef((size_t)nV * MD);
+  for (int sl = 0; sl < nV; ++sl) {
+    const int v = vlist[sl];
+    const int q0 = v_off[v], n = v_off[v + 1] - q0;
+    for (int q = 0; q < MD; ++q) {
+      ps_edge[(size_t)sl * MD + q] = v_edge[q0 + (q < n ? q : 0)];
+      ps_coef[(size_t)sl * MD + q] = q < n ? v_coef[q0 + q] : real(0);
+    }
+  }
+  P->maxdeg = MD;
+
   // ---- radial metric ----
   const double* r = G->radii_m;
   std::vector<real> invr(L + 1), rr(L + 1), mid(L), invm(L), invdr(L), invcd(L + 1);
@@ -291,9 +309,13 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(fe, face_e);
   UP(fv, face_v);
   UP(fw, face_w);
-  UP(v_off, v_off);
-  UP(v_edge, v_edge);
-  UP(v_coef, v_coef);
+  UP(ps_edge, ps_edge);
+  UP(ps_coef, ps_coef);
+  {
+    cudaError_t e1 = A.upload(v_off, &P->v_off);
+    cudaError_t e2 = A.upload(v_edge, &P->v_edge);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(IFDTD_ERR_CUDA, "upload of vertex incidence failed");
+  }
   UP(invr, invr);
   UP(rr, rr);
   UP(mid, mid);
@@ -328,8 +350,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->edge_th = R.edge_th;
   P->edge_lr = R.edge_lr;
   P->face_e = R.face_e;
-  P->v_off = R.v_off;
-  P->v_edge = R.v_edge;
 
   // ---- surface impedance ----
   P->T = X->si_terms;
@@ -372,22 +392,26 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       UP(bd, bdir);
     }
     const int W = X->vertex_face_width;
-    std::vector<int> vf_off(nV + 1, 0), vf_face;
-    std::vector<real> vf_wc;
-    for (int v = 0; v < nV; ++v) {
+    std::vector<int> ps_face((size_t)nV * MD, 0);
+    std::vector<real> ps_wc((size_t)nV * MD * 3, real(0));
+    for (int sl = 0; sl < nV; ++sl) {
+      const int v = vlist[sl];
+      int n = 0, first = -1;
       for (int q = 0; q < W; ++q) {
         const double w = X->vertex_face_weights[(size_t)v * W + q];
         if (w == 0.0) continue;
         const int64_t f = X->vertex_faces[(size_t)v * W + q];
         if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
-        vf_face.push_back((int)f);
-        for (int c = 0; c < 3; ++c) vf_wc.push_back((real)(w * X->face_centers[3 * f + c]));
+        if (n >= MD) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
+        if (first < 0) first = (int)f;
+        ps_face[(size_t)sl * MD + n] = (int)f;
+        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * MD + n) * 3 + c] = (real)(w * X->face_centers[3 * f + c]);
+        ++n;
       }
-      vf_off[v + 1] = (int)vf_face.size();
+      for (int q = n; q < MD; ++q) ps_face[(size_t)sl * MD + q] = first < 0 ? 0 : first;
     }
-    UP(vf_off, vf_off);
-    UP(vf_face, vf_face);
-    UP(vf_wc, vf_wc);
+    UP(ps_face, ps_face);
+    UP(ps_wc, ps_wc);
     if (S > 1) {
       cudaError_t e = A.alloc((size_t)nF * L * 3 * sizeof(real), &P->d_jtot);
       if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of summed plasma current failed");
@@ -415,6 +439,10 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.src_er_vmax = vmax;
   R.src_et_emin = emin;
   R.src_et_emax = emax;
+  R.maxdeg = MD;
+  R.layer_reals = layer_reals(L, R.coef_full, X->plasma_species, R.plasma_full, R.magnetized);
+  P->smem_bytes = (size_t)R.layer_reals * sizeof(real);
+  if (P->smem_bytes > 200 * 1024) return fail(IFDTD_ERR_UNSUPPORTED, "radial grid too fine for the shared per-layer rows");
   R.dtmu = (real)(G->time_step_s / 1.256637062120e-6);
   {
     void* cur = nullptr;
@@ -457,15 +485,59 @@ int bind_state(ifdtd_plan* P, const ifdtd_state* st, cudaStream_t stream) {
 }
 
 template <typename real>
+constexpr int run_for() {
+  return sizeof(real) == 4 ? 4 : 2;
+}
+
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename real, bool PL>
+cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, cudaStream_t st) {
+  auto k = kh_kernel<real, PL, run_for<real>()>;
+  cudaError_t e = allow_smem(k, P->smem_bytes);
+  if (e != cudaSuccess) return e;
+  k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members);
+  return cudaGetLastError();
+}
+
+template <typename real, bool PL, int MD>
+cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, int istep,
+                        cudaStream_t st) {
+  auto k = ke_kernel<real, PL, run_for<real>(), MD>;
+  cudaError_t e = allow_smem(k, P->smem_bytes);
+  if (e != cudaSuccess) return e;
+  k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members, istep);
+  return cudaGetLastError();
+}
+
+template <typename real>
+cudaError_t launch_kh(ifdtd_plan* P, cudaStream_t st) {
+  const Rec<real>* rec = (const Rec<real>*)P->d_rec;
+  return P->plasma ? launch_kh_t<real, true>(P, rec, nullptr, 1, P->n_patches, st)
+                   : launch_kh_t<real, false>(P, rec, nullptr, 1, P->n_patches, st);
+}
+
+template <typename real>
+cudaError_t launch_ke(ifdtd_plan* P, int istep, cudaStream_t st) {
+  const Rec<real>* rec = (const Rec<real>*)P->d_rec;
+  if (P->maxdeg == 6)
+    return P->plasma ? launch_ke_t<real, true, 6>(P, rec, nullptr, 1, P->n_patches, istep, st)
+                     : launch_ke_t<real, false, 6>(P, rec, nullptr, 1, P->n_patches, istep, st);
+  return P->plasma ? launch_ke_t<real, true, 12>(P, rec, nullptr, 1, P->n_patches, istep, st)
+                   : launch_ke_t<real, false, 12>(P, rec, nullptr, 1, P->n_patches, istep, st);
+}
+
+template <typename real>
 cudaError_t launch_step(ifdtd_plan* P, int istep, const ifdtd_probe* probe, int row, cudaStream_t st) {
   const Rec<real>* rec = (const Rec<real>*)P->d_rec;
-  if (P->plasma) {
-    kh_kernel<real, true><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1);
-    ke_kernel<real, true><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1, istep);
-  } else {
-    kh_kernel<real, false><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1);
-    ke_kernel<real, false><<<P->n_patches, P->threads, 0, st>>>(rec, nullptr, 1, istep);
-  }
+  cudaError_t e = launch_kh<real>(P, st);
+  if (e != cudaSuccess) return e;
+  e = launch_ke<real>(P, istep, st);
+  if (e != cudaSuccess) return e;
   if (probe) {
     const int blocks = (probe->rows * 32 + 255) / 256;
     sample_rec_kernel<real><<<blocks, 256, 0, st>>>(rec, probe->kind, probe->rows, probe->width, probe->index,
@@ -610,15 +682,7 @@ int32_t ifdtd_update_magnetic(ifdtd_plan* plan, const ifdtd_state* state, void* 
   cudaStream_t st = (cudaStream_t)stream;
   const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
   if (rc) return rc;
-  if (plan->dtype == 4) {
-    const Rec<float>* rec = (const Rec<float>*)plan->d_rec;
-    if (plan->plasma) kh_kernel<float, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
-    else kh_kernel<float, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
-  } else {
-    const Rec<double>* rec = (const Rec<double>*)plan->d_rec;
-    if (plan->plasma) kh_kernel<double, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
-    else kh_kernel<double, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1);
-  }
+  CUDA_TRY(plan->dtype == 4 ? launch_kh<float>(plan, st) : launch_kh<double>(plan, st));
   CUDA_TRY(cudaGetLastError());
   return IFDTD_OK;
 }
@@ -631,15 +695,7 @@ int32_t ifdtd_update_electric(ifdtd_plan* plan, const ifdtd_state* state, double
   if (rc) return rc;
   // pageable source: staged by the runtime before the call returns
   CUDA_TRY(cudaMemcpyAsync(plan->d_cur, &current, sizeof(double), cudaMemcpyHostToDevice, st));
-  if (plan->dtype == 4) {
-    const Rec<float>* rec = (const Rec<float>*)plan->d_rec;
-    if (plan->plasma) ke_kernel<float, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
-    else ke_kernel<float, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
-  } else {
-    const Rec<double>* rec = (const Rec<double>*)plan->d_rec;
-    if (plan->plasma) ke_kernel<double, true><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
-    else ke_kernel<double, false><<<plan->n_patches, plan->threads, 0, st>>>(rec, nullptr, 1, 0);
-  }
+  CUDA_TRY(plan->dtype == 4 ? launch_ke<float>(plan, 0, st) : launch_ke<double>(plan, 0, st));
   CUDA_TRY(cudaGetLastError());
   return IFDTD_OK;
 }

@@ -212,3 +212,14 @@ def test_c_abi_reports_missing_device_or_bad_arguments():
     count = ctypes.c_int32(-1)
     lib.ifdtd_device_count(ctypes.byref(count))
     assert count.value >= 0
+
+
+def test_kernel_division_by_magic_multiply_is_exact():
+    """The step kernels split flat work indices with q = umulhi(n, ceil(2^32/d))
+    (d = 1 encoded as the identity); exact for every divisor they use."""
+
+    for d in range(1, 1025):
+        m = 0 if d == 1 else (0xFFFFFFFF // d + 1)
+        n = np.arange(0, 1 << 16, dtype=np.uint64)
+        q = n if m == 0 else (n * np.uint64(m)) >> np.uint64(32)
+        assert np.array_equal(q, n // d), d
