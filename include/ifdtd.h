@@ -12,11 +12,16 @@
  * the calling thread.
  *
  * Layout contract: every field is a row-major (entity, radial) array with the
- * radial index contiguous, exactly the reference's er (V, L+1), et (E, L),
- * hr (F, L), ht (E, L+1) arrays (solver.py:315-322); surface-impedance memory
- * is (E, T) (surface_impedance.py:203); plasma current densities are
- * (F, L, 3) per species (plasma.py:411).  Element type is float (dtype 4) or
- * double (dtype 8) for a whole plan.
+ * radial index contiguous, as the reference's er (V, L+1), et (E, L),
+ * hr (F, L), ht (E, L+1) arrays (solver.py:315-322), but with a row pitch
+ * chosen by the plan (ifdtd_plan_layout): node arrays er/ht use node_pitch
+ * >= L+1, midpoint arrays et/hr use mid_pitch >= L, both multiples of 16
+ * bytes, so that every radial run is one aligned 16-byte vector access.  The
+ * padding elements of a row must be zero on entry and stay zero.  Plasma
+ * current densities, (F, L, 3) per species in the reference (plasma.py:411),
+ * are stored component-major as (F, 3, mid_pitch).  Surface-impedance memory
+ * is (E, T) (surface_impedance.py:203).  Base pointers are 16-byte aligned.
+ * Element type is float (dtype 4) or double (dtype 8) for a whole plan.
  */
 #ifndef IFDTD_H
 #define IFDTD_H
@@ -114,7 +119,7 @@ typedef struct ifdtd_tuning {
 typedef struct ifdtd_state {
   void *er, *et, *hr, *ht;
   void* si_memory;                          /* (E,T) or NULL */
-  void* plasma_current[IFDTD_MAX_SPECIES];  /* (F,L,3) each */
+  void* plasma_current[IFDTD_MAX_SPECIES];  /* (F,3,mid_pitch) each */
 } ifdtd_state;
 
 int32_t ifdtd_version(void);
@@ -127,6 +132,8 @@ int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* gr
                           const ifdtd_physics_desc* physics, const ifdtd_tuning* tuning,
                           int32_t dtype_bytes, int32_t device, ifdtd_plan** out);
 int32_t ifdtd_plan_destroy(ifdtd_plan* plan);
+/* Row pitches (in elements) the plan expects for node and midpoint arrays. */
+int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* mid_pitch);
 /* Bytes of device memory held by the plan (tables, staging, scratch). */
 int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);
 

@@ -114,6 +114,7 @@ _SIGNATURES = {
     ),
     "ifdtd_plan_destroy": ([_vp], _i32),
     "ifdtd_plan_bytes": ([_vp, C.POINTER(C.c_int64)], _i32),
+    "ifdtd_plan_layout": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_step": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_update_magnetic": ([_vp, C.POINTER(State), _vp], _i32),
     "ifdtd_update_electric": ([_vp, C.POINTER(State), C.c_double, _vp], _i32),
@@ -171,6 +172,13 @@ def check(status: int, what: str) -> None:
     if status == ERR_UNSUPPORTED:
         raise BackendUnavailableError(message)
     raise RuntimeError(message)
+
+
+def row_pitch(n: int) -> int:
+    """Row pitch (elements) the plan uses for a radial extent of n samples:
+    n rounded up to a multiple of 4, so rows are 16-byte aligned."""
+
+    return (int(n) + 3) // 4 * 4
 
 
 def i64(a) -> np.ndarray:

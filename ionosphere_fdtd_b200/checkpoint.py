@@ -200,7 +200,7 @@ def load_checkpoint(
                 raise CheckpointError(f"checkpoint plasma current {i} has shape {saved.shape}, expected {tuple(current.shape)}")
             if not np.issubdtype(saved.dtype, np.floating) or not np.all(np.isfinite(saved)):
                 raise CheckpointError(f"checkpoint plasma current {i} is invalid")
-            expected_currents[i] = simulation.backend.asarray(saved)
+            current.copy_(simulation.backend.asarray(saved))
     steps = metadata["state"]["steps"]
     if isinstance(steps, bool) or not isinstance(steps, int) or steps < 0:
         raise CheckpointError("checkpoint step count must be a non-negative integer")

@@ -84,7 +84,7 @@ struct ifdtd_plan {
   int dtype = 4;
   int device = 0;
   int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
-  int n_patches = 0, threads = 256, chunk = 32, maxdeg = 6;
+  int n_patches = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
   size_t smem_bytes = 0;
   bool plasma = false;
   DeviceArena arena;
@@ -126,6 +126,8 @@ bool in_range(const int64_t* p, size_t n, int64_t hi) {
   return true;
 }
 
+int round4(int n) { return (n + 3) / 4 * 4; }
+
 template <typename real>
 int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G, const ifdtd_physics_desc* X,
                const ifdtd_tuning* tune) {
@@ -133,7 +135,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   std::memset(&R, 0, sizeof(R));
   const int nV = M->n_vertices, nE = M->n_edges, nF = M->n_faces, L = G->radial_cells;
   if (nV < 4 || nE < 6 || nF < 4 || L < 2) return fail(IFDTD_ERR_ARGUMENT, "mesh or radial grid too small");
-  if ((int64_t)nE * (L + 1) >= (int64_t)1 << 31 || (int64_t)nF * L * 3 >= (int64_t)1 << 31)
+  const int Pn = round4(L + 1), Pm = round4(L);
+  if ((int64_t)nE * Pn >= (int64_t)1 << 31 || (int64_t)nF * 3 * Pm >= (int64_t)1 << 31)
     return fail(IFDTD_ERR_ARGUMENT, "problem exceeds 2^31 samples per array");
   if (!in_range(M->edges, 2 * (size_t)nE, nV) || !in_range(M->faces, 3 * (size_t)nF, nV) ||
       !in_range(M->face_edges, 3 * (size_t)nF, nE) || !in_range(M->edge_left_faces, nE, nF) ||
@@ -142,7 +145,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int fpp = (tune && tune->faces_per_patch > 0) ? tune->faces_per_patch : 32;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
   if (threads % 32 || threads > 256) return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 <= 256");
-  if ((int64_t)fpp * 3 * (L + 1) >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
+  if ((int64_t)fpp * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
   P->threads = threads;
   // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
   P->chunk = (tune && tune->graph_chunk >= 0) ? tune->graph_chunk : 32;
@@ -150,6 +153,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->nE = nE;
   P->nF = nF;
   P->L = L;
+  P->Pn = Pn;
+  P->Pm = Pm;
   DeviceArena& A = P->arena;
 
   // ---- edges ----
@@ -168,7 +173,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   // ---- faces ----
   std::vector<int4> fe(nF), fv(nF);
   std::vector<int> fsign(3 * (size_t)nF);
-  std::vector<real> fw(3 * (size_t)nF);
+  std::vector<real> fw(4 * (size_t)nF, real(0));
   for (int f = 0; f < nF; ++f) {
     fe[f] = make_int4((int)M->face_edges[3 * f], (int)M->face_edges[3 * f + 1], (int)M->face_edges[3 * f + 2], 0);
     fv[f] = make_int4((int)M->faces[3 * f], (int)M->faces[3 * f + 1], (int)M->faces[3 * f + 2], 0);
@@ -177,7 +182,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       const int64_t s = M->face_edge_signs[3 * f + i];
       if (s != 1 && s != -1) return fail(IFDTD_ERR_ARGUMENT, "face edge signs must be +1 or -1");
       fsign[3 * f + i] = (int)s;
-      fw[3 * f + i] = (real)((double)s * M->primal_edge_angles[M->face_edges[3 * f + i]] * inv_a);
+      fw[4 * f + i] = (real)((double)s * M->primal_edge_angles[M->face_edges[3 * f + i]] * inv_a);
     }
   }
   // ---- vertex incidence in reference slot order: tail uses, then head uses ----
@@ -190,14 +195,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   for (int v = 0; v < nV; ++v) v_off[v + 1] = v_off[v] + deg[v];
   std::vector<int> fill(v_off.begin(), v_off.end() - 1);
   std::vector<int> v_edge(2 * (size_t)nE), v_sign(2 * (size_t)nE);
-  std::vector<real> v_coef(2 * (size_t)nE);
+  std::vector<double> v_coef(2 * (size_t)nE);
   for (int pass = 0; pass < 2; ++pass)
     for (int e = 0; e < nE; ++e) {
       const int v = pass == 0 ? th[e].x : th[e].y;
       const int q = fill[v]++;
       v_edge[q] = e;
       v_sign[q] = pass == 0 ? 1 : -1;
-      v_coef[q] = (real)((pass == 0 ? 1.0 : -1.0) * M->dual_edge_angles[e] / M->dual_cell_solid_angles[v]);
+      v_coef[q] = (pass == 0 ? 1.0 : -1.0) * M->dual_edge_angles[e] / M->dual_cell_solid_angles[v];
     }
   // ---- patches: faces [p*fpp, (p+1)*fpp), edges by lowest adjacent face, vertices by lowest incident face ----
   const int n_patches = (nF + fpp - 1) / fpp;
@@ -232,21 +237,22 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   for (int v = 0; v < nV; ++v) maxdeg = std::max(maxdeg, deg[v]);
   const int MD = maxdeg <= 6 ? 6 : (maxdeg <= 12 ? 12 : 0);
   if (MD == 0) return fail(IFDTD_ERR_UNSUPPORTED, "vertex degree above 12 is not supported");
-  std::vector<int> ps_edge((size_t)nV * MD);
-  std::vector<real> ps_coef((size_t)nV * MD);
+  const int SW = round4(MD);
+  std::vector<int> ps_edge((size_t)nV * SW, 0);
+  std::vector<real> ps_coef((size_t)nV * SW, real(0));
   for (int sl = 0; sl < nV; ++sl) {
     const int v = vlist[sl];
     const int q0 = v_off[v], n = v_off[v + 1] - q0;
-    for (int q = 0; q < MD; ++q) {
-      ps_edge[(size_t)sl * MD + q] = v_edge[q0 + (q < n ? q : 0)];
-      ps_coef[(size_t)sl * MD + q] = q < n ? v_coef[q0 + q] : real(0);
+    for (int q = 0; q < SW; ++q) {
+      ps_edge[(size_t)sl * SW + q] = v_edge[q0 + (q < n ? q : 0)];
+      ps_coef[(size_t)sl * SW + q] = q < n ? (real)v_coef[q0 + q] : real(0);
     }
   }
   P->maxdeg = MD;
 
-  // ---- radial metric ----
+  // ---- radial metric rows, zero padded to Pn / Pm ----
   const double* r = G->radii_m;
-  std::vector<real> invr(L + 1), rr(L + 1), mid(L), invm(L), invdr(L), invcd(L + 1);
+  std::vector<real> invr(Pn, 0), rr(Pn, 0), invcd(Pn, 0), mid(Pm, 0), invm(Pm, 0), invdr(Pm, 0);
   std::vector<double> m(L);
   for (int k = 0; k <= L; ++k) {
     if (!(r[k] > 0.0) || (k > 0 && !(r[k] > r[k - 1]))) return fail(IFDTD_ERR_ARGUMENT, "radii must increase");
@@ -263,12 +269,17 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   invcd[L] = (real)(2.0 / (r[L] - r[L - 1]));
   for (int k = 1; k < L; ++k) invcd[k] = (real)(1.0 / (m[k] - m[k - 1]));
 
-  // ---- coefficients ----
+  // ---- loss coefficients, rows padded to Pn / Pm ----
   if (!(X->coef_rows_er == 1 || X->coef_rows_er == nV) || !(X->coef_rows_et == 1 || X->coef_rows_et == nE))
     return fail(IFDTD_ERR_ARGUMENT, "coefficient rows must be 1 or the entity count");
   if ((X->coef_rows_er == 1) != (X->coef_rows_et == 1))
     return fail(IFDTD_ERR_ARGUMENT, "er and et coefficients must both be compressed or both full");
-  const size_t ner = (size_t)X->coef_rows_er * (L + 1), net = (size_t)X->coef_rows_et * L;
+  auto pad_rows = [](const double* src, int rows, int cols, int pitch) {
+    std::vector<real> out((size_t)rows * pitch, real(0));
+    for (int i = 0; i < rows; ++i)
+      for (int j = 0; j < cols; ++j) out[(size_t)i * pitch + j] = (real)src[(size_t)i * cols + j];
+    return out;
+  };
 
   // ---- sources ----
   if (X->n_src_er < 0 || X->n_src_er > IFDTD_MAX_SOURCES || X->n_src_et < 0 || X->n_src_et > IFDTD_MAX_SOURCES)
@@ -293,11 +304,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   }
 
   // ---- upload ----
-#define UP(vec, field)                                                   \
-  do {                                                                   \
-    cudaError_t _e = A.upload(vec, &R.field);                            \
-    if (_e != cudaSuccess)                                               \
-      return fail(IFDTD_ERR_CUDA, std::string("upload ") + #field + ": " + cudaGetErrorString(_e)); \
+#define UP(vec, field)                                                                                  \
+  do {                                                                                                  \
+    cudaError_t _e = A.upload(vec, &R.field);                                                           \
+    if (_e != cudaSuccess)                                                                              \
+      return fail(IFDTD_ERR_CUDA, std::string("upload ") + #field + ": " + cudaGetErrorString(_e));     \
   } while (0)
   UP(eptr, eptr);
   UP(vptr, vptr);
@@ -311,11 +322,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(fw, face_w);
   UP(ps_edge, ps_edge);
   UP(ps_coef, ps_coef);
-  {
-    cudaError_t e1 = A.upload(v_off, &P->v_off);
-    cudaError_t e2 = A.upload(v_edge, &P->v_edge);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(IFDTD_ERR_CUDA, "upload of vertex incidence failed");
-  }
   UP(invr, invr);
   UP(rr, rr);
   UP(mid, mid);
@@ -323,8 +329,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(invdr, invdr);
   UP(invcd, invcd);
   {
-    auto ca = cast<real>(X->ca_er, ner), cb = cast<real>(X->cb_er, ner);
-    auto ct = cast<real>(X->ca_et, net), cu = cast<real>(X->cb_et, net);
+    auto ca = pad_rows(X->ca_er, X->coef_rows_er, L + 1, Pn), cb = pad_rows(X->cb_er, X->coef_rows_er, L + 1, Pn);
+    auto ct = pad_rows(X->ca_et, X->coef_rows_et, L, Pm), cu = pad_rows(X->cb_et, X->coef_rows_et, L, Pm);
     UP(ca, ca_er);
     UP(cb, cb_er);
     UP(ct, ca_et);
@@ -345,7 +351,10 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   {
     cudaError_t e1 = A.upload(fsign, &P->face_sign);
     cudaError_t e2 = A.upload(v_sign, &P->v_sign);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(IFDTD_ERR_CUDA, "upload of primitive tables failed");
+    cudaError_t e3 = A.upload(v_off, &P->v_off);
+    cudaError_t e4 = A.upload(v_edge, &P->v_edge);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
+      return fail(IFDTD_ERR_CUDA, "upload of primitive tables failed");
   }
   P->edge_th = R.edge_th;
   P->edge_lr = R.edge_lr;
@@ -373,27 +382,37 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->S = X->plasma_species;
   if (X->plasma_species < 0 || X->plasma_species > IFDTD_MAX_SPECIES)
     return fail(IFDTD_ERR_ARGUMENT, "plasma species count out of range");
+  int slot_faces_ok = 1;
   if (X->plasma_species > 0) {
-    const int S = X->plasma_species;
-    if (!(X->plasma_rows == 1 || X->plasma_rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
+    const int S = X->plasma_species, rows = X->plasma_rows;
+    if (!(rows == 1 || rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
     P->plasma = true;
-    auto rc = cast<real>(X->plasma_reconstruction, 9 * (size_t)nF);
-    auto ce = cast<real>(X->face_centers, 3 * (size_t)nF);
-    auto tl = cast<real>(X->plasma_tangent_left, 3 * (size_t)nE);
-    auto tr = cast<real>(X->plasma_tangent_right, 3 * (size_t)nE);
-    auto pc = cast<real>(X->plasma_coef, (size_t)S * 6 * X->plasma_rows * L);
-    UP(rc, recon);
-    UP(ce, centre);
-    UP(tl, tan_l);
-    UP(tr, tan_r);
+    std::vector<real> pl(12 * (size_t)nF);
+    for (int f = 0; f < nF; ++f)
+      for (int i = 0; i < 3; ++i) {
+        for (int c = 0; c < 3; ++c) pl[12 * (size_t)f + 4 * i + c] = (real)X->plasma_reconstruction[9 * (size_t)f + 3 * i + c];
+        pl[12 * (size_t)f + 4 * i + 3] = (real)X->face_centers[3 * (size_t)f + i];
+      }
+    std::vector<real> tn(8 * (size_t)nE, real(0));
+    for (int e = 0; e < nE; ++e)
+      for (int c = 0; c < 3; ++c) {
+        tn[8 * (size_t)e + c] = (real)X->plasma_tangent_left[3 * (size_t)e + c];
+        tn[8 * (size_t)e + 4 + c] = (real)X->plasma_tangent_right[3 * (size_t)e + c];
+      }
+    auto pc = pad_rows(X->plasma_coef, S * 6 * rows, L, Pm);
+    UP(pl, face_pl);
+    UP(tn, tan);
     UP(pc, pcoef);
     if (X->plasma_magnetized) {
-      auto bd = cast<real>(X->plasma_bdir, (size_t)X->plasma_rows * L * 3);
+      std::vector<real> bd((size_t)rows * 3 * Pm, real(0));  // component-major (rows, 3, Pm)
+      for (int i = 0; i < rows; ++i)
+        for (int j = 0; j < L; ++j)
+          for (int c = 0; c < 3; ++c) bd[((size_t)i * 3 + c) * Pm + j] = (real)X->plasma_bdir[((size_t)i * L + j) * 3 + c];
       UP(bd, bdir);
     }
     const int W = X->vertex_face_width;
-    std::vector<int> ps_face((size_t)nV * MD, 0);
-    std::vector<real> ps_wc((size_t)nV * MD * 3, real(0));
+    std::vector<int> ps_face((size_t)nV * SW, 0);
+    std::vector<real> ps_wc((size_t)nV * SW * 4, real(0));
     for (int sl = 0; sl < nV; ++sl) {
       const int v = vlist[sl];
       int n = 0, first = -1;
@@ -402,18 +421,22 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
         if (w == 0.0) continue;
         const int64_t f = X->vertex_faces[(size_t)v * W + q];
         if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
-        if (n >= MD) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
+        if (n >= MD) {
+          slot_faces_ok = 0;
+          break;
+        }
         if (first < 0) first = (int)f;
-        ps_face[(size_t)sl * MD + n] = (int)f;
-        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * MD + n) * 3 + c] = (real)(w * X->face_centers[3 * f + c]);
+        ps_face[(size_t)sl * SW + n] = (int)f;
+        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
         ++n;
       }
-      for (int q = n; q < MD; ++q) ps_face[(size_t)sl * MD + q] = first < 0 ? 0 : first;
+      for (int q = n; q < SW; ++q) ps_face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
     }
+    if (!slot_faces_ok) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
     UP(ps_face, ps_face);
     UP(ps_wc, ps_wc);
     if (S > 1) {
-      cudaError_t e = A.alloc((size_t)nF * L * 3 * sizeof(real), &P->d_jtot);
+      cudaError_t e = A.alloc((size_t)nF * 3 * Pm * sizeof(real), &P->d_jtot);
       if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of summed plasma current failed");
       R.Jtot = (real*)P->d_jtot;
     }
@@ -425,6 +448,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.nE = nE;
   R.nF = nF;
   R.L = L;
+  R.Pn = Pn;
+  R.Pm = Pm;
   R.n_patches = n_patches;
   R.fpp = fpp;
   R.full = G->full_spherical ? 1 : 0;
@@ -440,7 +465,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.src_et_emin = emin;
   R.src_et_emax = emax;
   R.maxdeg = MD;
-  R.layer_reals = layer_reals(L, R.coef_full, X->plasma_species, R.plasma_full, R.magnetized);
+  R.slot_width = SW;
+  R.layer_reals = layer_reals(Pn, Pm, R.coef_full, X->plasma_species, R.plasma_full, R.magnetized, X->si_terms);
   P->smem_bytes = (size_t)R.layer_reals * sizeof(real);
   if (P->smem_bytes > 200 * 1024) return fail(IFDTD_ERR_UNSUPPORTED, "radial grid too fine for the shared per-layer rows");
   R.dtmu = (real)(G->time_step_s / 1.256637062120e-6);
@@ -484,11 +510,6 @@ int bind_state(ifdtd_plan* P, const ifdtd_state* st, cudaStream_t stream) {
   return IFDTD_OK;
 }
 
-template <typename real>
-constexpr int run_for() {
-  return sizeof(real) == 4 ? 4 : 2;
-}
-
 template <typename K>
 cudaError_t allow_smem(K kernel, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
@@ -497,7 +518,7 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 template <typename real, bool PL>
 cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, cudaStream_t st) {
-  auto k = kh_kernel<real, PL, run_for<real>()>;
+  auto k = kh_kernel<real, PL>;
   cudaError_t e = allow_smem(k, P->smem_bytes);
   if (e != cudaSuccess) return e;
   k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members);
@@ -507,7 +528,7 @@ cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, in
 template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, int istep,
                         cudaStream_t st) {
-  auto k = ke_kernel<real, PL, run_for<real>(), MD>;
+  auto k = ke_kernel<real, PL, MD>;
   cudaError_t e = allow_smem(k, P->smem_bytes);
   if (e != cudaSuccess) return e;
   k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members, istep);
@@ -661,6 +682,13 @@ int32_t ifdtd_plan_destroy(ifdtd_plan* plan) {
   return IFDTD_OK;
 }
 
+int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* mid_pitch) {
+  if (!plan || !node_pitch || !mid_pitch) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  *node_pitch = plan->Pn;
+  *mid_pitch = plan->Pm;
+  return IFDTD_OK;
+}
+
 int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes) {
   if (!plan || !bytes) return fail(IFDTD_ERR_ARGUMENT, "null argument");
   *bytes = (int64_t)plan->arena.bytes;
@@ -770,7 +798,7 @@ int32_t ifdtd_sample(ifdtd_plan* plan, const ifdtd_state* state, const ifdtd_pro
   const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
   if (rc) return rc;
   const void* field = probe->kind == 0 ? state->er : probe->kind == 1 ? state->et : probe->kind == 2 ? state->hr : state->ht;
-  const int pitch = (probe->kind == 0 || probe->kind == 3) ? plan->L + 1 : plan->L;
+  const int pitch = (probe->kind == 0 || probe->kind == 3) ? plan->Pn : plan->Pm;
   const int blocks = (probe->rows * 32 + 255) / 256;
   if (plan->dtype == 4)
     sample_kernel<float><<<blocks, 256, 0, st>>>((const float*)field, pitch, probe->rows, probe->width, probe->index,
@@ -797,8 +825,8 @@ int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, 
   DeviceGuard guard(plan->device);
   cudaStream_t st = (cudaStream_t)stream;
   CUDA_TRY(cudaMemsetAsync(out4, 0, 4 * sizeof(double), st));
-  const size_t n0 = (size_t)plan->nV * (plan->L + 1), n1 = (size_t)plan->nE * plan->L;
-  const size_t n2 = (size_t)plan->nF * plan->L, n3 = (size_t)plan->nE * (plan->L + 1);
+  const size_t n0 = (size_t)plan->nV * plan->Pn, n1 = (size_t)plan->nE * plan->Pm;
+  const size_t n2 = (size_t)plan->nF * plan->Pm, n3 = (size_t)plan->nE * plan->Pn;
   dim3 grid(grid_for(std::max(std::max(n0, n1), std::max(n2, n3))), 4);
   if (plan->dtype == 4)
     max_abs_kernel<float><<<grid, 256, 0, st>>>((const float*)state->er, n0, (const float*)state->et, n1,

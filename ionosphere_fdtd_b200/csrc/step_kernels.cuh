@@ -7,16 +7,17 @@
 // face-scan order, mesh.py:674-708) and the vertices whose lowest-numbered
 // incident face lies in the range (listed in vlist).
 //
-// Work mapping: a thread owns a run of RUN consecutive radial samples of one
-// column (a "chunk").  Per-column indices and metric factors are loaded once
-// per chunk and the RUN samples of every gathered neighbour column are
-// independent loads, so each thread keeps many loads in flight; a warp covers
-// 32 chunks, i.e. a few columns of consecutive memory.  Vertex gathers use
-// fixed-width slot tables (MAXDEG slots, padded with coefficient 0 exactly as
-// the reference pads its incidence table, torch_backend.py:66-89), stored in
-// patch order so the index chain is two loads deep and the loops unroll.
-// Per-layer metric factors and altitude-only coefficient rows are staged in
-// shared memory.
+// Layout: rows of node arrays (er, ht) have pitch Pn >= L+1 and rows of
+// midpoint arrays (et, hr, plasma current components) pitch Pm >= L, both
+// multiples of 16 bytes, with zero padding that every kernel keeps zero.  A
+// thread owns one 16-byte run (4 floats or 2 doubles) of one column, so each
+// access to a gathered neighbour column is one aligned vector load and a warp
+// reads 512 contiguous bytes per column segment.  Per-entity tables are packed
+// for vector loads; vertex gathers use fixed-width slot tables (MAXDEG slots,
+// padded with coefficient 0 as the reference pads its incidence table,
+// torch_backend.py:66-89) stored in patch order, so index chains are two loads
+// deep and all gathers unroll.  Per-layer metric factors and altitude-only
+// coefficient rows are staged in shared memory.
 //
 // Two in-place launches form one leapfrog step, in the reference's order
 // (solver.py:867-989):
@@ -40,15 +41,15 @@ constexpr int kMaxSpecies = 4;
 template <typename real>
 struct Rec {
   // sizes and switches
-  int nV, nE, nF, L;
+  int nV, nE, nF, L, Pn, Pm;
   int n_patches, fpp;
   int full, si_terms, n_species, plasma_full, magnetized, coef_full;
   int n_src_er, n_src_et;
   int src_er_vmin, src_er_vmax, src_et_emin, src_et_emax;
-  int maxdeg, layer_reals;
+  int maxdeg, slot_width, layer_reals;
   // state
   real *er, *et, *hr, *ht, *si_mem;
-  real* J[kMaxSpecies];
+  real* J[kMaxSpecies];  // (F, 3, Pm) per species
   real* Jtot;            // summed species current when n_species > 1
   const double* cur;     // per-step source current (staging row)
   // patch ownership
@@ -56,18 +57,20 @@ struct Rec {
   // edges
   const int2 *edge_th, *edge_lr;
   const real *inv_theta, *inv_phi;
+  const real* tan;       // (E, 8): left tangent, 0, right tangent, 0
   // faces
   const int4 *face_e, *face_v;
-  const real* face_w;    // (F,3): sign_i * theta_i / A_f
-  // vertex slots in vlist order: (V, maxdeg) edges / coefficients / faces / weighted centres
+  const real* face_w;    // (F, 4): sign_i * theta_i / A_f, 0
+  const real* face_pl;   // (F, 12): reconstruction row i then centre component i
+  // vertex slots in vlist order, slot_width entries per vertex
   const int* ps_edge;
   const real* ps_coef;   // sign * phi_e / A*_v, 0 in padding slots
   const int* ps_face;
-  const real* ps_wc;     // (V, maxdeg, 3): area weight * face centre, 0 in padding slots
-  // radial metric (global copies; kernels stage them in shared memory)
+  const real* ps_wc;     // (V, slot_width, 4): area weight * face centre, 0 in padding slots
+  // radial metric rows (padded; staged in shared memory by the kernels)
   const real *invr, *rr, *mid, *invm, *invdr, *invcd;
   real dtmu;             // dt / mu0
-  // loss coefficients: (rows, L+1) / (rows, L), rows = 1 or V / E
+  // loss coefficients: (rows, Pn) / (rows, Pm), rows = 1 or V / E
   const real *ca_er, *cb_er, *ca_et, *cb_et;
   // sources
   const int *src_er_v, *src_er_k;
@@ -77,10 +80,70 @@ struct Rec {
   // surface impedance
   real si_metric, si_kappa, si_hist_sum;
   const real *si_scale, *si_decay, *si_drive, *si_hist;
-  // plasma
-  const real *recon, *centre, *tan_l, *tan_r;
+  // plasma: coefficients (S, 6, rows, Pm), unit B (rows, 3, Pm)
   const real *pcoef, *bdir;
 };
+
+template <typename real>
+struct Lanes;
+template <>
+struct Lanes<float> {
+  static constexpr int N = 4;
+};
+template <>
+struct Lanes<double> {
+  static constexpr int N = 2;
+};
+
+// One 16-byte radial run.
+template <typename real>
+struct Run {
+  real x[Lanes<real>::N];
+};
+
+template <typename real>
+__device__ __forceinline__ Run<real> ld16(const real* p) {
+  Run<real> r;
+  if constexpr (sizeof(real) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    r.x[0] = t.x; r.x[1] = t.y; r.x[2] = t.z; r.x[3] = t.w;
+  } else {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    r.x[0] = t.x; r.x[1] = t.y;
+  }
+  return r;
+}
+
+// Read-only (non-coherent) variant for arrays the kernel does not write.
+template <typename real>
+__device__ __forceinline__ Run<real> ldg16(const real* p) {
+  Run<real> r;
+  if constexpr (sizeof(real) == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    r.x[0] = t.x; r.x[1] = t.y; r.x[2] = t.z; r.x[3] = t.w;
+  } else {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    r.x[0] = t.x; r.x[1] = t.y;
+  }
+  return r;
+}
+
+template <typename real>
+__device__ __forceinline__ Run<real> zero_run() {
+  Run<real> r;
+#pragma unroll
+  for (int i = 0; i < Lanes<real>::N; ++i) r.x[i] = real(0);
+  return r;
+}
+
+template <typename real>
+__device__ __forceinline__ void st16(real* p, const Run<real>& r) {
+  if constexpr (sizeof(real) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
+  } else {
+    *reinterpret_cast<double2*>(p) = make_double2(r.x[0], r.x[1]);
+  }
+}
 
 // Shared-memory view of the per-layer rows of one record.
 template <typename real>
@@ -88,13 +151,16 @@ struct Layers {
   real *invr, *rr, *invcd, *mid, *invm, *invdr;
   real *ca_er, *cb_er, *ca_et, *cb_et;  // compressed coefficient rows (else null)
   real *pc, *bd;                        // compressed plasma rows (else null)
+  real *si_decay, *si_drive, *si_hist;  // surface-impedance pole rows (else null)
 };
 
 // Number of reals of per-layer data staged in shared memory (host and device).
-__host__ __device__ inline int layer_reals(int L, int coef_full, int species, int plasma_full, int magnetized) {
-  int n = 3 * (L + 1) + 3 * L;
-  if (!coef_full) n += 2 * (L + 1) + 2 * L;
-  if (species > 0 && !plasma_full) n += 6 * species * L + (magnetized ? 3 * L : 0);
+__host__ __device__ inline int layer_reals(int Pn, int Pm, int coef_full, int species, int plasma_full, int magnetized,
+                                           int si_terms) {
+  int n = 3 * Pn + 3 * Pm;
+  if (!coef_full) n += 2 * Pn + 2 * Pm;
+  if (species > 0 && !plasma_full) n += 6 * species * Pm + (magnetized ? 3 * Pm : 0);
+  n += 3 * si_terms;
   return n;
 }
 
@@ -117,39 +183,48 @@ __device__ __forceinline__ void copy_row(real* dst, const real* src, int n) {
 // Carve and fill the shared per-layer rows; ends with a barrier.
 template <typename real>
 __device__ __forceinline__ void load_layers(const Rec<real>& R, real* smem, Layers<real>& Ls) {
-  const int L = R.L, Lp1 = L + 1;
+  const int Pn = R.Pn, Pm = R.Pm;
   real* p = smem;
-  Ls.invr = p; p += Lp1;
-  Ls.rr = p; p += Lp1;
-  Ls.invcd = p; p += Lp1;
-  Ls.mid = p; p += L;
-  Ls.invm = p; p += L;
-  Ls.invdr = p; p += L;
-  copy_row(Ls.invr, R.invr, Lp1);
-  copy_row(Ls.rr, R.rr, Lp1);
-  copy_row(Ls.invcd, R.invcd, Lp1);
-  copy_row(Ls.mid, R.mid, L);
-  copy_row(Ls.invm, R.invm, L);
-  copy_row(Ls.invdr, R.invdr, L);
+  Ls.invr = p; p += Pn;
+  Ls.rr = p; p += Pn;
+  Ls.invcd = p; p += Pn;
+  Ls.mid = p; p += Pm;
+  Ls.invm = p; p += Pm;
+  Ls.invdr = p; p += Pm;
+  copy_row(Ls.invr, R.invr, Pn);
+  copy_row(Ls.rr, R.rr, Pn);
+  copy_row(Ls.invcd, R.invcd, Pn);
+  copy_row(Ls.mid, R.mid, Pm);
+  copy_row(Ls.invm, R.invm, Pm);
+  copy_row(Ls.invdr, R.invdr, Pm);
   Ls.ca_er = Ls.cb_er = Ls.ca_et = Ls.cb_et = nullptr;
   if (!R.coef_full) {
-    Ls.ca_er = p; p += Lp1;
-    Ls.cb_er = p; p += Lp1;
-    Ls.ca_et = p; p += L;
-    Ls.cb_et = p; p += L;
-    copy_row(Ls.ca_er, R.ca_er, Lp1);
-    copy_row(Ls.cb_er, R.cb_er, Lp1);
-    copy_row(Ls.ca_et, R.ca_et, L);
-    copy_row(Ls.cb_et, R.cb_et, L);
+    Ls.ca_er = p; p += Pn;
+    Ls.cb_er = p; p += Pn;
+    Ls.ca_et = p; p += Pm;
+    Ls.cb_et = p; p += Pm;
+    copy_row(Ls.ca_er, R.ca_er, Pn);
+    copy_row(Ls.cb_er, R.cb_er, Pn);
+    copy_row(Ls.ca_et, R.ca_et, Pm);
+    copy_row(Ls.cb_et, R.cb_et, Pm);
   }
   Ls.pc = Ls.bd = nullptr;
   if (R.n_species > 0 && !R.plasma_full) {
-    Ls.pc = p; p += 6 * R.n_species * L;
-    copy_row(Ls.pc, R.pcoef, 6 * R.n_species * L);
+    Ls.pc = p; p += 6 * R.n_species * Pm;
+    copy_row(Ls.pc, R.pcoef, 6 * R.n_species * Pm);
     if (R.magnetized) {
-      Ls.bd = p; p += 3 * L;
-      copy_row(Ls.bd, R.bdir, 3 * L);
+      Ls.bd = p; p += 3 * Pm;
+      copy_row(Ls.bd, R.bdir, 3 * Pm);
     }
+  }
+  Ls.si_decay = Ls.si_drive = Ls.si_hist = nullptr;
+  if (R.si_terms > 0) {
+    Ls.si_decay = p; p += R.si_terms;
+    Ls.si_drive = p; p += R.si_terms;
+    Ls.si_hist = p; p += R.si_terms;
+    copy_row(Ls.si_decay, R.si_decay, R.si_terms);
+    copy_row(Ls.si_drive, R.si_drive, R.si_terms);
+    copy_row(Ls.si_hist, R.si_hist, R.si_terms);
   }
   __syncthreads();
 }
@@ -161,8 +236,8 @@ __device__ __forceinline__ uint32_t div_magic(int d) { return d == 1 ? 0u : 0xFF
 
 template <typename real>
 __device__ __forceinline__ real pcoef_at(const Rec<real>& R, const Layers<real>& Ls, int s, int c, int f, int j) {
-  if (!R.plasma_full) return Ls.pc[(s * 6 + c) * R.L + j];
-  return __ldg(R.pcoef + (((size_t)(s * 6 + c) * R.nF + f) * R.L + j));
+  if (!R.plasma_full) return Ls.pc[(s * 6 + c) * R.Pm + j];
+  return __ldg(R.pcoef + (((size_t)(s * 6 + c) * R.nF + f) * R.Pm + j));
 }
 
 template <typename real>
@@ -185,9 +260,10 @@ __device__ __forceinline__ void member_patch(const int2* block_map, int n_member
 // cold-plasma current ADE (faces x midpoints).
 // solver.py:877-921; surface_impedance.py:225-270; plasma.py:413-442, 489-501.
 // ---------------------------------------------------------------------------
-template <typename real, bool PLASMA, int RUN>
+template <typename real, bool PLASMA>
 __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
                                                   int n_members) {
+  constexpr int N = Lanes<real>::N;
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   int member, patch;
@@ -195,8 +271,8 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
   load_rec(R, recs + member);
   Layers<real> Ls;
   load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-  const int L = R.L, Lp1 = L + 1;
-  const int cn = (Lp1 + RUN - 1) / RUN, cm = (L + RUN - 1) / RUN;
+  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm;
+  const int cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
   const real* __restrict__ er = R.er;
   const real* __restrict__ et = R.et;
@@ -206,72 +282,59 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
   const bool si = R.si_terms > 0;
   const bool full = R.full != 0;
 
-  // ---- Ht: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr) / mu0, odd (PEC) Et ghosts ----
+  // ---- Ht: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr) / mu0, odd (PEC) Et ghosts;
+  //      the run holding node 0 also advances the surface-impedance ADE ----
   const int ea = R.eptr[patch], eb = R.eptr[patch + 1];
   const int n_edge_items = (eb - ea) * cn;
   for (int it = threadIdx.x; it < n_edge_items; it += blockDim.x) {
     const int el = fast_div(it, mag_cn);
-    const int k0 = (it - el * cn) * RUN;
+    const int k0 = (it - el * cn) * N;
     const int e = ea + el;
     const int2 th = __ldg(R.edge_th + e);
     const real inv_t = __ldg(R.inv_theta + e);
-    const real* erh = er + (size_t)th.y * Lp1;
-    const real* ert = er + (size_t)th.x * Lp1;
-    const real* etr = et + (size_t)e * L;
-    real* htr = ht + (size_t)e * Lp1;
-    real vh[RUN], vt[RUN], vo[RUN], vu[RUN + 1];
+    const Run<real> vh = ldg16(er + (size_t)th.y * Pn + k0);
+    const Run<real> vt = ldg16(er + (size_t)th.x * Pn + k0);
+    real* htp = ht + (size_t)e * Pn + k0;
+    const Run<real> vo = ld16(htp);
+    const real* etr = et + (size_t)e * Pm;
+    const Run<real> vu = (k0 < Pm) ? ldg16(etr + k0) : zero_run<real>();  // Et at k0 .. k0+N-1
+    const real vprev = (k0 > 0 && k0 - 1 < L) ? __ldg(etr + k0 - 1) : real(0);
+    Run<real> out;
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) {
+    for (int r = 0; r < N; ++r) {
       const int k = k0 + r;
-      const bool ok = k < Lp1;
-      vh[r] = ok ? erh[k] : real(0);
-      vt[r] = ok ? ert[k] : real(0);
-      vo[r] = ok ? htr[k] : real(0);
-    }
-#pragma unroll
-    for (int r = 0; r <= RUN; ++r) {
-      const int k = k0 - 1 + r;
-      vu[r] = (k >= 0 && k < L) ? etr[k] : real(0);
-    }
-#pragma unroll
-    for (int r = 0; r < RUN; ++r) {
-      const int k = k0 + r;
-      if (k >= Lp1 || (si && k == 0)) continue;  // the surface ADE owns the lowest plane
-      const real g = (vh[r] - vt[r]) * inv_t * Ls.invr[k];
-      real up = vu[r + 1], dn = vu[r];
+      const real g = (vh.x[r] - vt.x[r]) * inv_t * Ls.invr[k];
+      real up = (k < L) ? vu.x[r] : real(0);
+      real dn = (k >= 1 && k - 1 < L) ? (r == 0 ? vprev : vu.x[r - 1]) : real(0);
       real d;
       if (full) {
         up = (k < L) ? up * Ls.mid[k] : real(0);
-        dn = (k > 0) ? dn * Ls.mid[k - 1] : real(0);
+        dn = (k >= 1 && k - 1 < L) ? dn * Ls.mid[k - 1] : real(0);
         d = (up - dn) * Ls.invcd[k] * Ls.invr[k];
       } else {
         d = (up - dn) * Ls.invcd[k];
       }
-      htr[k] = vo[r] + (g - d) * dtmu;
+      out.x[r] = (k < Lp1) ? vo.x[r] + (g - d) * dtmu : real(0);
     }
-  }
-
-  // ---- lower surface-impedance boundary (implicit, trapezoidal ADE) ----
-  if (si) {
-    const int T = R.si_terms;
-    for (int el = threadIdx.x; el < eb - ea; el += blockDim.x) {
-      const int e = ea + el;
-      const int2 th = __ldg(R.edge_th + e);
-      const real h_old = ht[(size_t)e * Lp1];
-      const real g0 = (er[(size_t)th.y * Lp1] - er[(size_t)th.x * Lp1]) * __ldg(R.inv_theta + e) * Ls.invr[0];
-      const real e1 = R.si_metric * et[(size_t)e * L];
+    if (si && k0 == 0) {
+      // lower boundary: implicit coupling of the curl to the passive impedance ADE
+      const int T = R.si_terms;
+      const real h_old = vo.x[0];
+      const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
+      const real e1 = R.si_metric * vu.x[0];
       const real s = __ldg(R.si_scale + e);
       real* mem = R.si_mem + (size_t)e * T;
       real hist = real(0);
-      for (int p = 0; p < T; ++p) hist += mem[p] * __ldg(R.si_hist + p);
+      for (int p = 0; p < T; ++p) hist += mem[p] * Ls.si_hist[p];
       hist *= s;
       const real kap = R.si_kappa;
       const real c = kap * (s * R.si_hist_sum);
       const real h_new = ((real(1) - real(0.5) * c) * h_old + dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
-      ht[(size_t)e * Lp1] = h_new;
       const real hs = h_new + h_old;
-      for (int p = 0; p < T; ++p) mem[p] = mem[p] * __ldg(R.si_decay + p) + hs * __ldg(R.si_drive + p);
+      for (int p = 0; p < T; ++p) mem[p] = mem[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
+      out.x[0] = h_new;
     }
+    st16(htp, out);
   }
 
   // ---- Hr and the plasma current on owned faces ----
@@ -280,70 +343,64 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
   const int n_face_items = (fb - fa) * cm;
   for (int it = threadIdx.x; it < n_face_items; it += blockDim.x) {
     const int fl = fast_div(it, mag_cm);
-    const int j0 = (it - fl * cm) * RUN;
+    const int j0 = (it - fl * cm) * N;
     const int f = fa + fl;
     const int4 fe = __ldg(R.face_e + f);
-    const real w0 = __ldg(R.face_w + 3 * (size_t)f), w1 = __ldg(R.face_w + 3 * (size_t)f + 1),
-               w2 = __ldg(R.face_w + 3 * (size_t)f + 2);
-    const real* et0 = et + (size_t)fe.x * L;
-    const real* et1 = et + (size_t)fe.y * L;
-    const real* et2 = et + (size_t)fe.z * L;
-    real* hrr = hr + (size_t)f * L;
-    real a0[RUN], a1[RUN], a2[RUN], hv[RUN];
+    const Run<real> a0 = ldg16(et + (size_t)fe.x * Pm + j0);
+    const Run<real> a1 = ldg16(et + (size_t)fe.y * Pm + j0);
+    const Run<real> a2 = ldg16(et + (size_t)fe.z * Pm + j0);
+    real* hrp = hr + (size_t)f * Pm + j0;
+    const Run<real> hv = ld16(hrp);
+    const real* fw = R.face_w + 4 * (size_t)f;
+    const real w0 = __ldg(fw), w1 = __ldg(fw + 1), w2 = __ldg(fw + 2);
+    Run<real> hn;
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) {
+    for (int r = 0; r < N; ++r) {
       const int j = j0 + r;
-      const bool ok = j < L;
-      a0[r] = ok ? et0[j] : real(0);
-      a1[r] = ok ? et1[j] : real(0);
-      a2[r] = ok ? et2[j] : real(0);
-      hv[r] = ok ? hrr[j] : real(0);
+      hn.x[r] = (j < L) ? hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * Ls.invm[j] * dtmu : real(0);
     }
-#pragma unroll
-    for (int r = 0; r < RUN; ++r) {
-      const int j = j0 + r;
-      if (j < L) hrr[j] = hv[r] - (w0 * a0[r] + w1 * a1[r] + w2 * a2[r]) * Ls.invm[j] * dtmu;
-    }
+    st16(hrp, hn);
     if (PLASMA) {
       const int4 fv = __ldg(R.face_v + f);
-      const real* va = er + (size_t)fv.x * Lp1;
-      const real* vb = er + (size_t)fv.y * Lp1;
-      const real* vc = er + (size_t)fv.z * Lp1;
-      real node[RUN + 1];
+      const real* pa = er + (size_t)fv.x * Pn;
+      const real* pb = er + (size_t)fv.y * Pn;
+      const real* pc = er + (size_t)fv.z * Pn;
+      const Run<real> na = ldg16(pa + j0), nb = ldg16(pb + j0), nc = ldg16(pc + j0);
+      const bool tail = j0 + N < Pn;
+      const real ta = tail ? __ldg(pa + j0 + N) : real(0), tb = tail ? __ldg(pb + j0 + N) : real(0),
+                 tc = tail ? __ldg(pc + j0 + N) : real(0);
       const real third = real(1) / real(3);
+      real node[N + 1];
 #pragma unroll
-      for (int r = 0; r <= RUN; ++r) {
-        const int k = j0 + r;
-        node[r] = (k <= L) ? (va[k] + vb[k] + vc[k]) * third : real(0);
+      for (int r = 0; r < N; ++r) node[r] = (na.x[r] + nb.x[r] + nc.x[r]) * third;
+      node[N] = (ta + tb + tc) * third;
+      const real* gp = R.face_pl + 12 * (size_t)f;
+      real rc[3][3], cf[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rc[i][c] = __ldg(gp + 4 * i + c);
+        cf[i] = __ldg(gp + 4 * i + 3);
       }
-      real rc[9], cf[3];
+      real E[N][3];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) rc[c] = __ldg(R.recon + 9 * (size_t)f + c);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) cf[c] = __ldg(R.centre + 3 * (size_t)f + c);
-      real E[RUN][3];
-#pragma unroll
-      for (int r = 0; r < RUN; ++r) {
+      for (int r = 0; r < N; ++r) {
         const real rad = real(0.5) * (node[r] + node[r + 1]);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) E[r][c] = a0[r] * rc[c] + a1[r] * rc[3 + c] + a2[r] * rc[6 + c] + rad * cf[c];
+        for (int c = 0; c < 3; ++c) E[r][c] = a0.x[r] * rc[0][c] + a1.x[r] * rc[1][c] + a2.x[r] * rc[2][c] + rad * cf[c];
       }
-      real tot[RUN][3];
+      real tot[N][3];
 #pragma unroll
-      for (int r = 0; r < RUN; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
+      for (int r = 0; r < N; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
       for (int s = 0; s < R.n_species; ++s) {
-        real* Js = R.J[s] + ((size_t)f * L) * 3;
-        real jv[RUN][3];
+        real* Js = R.J[s] + (size_t)f * 3 * Pm + j0;
+        Run<real> jc[3];
 #pragma unroll
-        for (int r = 0; r < RUN; ++r) {
+        for (int c = 0; c < 3; ++c) jc[c] = ld16(Js + c * Pm);
+        Run<real> jn[3];
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
           const int j = j0 + r;
-#pragma unroll
-          for (int c = 0; c < 3; ++c) jv[r][c] = (j < L) ? Js[3 * j + c] : real(0);
-        }
-#pragma unroll
-        for (int r = 0; r < RUN; ++r) {
-          const int j = j0 + r;
-          if (j >= L) continue;
           const real decay = pcoef_at(R, Ls, s, 0, f, j);
           const real cs = pcoef_at(R, Ls, s, 1, f, j);
           const real dre = pcoef_at(R, Ls, s, 4, f, j);
@@ -353,16 +410,9 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
             const real dpar = pcoef_at(R, Ls, s, 3, f, j);
             const real dim = pcoef_at(R, Ls, s, 5, f, j);
             real b[3];
-            if (R.plasma_full) {
-              const real* bp = R.bdir + 3 * ((size_t)f * L + j);
-              b[0] = __ldg(bp);
-              b[1] = __ldg(bp + 1);
-              b[2] = __ldg(bp + 2);
-            } else {
-              b[0] = Ls.bd[3 * j];
-              b[1] = Ls.bd[3 * j + 1];
-              b[2] = Ls.bd[3 * j + 2];
-            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              b[c] = R.plasma_full ? __ldg(R.bdir + ((size_t)f * 3 + c) * Pm + j) : Ls.bd[c * Pm + j];
             const real eb = E[r][0] * b[0] + E[r][1] * b[1] + E[r][2] * b[2];
             real Ep[3], Eq[3], Ex[3];
 #pragma unroll
@@ -373,13 +423,11 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
             Ex[0] = Eq[1] * b[2] - Eq[2] * b[1];
             Ex[1] = Eq[2] * b[0] - Eq[0] * b[2];
             Ex[2] = Eq[0] * b[1] - Eq[1] * b[0];
-            const real jb = jv[r][0] * b[0] + jv[r][1] * b[1] + jv[r][2] * b[2];
+            const real J0 = jc[0].x[r], J1 = jc[1].x[r], J2 = jc[2].x[r];
+            const real jb = J0 * b[0] + J1 * b[1] + J2 * b[2];
             real Jp[3], Jq[3], Jx[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              Jp[c] = jb * b[c];
-              Jq[c] = jv[r][c] - Jp[c];
-            }
+            Jp[0] = jb * b[0]; Jp[1] = jb * b[1]; Jp[2] = jb * b[2];
+            Jq[0] = J0 - Jp[0]; Jq[1] = J1 - Jp[1]; Jq[2] = J2 - Jp[2];
             Jx[0] = Jq[1] * b[2] - Jq[2] * b[1];
             Jx[1] = Jq[2] * b[0] - Jq[0] * b[2];
             Jx[2] = Jq[0] * b[1] - Jq[1] * b[0];
@@ -388,24 +436,26 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
               nj[c] = decay * Jp[c] + dpar * Ep[c] + decay * (cs * Jq[c] + sn * Jx[c]) + dre * Eq[c] + dim * Ex[c];
           } else {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) nj[c] = decay * (cs * jv[r][c]) + dre * E[r][c];
+            for (int c = 0; c < 3; ++c) nj[c] = decay * (cs * jc[c].x[r]) + dre * E[r][c];
           }
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            Js[3 * j + c] = nj[c];
-            tot[r][c] += nj[c];
+            const real v = (j < L) ? nj[c] : real(0);
+            jn[c].x[r] = v;
+            tot[r][c] += v;
           }
         }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) st16(Js + c * Pm, jn[c]);
       }
       if (R.n_species > 1) {
-        real* Jt = R.Jtot + ((size_t)f * L) * 3;
+        real* Jt = R.Jtot + (size_t)f * 3 * Pm + j0;
 #pragma unroll
-        for (int r = 0; r < RUN; ++r) {
-          const int j = j0 + r;
-          if (j < L) {
+        for (int c = 0; c < 3; ++c) {
+          Run<real> t;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) Jt[3 * j + c] = tot[r][c];
-          }
+          for (int r = 0; r < N; ++r) t.x[r] = tot[r][c];
+          st16(Jt + c * Pm, t);
         }
       }
     }
@@ -416,9 +466,10 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
 // E phase: Er (vertices x nodes) and Et (edges x midpoints).
 // solver.py:923-989; plasma.py:503-527.
 // ---------------------------------------------------------------------------
-template <typename real, bool PLASMA, int RUN, int MAXDEG>
+template <typename real, bool PLASMA, int MAXDEG>
 __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
                                                   int n_members, int istep) {
+  constexpr int N = Lanes<real>::N;
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   int member, patch;
@@ -426,8 +477,8 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
   load_rec(R, recs + member);
   Layers<real> Ls;
   load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-  const int L = R.L, Lp1 = L + 1;
-  const int cn = (Lp1 + RUN - 1) / RUN, cm = (L + RUN - 1) / RUN;
+  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
+  const int cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
   real* __restrict__ er = R.er;
   real* __restrict__ et = R.et;
@@ -443,69 +494,72 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
   const int n_vert_items = (vb - va) * cn;
   for (int it = threadIdx.x; it < n_vert_items; it += blockDim.x) {
     const int vl = fast_div(it, mag_cn);
-    const int k0 = (it - vl * cn) * RUN;
+    const int k0 = (it - vl * cn) * N;
     const int slot = va + vl;
     const int v = __ldg(R.vlist + slot);
-    real acc[RUN];
-#pragma unroll
-    for (int r = 0; r < RUN; ++r) acc[r] = real(0);
+    int eidx[MAXDEG];
+    real ecoef[MAXDEG];
 #pragma unroll
     for (int q = 0; q < MAXDEG; ++q) {
-      const int e = __ldg(R.ps_edge + (size_t)slot * MAXDEG + q);
-      const real c = __ldg(R.ps_coef + (size_t)slot * MAXDEG + q);
-      const real* hrow = ht + (size_t)e * Lp1;
-#pragma unroll
-      for (int r = 0; r < RUN; ++r) {
-        const int k = k0 + r;
-        acc[r] += c * ((k < Lp1) ? hrow[k] : real(0));
-      }
+      eidx[q] = __ldg(R.ps_edge + (size_t)slot * SW + q);
+      ecoef[q] = __ldg(R.ps_coef + (size_t)slot * SW + q);
     }
-    real* err = er + (size_t)v * Lp1;
-    real ev[RUN];
+    Run<real> hvals[MAXDEG];
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) ev[r] = (k0 + r < Lp1) ? err[k0 + r] : real(0);
-    real jr[RUN];
+    for (int q = 0; q < MAXDEG; ++q) hvals[q] = ldg16(ht + (size_t)eidx[q] * Pn + k0);
+    real* erp = er + (size_t)v * Pn + k0;
+    const Run<real> ev = ld16(erp);
+    real acc[N];
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) jr[r] = real(0);
+    for (int r = 0; r < N; ++r) {
+      acc[r] = real(0);
+#pragma unroll
+      for (int q = 0; q < MAXDEG; ++q) acc[r] += ecoef[q] * hvals[q].x[r];
+    }
+    real jr[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) jr[r] = real(0);
     if (PLASMA) {
-      // radial plasma current at faces, area-averaged to the vertex, then to nodes
-      real rav[RUN + 1];
+      // radial current at faces (J . centre), area-averaged to the vertex, then to nodes
+      real rav[N + 1];
 #pragma unroll
-      for (int r = 0; r <= RUN; ++r) rav[r] = real(0);
+      for (int r = 0; r <= N; ++r) rav[r] = real(0);
 #pragma unroll 2
       for (int q = 0; q < MAXDEG; ++q) {
-        const int f = __ldg(R.ps_face + (size_t)slot * MAXDEG + q);
-        const real* wc = R.ps_wc + ((size_t)slot * MAXDEG + q) * 3;
+        const int f = __ldg(R.ps_face + (size_t)slot * SW + q);
+        const real* wc = R.ps_wc + ((size_t)slot * SW + q) * 4;
         const real c0 = __ldg(wc), c1 = __ldg(wc + 1), c2 = __ldg(wc + 2);
-        const real* jf = Jsum + (size_t)f * L * 3;
+        const real* jf = Jsum + (size_t)f * 3 * Pm;
+        const bool in = k0 < Pm;
+        const Run<real> jx = in ? ldg16(jf + k0) : zero_run<real>();
+        const Run<real> jy = in ? ldg16(jf + Pm + k0) : zero_run<real>();
+        const Run<real> jz = in ? ldg16(jf + 2 * Pm + k0) : zero_run<real>();
+        const bool prev = k0 >= 1 && k0 - 1 < L;
+        if (prev) rav[0] += __ldg(jf + k0 - 1) * c0 + __ldg(jf + Pm + k0 - 1) * c1 + __ldg(jf + 2 * Pm + k0 - 1) * c2;
 #pragma unroll
-        for (int r = 0; r <= RUN; ++r) {
-          int j = k0 - 1 + r;
-          j = j < 0 ? 0 : (j >= L ? L - 1 : j);
-          rav[r] += jf[3 * j] * c0 + jf[3 * j + 1] * c1 + jf[3 * j + 2] * c2;
-        }
+        for (int r = 0; r < N; ++r) rav[r + 1] += jx.x[r] * c0 + jy.x[r] * c1 + jz.x[r] * c2;
       }
 #pragma unroll
-      for (int r = 0; r < RUN; ++r) {
+      for (int r = 0; r < N; ++r) {
         const int k = k0 + r;
         jr[r] = (k == 0) ? rav[r + 1] : (k == L ? rav[r] : real(0.5) * (rav[r] + rav[r + 1]));
       }
     }
+    Run<real> out;
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) {
+    for (int r = 0; r < N; ++r) {
       const int k = k0 + r;
-      if (k >= Lp1) continue;
-      const size_t o = (size_t)v * Lp1 + k;
-      const real ca = coef_full ? __ldg(R.ca_er + o) : Ls.ca_er[k];
-      const real cb = coef_full ? __ldg(R.cb_er + o) : Ls.cb_er[k];
-      real x = ca * ev[r] + cb * (acc[r] * Ls.invr[k]);
+      const real ca = coef_full ? __ldg(R.ca_er + (size_t)v * Pn + k) : Ls.ca_er[k];
+      const real cb = coef_full ? __ldg(R.cb_er + (size_t)v * Pn + k) : Ls.cb_er[k];
+      real x = ca * ev.x[r] + cb * (acc[r] * Ls.invr[k]);
       if (v >= R.src_er_vmin && v <= R.src_er_vmax) {
         for (int s = 0; s < R.n_src_er; ++s)
           if (__ldg(R.src_er_v + s) == v && __ldg(R.src_er_k + s) == k) x -= __ldg(R.src_er_c + s) * current;
       }
       if (PLASMA) x -= cb * jr[r];
-      err[k] = x;
+      out.x[r] = (k < Lp1) ? x : real(0);
     }
+    st16(erp, out);
   }
 
   // ---- Et: dual-edge difference of Hr minus (1/m) d(r Ht)/dr, loss, sources, Jt ----
@@ -513,62 +567,55 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
   const int n_edge_items = (eb - ea) * cm;
   for (int it = threadIdx.x; it < n_edge_items; it += blockDim.x) {
     const int el = fast_div(it, mag_cm);
-    const int j0 = (it - el * cm) * RUN;
+    const int j0 = (it - el * cm) * N;
     const int e = ea + el;
     const int2 lr = __ldg(R.edge_lr + e);
     const real inv_p = __ldg(R.inv_phi + e);
-    const real* hl = hr + (size_t)lr.x * L;
-    const real* hq = hr + (size_t)lr.y * L;
-    const real* htr = ht + (size_t)e * Lp1;
-    real* etr = et + (size_t)e * L;
-    real a[RUN], b[RUN], ev[RUN], hv[RUN + 1];
+    const Run<real> a = ldg16(hr + (size_t)lr.x * Pm + j0);
+    const Run<real> b = ldg16(hr + (size_t)lr.y * Pm + j0);
+    const real* htr = ht + (size_t)e * Pn;
+    const Run<real> hv = ldg16(htr + j0);
+    const real htail = (j0 + N < Pn) ? __ldg(htr + j0 + N) : real(0);
+    real* etp = et + (size_t)e * Pm + j0;
+    const Run<real> ev = ld16(etp);
+    real jt[N];
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) {
-      const int j = j0 + r;
-      const bool ok = j < L;
-      a[r] = ok ? hl[j] : real(0);
-      b[r] = ok ? hq[j] : real(0);
-      ev[r] = ok ? etr[j] : real(0);
-    }
-#pragma unroll
-    for (int r = 0; r <= RUN; ++r) hv[r] = (j0 + r <= L) ? htr[j0 + r] : real(0);
-    real jt[RUN];
-#pragma unroll
-    for (int r = 0; r < RUN; ++r) jt[r] = real(0);
+    for (int r = 0; r < N; ++r) jt[r] = real(0);
     if (PLASMA) {
-      const real* jl = Jsum + (size_t)lr.x * L * 3;
-      const real* jq = Jsum + (size_t)lr.y * L * 3;
-      const real* tl = R.tan_l + 3 * (size_t)e;
-      const real* tq = R.tan_r + 3 * (size_t)e;
-      const real l0 = __ldg(tl), l1 = __ldg(tl + 1), l2 = __ldg(tl + 2);
-      const real q0 = __ldg(tq), q1 = __ldg(tq + 1), q2 = __ldg(tq + 2);
+      const real* jl = Jsum + (size_t)lr.x * 3 * Pm + j0;
+      const real* jq = Jsum + (size_t)lr.y * 3 * Pm + j0;
+      const real* tp = R.tan + 8 * (size_t)e;
+      const real l0 = __ldg(tp), l1 = __ldg(tp + 1), l2 = __ldg(tp + 2);
+      const real q0 = __ldg(tp + 4), q1 = __ldg(tp + 5), q2 = __ldg(tp + 6);
+      const Run<real> lx = ldg16(jl), ly = ldg16(jl + Pm), lz = ldg16(jl + 2 * Pm);
+      const Run<real> qx = ldg16(jq), qy = ldg16(jq + Pm), qz = ldg16(jq + 2 * Pm);
 #pragma unroll
-      for (int r = 0; r < RUN; ++r) {
-        const int j = j0 + r < L ? j0 + r : L - 1;
-        const real left = jl[3 * j] * l0 + jl[3 * j + 1] * l1 + jl[3 * j + 2] * l2;
-        const real right = jq[3 * j] * q0 + jq[3 * j + 1] * q1 + jq[3 * j + 2] * q2;
+      for (int r = 0; r < N; ++r) {
+        const real left = lx.x[r] * l0 + ly.x[r] * l1 + lz.x[r] * l2;
+        const real right = qx.x[r] * q0 + qy.x[r] * q1 + qz.x[r] * q2;
         jt[r] = real(0.5) * (left + right);
       }
     }
+    Run<real> out;
 #pragma unroll
-    for (int r = 0; r < RUN; ++r) {
+    for (int r = 0; r < N; ++r) {
       const int j = j0 + r;
-      if (j >= L) continue;
-      real g = (a[r] - b[r]) * inv_p * Ls.invm[j];
-      const real d = full ? (Ls.rr[j + 1] * hv[r + 1] - Ls.rr[j] * hv[r]) * Ls.invdr[j] * Ls.invm[j]
-                          : (hv[r + 1] - hv[r]) * Ls.invdr[j];
+      const real hnext = (r + 1 < N) ? hv.x[r + 1] : htail;
+      real g = (a.x[r] - b.x[r]) * inv_p * Ls.invm[j];
+      const real d = full ? (Ls.rr[j + 1] * hnext - Ls.rr[j] * hv.x[r]) * Ls.invdr[j] * Ls.invm[j]
+                          : (hnext - hv.x[r]) * Ls.invdr[j];
       g -= d;
-      const size_t o = (size_t)e * L + j;
-      const real ca = coef_full ? __ldg(R.ca_et + o) : Ls.ca_et[j];
-      const real cb = coef_full ? __ldg(R.cb_et + o) : Ls.cb_et[j];
-      real x = ca * ev[r] + cb * g;
+      const real ca = coef_full ? __ldg(R.ca_et + (size_t)e * Pm + j) : Ls.ca_et[j];
+      const real cb = coef_full ? __ldg(R.cb_et + (size_t)e * Pm + j) : Ls.cb_et[j];
+      real x = ca * ev.x[r] + cb * g;
       if (e >= R.src_et_emin && e <= R.src_et_emax) {
         for (int s = 0; s < R.n_src_et; ++s)
           if (__ldg(R.src_et_e + s) == e && __ldg(R.src_et_j + s) == j) x -= __ldg(R.src_et_c + s) * current;
       }
       if (PLASMA) x -= cb * jt[r];
-      etr[j] = x;
+      out.x[r] = (j < L) ? x : real(0);
     }
+    st16(etp, out);
   }
 }
 
@@ -600,7 +647,7 @@ __global__ void sample_rec_kernel(const Rec<real>* __restrict__ rec, int kind, i
                                   const int* __restrict__ index, const int* __restrict__ layer,
                                   const double* __restrict__ weight, double* __restrict__ out) {
   const real* field = kind == 0 ? rec->er : kind == 1 ? rec->et : kind == 2 ? rec->hr : rec->ht;
-  const int pitch = (kind == 0 || kind == 3) ? rec->L + 1 : rec->L;
+  const int pitch = (kind == 0 || kind == 3) ? rec->Pn : rec->Pm;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= rows) return;
@@ -616,7 +663,8 @@ __global__ void sample_rec_kernel(const Rec<real>* __restrict__ rec, int kind, i
 
 // max |x| of up to four arrays; results combined with an order-independent
 // atomic max on the bit pattern of non-negative doubles (NaN sorts above +Inf,
-// so a non-finite field reports NaN or Inf).
+// so a non-finite field reports NaN or Inf).  Row padding is zero and does not
+// change a maximum of absolute values.
 template <typename real>
 __global__ void max_abs_kernel(const real* __restrict__ a0, size_t n0, const real* __restrict__ a1, size_t n1,
                                const real* __restrict__ a2, size_t n2, const real* __restrict__ a3, size_t n3,

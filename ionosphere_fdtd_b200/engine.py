@@ -154,6 +154,9 @@ class Engine:
                 "ifdtd_plan_create",
             )
         self.plan = handle
+        node_pitch, mid_pitch = C.c_int32(), C.c_int32()
+        N.check(lib.ifdtd_plan_layout(handle, C.byref(node_pitch), C.byref(mid_pitch)), "ifdtd_plan_layout")
+        self.node_pitch, self.mid_pitch = int(node_pitch.value), int(mid_pitch.value)
         self._keep = keep  # descriptors are copied by the plan; arrays kept for clarity of ownership
         self._state_key = None
         self._state = N.State()
@@ -182,31 +185,35 @@ class Engine:
     # -- state ------------------------------------------------------------------
 
     def state(self, er, et, hr, ht, si_memory=None, plasma_currents=()) -> N.State:
+        """Bind the padded state buffers: er/ht (V|E, node_pitch), et/hr
+        (E|F, mid_pitch), plasma currents (F, 3, mid_pitch), SI memory (E, T)."""
+
         tensors = (er, et, hr, ht, si_memory, *plasma_currents)
         key = tuple(0 if t is None else t.data_ptr() for t in tensors)
         if key == self._state_key:
             return self._state
         b = self.backend
         mesh = self.mesh
+        pn, pm = self.node_pitch, self.mid_pitch
         expect = {
-            "er": (er, (mesh.n_vertices, self.L + 1)),
-            "et": (et, (mesh.n_edges, self.L)),
-            "hr": (hr, (mesh.n_faces, self.L)),
-            "ht": (ht, (mesh.n_edges, self.L + 1)),
+            "er": (er, (mesh.n_vertices, pn)),
+            "et": (et, (mesh.n_edges, pm)),
+            "hr": (hr, (mesh.n_faces, pm)),
+            "ht": (ht, (mesh.n_edges, pn)),
         }
         if self.si_terms:
             expect["surface_impedance_memory"] = (si_memory, (mesh.n_edges, self.si_terms))
         for i in range(self.species):
-            expect[f"plasma_current_{i}"] = (plasma_currents[i], (mesh.n_faces, self.L, 3))
+            expect[f"plasma_current_{i}"] = (plasma_currents[i], (mesh.n_faces, 3, pm))
         for name, (t, shape) in expect.items():
             if t is None or not b.torch.is_tensor(t):
                 raise ValueError(f"{name} must be a device tensor")
             if tuple(t.shape) != shape:
-                raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shape}")
+                raise ValueError(f"{name} buffer has shape {tuple(t.shape)}, expected {shape}")
             if t.dtype != b.dtype or t.device != b.torch_device:
                 raise ValueError(f"{name} must be a {b.dtype_name} tensor on {b.device}")
-            if not t.is_contiguous():
-                raise ValueError(f"{name} must be contiguous")
+            if not t.is_contiguous() or t.data_ptr() % 16:
+                raise ValueError(f"{name} must be contiguous and 16-byte aligned")
         st = N.State()
         st.er, st.et, st.hr, st.ht = er.data_ptr(), et.data_ptr(), hr.data_ptr(), ht.data_ptr()
         st.si_memory = si_memory.data_ptr() if self.si_terms else None

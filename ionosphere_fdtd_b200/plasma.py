@@ -364,14 +364,21 @@ def vertex_face_average(mesh) -> tuple[NDArray[np.int64], NDArray[np.float64]]:
 
 
 class MagnetizedPlasmaADE:
-    """Species coefficients and device current densities (F, L, 3) per species."""
+    """Species coefficients and device current densities.
 
-    def __init__(self, model: MeshPlasmaModel, time_step_s: float, backend: Any):
+    Each species' current lives in a component-major buffer (F, 3, mid_pitch)
+    (16-byte aligned rows for the step kernels); ``current_density[s]`` is the
+    reference-shaped (F, L, 3) view of it, so reads, in-place writes and
+    checkpoints see the reference layout (plasma.py:411)."""
+
+    def __init__(self, model: MeshPlasmaModel, time_step_s: float, backend: Any, mid_pitch: int | None = None):
         self.model = model
         self.backend = backend
         self.coef, self.bdir, self.magnetized, self.rows = ade_coefficients(model, time_step_s)
-        shape = model.magnetic_field_t.shape[:2]
-        self.current_density = [backend.zeros((*shape, 3)) for _ in model.species]
+        n_faces, layers = model.magnetic_field_t.shape[:2]
+        pitch = mid_pitch or (layers + 3) // 4 * 4
+        self.buffers = [backend.zeros((n_faces, 3, pitch)) for _ in model.species]
+        self.current_density = [buf[:, :, :layers].permute(0, 2, 1) for buf in self.buffers]
 
     @property
     def state_bytes(self) -> int:
@@ -386,7 +393,7 @@ class MagnetizedPlasmaADE:
 class GeodesicPlasmaCoupler:
     """Reconstruction and scatter tables of the plasma coupling (plasma.py:455-545)."""
 
-    def __init__(self, model: MeshPlasmaModel, mesh, radial_midpoint_altitudes_m, time_step_s: float, backend: Any) -> None:
+    def __init__(self, model: MeshPlasmaModel, mesh, radial_midpoint_altitudes_m, time_step_s: float, backend: Any, mid_pitch: int | None = None) -> None:
         model.validate_grid(mesh, radial_midpoint_altitudes_m)
         self.mesh = mesh
         self.backend = backend
@@ -397,7 +404,7 @@ class GeodesicPlasmaCoupler:
         self.left_tangents = np.ascontiguousarray(tangents[mesh.edge_left_faces, left_slots])
         self.right_tangents = np.ascontiguousarray(tangents[mesh.edge_right_faces, right_slots])
         self.vertex_faces, self.vertex_face_weights = vertex_face_average(mesh)
-        self.ade = MagnetizedPlasmaADE(model, time_step_s, backend)
+        self.ade = MagnetizedPlasmaADE(model, time_step_s, backend, mid_pitch)
 
     @property
     def persistent_bytes(self) -> int:

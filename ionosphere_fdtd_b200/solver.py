@@ -22,6 +22,7 @@ from numpy.typing import NDArray
 
 from .backend import CudaBackend, create_backend
 from .constants import C_0, EARTH_RADIUS_M, EPSILON_0, MU_0
+from ._native import row_pitch
 from .engine import Engine, Physics, Tuning, plasma_inputs, surface_inputs
 from .materials import EarthIonosphereMaterial
 from .mesh import GeodesicMesh, build_geodesic_mesh
@@ -236,17 +237,31 @@ class GeodesicFDTD:
             raise ValueError("source carrier frequency must be below the time-step Nyquist limit")
 
         b = self.backend
-        self.er = b.zeros((self.mesh.n_vertices, len(self.radii_m)))
-        self.ht = b.zeros((self.mesh.n_edges, len(self.radii_m)))
-        self.et = b.zeros((self.mesh.n_edges, len(self.radial_midpoints_m)))
-        self.hr = b.zeros((self.mesh.n_faces, len(self.radial_midpoints_m)))
+        L = len(self.radial_midpoints_m)
+        self._node_pitch, self._mid_pitch = row_pitch(L + 1), row_pitch(L)
+        # padded, 16-byte aligned rows for the step kernels; the public fields
+        # are exact-shape views (padding stays zero)
+        self._buffers = {
+            "er": b.zeros((self.mesh.n_vertices, self._node_pitch)),
+            "et": b.zeros((self.mesh.n_edges, self._mid_pitch)),
+            "hr": b.zeros((self.mesh.n_faces, self._mid_pitch)),
+            "ht": b.zeros((self.mesh.n_edges, self._node_pitch)),
+        }
+        self._views = {
+            "er": self._buffers["er"][:, : L + 1],
+            "et": self._buffers["et"][:, :L],
+            "hr": self._buffers["hr"][:, :L],
+            "ht": self._buffers["ht"][:, : L + 1],
+        }
         self._surface_impedance_ade = (
             SurfaceImpedanceADE(surface_impedance, edge_count=self.mesh.n_edges, time_step_s=self.time_step_s, backend=b)
             if surface_impedance is not None
             else None
         )
         self._plasma_coupler = (
-            GeodesicPlasmaCoupler(plasma, self.mesh, self.radial_midpoint_altitudes_m, self.time_step_s, b) if plasma is not None else None
+            GeodesicPlasmaCoupler(plasma, self.mesh, self.radial_midpoint_altitudes_m, self.time_step_s, b, self._mid_pitch)
+            if plasma is not None
+            else None
         )
         self._prepare_geometry()
         self._prepare_material_coefficients()
@@ -264,7 +279,25 @@ class GeodesicFDTD:
         self._engine = Engine(
             self.mesh, self.radii_m, cfg.geometry_mode == "full-spherical", self.time_step_s, self._physics(), b, tuning
         )
+        if (self._engine.node_pitch, self._engine.mid_pitch) != (self._node_pitch, self._mid_pitch):
+            raise RuntimeError("native plan chose a different row pitch than the host layout")
         b._engine = self._engine
+
+    # -- fields: exact-shape views of padded device buffers -----------------------
+
+    def _assign_field(self, name: str, value: Any) -> None:
+        view = self._views[name]
+        torch = self.backend.torch
+        t = value if torch.is_tensor(value) else torch.as_tensor(np.asarray(value))
+        if tuple(t.shape) != tuple(view.shape):
+            raise ValueError(f"{name} must have shape {tuple(view.shape)}, got {tuple(t.shape)}")
+        if t.data_ptr() != view.data_ptr():
+            view.copy_(t.to(device=view.device, dtype=view.dtype))
+
+    er = property(lambda self: self._views["er"], lambda self, v: self._assign_field("er", v))
+    et = property(lambda self: self._views["et"], lambda self, v: self._assign_field("et", v))
+    hr = property(lambda self: self._views["hr"], lambda self, v: self._assign_field("hr", v))
+    ht = property(lambda self: self._views["ht"], lambda self, v: self._assign_field("ht", v))
 
     # -- setup (host, float64) ----------------------------------------------------
 
@@ -413,8 +446,12 @@ class GeodesicFDTD:
 
     def _state(self):
         ade = self._surface_impedance_ade
-        currents = tuple(self._plasma_coupler.ade.current_density) if self._plasma_coupler else ()
-        return self._engine.state(self.er, self.et, self.hr, self.ht, ade.memory if ade else None, currents)
+        currents = tuple(self._plasma_coupler.ade.buffers) if self._plasma_coupler else ()
+        buf = self._buffers
+        memory = ade.memory.contiguous() if ade is not None else None
+        if ade is not None and memory.data_ptr() != ade.memory.data_ptr():
+            ade.memory = memory
+        return self._engine.state(buf["er"], buf["et"], buf["hr"], buf["ht"], memory, currents)
 
     def _source_currents(self, count: int) -> NDArray[np.float64] | None:
         """I((n + 1/2) dt) for the next ``count`` steps, float64 (solver.py:851-865)."""
@@ -673,11 +710,12 @@ class GeodesicFDTD:
             "_radial_midpoints", "_inverse_radial_midpoints", "_radial_steps", "_radial_node_control_lengths",
             "_radial_center_distances",
         )
-        unique = {id(getattr(self, n)): getattr(self, n) for n in names}
+        unique = {id(getattr(self, n)): getattr(self, n) for n in names[4:]}
         total = sum(self.backend.nbytes(a) for a in unique.values())
+        total += sum(self.backend.nbytes(a) for a in self._buffers.values())
         total += self._engine.plan_bytes
         if self._surface_impedance_ade is not None:
             total += self._surface_impedance_ade.persistent_bytes
         if self._plasma_coupler is not None:
-            total += self._plasma_coupler.ade.state_bytes
+            total += sum(self.backend.nbytes(j) for j in self._plasma_coupler.ade.buffers)
         return total
