@@ -110,9 +110,11 @@ typedef struct ifdtd_physics_desc {
 
 /* Tuning of the launch geometry (0 = defaults). */
 typedef struct ifdtd_tuning {
-  int32_t faces_per_patch; /* faces owned by one CTA (default 32) */
-  int32_t threads;         /* threads per CTA (default 256) */
-  int32_t graph_chunk;     /* steps captured per CUDA graph (default 32; 0 disables) */
+  int32_t faces_per_patch;   /* faces owned by one H-phase CTA (default 32) */
+  int32_t threads;           /* threads per CTA (default 256) */
+  int32_t graph_chunk;       /* steps captured per CUDA graph (default 32; 0 disables) */
+  int32_t e_faces_per_patch; /* faces whose vertices/edges one E-phase CTA owns (default 16) */
+  int32_t staging;           /* 0 auto, 1 direct global gathers, 2 shared-memory staging */
 } ifdtd_tuning;
 
 /* Mutable state of one simulation: device pointers owned by the caller. */
@@ -134,6 +136,12 @@ int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* gr
 int32_t ifdtd_plan_destroy(ifdtd_plan* plan);
 /* Row pitches (in elements) the plan expects for node and midpoint arrays. */
 int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* mid_pitch);
+/* Device status word: bit 0 set when a staging wait hit its iteration limit
+ * (the step's results are then invalid).  Reading it synchronises the plan's
+ * device; reset != 0 clears it. */
+int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out);
+/* Which step kernels the plan launches: 1 direct, 2 staged (H phase, E phase). */
+int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode);
 /* Bytes of device memory held by the plan (tables, staging, scratch). */
 int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);
 

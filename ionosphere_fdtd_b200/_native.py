@@ -90,7 +90,7 @@ class PhysicsDesc(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("faces_per_patch", _i32), ("threads", _i32), ("graph_chunk", _i32)]
+    _fields_ = [("faces_per_patch", _i32), ("threads", _i32), ("graph_chunk", _i32), ("e_faces_per_patch", _i32), ("staging", _i32)]
 
 
 class State(C.Structure):
@@ -115,6 +115,8 @@ _SIGNATURES = {
     "ifdtd_plan_destroy": ([_vp], _i32),
     "ifdtd_plan_bytes": ([_vp, C.POINTER(C.c_int64)], _i32),
     "ifdtd_plan_layout": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
+    "ifdtd_status_word": ([_vp, _i32, C.POINTER(_i32)], _i32),
+    "ifdtd_plan_kernels": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_step": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_update_magnetic": ([_vp, C.POINTER(State), _vp], _i32),
     "ifdtd_update_electric": ([_vp, C.POINTER(State), C.c_double, _vp], _i32),

@@ -84,8 +84,10 @@ struct ifdtd_plan {
   int dtype = 4;
   int device = 0;
   int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
-  int n_patches = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
-  size_t smem_bytes = 0;
+  int n_patches = 0, n_patches_e = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
+  int h_mode = 1, e_mode = 1;  // 1 direct, 2 staged
+  size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
+  int* d_status = nullptr;
   bool plasma = false;
   DeviceArena arena;
   void* d_rec = nullptr;               // Rec<real> in device memory
@@ -143,9 +145,12 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       !in_range(M->edge_right_faces, nE, nF))
     return fail(IFDTD_ERR_ARGUMENT, "mesh index table out of range");
   const int fpp = (tune && tune->faces_per_patch > 0) ? tune->faces_per_patch : 32;
+  const int fpp_e = (tune && tune->e_faces_per_patch > 0) ? tune->e_faces_per_patch : 16;
+  const int staging = tune ? tune->staging : 0;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
   if (threads % 32 || threads > 256) return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 <= 256");
-  if ((int64_t)fpp * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
+  if (staging < 0 || staging > 2) return fail(IFDTD_ERR_ARGUMENT, "staging must be 0 (auto), 1 (direct) or 2 (staged)");
+  if ((int64_t)std::max(fpp, fpp_e) * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
   P->threads = threads;
   // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
   P->chunk = (tune && tune->graph_chunk >= 0) ? tune->graph_chunk : 32;
@@ -205,33 +210,41 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       v_coef[q] = (pass == 0 ? 1.0 : -1.0) * M->dual_edge_angles[e] / M->dual_cell_solid_angles[v];
     }
   // ---- patches: faces [p*fpp, (p+1)*fpp), edges by lowest adjacent face, vertices by lowest incident face ----
-  const int n_patches = (nF + fpp - 1) / fpp;
-  P->n_patches = n_patches;
-  std::vector<int> eptr(n_patches + 1);
-  {
-    int e = 0;
-    for (int p = 0; p <= n_patches; ++p) {
-      const int bound = std::min(p * fpp, nF);
-      while (e < nE && owner_e[e] < bound) ++e;
-      eptr[p] = (p == n_patches) ? nE : e;
-    }
-  }
   std::vector<int> owner_v(nV, nF);
   for (int f = 0; f < nF; ++f) {
     owner_v[fv[f].x] = std::min(owner_v[fv[f].x], f);
     owner_v[fv[f].y] = std::min(owner_v[fv[f].y], f);
     owner_v[fv[f].z] = std::min(owner_v[fv[f].z], f);
   }
-  std::vector<int> vptr(n_patches + 1, 0), vlist(nV);
-  for (int v = 0; v < nV; ++v) {
+  for (int v = 0; v < nV; ++v)
     if (owner_v[v] >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex without incident face");
-    vptr[owner_v[v] / fpp + 1]++;
-  }
-  for (int p = 0; p < n_patches; ++p) vptr[p + 1] += vptr[p];
-  {
-    std::vector<int> cursor(vptr.begin(), vptr.end() - 1);
-    for (int v = 0; v < nV; ++v) vlist[cursor[owner_v[v] / fpp]++] = v;
-  }
+  struct Own {
+    int fpp = 0, n = 0;
+    std::vector<int> eptr, vptr, vlist;
+  };
+  auto ownership = [&](int f_per) {
+    Own o;
+    o.fpp = f_per;
+    o.n = (nF + f_per - 1) / f_per;
+    o.eptr.assign(o.n + 1, 0);
+    int e = 0;
+    for (int q = 0; q <= o.n; ++q) {
+      const int bound = std::min(q * f_per, nF);
+      while (e < nE && owner_e[e] < bound) ++e;
+      o.eptr[q] = (q == o.n) ? nE : e;
+    }
+    o.vptr.assign(o.n + 1, 0);
+    o.vlist.assign(nV, 0);
+    for (int v = 0; v < nV; ++v) o.vptr[owner_v[v] / f_per + 1]++;
+    for (int q = 0; q < o.n; ++q) o.vptr[q + 1] += o.vptr[q];
+    std::vector<int> cursor(o.vptr.begin(), o.vptr.end() - 1);
+    for (int v = 0; v < nV; ++v) o.vlist[cursor[owner_v[v] / f_per]++] = v;
+    return o;
+  };
+  const Own oh = ownership(fpp), oe = ownership(fpp_e);
+  const std::vector<int>& vlist = oe.vlist;
+  P->n_patches = oh.n;
+  P->n_patches_e = oe.n;
   // ---- fixed-width vertex slots in vlist order (reference slot order, zero-padded) ----
   int maxdeg = 0;
   for (int v = 0; v < nV; ++v) maxdeg = std::max(maxdeg, deg[v]);
@@ -249,6 +262,121 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     }
   }
   P->maxdeg = MD;
+  std::vector<int> ps_face;
+  std::vector<real> ps_wc;
+  if (X->plasma_species > 0) {
+    const int W = X->vertex_face_width;
+    ps_face.assign((size_t)nV * SW, 0);
+    ps_wc.assign((size_t)nV * SW * 4, real(0));
+    for (int sl = 0; sl < nV; ++sl) {
+      const int v = vlist[sl];
+      int n = 0, first = -1;
+      for (int q = 0; q < W; ++q) {
+        const double w = X->vertex_face_weights[(size_t)v * W + q];
+        if (w == 0.0) continue;
+        const int64_t f = X->vertex_faces[(size_t)v * W + q];
+        if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
+        if (n >= MD) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
+        if (first < 0) first = (int)f;
+        ps_face[(size_t)sl * SW + n] = (int)f;
+        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
+        ++n;
+      }
+      for (int q = n; q < SW; ++q) ps_face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
+    }
+  }
+
+  // ---- shared-memory staging lists and local indices ----
+  const int S = std::max(0, X->plasma_species);
+  const bool plasma = S > 0;
+  std::vector<int> stampA(std::max(nV, std::max(nE, nF)), -1), locA(std::max(nV, std::max(nE, nF)), 0);
+  std::vector<int> stampB(std::max(nE, nF), -1), locB(std::max(nE, nF), 0);
+  std::vector<int> stampC(nF, -1), locC(nF, 0);
+  auto add = [](std::vector<int>& stamp, std::vector<int>& loc, std::vector<int>& rows, int base, int p, int id) {
+    if (stamp[id] != p) {
+      stamp[id] = p;
+      loc[id] = (int)rows.size() - base;
+      rows.push_back(id);
+    }
+    return loc[id];
+  };
+  // H phase: er rows (vertices) and et rows (edges) per patch
+  std::vector<int> khv_off(oh.n + 1, 0), khv_rows, khe_off(oh.n + 1, 0), khe_rows;
+  std::vector<int4> kh_edge_loc(nE), kh_face_loc(2 * (size_t)nF);
+  size_t kh_max = 0;
+  for (int q = 0; q < oh.n; ++q) {
+    const int fa = q * fpp, fb = std::min(fa + fpp, nF), ea = oh.eptr[q], eb = oh.eptr[q + 1];
+    khv_off[q] = (int)khv_rows.size();
+    khe_off[q] = (int)khe_rows.size();
+    for (int f = fa; f < fb; ++f) {
+      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].x);
+      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].y);
+      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].z);
+    }
+    for (int e = ea; e < eb; ++e) {
+      add(stampA, locA, khv_rows, khv_off[q], q, th[e].x);
+      add(stampA, locA, khv_rows, khv_off[q], q, th[e].y);
+    }
+    if (plasma)
+      for (int f = fa; f < fb; ++f) {
+        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].x);
+        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].y);
+        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].z);
+      }
+    for (int e = ea; e < eb; ++e) {
+      if (stampB[e] != q) return fail(IFDTD_ERR_ARGUMENT, "owned edge is not an edge of its patch's faces");
+      kh_edge_loc[e] = make_int4(locA[th[e].x], locA[th[e].y], locB[e], 0);
+    }
+    for (int f = fa; f < fb; ++f) {
+      kh_face_loc[2 * (size_t)f] = make_int4(locB[fe[f].x], locB[fe[f].y], locB[fe[f].z], plasma ? locA[fv[f].x] : 0);
+      kh_face_loc[2 * (size_t)f + 1] = make_int4(plasma ? locA[fv[f].y] : 0, plasma ? locA[fv[f].z] : 0, 0, 0);
+    }
+    const size_t nv = khv_rows.size() - khv_off[q], ne = khe_rows.size() - khe_off[q];
+    kh_max = std::max(kh_max, nv * Pn + ne * Pm + (size_t)(eb - ea) * Pn + (size_t)(fb - fa) * Pm +
+                                  (size_t)S * (fb - fa) * 3 * Pm);
+  }
+  khv_off[oh.n] = (int)khv_rows.size();
+  khe_off[oh.n] = (int)khe_rows.size();
+  // E phase: ht rows (edges), hr rows (faces), summed current rows (faces) per patch
+  std::fill(stampA.begin(), stampA.end(), -1);
+  std::fill(stampB.begin(), stampB.end(), -1);
+  std::vector<int> keh_off(oe.n + 1, 0), keh_rows, kef_off(oe.n + 1, 0), kef_rows, kej_off(oe.n + 1, 0), kej_rows;
+  std::vector<int> ke_slot_h((size_t)nV * SW, 0), ke_slot_j(plasma ? (size_t)nV * SW : 0, 0);
+  std::vector<int4> ke_edge_loc(nE);
+  std::vector<int> ke_edge_jr(plasma ? nE : 0, 0);
+  size_t ke_max = 0;
+  for (int q = 0; q < oe.n; ++q) {
+    const int va = oe.vptr[q], vb = oe.vptr[q + 1], ea = oe.eptr[q], eb = oe.eptr[q + 1];
+    keh_off[q] = (int)keh_rows.size();
+    kef_off[q] = (int)kef_rows.size();
+    kej_off[q] = (int)kej_rows.size();
+    for (int sl = va; sl < vb; ++sl)
+      for (int k = 0; k < SW; ++k)
+        ke_slot_h[(size_t)sl * SW + k] = add(stampA, locA, keh_rows, keh_off[q], q, ps_edge[(size_t)sl * SW + k]);
+    for (int e = ea; e < eb; ++e) add(stampA, locA, keh_rows, keh_off[q], q, e);
+    for (int e = ea; e < eb; ++e) {
+      add(stampB, locB, kef_rows, kef_off[q], q, lr[e].x);
+      add(stampB, locB, kef_rows, kef_off[q], q, lr[e].y);
+    }
+    if (plasma) {
+      for (int sl = va; sl < vb; ++sl)
+        for (int k = 0; k < SW; ++k)
+          ke_slot_j[(size_t)sl * SW + k] = add(stampC, locC, kej_rows, kej_off[q], q, ps_face[(size_t)sl * SW + k]);
+      for (int e = ea; e < eb; ++e) {
+        add(stampC, locC, kej_rows, kej_off[q], q, lr[e].x);
+        add(stampC, locC, kej_rows, kej_off[q], q, lr[e].y);
+      }
+    }
+    for (int e = ea; e < eb; ++e) {
+      ke_edge_loc[e] = make_int4(locA[e], locB[lr[e].x], locB[lr[e].y], plasma ? locC[lr[e].x] : 0);
+      if (plasma) ke_edge_jr[e] = locC[lr[e].y];
+    }
+    const size_t nh = keh_rows.size() - keh_off[q], nf = kef_rows.size() - kef_off[q], nj = kej_rows.size() - kej_off[q];
+    ke_max = std::max(ke_max, nh * Pn + nf * Pm + nj * 3 * Pm + (size_t)(vb - va) * Pn + (size_t)(eb - ea) * Pm);
+  }
+  keh_off[oe.n] = (int)keh_rows.size();
+  kef_off[oe.n] = (int)kef_rows.size();
+  kej_off[oe.n] = (int)kej_rows.size();
 
   // ---- radial metric rows, zero padded to Pn / Pm ----
   const double* r = G->radii_m;
@@ -310,9 +438,28 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     if (_e != cudaSuccess)                                                                              \
       return fail(IFDTD_ERR_CUDA, std::string("upload ") + #field + ": " + cudaGetErrorString(_e));     \
   } while (0)
-  UP(eptr, eptr);
-  UP(vptr, vptr);
-  UP(vlist, vlist);
+  UP(oh.eptr, eptr_h);
+  UP(oe.eptr, eptr_e);
+  UP(oe.vptr, vptr);
+  UP(oe.vlist, vlist);
+  UP(khv_off, khv_off);
+  UP(khv_rows, khv_rows);
+  UP(khe_off, khe_off);
+  UP(khe_rows, khe_rows);
+  UP(kh_edge_loc, kh_edge_loc);
+  UP(kh_face_loc, kh_face_loc);
+  UP(keh_off, keh_off);
+  UP(keh_rows, keh_rows);
+  UP(kef_off, kef_off);
+  UP(kef_rows, kef_rows);
+  UP(ke_slot_h, ke_slot_h);
+  UP(ke_edge_loc, ke_edge_loc);
+  if (plasma) {
+    UP(kej_off, kej_off);
+    UP(kej_rows, kej_rows);
+    UP(ke_slot_j, ke_slot_j);
+    UP(ke_edge_jr, ke_edge_jr);
+  }
   UP(th, edge_th);
   UP(lr, edge_lr);
   UP(inv_theta, inv_theta);
@@ -382,7 +529,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->S = X->plasma_species;
   if (X->plasma_species < 0 || X->plasma_species > IFDTD_MAX_SPECIES)
     return fail(IFDTD_ERR_ARGUMENT, "plasma species count out of range");
-  int slot_faces_ok = 1;
   if (X->plasma_species > 0) {
     const int S = X->plasma_species, rows = X->plasma_rows;
     if (!(rows == 1 || rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
@@ -410,29 +556,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
           for (int c = 0; c < 3; ++c) bd[((size_t)i * 3 + c) * Pm + j] = (real)X->plasma_bdir[((size_t)i * L + j) * 3 + c];
       UP(bd, bdir);
     }
-    const int W = X->vertex_face_width;
-    std::vector<int> ps_face((size_t)nV * SW, 0);
-    std::vector<real> ps_wc((size_t)nV * SW * 4, real(0));
-    for (int sl = 0; sl < nV; ++sl) {
-      const int v = vlist[sl];
-      int n = 0, first = -1;
-      for (int q = 0; q < W; ++q) {
-        const double w = X->vertex_face_weights[(size_t)v * W + q];
-        if (w == 0.0) continue;
-        const int64_t f = X->vertex_faces[(size_t)v * W + q];
-        if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
-        if (n >= MD) {
-          slot_faces_ok = 0;
-          break;
-        }
-        if (first < 0) first = (int)f;
-        ps_face[(size_t)sl * SW + n] = (int)f;
-        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
-        ++n;
-      }
-      for (int q = n; q < SW; ++q) ps_face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
-    }
-    if (!slot_faces_ok) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
     UP(ps_face, ps_face);
     UP(ps_wc, ps_wc);
     if (S > 1) {
@@ -450,8 +573,10 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.L = L;
   R.Pn = Pn;
   R.Pm = Pm;
-  R.n_patches = n_patches;
-  R.fpp = fpp;
+  R.n_patches_h = oh.n;
+  R.fpp_h = fpp;
+  R.n_patches_e = oe.n;
+  R.fpp_e = fpp_e;
   R.full = G->full_spherical ? 1 : 0;
   R.si_terms = X->si_terms;
   R.n_species = X->plasma_species;
@@ -469,6 +594,29 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.layer_reals = layer_reals(Pn, Pm, R.coef_full, X->plasma_species, R.plasma_full, R.magnetized, X->si_terms);
   P->smem_bytes = (size_t)R.layer_reals * sizeof(real);
   if (P->smem_bytes > 200 * 1024) return fail(IFDTD_ERR_UNSUPPORTED, "radial grid too fine for the shared per-layer rows");
+  {
+    // staged kernels: per-layer rows (rounded to 16 bytes) + the largest patch's rows
+    const size_t layer_block = (size_t)((R.layer_reals + 3) / 4 * 4) * sizeof(real);
+    P->kh_smem = layer_block + kh_max * sizeof(real);
+    P->ke_smem = layer_block + ke_max * sizeof(real);
+    const size_t auto_limit = 113 * 1024, hard_limit = 220 * 1024;
+    auto pick = [&](size_t need) {
+      if (staging == 1) return 1;
+      if (staging == 2) return need <= hard_limit ? 2 : 0;
+      return need <= auto_limit ? 2 : 1;
+    };
+    P->h_mode = pick(P->kh_smem);
+    P->e_mode = pick(P->ke_smem);
+    if (P->h_mode == 0 || P->e_mode == 0) return fail(IFDTD_ERR_UNSUPPORTED, "staged rows do not fit in shared memory");
+  }
+  {
+    void* st = nullptr;
+    cudaError_t e = A.alloc(sizeof(int), &st);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of the status word failed");
+    CUDA_TRY(cudaMemset(st, 0, sizeof(int)));
+    P->d_status = (int*)st;
+    R.status = (int*)st;
+  }
   R.dtmu = (real)(G->time_step_s / 1.256637062120e-6);
   {
     void* cur = nullptr;
@@ -518,20 +666,34 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 template <typename real, bool PL>
 cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, cudaStream_t st) {
-  auto k = kh_kernel<real, PL>;
-  cudaError_t e = allow_smem(k, P->smem_bytes);
-  if (e != cudaSuccess) return e;
-  k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members);
+  if (P->h_mode == 2) {
+    auto k = kh_staged<real, PL>;
+    cudaError_t e = allow_smem(k, P->kh_smem);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, P->threads, P->kh_smem, st>>>(rec, map, members);
+  } else {
+    auto k = kh_kernel<real, PL>;
+    cudaError_t e = allow_smem(k, P->smem_bytes);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members);
+  }
   return cudaGetLastError();
 }
 
 template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, int istep,
                         cudaStream_t st) {
-  auto k = ke_kernel<real, PL, MD>;
-  cudaError_t e = allow_smem(k, P->smem_bytes);
-  if (e != cudaSuccess) return e;
-  k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members, istep);
+  if (P->e_mode == 2) {
+    auto k = ke_staged<real, PL, MD>;
+    cudaError_t e = allow_smem(k, P->ke_smem);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, P->threads, P->ke_smem, st>>>(rec, map, members, istep);
+  } else {
+    auto k = ke_kernel<real, PL, MD>;
+    cudaError_t e = allow_smem(k, P->smem_bytes);
+    if (e != cudaSuccess) return e;
+    k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members, istep);
+  }
   return cudaGetLastError();
 }
 
@@ -545,11 +707,12 @@ cudaError_t launch_kh(ifdtd_plan* P, cudaStream_t st) {
 template <typename real>
 cudaError_t launch_ke(ifdtd_plan* P, int istep, cudaStream_t st) {
   const Rec<real>* rec = (const Rec<real>*)P->d_rec;
+  const int nb = P->n_patches_e;
   if (P->maxdeg == 6)
-    return P->plasma ? launch_ke_t<real, true, 6>(P, rec, nullptr, 1, P->n_patches, istep, st)
-                     : launch_ke_t<real, false, 6>(P, rec, nullptr, 1, P->n_patches, istep, st);
-  return P->plasma ? launch_ke_t<real, true, 12>(P, rec, nullptr, 1, P->n_patches, istep, st)
-                   : launch_ke_t<real, false, 12>(P, rec, nullptr, 1, P->n_patches, istep, st);
+    return P->plasma ? launch_ke_t<real, true, 6>(P, rec, nullptr, 1, nb, istep, st)
+                     : launch_ke_t<real, false, 6>(P, rec, nullptr, 1, nb, istep, st);
+  return P->plasma ? launch_ke_t<real, true, 12>(P, rec, nullptr, 1, nb, istep, st)
+                   : launch_ke_t<real, false, 12>(P, rec, nullptr, 1, nb, istep, st);
 }
 
 template <typename real>
@@ -686,6 +849,24 @@ int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* 
   if (!plan || !node_pitch || !mid_pitch) return fail(IFDTD_ERR_ARGUMENT, "null argument");
   *node_pitch = plan->Pn;
   *mid_pitch = plan->Pm;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out) {
+  if (!plan || !out) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  DeviceGuard guard(plan->device);
+  CUDA_TRY(cudaDeviceSynchronize());
+  int value = 0;
+  CUDA_TRY(cudaMemcpy(&value, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset) CUDA_TRY(cudaMemset(plan->d_status, 0, sizeof(int)));
+  *out = value;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode) {
+  if (!plan || !h_mode || !e_mode) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  *h_mode = plan->h_mode;
+  *e_mode = plan->e_mode;
   return IFDTD_OK;
 }
 

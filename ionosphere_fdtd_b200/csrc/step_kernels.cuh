@@ -42,7 +42,7 @@ template <typename real>
 struct Rec {
   // sizes and switches
   int nV, nE, nF, L, Pn, Pm;
-  int n_patches, fpp;
+  int n_patches_h, fpp_h, n_patches_e, fpp_e;
   int full, si_terms, n_species, plasma_full, magnetized, coef_full;
   int n_src_er, n_src_et;
   int src_er_vmin, src_er_vmax, src_et_emin, src_et_emax;
@@ -52,8 +52,10 @@ struct Rec {
   real* J[kMaxSpecies];  // (F, 3, Pm) per species
   real* Jtot;            // summed species current when n_species > 1
   const double* cur;     // per-step source current (staging row)
-  // patch ownership
-  const int *eptr, *vptr, *vlist;
+  int* status;           // device status word (bit 0: a staging wait timed out)
+  // ownership: H phase patches own faces [p*fpp_h, ...) and eptr_h edges;
+  // E phase patches own vertices vlist[vptr[p]..] and eptr_e edges
+  const int *eptr_h, *eptr_e, *vptr, *vlist;
   // edges
   const int2 *edge_th, *edge_lr;
   const real *inv_theta, *inv_phi;
@@ -67,6 +69,14 @@ struct Rec {
   const real* ps_coef;   // sign * phi_e / A*_v, 0 in padding slots
   const int* ps_face;
   const real* ps_wc;     // (V, slot_width, 4): area weight * face centre, 0 in padding slots
+  // shared-memory staging (per patch row lists and local indices into them)
+  const int *khv_off, *khv_rows, *khe_off, *khe_rows;  // H phase: er rows (vertices), et rows (edges)
+  const int4* kh_edge_loc;                             // per edge: tail, head (er rows), own et row, 0
+  const int4* kh_face_loc;                             // per face, 2 x int4: et rows x3, er rows x3
+  const int *keh_off, *keh_rows, *kef_off, *kef_rows, *kej_off, *kej_rows;  // E phase: ht, hr, J rows
+  const int *ke_slot_h, *ke_slot_j;                    // per vertex slot: local ht row / local J row
+  const int4* ke_edge_loc;                             // per edge: own ht row, left/right hr rows, left J row
+  const int* ke_edge_jr;                               // per edge: right J row
   // radial metric rows (padded; staged in shared memory by the kernels)
   const real *invr, *rr, *mid, *invm, *invdr, *invcd;
   real dtmu;             // dt / mu0
@@ -256,9 +266,355 @@ __device__ __forceinline__ void member_patch(const int2* block_map, int n_member
 }
 
 // ---------------------------------------------------------------------------
-// H phase: Ht (edges x nodes), surface-impedance ADE, Hr (faces x midpoints),
-// cold-plasma current ADE (faces x midpoints).
-// solver.py:877-921; surface_impedance.py:225-270; plasma.py:413-442, 489-501.
+// Bulk asynchronous copies (TMA, cp.async.bulk) into shared memory, completed
+// on an mbarrier.  Sources are always this GPU's global memory; no multicast.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kWaitLimit = 1u << 22;  // bounded spin on the staging barrier
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the staged rows with an iteration limit.  On timeout the CTA flags
+// the status word, waits once more (bounded) for its own copies and reports
+// failure so the caller skips the compute phase.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (threadIdx.x == 0) atomicOr(status, 1);
+  for (uint32_t i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) break;
+  return false;
+}
+
+// Start of the staged-row area after the per-layer rows (16-byte aligned).
+template <typename real>
+__device__ __forceinline__ real* staged_base(const Rec<real>& R, unsigned char* dyn) {
+  return reinterpret_cast<real*>(dyn) + ((R.layer_reals + 3) / 4) * 4;
+}
+
+// ---------------------------------------------------------------------------
+// Per-run arithmetic shared by the direct and the staged kernels.  Input row
+// pointers may address shared or global memory; outputs are global.
+// ---------------------------------------------------------------------------
+
+// Ht on nodes k0..k0+N-1 of edge e: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr)/mu0
+// with odd (PEC) Et ghosts (solver.py:877-899, 443-456); the run holding node 0
+// also advances the surface-impedance ADE (surface_impedance.py:225-270).
+template <typename real>
+__device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
+                                           const real* ert, const real* etr, const real* hto, real* htout) {
+  constexpr int N = Lanes<real>::N;
+  const int L = R.L, Lp1 = L + 1, Pm = R.Pm;
+  const real inv_t = __ldg(R.inv_theta + e);
+  const real dtmu = R.dtmu;
+  const Run<real> vh = ld16(erh + k0);
+  const Run<real> vt = ld16(ert + k0);
+  const Run<real> vo = ld16(hto + k0);
+  const Run<real> vu = (k0 < Pm) ? ld16(etr + k0) : zero_run<real>();
+  const real vprev = (k0 > 0 && k0 - 1 < L) ? etr[k0 - 1] : real(0);
+  Run<real> out;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const int k = k0 + r;
+    const real g = (vh.x[r] - vt.x[r]) * inv_t * Ls.invr[k];
+    real up = (k < L) ? vu.x[r] : real(0);
+    real dn = (k >= 1 && k - 1 < L) ? (r == 0 ? vprev : vu.x[r - 1]) : real(0);
+    real d;
+    if (R.full) {
+      up = (k < L) ? up * Ls.mid[k] : real(0);
+      dn = (k >= 1 && k - 1 < L) ? dn * Ls.mid[k - 1] : real(0);
+      d = (up - dn) * Ls.invcd[k] * Ls.invr[k];
+    } else {
+      d = (up - dn) * Ls.invcd[k];
+    }
+    out.x[r] = (k < Lp1) ? vo.x[r] + (g - d) * dtmu : real(0);
+  }
+  if (R.si_terms > 0 && k0 == 0) {
+    const int T = R.si_terms;
+    const real h_old = vo.x[0];
+    const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
+    const real e1 = R.si_metric * vu.x[0];
+    const real s = __ldg(R.si_scale + e);
+    real* mem = R.si_mem + (size_t)e * T;
+    real hist = real(0);
+    for (int p = 0; p < T; ++p) hist += mem[p] * Ls.si_hist[p];
+    hist *= s;
+    const real kap = R.si_kappa;
+    const real c = kap * (s * R.si_hist_sum);
+    const real h_new = ((real(1) - real(0.5) * c) * h_old + dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
+    const real hs = h_new + h_old;
+    for (int p = 0; p < T; ++p) mem[p] = mem[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
+    out.x[0] = h_new;
+  }
+  st16(htout + k0, out);
+}
+
+// Hr and the plasma current on midpoints j0..j0+N-1 of face f
+// (solver.py:915-921; plasma.py:413-442, 489-501).  jin[s] / jout[s] are the
+// face's (3, Pm) current rows of species s.
+template <typename real, bool PLASMA>
+__device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real>& Ls, int f, int j0, const real* et0,
+                                           const real* et1, const real* et2, const real* hro, real* hrout,
+                                           const real* pa, const real* pb, const real* pc, const real* const* jin,
+                                           real* const* jout, real* jtot) {
+  constexpr int N = Lanes<real>::N;
+  const int L = R.L, Pn = R.Pn, Pm = R.Pm;
+  const real dtmu = R.dtmu;
+  const Run<real> a0 = ld16(et0 + j0);
+  const Run<real> a1 = ld16(et1 + j0);
+  const Run<real> a2 = ld16(et2 + j0);
+  const Run<real> hv = ld16(hro + j0);
+  const real* fw = R.face_w + 4 * (size_t)f;
+  const real w0 = __ldg(fw), w1 = __ldg(fw + 1), w2 = __ldg(fw + 2);
+  Run<real> hn;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const int j = j0 + r;
+    hn.x[r] = (j < L) ? hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * Ls.invm[j] * dtmu : real(0);
+  }
+  st16(hrout + j0, hn);
+  if (!PLASMA) return;
+  const Run<real> na = ld16(pa + j0), nb = ld16(pb + j0), nc = ld16(pc + j0);
+  const bool tail = j0 + N < Pn;
+  const real ta = tail ? pa[j0 + N] : real(0), tb = tail ? pb[j0 + N] : real(0), tc = tail ? pc[j0 + N] : real(0);
+  const real third = real(1) / real(3);
+  real node[N + 1];
+#pragma unroll
+  for (int r = 0; r < N; ++r) node[r] = (na.x[r] + nb.x[r] + nc.x[r]) * third;
+  node[N] = (ta + tb + tc) * third;
+  const real* gp = R.face_pl + 12 * (size_t)f;
+  real rc[3][3], cf[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rc[i][c] = __ldg(gp + 4 * i + c);
+    cf[i] = __ldg(gp + 4 * i + 3);
+  }
+  real E[N][3];
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const real rad = real(0.5) * (node[r] + node[r + 1]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) E[r][c] = a0.x[r] * rc[0][c] + a1.x[r] * rc[1][c] + a2.x[r] * rc[2][c] + rad * cf[c];
+  }
+  real tot[N][3];
+#pragma unroll
+  for (int r = 0; r < N; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
+  for (int s = 0; s < R.n_species; ++s) {
+    Run<real> jc[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) jc[c] = ld16(jin[s] + c * Pm + j0);
+    Run<real> jn[3];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      const int j = j0 + r;
+      const real decay = pcoef_at(R, Ls, s, 0, f, j);
+      const real cs = pcoef_at(R, Ls, s, 1, f, j);
+      const real dre = pcoef_at(R, Ls, s, 4, f, j);
+      real nj[3];
+      if (R.magnetized) {
+        const real sn = pcoef_at(R, Ls, s, 2, f, j);
+        const real dpar = pcoef_at(R, Ls, s, 3, f, j);
+        const real dim = pcoef_at(R, Ls, s, 5, f, j);
+        real b[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          b[c] = R.plasma_full ? __ldg(R.bdir + ((size_t)f * 3 + c) * Pm + j) : Ls.bd[c * Pm + j];
+        const real eb = E[r][0] * b[0] + E[r][1] * b[1] + E[r][2] * b[2];
+        real Ep[3], Eq[3], Ex[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Ep[c] = eb * b[c];
+          Eq[c] = E[r][c] - Ep[c];
+        }
+        Ex[0] = Eq[1] * b[2] - Eq[2] * b[1];
+        Ex[1] = Eq[2] * b[0] - Eq[0] * b[2];
+        Ex[2] = Eq[0] * b[1] - Eq[1] * b[0];
+        const real J0 = jc[0].x[r], J1 = jc[1].x[r], J2 = jc[2].x[r];
+        const real jb = J0 * b[0] + J1 * b[1] + J2 * b[2];
+        real Jp[3], Jq[3], Jx[3];
+        Jp[0] = jb * b[0];
+        Jp[1] = jb * b[1];
+        Jp[2] = jb * b[2];
+        Jq[0] = J0 - Jp[0];
+        Jq[1] = J1 - Jp[1];
+        Jq[2] = J2 - Jp[2];
+        Jx[0] = Jq[1] * b[2] - Jq[2] * b[1];
+        Jx[1] = Jq[2] * b[0] - Jq[0] * b[2];
+        Jx[2] = Jq[0] * b[1] - Jq[1] * b[0];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          nj[c] = decay * Jp[c] + dpar * Ep[c] + decay * (cs * Jq[c] + sn * Jx[c]) + dre * Eq[c] + dim * Ex[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nj[c] = decay * (cs * jc[c].x[r]) + dre * E[r][c];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const real v = (j < L) ? nj[c] : real(0);
+        jn[c].x[r] = v;
+        tot[r][c] += v;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st16(jout[s] + c * Pm + j0, jn[c]);
+  }
+  if (R.n_species > 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Run<real> t;
+#pragma unroll
+      for (int r = 0; r < N; ++r) t.x[r] = tot[r][c];
+      st16(jtot + c * Pm + j0, t);
+    }
+  }
+}
+
+// Er on nodes k0..k0+N-1 of vertex v (solver.py:929-962; plasma.py:511-526).
+// hrows[q]: Ht row of slot q's edge; jrows[q]: (3, Pm) summed current rows of
+// slot q's face; slot coefficients come from the slot tables at `slot`.
+template <typename real, bool PLASMA, int MAXDEG>
+__device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int slot, int k0,
+                                             const real* const* hrows, const real* const* jrows, const real* ero,
+                                             real* erout, real current) {
+  constexpr int N = Lanes<real>::N;
+  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
+  Run<real> hv[MAXDEG];
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) hv[q] = ld16(hrows[q] + k0);
+  const Run<real> ev = ld16(ero + k0);
+  real acc[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    acc[r] = real(0);
+#pragma unroll
+    for (int q = 0; q < MAXDEG; ++q) acc[r] += __ldg(R.ps_coef + (size_t)slot * SW + q) * hv[q].x[r];
+  }
+  real jr[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) jr[r] = real(0);
+  if (PLASMA) {
+    // radial current at faces (J . centre), area-averaged to the vertex, then to nodes
+    real rav[N + 1];
+#pragma unroll
+    for (int r = 0; r <= N; ++r) rav[r] = real(0);
+#pragma unroll 2
+    for (int q = 0; q < MAXDEG; ++q) {
+      const real* wc = R.ps_wc + ((size_t)slot * SW + q) * 4;
+      const real c0 = __ldg(wc), c1 = __ldg(wc + 1), c2 = __ldg(wc + 2);
+      const real* jf = jrows[q];
+      const bool in = k0 < Pm;
+      const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
+      const Run<real> jy = in ? ld16(jf + Pm + k0) : zero_run<real>();
+      const Run<real> jz = in ? ld16(jf + 2 * Pm + k0) : zero_run<real>();
+      if (k0 >= 1 && k0 - 1 < L) rav[0] += jf[k0 - 1] * c0 + jf[Pm + k0 - 1] * c1 + jf[2 * Pm + k0 - 1] * c2;
+#pragma unroll
+      for (int r = 0; r < N; ++r) rav[r + 1] += jx.x[r] * c0 + jy.x[r] * c1 + jz.x[r] * c2;
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      const int k = k0 + r;
+      jr[r] = (k == 0) ? rav[r + 1] : (k == L ? rav[r] : real(0.5) * (rav[r] + rav[r + 1]));
+    }
+  }
+  Run<real> out;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const int k = k0 + r;
+    const real ca = R.coef_full ? __ldg(R.ca_er + (size_t)v * Pn + k) : Ls.ca_er[k];
+    const real cb = R.coef_full ? __ldg(R.cb_er + (size_t)v * Pn + k) : Ls.cb_er[k];
+    real x = ca * ev.x[r] + cb * (acc[r] * Ls.invr[k]);
+    if (v >= R.src_er_vmin && v <= R.src_er_vmax) {
+      for (int s = 0; s < R.n_src_er; ++s)
+        if (__ldg(R.src_er_v + s) == v && __ldg(R.src_er_k + s) == k) x -= __ldg(R.src_er_c + s) * current;
+    }
+    if (PLASMA) x -= cb * jr[r];
+    out.x[r] = (k < Lp1) ? x : real(0);
+  }
+  st16(erout + k0, out);
+}
+
+// Et on midpoints j0..j0+N-1 of edge e (solver.py:964-989; plasma.py:503-509).
+template <typename real, bool PLASMA>
+__device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int j0, const real* hl,
+                                           const real* hq, const real* hto, const real* jl, const real* jq,
+                                           const real* eto, real* etout, real current) {
+  constexpr int N = Lanes<real>::N;
+  const int L = R.L, Pn = R.Pn, Pm = R.Pm;
+  const real inv_p = __ldg(R.inv_phi + e);
+  const Run<real> a = ld16(hl + j0);
+  const Run<real> b = ld16(hq + j0);
+  const Run<real> hv = ld16(hto + j0);
+  const real htail = (j0 + N < Pn) ? hto[j0 + N] : real(0);
+  const Run<real> ev = ld16(eto + j0);
+  real jt[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) jt[r] = real(0);
+  if (PLASMA) {
+    const real* tp = R.tan + 8 * (size_t)e;
+    const real l0 = __ldg(tp), l1 = __ldg(tp + 1), l2 = __ldg(tp + 2);
+    const real q0 = __ldg(tp + 4), q1 = __ldg(tp + 5), q2 = __ldg(tp + 6);
+    const Run<real> lx = ld16(jl + j0), ly = ld16(jl + Pm + j0), lz = ld16(jl + 2 * Pm + j0);
+    const Run<real> qx = ld16(jq + j0), qy = ld16(jq + Pm + j0), qz = ld16(jq + 2 * Pm + j0);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      const real left = lx.x[r] * l0 + ly.x[r] * l1 + lz.x[r] * l2;
+      const real right = qx.x[r] * q0 + qy.x[r] * q1 + qz.x[r] * q2;
+      jt[r] = real(0.5) * (left + right);
+    }
+  }
+  Run<real> out;
+#pragma unroll
+  for (int r = 0; r < N; ++r) {
+    const int j = j0 + r;
+    const real hnext = (r + 1 < N) ? hv.x[r + 1] : htail;
+    real g = (a.x[r] - b.x[r]) * inv_p * Ls.invm[j];
+    const real d = R.full ? (Ls.rr[j + 1] * hnext - Ls.rr[j] * hv.x[r]) * Ls.invdr[j] * Ls.invm[j]
+                          : (hnext - hv.x[r]) * Ls.invdr[j];
+    g -= d;
+    const real ca = R.coef_full ? __ldg(R.ca_et + (size_t)e * Pm + j) : Ls.ca_et[j];
+    const real cb = R.coef_full ? __ldg(R.cb_et + (size_t)e * Pm + j) : Ls.cb_et[j];
+    real x = ca * ev.x[r] + cb * g;
+    if (e >= R.src_et_emin && e <= R.src_et_emax) {
+      for (int s = 0; s < R.n_src_et; ++s)
+        if (__ldg(R.src_et_e + s) == e && __ldg(R.src_et_j + s) == j) x -= __ldg(R.src_et_c + s) * current;
+    }
+    if (PLASMA) x -= cb * jt[r];
+    out.x[r] = (j < L) ? x : real(0);
+  }
+  st16(etout + j0, out);
+}
+
+// ---------------------------------------------------------------------------
+// Direct kernels: neighbour rows read straight from global memory (used when a
+// patch's staged rows would not fit in shared memory).
 // ---------------------------------------------------------------------------
 template <typename real, bool PLASMA>
 __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
@@ -271,201 +627,31 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
   load_rec(R, recs + member);
   Layers<real> Ls;
   load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm;
-  const int cn = Pn / N, cm = Pm / N;
+  const int Pn = R.Pn, Pm = R.Pm, cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  const real* __restrict__ er = R.er;
-  const real* __restrict__ et = R.et;
-  real* __restrict__ ht = R.ht;
-  real* __restrict__ hr = R.hr;
-  const real dtmu = R.dtmu;
-  const bool si = R.si_terms > 0;
-  const bool full = R.full != 0;
-
-  // ---- Ht: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr) / mu0, odd (PEC) Et ghosts;
-  //      the run holding node 0 also advances the surface-impedance ADE ----
-  const int ea = R.eptr[patch], eb = R.eptr[patch + 1];
-  const int n_edge_items = (eb - ea) * cn;
-  for (int it = threadIdx.x; it < n_edge_items; it += blockDim.x) {
+  const int ea = R.eptr_h[patch], eb = R.eptr_h[patch + 1];
+  for (int it = threadIdx.x; it < (eb - ea) * cn; it += blockDim.x) {
     const int el = fast_div(it, mag_cn);
-    const int k0 = (it - el * cn) * N;
     const int e = ea + el;
     const int2 th = __ldg(R.edge_th + e);
-    const real inv_t = __ldg(R.inv_theta + e);
-    const Run<real> vh = ldg16(er + (size_t)th.y * Pn + k0);
-    const Run<real> vt = ldg16(er + (size_t)th.x * Pn + k0);
-    real* htp = ht + (size_t)e * Pn + k0;
-    const Run<real> vo = ld16(htp);
-    const real* etr = et + (size_t)e * Pm;
-    const Run<real> vu = (k0 < Pm) ? ldg16(etr + k0) : zero_run<real>();  // Et at k0 .. k0+N-1
-    const real vprev = (k0 > 0 && k0 - 1 < L) ? __ldg(etr + k0 - 1) : real(0);
-    Run<real> out;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int k = k0 + r;
-      const real g = (vh.x[r] - vt.x[r]) * inv_t * Ls.invr[k];
-      real up = (k < L) ? vu.x[r] : real(0);
-      real dn = (k >= 1 && k - 1 < L) ? (r == 0 ? vprev : vu.x[r - 1]) : real(0);
-      real d;
-      if (full) {
-        up = (k < L) ? up * Ls.mid[k] : real(0);
-        dn = (k >= 1 && k - 1 < L) ? dn * Ls.mid[k - 1] : real(0);
-        d = (up - dn) * Ls.invcd[k] * Ls.invr[k];
-      } else {
-        d = (up - dn) * Ls.invcd[k];
-      }
-      out.x[r] = (k < Lp1) ? vo.x[r] + (g - d) * dtmu : real(0);
-    }
-    if (si && k0 == 0) {
-      // lower boundary: implicit coupling of the curl to the passive impedance ADE
-      const int T = R.si_terms;
-      const real h_old = vo.x[0];
-      const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
-      const real e1 = R.si_metric * vu.x[0];
-      const real s = __ldg(R.si_scale + e);
-      real* mem = R.si_mem + (size_t)e * T;
-      real hist = real(0);
-      for (int p = 0; p < T; ++p) hist += mem[p] * Ls.si_hist[p];
-      hist *= s;
-      const real kap = R.si_kappa;
-      const real c = kap * (s * R.si_hist_sum);
-      const real h_new = ((real(1) - real(0.5) * c) * h_old + dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
-      const real hs = h_new + h_old;
-      for (int p = 0; p < T; ++p) mem[p] = mem[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
-      out.x[0] = h_new;
-    }
-    st16(htp, out);
+    h_edge_run(R, Ls, e, (it - el * cn) * N, R.er + (size_t)th.y * Pn, R.er + (size_t)th.x * Pn, R.et + (size_t)e * Pm,
+               R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn);
   }
-
-  // ---- Hr and the plasma current on owned faces ----
-  const int fa = patch * R.fpp;
-  const int fb = min(fa + R.fpp, R.nF);
-  const int n_face_items = (fb - fa) * cm;
-  for (int it = threadIdx.x; it < n_face_items; it += blockDim.x) {
+  const int fa = patch * R.fpp_h, fb = min(fa + R.fpp_h, R.nF);
+  for (int it = threadIdx.x; it < (fb - fa) * cm; it += blockDim.x) {
     const int fl = fast_div(it, mag_cm);
-    const int j0 = (it - fl * cm) * N;
     const int f = fa + fl;
     const int4 fe = __ldg(R.face_e + f);
-    const Run<real> a0 = ldg16(et + (size_t)fe.x * Pm + j0);
-    const Run<real> a1 = ldg16(et + (size_t)fe.y * Pm + j0);
-    const Run<real> a2 = ldg16(et + (size_t)fe.z * Pm + j0);
-    real* hrp = hr + (size_t)f * Pm + j0;
-    const Run<real> hv = ld16(hrp);
-    const real* fw = R.face_w + 4 * (size_t)f;
-    const real w0 = __ldg(fw), w1 = __ldg(fw + 1), w2 = __ldg(fw + 2);
-    Run<real> hn;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int j = j0 + r;
-      hn.x[r] = (j < L) ? hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * Ls.invm[j] * dtmu : real(0);
-    }
-    st16(hrp, hn);
-    if (PLASMA) {
-      const int4 fv = __ldg(R.face_v + f);
-      const real* pa = er + (size_t)fv.x * Pn;
-      const real* pb = er + (size_t)fv.y * Pn;
-      const real* pc = er + (size_t)fv.z * Pn;
-      const Run<real> na = ldg16(pa + j0), nb = ldg16(pb + j0), nc = ldg16(pc + j0);
-      const bool tail = j0 + N < Pn;
-      const real ta = tail ? __ldg(pa + j0 + N) : real(0), tb = tail ? __ldg(pb + j0 + N) : real(0),
-                 tc = tail ? __ldg(pc + j0 + N) : real(0);
-      const real third = real(1) / real(3);
-      real node[N + 1];
-#pragma unroll
-      for (int r = 0; r < N; ++r) node[r] = (na.x[r] + nb.x[r] + nc.x[r]) * third;
-      node[N] = (ta + tb + tc) * third;
-      const real* gp = R.face_pl + 12 * (size_t)f;
-      real rc[3][3], cf[3];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) rc[i][c] = __ldg(gp + 4 * i + c);
-        cf[i] = __ldg(gp + 4 * i + 3);
-      }
-      real E[N][3];
-#pragma unroll
-      for (int r = 0; r < N; ++r) {
-        const real rad = real(0.5) * (node[r] + node[r + 1]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) E[r][c] = a0.x[r] * rc[0][c] + a1.x[r] * rc[1][c] + a2.x[r] * rc[2][c] + rad * cf[c];
-      }
-      real tot[N][3];
-#pragma unroll
-      for (int r = 0; r < N; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
-      for (int s = 0; s < R.n_species; ++s) {
-        real* Js = R.J[s] + (size_t)f * 3 * Pm + j0;
-        Run<real> jc[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) jc[c] = ld16(Js + c * Pm);
-        Run<real> jn[3];
-#pragma unroll
-        for (int r = 0; r < N; ++r) {
-          const int j = j0 + r;
-          const real decay = pcoef_at(R, Ls, s, 0, f, j);
-          const real cs = pcoef_at(R, Ls, s, 1, f, j);
-          const real dre = pcoef_at(R, Ls, s, 4, f, j);
-          real nj[3];
-          if (R.magnetized) {
-            const real sn = pcoef_at(R, Ls, s, 2, f, j);
-            const real dpar = pcoef_at(R, Ls, s, 3, f, j);
-            const real dim = pcoef_at(R, Ls, s, 5, f, j);
-            real b[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              b[c] = R.plasma_full ? __ldg(R.bdir + ((size_t)f * 3 + c) * Pm + j) : Ls.bd[c * Pm + j];
-            const real eb = E[r][0] * b[0] + E[r][1] * b[1] + E[r][2] * b[2];
-            real Ep[3], Eq[3], Ex[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              Ep[c] = eb * b[c];
-              Eq[c] = E[r][c] - Ep[c];
-            }
-            Ex[0] = Eq[1] * b[2] - Eq[2] * b[1];
-            Ex[1] = Eq[2] * b[0] - Eq[0] * b[2];
-            Ex[2] = Eq[0] * b[1] - Eq[1] * b[0];
-            const real J0 = jc[0].x[r], J1 = jc[1].x[r], J2 = jc[2].x[r];
-            const real jb = J0 * b[0] + J1 * b[1] + J2 * b[2];
-            real Jp[3], Jq[3], Jx[3];
-            Jp[0] = jb * b[0]; Jp[1] = jb * b[1]; Jp[2] = jb * b[2];
-            Jq[0] = J0 - Jp[0]; Jq[1] = J1 - Jp[1]; Jq[2] = J2 - Jp[2];
-            Jx[0] = Jq[1] * b[2] - Jq[2] * b[1];
-            Jx[1] = Jq[2] * b[0] - Jq[0] * b[2];
-            Jx[2] = Jq[0] * b[1] - Jq[1] * b[0];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              nj[c] = decay * Jp[c] + dpar * Ep[c] + decay * (cs * Jq[c] + sn * Jx[c]) + dre * Eq[c] + dim * Ex[c];
-          } else {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) nj[c] = decay * (cs * jc[c].x[r]) + dre * E[r][c];
-          }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const real v = (j < L) ? nj[c] : real(0);
-            jn[c].x[r] = v;
-            tot[r][c] += v;
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) st16(Js + c * Pm, jn[c]);
-      }
-      if (R.n_species > 1) {
-        real* Jt = R.Jtot + (size_t)f * 3 * Pm + j0;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          Run<real> t;
-#pragma unroll
-          for (int r = 0; r < N; ++r) t.x[r] = tot[r][c];
-          st16(Jt + c * Pm, t);
-        }
-      }
-    }
+    const int4 fv = PLASMA ? __ldg(R.face_v + f) : make_int4(0, 0, 0, 0);
+    real* jrow[kMaxSpecies];
+    for (int s = 0; s < kMaxSpecies; ++s) jrow[s] = s < R.n_species ? R.J[s] + (size_t)f * 3 * Pm : nullptr;
+    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, R.et + (size_t)fe.x * Pm, R.et + (size_t)fe.y * Pm,
+                             R.et + (size_t)fe.z * Pm, R.hr + (size_t)f * Pm, R.hr + (size_t)f * Pm,
+                             R.er + (size_t)fv.x * Pn, R.er + (size_t)fv.y * Pn, R.er + (size_t)fv.z * Pn, jrow, jrow,
+                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr);
   }
 }
 
-// ---------------------------------------------------------------------------
-// E phase: Er (vertices x nodes) and Et (edges x midpoints).
-// solver.py:923-989; plasma.py:503-527.
-// ---------------------------------------------------------------------------
 template <typename real, bool PLASMA, int MAXDEG>
 __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
                                                   int n_members, int istep) {
@@ -477,145 +663,182 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
   load_rec(R, recs + member);
   Layers<real> Ls;
   load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
-  const int cn = Pn / N, cm = Pm / N;
+  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  real* __restrict__ er = R.er;
-  real* __restrict__ et = R.et;
-  const real* __restrict__ ht = R.ht;
-  const real* __restrict__ hr = R.hr;
   const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
-  const real* __restrict__ Jsum = PLASMA ? jsum(R) : nullptr;
-  const bool full = R.full != 0;
-  const bool coef_full = R.coef_full != 0;
-
-  // ---- Er: dual-cell circulation of Ht, exponential loss, sources, Jr ----
+  const real* Jsum = PLASMA ? jsum(R) : nullptr;
   const int va = R.vptr[patch], vb = R.vptr[patch + 1];
-  const int n_vert_items = (vb - va) * cn;
-  for (int it = threadIdx.x; it < n_vert_items; it += blockDim.x) {
+  for (int it = threadIdx.x; it < (vb - va) * cn; it += blockDim.x) {
     const int vl = fast_div(it, mag_cn);
-    const int k0 = (it - vl * cn) * N;
     const int slot = va + vl;
     const int v = __ldg(R.vlist + slot);
-    int eidx[MAXDEG];
-    real ecoef[MAXDEG];
+    const real* hrows[MAXDEG];
+    const real* jrows[MAXDEG];
 #pragma unroll
     for (int q = 0; q < MAXDEG; ++q) {
-      eidx[q] = __ldg(R.ps_edge + (size_t)slot * SW + q);
-      ecoef[q] = __ldg(R.ps_coef + (size_t)slot * SW + q);
+      hrows[q] = R.ht + (size_t)__ldg(R.ps_edge + (size_t)slot * SW + q) * Pn;
+      jrows[q] = PLASMA ? Jsum + (size_t)__ldg(R.ps_face + (size_t)slot * SW + q) * 3 * Pm : nullptr;
     }
-    Run<real> hvals[MAXDEG];
-#pragma unroll
-    for (int q = 0; q < MAXDEG; ++q) hvals[q] = ldg16(ht + (size_t)eidx[q] * Pn + k0);
-    real* erp = er + (size_t)v * Pn + k0;
-    const Run<real> ev = ld16(erp);
-    real acc[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      acc[r] = real(0);
-#pragma unroll
-      for (int q = 0; q < MAXDEG; ++q) acc[r] += ecoef[q] * hvals[q].x[r];
-    }
-    real jr[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) jr[r] = real(0);
-    if (PLASMA) {
-      // radial current at faces (J . centre), area-averaged to the vertex, then to nodes
-      real rav[N + 1];
-#pragma unroll
-      for (int r = 0; r <= N; ++r) rav[r] = real(0);
-#pragma unroll 2
-      for (int q = 0; q < MAXDEG; ++q) {
-        const int f = __ldg(R.ps_face + (size_t)slot * SW + q);
-        const real* wc = R.ps_wc + ((size_t)slot * SW + q) * 4;
-        const real c0 = __ldg(wc), c1 = __ldg(wc + 1), c2 = __ldg(wc + 2);
-        const real* jf = Jsum + (size_t)f * 3 * Pm;
-        const bool in = k0 < Pm;
-        const Run<real> jx = in ? ldg16(jf + k0) : zero_run<real>();
-        const Run<real> jy = in ? ldg16(jf + Pm + k0) : zero_run<real>();
-        const Run<real> jz = in ? ldg16(jf + 2 * Pm + k0) : zero_run<real>();
-        const bool prev = k0 >= 1 && k0 - 1 < L;
-        if (prev) rav[0] += __ldg(jf + k0 - 1) * c0 + __ldg(jf + Pm + k0 - 1) * c1 + __ldg(jf + 2 * Pm + k0 - 1) * c2;
-#pragma unroll
-        for (int r = 0; r < N; ++r) rav[r + 1] += jx.x[r] * c0 + jy.x[r] * c1 + jz.x[r] * c2;
-      }
-#pragma unroll
-      for (int r = 0; r < N; ++r) {
-        const int k = k0 + r;
-        jr[r] = (k == 0) ? rav[r + 1] : (k == L ? rav[r] : real(0.5) * (rav[r] + rav[r + 1]));
-      }
-    }
-    Run<real> out;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int k = k0 + r;
-      const real ca = coef_full ? __ldg(R.ca_er + (size_t)v * Pn + k) : Ls.ca_er[k];
-      const real cb = coef_full ? __ldg(R.cb_er + (size_t)v * Pn + k) : Ls.cb_er[k];
-      real x = ca * ev.x[r] + cb * (acc[r] * Ls.invr[k]);
-      if (v >= R.src_er_vmin && v <= R.src_er_vmax) {
-        for (int s = 0; s < R.n_src_er; ++s)
-          if (__ldg(R.src_er_v + s) == v && __ldg(R.src_er_k + s) == k) x -= __ldg(R.src_er_c + s) * current;
-      }
-      if (PLASMA) x -= cb * jr[r];
-      out.x[r] = (k < Lp1) ? x : real(0);
-    }
-    st16(erp, out);
+    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, slot, (it - vl * cn) * N, hrows, jrows, R.er + (size_t)v * Pn,
+                                       R.er + (size_t)v * Pn, current);
   }
-
-  // ---- Et: dual-edge difference of Hr minus (1/m) d(r Ht)/dr, loss, sources, Jt ----
-  const int ea = R.eptr[patch], eb = R.eptr[patch + 1];
-  const int n_edge_items = (eb - ea) * cm;
-  for (int it = threadIdx.x; it < n_edge_items; it += blockDim.x) {
+  const int ea = R.eptr_e[patch], eb = R.eptr_e[patch + 1];
+  for (int it = threadIdx.x; it < (eb - ea) * cm; it += blockDim.x) {
     const int el = fast_div(it, mag_cm);
-    const int j0 = (it - el * cm) * N;
     const int e = ea + el;
     const int2 lr = __ldg(R.edge_lr + e);
-    const real inv_p = __ldg(R.inv_phi + e);
-    const Run<real> a = ldg16(hr + (size_t)lr.x * Pm + j0);
-    const Run<real> b = ldg16(hr + (size_t)lr.y * Pm + j0);
-    const real* htr = ht + (size_t)e * Pn;
-    const Run<real> hv = ldg16(htr + j0);
-    const real htail = (j0 + N < Pn) ? __ldg(htr + j0 + N) : real(0);
-    real* etp = et + (size_t)e * Pm + j0;
-    const Run<real> ev = ld16(etp);
-    real jt[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) jt[r] = real(0);
-    if (PLASMA) {
-      const real* jl = Jsum + (size_t)lr.x * 3 * Pm + j0;
-      const real* jq = Jsum + (size_t)lr.y * 3 * Pm + j0;
-      const real* tp = R.tan + 8 * (size_t)e;
-      const real l0 = __ldg(tp), l1 = __ldg(tp + 1), l2 = __ldg(tp + 2);
-      const real q0 = __ldg(tp + 4), q1 = __ldg(tp + 5), q2 = __ldg(tp + 6);
-      const Run<real> lx = ldg16(jl), ly = ldg16(jl + Pm), lz = ldg16(jl + 2 * Pm);
-      const Run<real> qx = ldg16(jq), qy = ldg16(jq + Pm), qz = ldg16(jq + 2 * Pm);
-#pragma unroll
-      for (int r = 0; r < N; ++r) {
-        const real left = lx.x[r] * l0 + ly.x[r] * l1 + lz.x[r] * l2;
-        const real right = qx.x[r] * q0 + qy.x[r] * q1 + qz.x[r] * q2;
-        jt[r] = real(0.5) * (left + right);
-      }
+    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, R.hr + (size_t)lr.x * Pm, R.hr + (size_t)lr.y * Pm,
+                             R.ht + (size_t)e * Pn, PLASMA ? Jsum + (size_t)lr.x * 3 * Pm : nullptr,
+                             PLASMA ? Jsum + (size_t)lr.y * 3 * Pm : nullptr, R.et + (size_t)e * Pm,
+                             R.et + (size_t)e * Pm, current);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Staged kernels: each CTA bulk-copies every row its patch reads (gathered
+// neighbour columns and its own contiguous ranges) into shared memory with
+// cp.async.bulk on one mbarrier, then computes from shared memory.  The copy
+// engine, not registers, holds the bytes in flight.
+// ---------------------------------------------------------------------------
+template <typename real, bool PLASMA>
+__global__ void __launch_bounds__(256) kh_staged(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
+                                                  int n_members) {
+  constexpr int N = Lanes<real>::N;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t bar;
+  int member, patch;
+  member_patch(block_map, n_members, member, patch);
+  load_rec(R, recs + member);
+  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0;
+  const int ea = R.eptr_h[patch], eb = R.eptr_h[patch + 1];
+  const int fa = patch * R.fpp_h, fb = min(fa + R.fpp_h, R.nF);
+  const int nE_own = eb - ea, nF_own = fb - fa;
+  const int v0 = R.khv_off[patch], nv = R.khv_off[patch + 1] - v0;
+  const int e0 = R.khe_off[patch], ne = R.khe_off[patch + 1] - e0;
+  real* s_er = staged_base(R, dyn_smem);
+  real* s_et = s_er + (size_t)nv * Pn;
+  real* s_ht = s_et + (size_t)ne * Pm;
+  real* s_hr = s_ht + (size_t)nE_own * Pn;
+  real* s_J = s_hr + (size_t)nF_own * Pm;
+  const uint32_t bytes =
+      (uint32_t)sizeof(real) * ((uint32_t)nv * Pn + (uint32_t)ne * Pm + (uint32_t)nE_own * Pn + (uint32_t)nF_own * Pm +
+                                (uint32_t)S * nF_own * 3 * Pm);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, bytes);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nv; i += blockDim.x)
+    bulk_load(s_er + (size_t)i * Pn, R.er + (size_t)__ldg(R.khv_rows + v0 + i) * Pn, Pn * sizeof(real), &bar);
+  for (int i = threadIdx.x; i < ne; i += blockDim.x)
+    bulk_load(s_et + (size_t)i * Pm, R.et + (size_t)__ldg(R.khe_rows + e0 + i) * Pm, Pm * sizeof(real), &bar);
+  if (threadIdx.x == blockDim.x - 1) {
+    if (nE_own) bulk_load(s_ht, R.ht + (size_t)ea * Pn, (uint32_t)nE_own * Pn * sizeof(real), &bar);
+    if (nF_own) bulk_load(s_hr, R.hr + (size_t)fa * Pm, (uint32_t)nF_own * Pm * sizeof(real), &bar);
+    for (int s = 0; s < S; ++s)
+      bulk_load(s_J + (size_t)s * nF_own * 3 * Pm, R.J[s] + (size_t)fa * 3 * Pm, (uint32_t)nF_own * 3 * Pm * sizeof(real),
+                &bar);
+  }
+  Layers<real> Ls;
+  load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);  // overlaps the copies; ends with a barrier
+  if (!mbar_wait_bounded(&bar, 0, R.status)) return;
+  const int cn = Pn / N, cm = Pm / N;
+  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  for (int it = threadIdx.x; it < nE_own * cn; it += blockDim.x) {
+    const int el = fast_div(it, mag_cn);
+    const int e = ea + el;
+    const int4 loc = __ldg(R.kh_edge_loc + e);
+    h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + (size_t)loc.y * Pn, s_er + (size_t)loc.x * Pn,
+               s_et + (size_t)loc.z * Pm, s_ht + (size_t)el * Pn, R.ht + (size_t)e * Pn);
+  }
+  for (int it = threadIdx.x; it < nF_own * cm; it += blockDim.x) {
+    const int fl = fast_div(it, mag_cm);
+    const int f = fa + fl;
+    const int4 l0 = __ldg(R.kh_face_loc + 2 * (size_t)f);
+    const int4 l1 = __ldg(R.kh_face_loc + 2 * (size_t)f + 1);
+    const real* jin[kMaxSpecies];
+    real* jout[kMaxSpecies];
+    for (int s = 0; s < kMaxSpecies; ++s) {
+      jin[s] = s < S ? s_J + ((size_t)s * nF_own + fl) * 3 * Pm : nullptr;
+      jout[s] = s < S ? R.J[s] + (size_t)f * 3 * Pm : nullptr;
     }
-    Run<real> out;
+    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, s_et + (size_t)l0.x * Pm, s_et + (size_t)l0.y * Pm,
+                             s_et + (size_t)l0.z * Pm, s_hr + (size_t)fl * Pm, R.hr + (size_t)f * Pm,
+                             s_er + (size_t)l0.w * Pn, s_er + (size_t)l1.x * Pn, s_er + (size_t)l1.y * Pn, jin, jout,
+                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr);
+  }
+}
+
+template <typename real, bool PLASMA, int MAXDEG>
+__global__ void __launch_bounds__(256) ke_staged(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
+                                                  int n_members, int istep) {
+  constexpr int N = Lanes<real>::N;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t bar;
+  int member, patch;
+  member_patch(block_map, n_members, member, patch);
+  load_rec(R, recs + member);
+  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
+  const int va = R.vptr[patch], vb = R.vptr[patch + 1];
+  const int ea = R.eptr_e[patch], eb = R.eptr_e[patch + 1];
+  const int nV_own = vb - va, nE_own = eb - ea;
+  const int h0 = R.keh_off[patch], nh = R.keh_off[patch + 1] - h0;
+  const int f0 = R.kef_off[patch], nf = R.kef_off[patch + 1] - f0;
+  const int j0 = PLASMA ? R.kej_off[patch] : 0, nj = PLASMA ? R.kej_off[patch + 1] - j0 : 0;
+  const real* Jsum = PLASMA ? jsum(R) : nullptr;
+  real* s_ht = staged_base(R, dyn_smem);
+  real* s_hr = s_ht + (size_t)nh * Pn;
+  real* s_J = s_hr + (size_t)nf * Pm;
+  real* s_er = s_J + (size_t)nj * 3 * Pm;
+  real* s_et = s_er + (size_t)nV_own * Pn;
+  const uint32_t bytes = (uint32_t)sizeof(real) * ((uint32_t)nh * Pn + (uint32_t)nf * Pm + (uint32_t)nj * 3 * Pm +
+                                                   (uint32_t)nV_own * Pn + (uint32_t)nE_own * Pm);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_expect_tx(&bar, bytes);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nh; i += blockDim.x)
+    bulk_load(s_ht + (size_t)i * Pn, R.ht + (size_t)__ldg(R.keh_rows + h0 + i) * Pn, Pn * sizeof(real), &bar);
+  for (int i = threadIdx.x; i < nf; i += blockDim.x)
+    bulk_load(s_hr + (size_t)i * Pm, R.hr + (size_t)__ldg(R.kef_rows + f0 + i) * Pm, Pm * sizeof(real), &bar);
+  for (int i = threadIdx.x; i < nj; i += blockDim.x)
+    bulk_load(s_J + (size_t)i * 3 * Pm, Jsum + (size_t)__ldg(R.kej_rows + j0 + i) * 3 * Pm, 3 * Pm * sizeof(real), &bar);
+  for (int i = threadIdx.x; i < nV_own; i += blockDim.x)
+    bulk_load(s_er + (size_t)i * Pn, R.er + (size_t)__ldg(R.vlist + va + i) * Pn, Pn * sizeof(real), &bar);
+  if (threadIdx.x == blockDim.x - 1 && nE_own)
+    bulk_load(s_et, R.et + (size_t)ea * Pm, (uint32_t)nE_own * Pm * sizeof(real), &bar);
+  Layers<real> Ls;
+  load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
+  if (!mbar_wait_bounded(&bar, 0, R.status)) return;
+  const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+  const int cn = Pn / N, cm = Pm / N;
+  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  for (int it = threadIdx.x; it < nV_own * cn; it += blockDim.x) {
+    const int vl = fast_div(it, mag_cn);
+    const int slot = va + vl;
+    const int v = __ldg(R.vlist + slot);
+    const real* hrows[MAXDEG];
+    const real* jrows[MAXDEG];
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int j = j0 + r;
-      const real hnext = (r + 1 < N) ? hv.x[r + 1] : htail;
-      real g = (a.x[r] - b.x[r]) * inv_p * Ls.invm[j];
-      const real d = full ? (Ls.rr[j + 1] * hnext - Ls.rr[j] * hv.x[r]) * Ls.invdr[j] * Ls.invm[j]
-                          : (hnext - hv.x[r]) * Ls.invdr[j];
-      g -= d;
-      const real ca = coef_full ? __ldg(R.ca_et + (size_t)e * Pm + j) : Ls.ca_et[j];
-      const real cb = coef_full ? __ldg(R.cb_et + (size_t)e * Pm + j) : Ls.cb_et[j];
-      real x = ca * ev.x[r] + cb * g;
-      if (e >= R.src_et_emin && e <= R.src_et_emax) {
-        for (int s = 0; s < R.n_src_et; ++s)
-          if (__ldg(R.src_et_e + s) == e && __ldg(R.src_et_j + s) == j) x -= __ldg(R.src_et_c + s) * current;
-      }
-      if (PLASMA) x -= cb * jt[r];
-      out.x[r] = (j < L) ? x : real(0);
+    for (int q = 0; q < MAXDEG; ++q) {
+      hrows[q] = s_ht + (size_t)__ldg(R.ke_slot_h + (size_t)slot * SW + q) * Pn;
+      jrows[q] = PLASMA ? s_J + (size_t)__ldg(R.ke_slot_j + (size_t)slot * SW + q) * 3 * Pm : nullptr;
     }
-    st16(etp, out);
+    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, slot, (it - vl * cn) * N, hrows, jrows, s_er + (size_t)vl * Pn,
+                                       R.er + (size_t)v * Pn, current);
+  }
+  for (int it = threadIdx.x; it < nE_own * cm; it += blockDim.x) {
+    const int el = fast_div(it, mag_cm);
+    const int e = ea + el;
+    const int4 loc = __ldg(R.ke_edge_loc + e);
+    const int jr = PLASMA ? __ldg(R.ke_edge_jr + e) : 0;
+    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, s_hr + (size_t)loc.y * Pm, s_hr + (size_t)loc.z * Pm,
+                             s_ht + (size_t)loc.x * Pn, PLASMA ? s_J + (size_t)loc.w * 3 * Pm : nullptr,
+                             PLASMA ? s_J + (size_t)jr * 3 * Pm : nullptr, s_et + (size_t)el * Pm, R.et + (size_t)e * Pm,
+                             current);
   }
 }
 

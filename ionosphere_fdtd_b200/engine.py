@@ -35,9 +35,15 @@ class Physics:
 
 @dataclass
 class Tuning:
+    """Launch geometry of a plan: faces per H-phase and E-phase CTA, threads per
+    CTA, steps per captured CUDA graph, and the gather mode (0 auto, 1 direct
+    global loads, 2 shared-memory staging with bulk copies)."""
+
     faces_per_patch: int = 32
     threads: int = 256
     graph_chunk: int = 32
+    e_faces_per_patch: int = 16
+    staging: int = 0
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -146,7 +152,8 @@ class Engine:
             pd.vertex_face_width = int(p["vertex_faces"].shape[1])
             pd.vertex_faces = i64(p["vertex_faces"])
             pd.vertex_face_weights = f64(p["vertex_face_weights"])
-        td = N.Tuning(self.tuning.faces_per_patch, self.tuning.threads, self.tuning.graph_chunk)
+        t = self.tuning
+        td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(
@@ -175,6 +182,20 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+    @property
+    def kernel_modes(self) -> tuple[str, str]:
+        """("direct" | "staged") for the H and E phases."""
+
+        h, e = C.c_int32(), C.c_int32()
+        N.check(N.load().ifdtd_plan_kernels(self.plan, C.byref(h), C.byref(e)), "ifdtd_plan_kernels")
+        name = {1: "direct", 2: "staged"}
+        return name[h.value], name[e.value]
+
+    def status_word(self, reset: bool = False) -> int:
+        out = C.c_int32()
+        N.check(N.load().ifdtd_status_word(self.plan, 1 if reset else 0, C.byref(out)), "ifdtd_status_word")
+        return int(out.value)
 
     @property
     def plan_bytes(self) -> int:

@@ -119,3 +119,20 @@ def test_patch_size_does_not_change_results(fpp):
     other = run_product(case, "float64", tuning=Tuning(faces_per_patch=fpp, threads=128))
     for f in STATE:
         np.testing.assert_array_equal(ref[f], other[f])
+
+
+@pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "tangential_s1", "thin_shell_s1"])
+def test_staged_and_direct_gathers_agree_bitwise(name):
+    """Shared-memory staging (bulk copies) and direct global gathers run the
+    same per-run arithmetic: results must be identical bit for bit."""
+
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    direct = run_product(C.CASES[name], "float32", tuning=Tuning(staging=1))
+    staged = run_product(C.CASES[name], "float32", tuning=Tuning(staging=2, faces_per_patch=16, e_faces_per_patch=8))
+    assert direct["_sim"]._engine.kernel_modes == ("direct", "direct")
+    assert staged["_sim"]._engine.kernel_modes == ("staged", "staged")
+    for key in ("er", "et", "hr", "ht", "si_memory", "plasma_current_0", "traces"):
+        if key in direct:
+            np.testing.assert_array_equal(direct[key], staged[key], err_msg=key)
+    assert staged["_sim"]._engine.status_word() == 0
