@@ -85,7 +85,8 @@ struct ifdtd_plan {
   int device = 0;
   int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
   int n_patches = 0, n_patches_e = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
-  int h_mode = 1, e_mode = 1;  // 1 direct, 2 staged
+  int h_mode = 1, e_mode = 1;  // 1 direct, 2 bulk-copy pipeline, 3 cp.async pipeline
+  int kh_stage = 0, ke_stage = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
   int* d_status = nullptr;
   bool plasma = false;
@@ -149,7 +150,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int staging = tune ? tune->staging : 0;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
   if (threads % 32 || threads > 256) return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 <= 256");
-  if (staging < 0 || staging > 2) return fail(IFDTD_ERR_ARGUMENT, "staging must be 0 (auto), 1 (direct) or 2 (staged)");
+  if (staging < 0 || staging > 3)
+    return fail(IFDTD_ERR_ARGUMENT, "staging must be 0 (auto), 1 (direct), 2 (bulk-copy pipeline) or 3 (cp.async pipeline)");
   if ((int64_t)std::max(fpp, fpp_e) * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
   P->threads = threads;
   // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
@@ -597,12 +599,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   {
     // staged kernels: per-layer rows (rounded to 16 bytes) + the largest patch's rows
     const size_t layer_block = (size_t)((R.layer_reals + 3) / 4 * 4) * sizeof(real);
-    P->kh_smem = layer_block + kh_max * sizeof(real);
-    P->ke_smem = layer_block + ke_max * sizeof(real);
+    P->kh_stage = (int)((kh_max + 3) / 4 * 4);
+    P->ke_stage = (int)((ke_max + 3) / 4 * 4);
+    P->kh_smem = layer_block + 2 * (size_t)P->kh_stage * sizeof(real);
+    P->ke_smem = layer_block + 2 * (size_t)P->ke_stage * sizeof(real);
     const size_t auto_limit = 113 * 1024, hard_limit = 220 * 1024;
     auto pick = [&](size_t need) {
       if (staging == 1) return 1;
-      if (staging == 2) return need <= hard_limit ? 2 : 0;
+      if (staging >= 2) return need <= hard_limit ? staging : 0;
       return need <= auto_limit ? 2 : 1;
     };
     P->h_mode = pick(P->kh_smem);
@@ -664,35 +668,47 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Persistent grid: SM count x resident CTAs (from the occupancy calculator).
+template <typename K>
+cudaError_t persistent_grid(ifdtd_plan* P, K kernel, size_t smem, int n_patches, int* grid) {
+  if (*grid > 0) return cudaSuccess;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, P->threads, smem);
+  if (e != cudaSuccess) return e;
+  *grid = std::max(1, std::min(n_patches, P->sm_count * std::max(per_sm, 1)));
+  return cudaSuccess;
+}
+
 template <typename real, bool PL>
-cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, cudaStream_t st) {
-  if (P->h_mode == 2) {
-    auto k = kh_staged<real, PL>;
+cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
+  if (P->h_mode >= 2) {
+    auto k = P->h_mode == 2 ? kh_pipe<real, PL, 0> : kh_pipe<real, PL, 1>;
     cudaError_t e = allow_smem(k, P->kh_smem);
+    if (e == cudaSuccess) e = persistent_grid(P, k, P->kh_smem, P->n_patches, &P->kh_grid);
     if (e != cudaSuccess) return e;
-    k<<<blocks, P->threads, P->kh_smem, st>>>(rec, map, members);
+    k<<<P->kh_grid, P->threads, P->kh_smem, st>>>(rec, P->kh_stage);
   } else {
     auto k = kh_kernel<real, PL>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
     if (e != cudaSuccess) return e;
-    k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members);
+    k<<<P->n_patches, P->threads, P->smem_bytes, st>>>(rec, nullptr, 1);
   }
   return cudaGetLastError();
 }
 
 template <typename real, bool PL, int MD>
-cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, int members, int blocks, int istep,
-                        cudaStream_t st) {
-  if (P->e_mode == 2) {
-    auto k = ke_staged<real, PL, MD>;
+cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, int istep, cudaStream_t st) {
+  if (P->e_mode >= 2) {
+    auto k = P->e_mode == 2 ? ke_pipe<real, PL, MD, 0> : ke_pipe<real, PL, MD, 1>;
     cudaError_t e = allow_smem(k, P->ke_smem);
+    if (e == cudaSuccess) e = persistent_grid(P, k, P->ke_smem, P->n_patches_e, &P->ke_grid);
     if (e != cudaSuccess) return e;
-    k<<<blocks, P->threads, P->ke_smem, st>>>(rec, map, members, istep);
+    k<<<P->ke_grid, P->threads, P->ke_smem, st>>>(rec, P->ke_stage, istep);
   } else {
     auto k = ke_kernel<real, PL, MD>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
     if (e != cudaSuccess) return e;
-    k<<<blocks, P->threads, P->smem_bytes, st>>>(rec, map, members, istep);
+    k<<<P->n_patches_e, P->threads, P->smem_bytes, st>>>(rec, nullptr, 1, istep);
   }
   return cudaGetLastError();
 }
@@ -700,19 +716,15 @@ cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, const int2* map, in
 template <typename real>
 cudaError_t launch_kh(ifdtd_plan* P, cudaStream_t st) {
   const Rec<real>* rec = (const Rec<real>*)P->d_rec;
-  return P->plasma ? launch_kh_t<real, true>(P, rec, nullptr, 1, P->n_patches, st)
-                   : launch_kh_t<real, false>(P, rec, nullptr, 1, P->n_patches, st);
+  return P->plasma ? launch_kh_t<real, true>(P, rec, st) : launch_kh_t<real, false>(P, rec, st);
 }
 
 template <typename real>
 cudaError_t launch_ke(ifdtd_plan* P, int istep, cudaStream_t st) {
   const Rec<real>* rec = (const Rec<real>*)P->d_rec;
-  const int nb = P->n_patches_e;
   if (P->maxdeg == 6)
-    return P->plasma ? launch_ke_t<real, true, 6>(P, rec, nullptr, 1, nb, istep, st)
-                     : launch_ke_t<real, false, 6>(P, rec, nullptr, 1, nb, istep, st);
-  return P->plasma ? launch_ke_t<real, true, 12>(P, rec, nullptr, 1, nb, istep, st)
-                   : launch_ke_t<real, false, 12>(P, rec, nullptr, 1, nb, istep, st);
+    return P->plasma ? launch_ke_t<real, true, 6>(P, rec, istep, st) : launch_ke_t<real, false, 6>(P, rec, istep, st);
+  return P->plasma ? launch_ke_t<real, true, 12>(P, rec, istep, st) : launch_ke_t<real, false, 12>(P, rec, istep, st);
 }
 
 template <typename real>
@@ -826,6 +838,7 @@ int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* gr
   ifdtd_plan* P = new ifdtd_plan();
   P->dtype = dtype_bytes;
   P->device = device;
+  P->sm_count = prop.multiProcessorCount;
   const int rc = dtype_bytes == 4 ? build_plan<float>(P, mesh, grid, physics, tuning)
                                   : build_plan<double>(P, mesh, grid, physics, tuning);
   if (rc != IFDTD_OK) {

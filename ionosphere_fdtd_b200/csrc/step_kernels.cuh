@@ -695,72 +695,114 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
 }
 
 // ---------------------------------------------------------------------------
-// Staged kernels: each CTA bulk-copies every row its patch reads (gathered
-// neighbour columns and its own contiguous ranges) into shared memory with
-// cp.async.bulk on one mbarrier, then computes from shared memory.  The copy
-// engine, not registers, holds the bytes in flight.
+// Pipelined staged kernels.  A persistent CTA walks patches p = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; every row a patch reads (gathered neighbour
+// columns and its own contiguous ranges) is copied into one of two shared-
+// memory stages while the CTA computes the previous patch from the other
+// stage, so the copies of the next patch are always in flight.  COPY selects
+// the copy engine: 0 = TMA bulk copies (cp.async.bulk) completing on a per-stage
+// mbarrier, 1 = per-thread 16-byte asynchronous copies (cp.async) completing in
+// commit groups.  Sources are this GPU's memory only; nothing is multicast.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Copies `rows` rows of `len` reals each from global rows src(i) to contiguous
+// shared rows of the same length.  COPY 0: one bulk copy per row from warp 0
+// (lane-strided); COPY 1: 16-byte pieces strided over the whole CTA.
+template <int COPY, typename real, typename SrcRow>
+__device__ __forceinline__ void stage_rows(real* dst, int rows, int len, SrcRow src, uint64_t* bar) {
+  constexpr int V = 16 / sizeof(real);
+  if (rows <= 0 || len <= 0) return;
+  if (COPY == 0) {
+    if (threadIdx.x < 32)
+      for (int i = threadIdx.x; i < rows; i += 32) bulk_load(dst + (size_t)i * len, src(i), len * sizeof(real), bar);
+  } else {
+    const int per = len / V;
+    for (int t = threadIdx.x; t < rows * per; t += blockDim.x) {
+      const int i = t / per, c = t - i * per;
+      cp16_async(dst + (size_t)i * len + c * V, src(i) + c * V);
+    }
+  }
+}
+
 template <typename real, bool PLASMA>
-__global__ void __launch_bounds__(256) kh_staged(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
-                                                  int n_members) {
+struct KhPatch {
+  int ea, eb, fa, fb, v0, nv, e0, ne;
+  __device__ __forceinline__ void init(const Rec<real>& R, int p) {
+    ea = R.eptr_h[p];
+    eb = R.eptr_h[p + 1];
+    fa = p * R.fpp_h;
+    fb = min(fa + R.fpp_h, R.nF);
+    v0 = R.khv_off[p];
+    nv = R.khv_off[p + 1] - v0;
+    e0 = R.khe_off[p];
+    ne = R.khe_off[p + 1] - e0;
+  }
+  __device__ __forceinline__ uint32_t reals(const Rec<real>& R) const {
+    const int S = PLASMA ? R.n_species : 0;
+    return (uint32_t)nv * R.Pn + (uint32_t)ne * R.Pm + (uint32_t)(eb - ea) * R.Pn + (uint32_t)(fb - fa) * R.Pm +
+           (uint32_t)S * (fb - fa) * 3 * R.Pm;
+  }
+};
+
+template <int COPY, typename real, bool PLASMA>
+__device__ __forceinline__ void kh_issue(const Rec<real>& R, int p, real* st, uint64_t* bar) {
+  KhPatch<real, PLASMA> P;
+  P.init(R, p);
+  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0, nEo = P.eb - P.ea, nFo = P.fb - P.fa;
+  if (COPY == 0 && threadIdx.x == 0) mbar_expect_tx(bar, P.reals(R) * sizeof(real));
+  if (COPY == 0) __syncwarp();
+  real* s_er = st;
+  real* s_et = s_er + (size_t)P.nv * Pn;
+  real* s_ht = s_et + (size_t)P.ne * Pm;
+  real* s_hr = s_ht + (size_t)nEo * Pn;
+  real* s_J = s_hr + (size_t)nFo * Pm;
+  stage_rows<COPY>(s_er, P.nv, Pn, [&](int i) { return R.er + (size_t)__ldg(R.khv_rows + P.v0 + i) * Pn; }, bar);
+  stage_rows<COPY>(s_et, P.ne, Pm, [&](int i) { return R.et + (size_t)__ldg(R.khe_rows + P.e0 + i) * Pm; }, bar);
+  stage_rows<COPY>(s_ht, 1, nEo * Pn, [&](int) { return R.ht + (size_t)P.ea * Pn; }, bar);
+  stage_rows<COPY>(s_hr, 1, nFo * Pm, [&](int) { return R.hr + (size_t)P.fa * Pm; }, bar);
+  for (int s = 0; s < S; ++s)
+    stage_rows<COPY>(s_J + (size_t)s * nFo * 3 * Pm, 1, nFo * 3 * Pm,
+                     [&](int) { return (const real*)R.J[s] + (size_t)P.fa * 3 * Pm; }, bar);
+}
+
+template <typename real, bool PLASMA>
+__device__ __forceinline__ void kh_compute(const Rec<real>& R, const Layers<real>& Ls, int p, const real* st) {
   constexpr int N = Lanes<real>::N;
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t bar;
-  int member, patch;
-  member_patch(block_map, n_members, member, patch);
-  load_rec(R, recs + member);
-  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0;
-  const int ea = R.eptr_h[patch], eb = R.eptr_h[patch + 1];
-  const int fa = patch * R.fpp_h, fb = min(fa + R.fpp_h, R.nF);
-  const int nE_own = eb - ea, nF_own = fb - fa;
-  const int v0 = R.khv_off[patch], nv = R.khv_off[patch + 1] - v0;
-  const int e0 = R.khe_off[patch], ne = R.khe_off[patch + 1] - e0;
-  real* s_er = staged_base(R, dyn_smem);
-  real* s_et = s_er + (size_t)nv * Pn;
-  real* s_ht = s_et + (size_t)ne * Pm;
-  real* s_hr = s_ht + (size_t)nE_own * Pn;
-  real* s_J = s_hr + (size_t)nF_own * Pm;
-  const uint32_t bytes =
-      (uint32_t)sizeof(real) * ((uint32_t)nv * Pn + (uint32_t)ne * Pm + (uint32_t)nE_own * Pn + (uint32_t)nF_own * Pm +
-                                (uint32_t)S * nF_own * 3 * Pm);
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    mbar_expect_tx(&bar, bytes);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nv; i += blockDim.x)
-    bulk_load(s_er + (size_t)i * Pn, R.er + (size_t)__ldg(R.khv_rows + v0 + i) * Pn, Pn * sizeof(real), &bar);
-  for (int i = threadIdx.x; i < ne; i += blockDim.x)
-    bulk_load(s_et + (size_t)i * Pm, R.et + (size_t)__ldg(R.khe_rows + e0 + i) * Pm, Pm * sizeof(real), &bar);
-  if (threadIdx.x == blockDim.x - 1) {
-    if (nE_own) bulk_load(s_ht, R.ht + (size_t)ea * Pn, (uint32_t)nE_own * Pn * sizeof(real), &bar);
-    if (nF_own) bulk_load(s_hr, R.hr + (size_t)fa * Pm, (uint32_t)nF_own * Pm * sizeof(real), &bar);
-    for (int s = 0; s < S; ++s)
-      bulk_load(s_J + (size_t)s * nF_own * 3 * Pm, R.J[s] + (size_t)fa * 3 * Pm, (uint32_t)nF_own * 3 * Pm * sizeof(real),
-                &bar);
-  }
-  Layers<real> Ls;
-  load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);  // overlaps the copies; ends with a barrier
-  if (!mbar_wait_bounded(&bar, 0, R.status)) return;
+  KhPatch<real, PLASMA> P;
+  P.init(R, p);
+  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0, nEo = P.eb - P.ea, nFo = P.fb - P.fa;
+  const real* s_er = st;
+  const real* s_et = s_er + (size_t)P.nv * Pn;
+  const real* s_ht = s_et + (size_t)P.ne * Pm;
+  const real* s_hr = s_ht + (size_t)nEo * Pn;
+  const real* s_J = s_hr + (size_t)nFo * Pm;
   const int cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  for (int it = threadIdx.x; it < nE_own * cn; it += blockDim.x) {
+  for (int it = threadIdx.x; it < nEo * cn; it += blockDim.x) {
     const int el = fast_div(it, mag_cn);
-    const int e = ea + el;
+    const int e = P.ea + el;
     const int4 loc = __ldg(R.kh_edge_loc + e);
     h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + (size_t)loc.y * Pn, s_er + (size_t)loc.x * Pn,
                s_et + (size_t)loc.z * Pm, s_ht + (size_t)el * Pn, R.ht + (size_t)e * Pn);
   }
-  for (int it = threadIdx.x; it < nF_own * cm; it += blockDim.x) {
+  for (int it = threadIdx.x; it < nFo * cm; it += blockDim.x) {
     const int fl = fast_div(it, mag_cm);
-    const int f = fa + fl;
+    const int f = P.fa + fl;
     const int4 l0 = __ldg(R.kh_face_loc + 2 * (size_t)f);
     const int4 l1 = __ldg(R.kh_face_loc + 2 * (size_t)f + 1);
     const real* jin[kMaxSpecies];
     real* jout[kMaxSpecies];
     for (int s = 0; s < kMaxSpecies; ++s) {
-      jin[s] = s < S ? s_J + ((size_t)s * nF_own + fl) * 3 * Pm : nullptr;
+      jin[s] = s < S ? s_J + ((size_t)s * nFo + fl) * 3 * Pm : nullptr;
       jout[s] = s < S ? R.J[s] + (size_t)f * 3 * Pm : nullptr;
     }
     h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, s_et + (size_t)l0.x * Pm, s_et + (size_t)l0.y * Pm,
@@ -770,55 +812,66 @@ __global__ void __launch_bounds__(256) kh_staged(const Rec<real>* __restrict__ r
   }
 }
 
-template <typename real, bool PLASMA, int MAXDEG>
-__global__ void __launch_bounds__(256) ke_staged(const Rec<real>* __restrict__ recs, const int2* __restrict__ block_map,
-                                                  int n_members, int istep) {
-  constexpr int N = Lanes<real>::N;
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t bar;
-  int member, patch;
-  member_patch(block_map, n_members, member, patch);
-  load_rec(R, recs + member);
-  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
-  const int va = R.vptr[patch], vb = R.vptr[patch + 1];
-  const int ea = R.eptr_e[patch], eb = R.eptr_e[patch + 1];
-  const int nV_own = vb - va, nE_own = eb - ea;
-  const int h0 = R.keh_off[patch], nh = R.keh_off[patch + 1] - h0;
-  const int f0 = R.kef_off[patch], nf = R.kef_off[patch + 1] - f0;
-  const int j0 = PLASMA ? R.kej_off[patch] : 0, nj = PLASMA ? R.kej_off[patch + 1] - j0 : 0;
-  const real* Jsum = PLASMA ? jsum(R) : nullptr;
-  real* s_ht = staged_base(R, dyn_smem);
-  real* s_hr = s_ht + (size_t)nh * Pn;
-  real* s_J = s_hr + (size_t)nf * Pm;
-  real* s_er = s_J + (size_t)nj * 3 * Pm;
-  real* s_et = s_er + (size_t)nV_own * Pn;
-  const uint32_t bytes = (uint32_t)sizeof(real) * ((uint32_t)nh * Pn + (uint32_t)nf * Pm + (uint32_t)nj * 3 * Pm +
-                                                   (uint32_t)nV_own * Pn + (uint32_t)nE_own * Pm);
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    mbar_expect_tx(&bar, bytes);
+template <typename real, bool PLASMA>
+struct KePatch {
+  int va, vb, ea, eb, h0, nh, f0, nf, j0, nj;
+  __device__ __forceinline__ void init(const Rec<real>& R, int p) {
+    va = R.vptr[p];
+    vb = R.vptr[p + 1];
+    ea = R.eptr_e[p];
+    eb = R.eptr_e[p + 1];
+    h0 = R.keh_off[p];
+    nh = R.keh_off[p + 1] - h0;
+    f0 = R.kef_off[p];
+    nf = R.kef_off[p + 1] - f0;
+    j0 = PLASMA ? R.kej_off[p] : 0;
+    nj = PLASMA ? R.kej_off[p + 1] - j0 : 0;
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nh; i += blockDim.x)
-    bulk_load(s_ht + (size_t)i * Pn, R.ht + (size_t)__ldg(R.keh_rows + h0 + i) * Pn, Pn * sizeof(real), &bar);
-  for (int i = threadIdx.x; i < nf; i += blockDim.x)
-    bulk_load(s_hr + (size_t)i * Pm, R.hr + (size_t)__ldg(R.kef_rows + f0 + i) * Pm, Pm * sizeof(real), &bar);
-  for (int i = threadIdx.x; i < nj; i += blockDim.x)
-    bulk_load(s_J + (size_t)i * 3 * Pm, Jsum + (size_t)__ldg(R.kej_rows + j0 + i) * 3 * Pm, 3 * Pm * sizeof(real), &bar);
-  for (int i = threadIdx.x; i < nV_own; i += blockDim.x)
-    bulk_load(s_er + (size_t)i * Pn, R.er + (size_t)__ldg(R.vlist + va + i) * Pn, Pn * sizeof(real), &bar);
-  if (threadIdx.x == blockDim.x - 1 && nE_own)
-    bulk_load(s_et, R.et + (size_t)ea * Pm, (uint32_t)nE_own * Pm * sizeof(real), &bar);
-  Layers<real> Ls;
-  load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-  if (!mbar_wait_bounded(&bar, 0, R.status)) return;
-  const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+  __device__ __forceinline__ uint32_t reals(const Rec<real>& R) const {
+    return (uint32_t)nh * R.Pn + (uint32_t)nf * R.Pm + (uint32_t)nj * 3 * R.Pm + (uint32_t)(vb - va) * R.Pn +
+           (uint32_t)(eb - ea) * R.Pm;
+  }
+};
+
+template <int COPY, typename real, bool PLASMA>
+__device__ __forceinline__ void ke_issue(const Rec<real>& R, int p, real* st, uint64_t* bar) {
+  KePatch<real, PLASMA> P;
+  P.init(R, p);
+  const int Pn = R.Pn, Pm = R.Pm;
+  const real* Jsum = PLASMA ? jsum(R) : nullptr;
+  if (COPY == 0 && threadIdx.x == 0) mbar_expect_tx(bar, P.reals(R) * sizeof(real));
+  if (COPY == 0) __syncwarp();
+  real* s_ht = st;
+  real* s_hr = s_ht + (size_t)P.nh * Pn;
+  real* s_J = s_hr + (size_t)P.nf * Pm;
+  real* s_er = s_J + (size_t)P.nj * 3 * Pm;
+  real* s_et = s_er + (size_t)(P.vb - P.va) * Pn;
+  stage_rows<COPY>(s_ht, P.nh, Pn, [&](int i) { return (const real*)R.ht + (size_t)__ldg(R.keh_rows + P.h0 + i) * Pn; }, bar);
+  stage_rows<COPY>(s_hr, P.nf, Pm, [&](int i) { return (const real*)R.hr + (size_t)__ldg(R.kef_rows + P.f0 + i) * Pm; }, bar);
+  if (PLASMA)
+    stage_rows<COPY>(s_J, P.nj, 3 * Pm, [&](int i) { return Jsum + (size_t)__ldg(R.kej_rows + P.j0 + i) * 3 * Pm; }, bar);
+  stage_rows<COPY>(s_er, P.vb - P.va, Pn, [&](int i) { return (const real*)R.er + (size_t)__ldg(R.vlist + P.va + i) * Pn; },
+                   bar);
+  stage_rows<COPY>(s_et, 1, (P.eb - P.ea) * Pm, [&](int) { return (const real*)R.et + (size_t)P.ea * Pm; }, bar);
+}
+
+template <typename real, bool PLASMA, int MAXDEG>
+__device__ __forceinline__ void ke_compute(const Rec<real>& R, const Layers<real>& Ls, int p, const real* st,
+                                           real current) {
+  constexpr int N = Lanes<real>::N;
+  KePatch<real, PLASMA> P;
+  P.init(R, p);
+  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
+  const real* s_ht = st;
+  const real* s_hr = s_ht + (size_t)P.nh * Pn;
+  const real* s_J = s_hr + (size_t)P.nf * Pm;
+  const real* s_er = s_J + (size_t)P.nj * 3 * Pm;
+  const real* s_et = s_er + (size_t)(P.vb - P.va) * Pn;
   const int cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  for (int it = threadIdx.x; it < nV_own * cn; it += blockDim.x) {
+  for (int it = threadIdx.x; it < (P.vb - P.va) * cn; it += blockDim.x) {
     const int vl = fast_div(it, mag_cn);
-    const int slot = va + vl;
+    const int slot = P.va + vl;
     const int v = __ldg(R.vlist + slot);
     const real* hrows[MAXDEG];
     const real* jrows[MAXDEG];
@@ -830,9 +883,9 @@ __global__ void __launch_bounds__(256) ke_staged(const Rec<real>* __restrict__ r
     e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, slot, (it - vl * cn) * N, hrows, jrows, s_er + (size_t)vl * Pn,
                                        R.er + (size_t)v * Pn, current);
   }
-  for (int it = threadIdx.x; it < nE_own * cm; it += blockDim.x) {
+  for (int it = threadIdx.x; it < (P.eb - P.ea) * cm; it += blockDim.x) {
     const int el = fast_div(it, mag_cm);
-    const int e = ea + el;
+    const int e = P.ea + el;
     const int4 loc = __ldg(R.ke_edge_loc + e);
     const int jr = PLASMA ? __ldg(R.ke_edge_jr + e) : 0;
     e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, s_hr + (size_t)loc.y * Pm, s_hr + (size_t)loc.z * Pm,
@@ -840,6 +893,89 @@ __global__ void __launch_bounds__(256) ke_staged(const Rec<real>* __restrict__ r
                              PLASMA ? s_J + (size_t)jr * 3 * Pm : nullptr, s_et + (size_t)el * Pm, R.et + (size_t)e * Pm,
                              current);
   }
+}
+
+// The persistent double-buffered loop shared by both phases.  stage_reals is
+// the largest patch's staged size (host-computed, a multiple of 4 reals).
+template <int COPY, typename real, typename Issue, typename Compute>
+__device__ __forceinline__ void pipeline(const Rec<real>& R, int n_patches, int stage_reals, real* stages,
+                                         uint64_t* bars, Issue issue, Compute compute) {
+  const int first = blockIdx.x, step = gridDim.x;
+  // prologue: patches first and first + step into stages 0 and 1
+  for (int s = 0; s < 2; ++s) {
+    const int p = first + s * step;
+    if (p < n_patches) issue(p, stages + (size_t)s * stage_reals, bars + s);
+    if (COPY == 1) cp_async_commit();
+  }
+  int i = 0;
+  for (int p = first; p < n_patches; p += step, ++i) {
+    const int s = i & 1;
+    real* st = stages + (size_t)s * stage_reals;
+    if (COPY == 0) {
+      if (!mbar_wait_bounded(bars + s, (uint32_t)((i >> 1) & 1), R.status)) return;
+    } else {
+      cp_async_wait<1>();
+      __syncthreads();
+    }
+    compute(p, st);
+    __syncthreads();  // the stage is free again
+    const int next = p + 2 * step;
+    if (next < n_patches) {
+      if (COPY == 0) fence_proxy_async();
+      issue(next, st, bars + s);
+    }
+    if (COPY == 1) cp_async_commit();
+  }
+  if (COPY == 1) cp_async_wait<0>();
+}
+
+template <typename real, bool PLASMA, int COPY>
+__global__ void __launch_bounds__(256) kh_pipe(const Rec<real>* __restrict__ recs, int stage_reals) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t bars[2];
+  load_rec(R, recs);
+  if (COPY == 0 && threadIdx.x == 0) {
+    mbar_init(bars, 1);
+    mbar_init(bars + 1, 1);
+  }
+  __syncthreads();
+  Layers<real> Ls;
+  Ls.invr = nullptr;
+  real* stages = staged_base(R, dyn_smem);
+  const int n = R.n_patches_h;
+  // issue the prologue copies before staging the per-layer rows so they overlap
+  pipeline<COPY>(
+      R, n, stage_reals, stages, bars,
+      [&](int p, real* st, uint64_t* bar) { kh_issue<COPY, real, PLASMA>(R, p, st, bar); },
+      [&](int p, const real* st) {
+        if (Ls.invr == nullptr) load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
+        kh_compute<real, PLASMA>(R, Ls, p, st);
+      });
+}
+
+template <typename real, bool PLASMA, int MAXDEG, int COPY>
+__global__ void __launch_bounds__(256) ke_pipe(const Rec<real>* __restrict__ recs, int stage_reals, int istep) {
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t bars[2];
+  load_rec(R, recs);
+  if (COPY == 0 && threadIdx.x == 0) {
+    mbar_init(bars, 1);
+    mbar_init(bars + 1, 1);
+  }
+  __syncthreads();
+  Layers<real> Ls;
+  Ls.invr = nullptr;
+  real* stages = staged_base(R, dyn_smem);
+  const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+  pipeline<COPY>(
+      R, R.n_patches_e, stage_reals, stages, bars,
+      [&](int p, real* st, uint64_t* bar) { ke_issue<COPY, real, PLASMA>(R, p, st, bar); },
+      [&](int p, const real* st) {
+        if (Ls.invr == nullptr) load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
+        ke_compute<real, PLASMA, MAXDEG>(R, Ls, p, st, current);
+      });
 }
 
 // ---------------------------------------------------------------------------

@@ -35,9 +35,10 @@ class Physics:
 
 @dataclass
 class Tuning:
-    """Launch geometry of a plan: faces per H-phase and E-phase CTA, threads per
-    CTA, steps per captured CUDA graph, and the gather mode (0 auto, 1 direct
-    global loads, 2 shared-memory staging with bulk copies)."""
+    """Launch geometry of a plan: faces per H-phase and E-phase patch, threads
+    per CTA, steps per captured CUDA graph, and the gather mode (0 auto,
+    1 direct global loads, 2 shared-memory pipeline fed by TMA bulk copies,
+    3 shared-memory pipeline fed by 16-byte cp.async copies)."""
 
     faces_per_patch: int = 32
     threads: int = 256
@@ -185,11 +186,12 @@ class Engine:
 
     @property
     def kernel_modes(self) -> tuple[str, str]:
-        """("direct" | "staged") for the H and E phases."""
+        """Gather mode of the H and E phases: "direct", "bulk" (TMA bulk-copy
+        pipeline) or "cp.async" (16-byte asynchronous-copy pipeline)."""
 
         h, e = C.c_int32(), C.c_int32()
         N.check(N.load().ifdtd_plan_kernels(self.plan, C.byref(h), C.byref(e)), "ifdtd_plan_kernels")
-        name = {1: "direct", 2: "staged"}
+        name = {1: "direct", 2: "bulk", 3: "cp.async"}
         return name[h.value], name[e.value]
 
     def status_word(self, reset: bool = False) -> int:
