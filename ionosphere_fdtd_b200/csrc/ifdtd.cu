@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/ifdtd.h"
+#include "pipe_kernels.cuh"
 #include "step_kernels.cuh"
 
 using namespace ifdtd;
@@ -85,8 +86,10 @@ struct ifdtd_plan {
   int device = 0;
   int nV = 0, nE = 0, nF = 0, L = 0, T = 0, S = 0;
   int n_patches = 0, n_patches_e = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
-  int h_mode = 1, e_mode = 1;  // 1 direct, 2 bulk-copy pipeline, 3 cp.async pipeline
-  int kh_stage = 0, ke_stage = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
+  int h_mode = 1, e_mode = 1;  // 1 direct gathers, 2 pipeline
+  int pipe_copy = 0;           // pipeline copy engine: 0 TMA bulk copies, 1 cp.async
+  bool pipe_h_ok = false, pipe_e_ok = false;
+  int kh_stage = 0, ke_stage = 0, kh_stages = 0, ke_stages = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
   int* d_status = nullptr;
   bool plasma = false;
@@ -131,6 +134,265 @@ bool in_range(const int64_t* p, size_t n, int64_t hi) {
 
 int round4(int n) { return (n + 3) / 4 * 4; }
 
+// ---------------------------------------------------------------------------
+// Pipelined kernels: per patch, the rows it reads as copy descriptors (runs of
+// consecutive rows of one source array) and a table blob whose local indices
+// address the rows inside the patch's shared-memory stage.  Stage layout:
+// [blob][gathered rows ...][own contiguous rows ...], every part 16-byte
+// aligned (rows are padded to 16-byte pitches).
+// ---------------------------------------------------------------------------
+constexpr int kSmemPerBlock = 232448;  // opt-in dynamic shared memory per CTA on sm_100
+
+struct PipeTables {
+  std::vector<int> dptr{0};
+  std::vector<int4> desc;
+  std::vector<unsigned char> tab;
+  int stage_bytes = 0;
+};
+
+// Sorted unique ids -> runs of consecutive rows, bridging gaps of at most
+// `gap` rows; loc[id] = the id's position among the staged rows.  Returns the
+// number of staged rows.
+int make_runs(const std::vector<int>& ids, int gap, std::vector<std::pair<int, int>>& runs, std::vector<int>& loc) {
+  runs.clear();
+  int before = 0;
+  for (const int id : ids) {
+    if (!runs.empty() && id - (runs.back().first + runs.back().second) <= gap) {
+      runs.back().second = id - runs.back().first + 1;
+    } else {
+      if (!runs.empty()) before += runs.back().second;
+      runs.push_back({id, 1});
+    }
+    loc[id] = before + (id - runs.back().first);
+  }
+  return runs.empty() ? 0 : before + runs.back().second;
+}
+
+void sort_unique(std::vector<int>& v) {
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+}
+
+// Append bytes to the blob (16-byte padded); returns the offset from `base`.
+int blob_put(std::vector<unsigned char>& tab, size_t base, const void* src, size_t bytes) {
+  const int off = (int)(tab.size() - base);
+  const unsigned char* p = static_cast<const unsigned char*>(src);
+  tab.insert(tab.end(), p, p + bytes);
+  tab.resize((tab.size() + 15) / 16 * 16, 0);
+  return off;
+}
+
+void add_runs(std::vector<int4>& desc, int src, const std::vector<std::pair<int, int>>& runs, int dst, int row_bytes) {
+  int pos = 0;
+  for (const auto& r : runs) {
+    desc.push_back(make_int4(src, r.first, dst + pos * row_bytes, r.second * row_bytes));
+    pos += r.second;
+  }
+}
+
+int round128(int n) { return (n + 127) / 128 * 128; }
+
+// H phase (patch = faces [q*fpp, ...) and edges eptr[q]..eptr[q+1]).  Stage:
+// blob, er rows (edge ends and, with plasma, face vertices), et rows (face
+// edges, which include the owned edges), own ht rows, own hr rows, own
+// current rows per species.
+template <typename real>
+bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>& eptr, const std::vector<int2>& th,
+                  const std::vector<int4>& fe, const std::vector<int4>& fv, const std::vector<real>& inv_theta,
+                  const std::vector<real>& fw, const std::vector<real>& pl, int S, int Pn, int Pm,
+                  std::vector<int>& locA, std::vector<int>& locB) {
+  using namespace pipe;
+  const int rb = (int)sizeof(real);
+  std::vector<int> er_ids, et_ids;
+  std::vector<std::pair<int, int>> er_runs, et_runs;
+  std::vector<int4> eloc, floc;
+  for (int q = 0; q < n; ++q) {
+    const int fa = q * fpp, fb = std::min(fa + fpp, nF), ea = eptr[q], eb = eptr[q + 1], ne = eb - ea, nf = fb - fa;
+    er_ids.clear();
+    et_ids.clear();
+    for (int e = ea; e < eb; ++e) {
+      er_ids.push_back(th[e].x);
+      er_ids.push_back(th[e].y);
+    }
+    for (int f = fa; f < fb; ++f) {
+      et_ids.push_back(fe[f].x);
+      et_ids.push_back(fe[f].y);
+      et_ids.push_back(fe[f].z);
+      if (S > 0) {
+        er_ids.push_back(fv[f].x);
+        er_ids.push_back(fv[f].y);
+        er_ids.push_back(fv[f].z);
+      }
+    }
+    sort_unique(er_ids);
+    sort_unique(et_ids);
+    for (int e = ea; e < eb; ++e)
+      if (!std::binary_search(et_ids.begin(), et_ids.end(), e)) return false;
+    int gap = 0, n_er = 0, n_et = 0, nd = 0;
+    for (;;) {
+      n_er = make_runs(er_ids, gap, er_runs, locA);
+      n_et = make_runs(et_ids, gap, et_runs, locB);
+      nd = 1 + (int)er_runs.size() + (int)et_runs.size() + (ne > 0) + (nf > 0 ? 1 + S : 0);
+      if (nd <= kMaxDesc || gap >= 64) break;
+      gap = 2 * gap + 1;
+    }
+    if (nd > kMaxDesc) return false;
+    const size_t base = T.tab.size();
+    int head[kh_head_ints] = {0};
+    T.tab.resize(base + sizeof(head), 0);
+    eloc.resize(ne);
+    for (int el = 0; el < ne; ++el) {
+      const int e = ea + el;
+      eloc[el] = make_int4(locA[th[e].x], locA[th[e].y], locB[e], 0);
+    }
+    floc.resize(2 * (size_t)nf);
+    for (int fl = 0; fl < nf; ++fl) {
+      const int f = fa + fl;
+      floc[2 * fl] = make_int4(locB[fe[f].x], locB[fe[f].y], locB[fe[f].z], S > 0 ? locA[fv[f].x] : 0);
+      floc[2 * fl + 1] = make_int4(S > 0 ? locA[fv[f].y] : 0, S > 0 ? locA[fv[f].z] : 0, 0, 0);
+    }
+    head[kh_o_eloc] = blob_put(T.tab, base, eloc.data(), ne * sizeof(int4));
+    head[kh_o_einv] = blob_put(T.tab, base, inv_theta.data() + ea, ne * (size_t)rb);
+    head[kh_o_floc] = blob_put(T.tab, base, floc.data(), floc.size() * sizeof(int4));
+    head[kh_o_fw] = blob_put(T.tab, base, fw.data() + 4 * (size_t)fa, 4 * (size_t)nf * rb);
+    head[kh_o_fpl] = S > 0 ? blob_put(T.tab, base, pl.data() + 12 * (size_t)fa, 12 * (size_t)nf * rb) : head[kh_o_fw];
+    const int B = (int)(T.tab.size() - base);
+    head[kh_ea] = ea;
+    head[kh_ne] = ne;
+    head[kh_fa] = fa;
+    head[kh_nf] = nf;
+    head[kh_o_er] = B;
+    head[kh_o_et] = head[kh_o_er] + n_er * Pn * rb;
+    head[kh_o_ht] = head[kh_o_et] + n_et * Pm * rb;
+    head[kh_o_hr] = head[kh_o_ht] + ne * Pn * rb;
+    head[kh_o_J] = head[kh_o_hr] + nf * Pm * rb;
+    const int end = head[kh_o_J] + S * nf * 3 * Pm * rb;
+    std::memcpy(T.tab.data() + base, head, sizeof(head));
+    T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
+    add_runs(T.desc, kSrcEr, er_runs, head[kh_o_er], Pn * rb);
+    add_runs(T.desc, kSrcEt, et_runs, head[kh_o_et], Pm * rb);
+    if (ne > 0) T.desc.push_back(make_int4(kSrcHt, ea, head[kh_o_ht], ne * Pn * rb));
+    if (nf > 0) {
+      T.desc.push_back(make_int4(kSrcHr, fa, head[kh_o_hr], nf * Pm * rb));
+      for (int s = 0; s < S; ++s)
+        T.desc.push_back(make_int4(kSrcJ0 + s, fa, head[kh_o_J] + s * nf * 3 * Pm * rb, nf * 3 * Pm * rb));
+    }
+    T.dptr.push_back((int)T.desc.size());
+    T.stage_bytes = std::max(T.stage_bytes, round128(end));
+    if (T.tab.size() / 16 >= (size_t)1 << 31) return false;
+  }
+  return true;
+}
+
+// E phase (patch = vertices vlist[vptr[q]..vptr[q+1]) and edges eptr[q]..).
+// Stage: blob, ht rows (slot edges and owned edges), hr rows and summed
+// current rows of one face set (faces beside owned edges and, with plasma,
+// slot faces), own er rows (vertices in increasing order), own et rows.
+template <typename real>
+bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std::vector<int>& vlist,
+                  const std::vector<int>& eptr, const std::vector<int2>& lr, int SW, const std::vector<int>& ps_edge,
+                  const std::vector<int>& ps_face, const std::vector<real>& ps_coef, const std::vector<real>& ps_wc,
+                  const std::vector<real>& inv_phi, const std::vector<real>& tn, bool plasma, int Pn, int Pm,
+                  std::vector<int>& locA, std::vector<int>& locB) {
+  using namespace pipe;
+  const int rb = (int)sizeof(real);
+  std::vector<int> h_ids, f_ids, v_ids, vloc;
+  std::vector<std::pair<int, int>> h_runs, f_runs, v_runs;
+  std::vector<std::pair<int, int>> own;  // (vertex, slot)
+  std::vector<int> vid, vh, vj;
+  std::vector<real> vcoef, vwc;
+  std::vector<int4> eloc;
+  vloc.assign(vlist.size(), 0);
+  for (int q = 0; q < n; ++q) {
+    const int va = vptr[q], vb = vptr[q + 1], ea = eptr[q], eb = eptr[q + 1], nv = vb - va, ne = eb - ea;
+    own.clear();
+    for (int sl = va; sl < vb; ++sl) own.push_back({vlist[sl], sl});
+    std::sort(own.begin(), own.end());
+    h_ids.clear();
+    f_ids.clear();
+    v_ids.clear();
+    for (const auto& o : own) {
+      v_ids.push_back(o.first);
+      for (int k = 0; k < SW; ++k) {
+        h_ids.push_back(ps_edge[(size_t)o.second * SW + k]);
+        if (plasma) f_ids.push_back(ps_face[(size_t)o.second * SW + k]);
+      }
+    }
+    for (int e = ea; e < eb; ++e) {
+      h_ids.push_back(e);
+      f_ids.push_back(lr[e].x);
+      f_ids.push_back(lr[e].y);
+    }
+    sort_unique(h_ids);
+    sort_unique(f_ids);
+    make_runs(v_ids, 0, v_runs, vloc);
+    int gap = 0, n_h = 0, n_f = 0, nd = 0;
+    for (;;) {
+      n_h = make_runs(h_ids, gap, h_runs, locA);
+      n_f = make_runs(f_ids, gap, f_runs, locB);
+      nd = 1 + (int)h_runs.size() + (int)f_runs.size() * (plasma ? 2 : 1) + (int)v_runs.size() + (ne > 0);
+      if (nd <= kMaxDesc || gap >= 64) break;
+      gap = 2 * gap + 1;
+    }
+    if (nd > kMaxDesc) return false;
+    const size_t base = T.tab.size();
+    int head[ke_head_ints] = {0};
+    T.tab.resize(base + sizeof(head), 0);
+    vid.assign(nv, 0);
+    vh.assign((size_t)nv * SW, 0);
+    vj.assign((size_t)nv * SW, 0);
+    vcoef.assign((size_t)nv * SW, real(0));
+    vwc.assign(plasma ? (size_t)nv * SW * 4 : 0, real(0));
+    for (int vl = 0; vl < nv; ++vl) {
+      const int sl = own[vl].second;
+      vid[vl] = own[vl].first;
+      for (int k = 0; k < SW; ++k) {
+        const size_t i = (size_t)sl * SW + k, o = (size_t)vl * SW + k;
+        vh[o] = locA[ps_edge[i]];
+        vcoef[o] = ps_coef[i];
+        if (plasma) {
+          vj[o] = locB[ps_face[i]];
+          for (int c = 0; c < 4; ++c) vwc[o * 4 + c] = ps_wc[i * 4 + c];
+        }
+      }
+    }
+    eloc.resize(ne);
+    for (int el = 0; el < ne; ++el) {
+      const int e = ea + el;
+      eloc[el] = make_int4(locA[e], locB[lr[e].x], locB[lr[e].y], 0);
+    }
+    head[ke_o_vid] = blob_put(T.tab, base, vid.data(), nv * sizeof(int));
+    head[ke_o_vh] = blob_put(T.tab, base, vh.data(), vh.size() * sizeof(int));
+    head[ke_o_vj] = plasma ? blob_put(T.tab, base, vj.data(), vj.size() * sizeof(int)) : head[ke_o_vh];
+    head[ke_o_vcoef] = blob_put(T.tab, base, vcoef.data(), vcoef.size() * (size_t)rb);
+    head[ke_o_vwc] = plasma ? blob_put(T.tab, base, vwc.data(), vwc.size() * (size_t)rb) : head[ke_o_vcoef];
+    head[ke_o_eloc] = blob_put(T.tab, base, eloc.data(), ne * sizeof(int4));
+    head[ke_o_einv] = blob_put(T.tab, base, inv_phi.data() + ea, ne * (size_t)rb);
+    head[ke_o_etan] = plasma ? blob_put(T.tab, base, tn.data() + 8 * (size_t)ea, 8 * (size_t)ne * rb) : head[ke_o_einv];
+    const int B = (int)(T.tab.size() - base);
+    head[ke_nv] = nv;
+    head[ke_ea] = ea;
+    head[ke_ne] = ne;
+    head[ke_o_ht] = B;
+    head[ke_o_hr] = head[ke_o_ht] + n_h * Pn * rb;
+    head[ke_o_J] = head[ke_o_hr] + n_f * Pm * rb;
+    head[ke_o_er] = head[ke_o_J] + (plasma ? n_f * 3 * Pm * rb : 0);
+    head[ke_o_et] = head[ke_o_er] + nv * Pn * rb;
+    const int end = head[ke_o_et] + ne * Pm * rb;
+    std::memcpy(T.tab.data() + base, head, sizeof(head));
+    T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
+    add_runs(T.desc, kSrcHt, h_runs, head[ke_o_ht], Pn * rb);
+    add_runs(T.desc, kSrcHr, f_runs, head[ke_o_hr], Pm * rb);
+    if (plasma) add_runs(T.desc, kSrcJsum, f_runs, head[ke_o_J], 3 * Pm * rb);
+    add_runs(T.desc, kSrcEr, v_runs, head[ke_o_er], Pn * rb);
+    if (ne > 0) T.desc.push_back(make_int4(kSrcEt, ea, head[ke_o_et], ne * Pm * rb));
+    T.dptr.push_back((int)T.desc.size());
+    T.stage_bytes = std::max(T.stage_bytes, round128(end));
+    if (T.tab.size() / 16 >= (size_t)1 << 31) return false;
+  }
+  return true;
+}
+
 template <typename real>
 int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G, const ifdtd_physics_desc* X,
                const ifdtd_tuning* tune) {
@@ -149,9 +411,12 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int fpp_e = (tune && tune->e_faces_per_patch > 0) ? tune->e_faces_per_patch : 16;
   const int staging = tune ? tune->staging : 0;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
-  if (threads % 32 || threads > 256) return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 <= 256");
+  if (threads % 32 || threads < 32 || threads > pipe::kMaxThreads - 32)
+    return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 in [32, 352]");
   if (staging < 0 || staging > 3)
-    return fail(IFDTD_ERR_ARGUMENT, "staging must be 0 (auto), 1 (direct), 2 (bulk-copy pipeline) or 3 (cp.async pipeline)");
+    return fail(IFDTD_ERR_ARGUMENT,
+                "staging must be 0 (auto), 1 (direct gathers), 2 (pipeline, TMA bulk copies) or 3 (pipeline, cp.async)");
+  P->pipe_copy = staging == 3 ? 1 : 0;
   if ((int64_t)std::max(fpp, fpp_e) * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
   P->threads = threads;
   // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
@@ -288,97 +553,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     }
   }
 
-  // ---- shared-memory staging lists and local indices ----
   const int S = std::max(0, X->plasma_species);
   const bool plasma = S > 0;
-  std::vector<int> stampA(std::max(nV, std::max(nE, nF)), -1), locA(std::max(nV, std::max(nE, nF)), 0);
-  std::vector<int> stampB(std::max(nE, nF), -1), locB(std::max(nE, nF), 0);
-  std::vector<int> stampC(nF, -1), locC(nF, 0);
-  auto add = [](std::vector<int>& stamp, std::vector<int>& loc, std::vector<int>& rows, int base, int p, int id) {
-    if (stamp[id] != p) {
-      stamp[id] = p;
-      loc[id] = (int)rows.size() - base;
-      rows.push_back(id);
-    }
-    return loc[id];
-  };
-  // H phase: er rows (vertices) and et rows (edges) per patch
-  std::vector<int> khv_off(oh.n + 1, 0), khv_rows, khe_off(oh.n + 1, 0), khe_rows;
-  std::vector<int4> kh_edge_loc(nE), kh_face_loc(2 * (size_t)nF);
-  size_t kh_max = 0;
-  for (int q = 0; q < oh.n; ++q) {
-    const int fa = q * fpp, fb = std::min(fa + fpp, nF), ea = oh.eptr[q], eb = oh.eptr[q + 1];
-    khv_off[q] = (int)khv_rows.size();
-    khe_off[q] = (int)khe_rows.size();
-    for (int f = fa; f < fb; ++f) {
-      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].x);
-      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].y);
-      add(stampB, locB, khe_rows, khe_off[q], q, fe[f].z);
-    }
-    for (int e = ea; e < eb; ++e) {
-      add(stampA, locA, khv_rows, khv_off[q], q, th[e].x);
-      add(stampA, locA, khv_rows, khv_off[q], q, th[e].y);
-    }
-    if (plasma)
-      for (int f = fa; f < fb; ++f) {
-        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].x);
-        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].y);
-        add(stampA, locA, khv_rows, khv_off[q], q, fv[f].z);
-      }
-    for (int e = ea; e < eb; ++e) {
-      if (stampB[e] != q) return fail(IFDTD_ERR_ARGUMENT, "owned edge is not an edge of its patch's faces");
-      kh_edge_loc[e] = make_int4(locA[th[e].x], locA[th[e].y], locB[e], 0);
-    }
-    for (int f = fa; f < fb; ++f) {
-      kh_face_loc[2 * (size_t)f] = make_int4(locB[fe[f].x], locB[fe[f].y], locB[fe[f].z], plasma ? locA[fv[f].x] : 0);
-      kh_face_loc[2 * (size_t)f + 1] = make_int4(plasma ? locA[fv[f].y] : 0, plasma ? locA[fv[f].z] : 0, 0, 0);
-    }
-    const size_t nv = khv_rows.size() - khv_off[q], ne = khe_rows.size() - khe_off[q];
-    kh_max = std::max(kh_max, nv * Pn + ne * Pm + (size_t)(eb - ea) * Pn + (size_t)(fb - fa) * Pm +
-                                  (size_t)S * (fb - fa) * 3 * Pm);
-  }
-  khv_off[oh.n] = (int)khv_rows.size();
-  khe_off[oh.n] = (int)khe_rows.size();
-  // E phase: ht rows (edges), hr rows (faces), summed current rows (faces) per patch
-  std::fill(stampA.begin(), stampA.end(), -1);
-  std::fill(stampB.begin(), stampB.end(), -1);
-  std::vector<int> keh_off(oe.n + 1, 0), keh_rows, kef_off(oe.n + 1, 0), kef_rows, kej_off(oe.n + 1, 0), kej_rows;
-  std::vector<int> ke_slot_h((size_t)nV * SW, 0), ke_slot_j(plasma ? (size_t)nV * SW : 0, 0);
-  std::vector<int4> ke_edge_loc(nE);
-  std::vector<int> ke_edge_jr(plasma ? nE : 0, 0);
-  size_t ke_max = 0;
-  for (int q = 0; q < oe.n; ++q) {
-    const int va = oe.vptr[q], vb = oe.vptr[q + 1], ea = oe.eptr[q], eb = oe.eptr[q + 1];
-    keh_off[q] = (int)keh_rows.size();
-    kef_off[q] = (int)kef_rows.size();
-    kej_off[q] = (int)kej_rows.size();
-    for (int sl = va; sl < vb; ++sl)
-      for (int k = 0; k < SW; ++k)
-        ke_slot_h[(size_t)sl * SW + k] = add(stampA, locA, keh_rows, keh_off[q], q, ps_edge[(size_t)sl * SW + k]);
-    for (int e = ea; e < eb; ++e) add(stampA, locA, keh_rows, keh_off[q], q, e);
-    for (int e = ea; e < eb; ++e) {
-      add(stampB, locB, kef_rows, kef_off[q], q, lr[e].x);
-      add(stampB, locB, kef_rows, kef_off[q], q, lr[e].y);
-    }
-    if (plasma) {
-      for (int sl = va; sl < vb; ++sl)
-        for (int k = 0; k < SW; ++k)
-          ke_slot_j[(size_t)sl * SW + k] = add(stampC, locC, kej_rows, kej_off[q], q, ps_face[(size_t)sl * SW + k]);
-      for (int e = ea; e < eb; ++e) {
-        add(stampC, locC, kej_rows, kej_off[q], q, lr[e].x);
-        add(stampC, locC, kej_rows, kej_off[q], q, lr[e].y);
-      }
-    }
-    for (int e = ea; e < eb; ++e) {
-      ke_edge_loc[e] = make_int4(locA[e], locB[lr[e].x], locB[lr[e].y], plasma ? locC[lr[e].x] : 0);
-      if (plasma) ke_edge_jr[e] = locC[lr[e].y];
-    }
-    const size_t nh = keh_rows.size() - keh_off[q], nf = kef_rows.size() - kef_off[q], nj = kej_rows.size() - kej_off[q];
-    ke_max = std::max(ke_max, nh * Pn + nf * Pm + nj * 3 * Pm + (size_t)(vb - va) * Pn + (size_t)(eb - ea) * Pm);
-  }
-  keh_off[oe.n] = (int)keh_rows.size();
-  kef_off[oe.n] = (int)kef_rows.size();
-  kej_off[oe.n] = (int)kej_rows.size();
 
   // ---- radial metric rows, zero padded to Pn / Pm ----
   const double* r = G->radii_m;
@@ -444,24 +620,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(oe.eptr, eptr_e);
   UP(oe.vptr, vptr);
   UP(oe.vlist, vlist);
-  UP(khv_off, khv_off);
-  UP(khv_rows, khv_rows);
-  UP(khe_off, khe_off);
-  UP(khe_rows, khe_rows);
-  UP(kh_edge_loc, kh_edge_loc);
-  UP(kh_face_loc, kh_face_loc);
-  UP(keh_off, keh_off);
-  UP(keh_rows, keh_rows);
-  UP(kef_off, kef_off);
-  UP(kef_rows, kef_rows);
-  UP(ke_slot_h, ke_slot_h);
-  UP(ke_edge_loc, ke_edge_loc);
-  if (plasma) {
-    UP(kej_off, kej_off);
-    UP(kej_rows, kej_rows);
-    UP(ke_slot_j, ke_slot_j);
-    UP(ke_edge_jr, ke_edge_jr);
-  }
   UP(th, edge_th);
   UP(lr, edge_lr);
   UP(inv_theta, inv_theta);
@@ -528,6 +686,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   }
 
   // ---- plasma ----
+  std::vector<real> pl, tn;  // (F, 12) reconstruction rows, (E, 8) edge tangents
   P->S = X->plasma_species;
   if (X->plasma_species < 0 || X->plasma_species > IFDTD_MAX_SPECIES)
     return fail(IFDTD_ERR_ARGUMENT, "plasma species count out of range");
@@ -535,13 +694,13 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     const int S = X->plasma_species, rows = X->plasma_rows;
     if (!(rows == 1 || rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
     P->plasma = true;
-    std::vector<real> pl(12 * (size_t)nF);
+    pl.assign(12 * (size_t)nF, real(0));
     for (int f = 0; f < nF; ++f)
       for (int i = 0; i < 3; ++i) {
         for (int c = 0; c < 3; ++c) pl[12 * (size_t)f + 4 * i + c] = (real)X->plasma_reconstruction[9 * (size_t)f + 3 * i + c];
         pl[12 * (size_t)f + 4 * i + 3] = (real)X->face_centers[3 * (size_t)f + i];
       }
-    std::vector<real> tn(8 * (size_t)nE, real(0));
+    tn.assign(8 * (size_t)nE, real(0));
     for (int e = 0; e < nE; ++e)
       for (int c = 0; c < 3; ++c) {
         tn[8 * (size_t)e + c] = (real)X->plasma_tangent_left[3 * (size_t)e + c];
@@ -564,6 +723,28 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       cudaError_t e = A.alloc((size_t)nF * 3 * Pm * sizeof(real), &P->d_jtot);
       if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of summed plasma current failed");
       R.Jtot = (real*)P->d_jtot;
+    }
+  }
+
+  // ---- pipelined kernels: copy descriptors and table blobs per patch ----
+  if (staging != 1) {
+    PipeTables th_tab, te_tab;
+    std::vector<int> locA(std::max(nV, std::max(nE, nF)), 0), locB(std::max(nE, nF), 0);
+    P->pipe_h_ok = build_pipe_h<real>(th_tab, oh.n, fpp, nF, oh.eptr, th, fe, fv, inv_theta, fw, pl, S, Pn, Pm, locA,
+                                      locB);
+    P->pipe_e_ok = build_pipe_e<real>(te_tab, oe.n, oe.vptr, oe.vlist, oe.eptr, lr, SW, ps_edge, ps_face, ps_coef,
+                                      ps_wc, inv_phi, tn, plasma, Pn, Pm, locA, locB);
+    P->kh_stage = th_tab.stage_bytes;
+    P->ke_stage = te_tab.stage_bytes;
+    if (P->pipe_h_ok) {
+      UP(th_tab.dptr, dptr_h);
+      UP(th_tab.desc, desc_h);
+      UP(th_tab.tab, tab_h);
+    }
+    if (P->pipe_e_ok) {
+      UP(te_tab.dptr, dptr_e);
+      UP(te_tab.desc, desc_e);
+      UP(te_tab.tab, tab_e);
     }
   }
 #undef UP
@@ -597,21 +778,21 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->smem_bytes = (size_t)R.layer_reals * sizeof(real);
   if (P->smem_bytes > 200 * 1024) return fail(IFDTD_ERR_UNSUPPORTED, "radial grid too fine for the shared per-layer rows");
   {
-    // staged kernels: per-layer rows (rounded to 16 bytes) + the largest patch's rows
-    const size_t layer_block = (size_t)((R.layer_reals + 3) / 4 * 4) * sizeof(real);
-    P->kh_stage = (int)((kh_max + 3) / 4 * 4);
-    P->ke_stage = (int)((ke_max + 3) / 4 * 4);
-    P->kh_smem = layer_block + 2 * (size_t)P->kh_stage * sizeof(real);
-    P->ke_smem = layer_block + 2 * (size_t)P->ke_stage * sizeof(real);
-    const size_t auto_limit = 113 * 1024, hard_limit = 220 * 1024;
-    auto pick = [&](size_t need) {
-      if (staging == 1) return 1;
-      if (staging >= 2) return need <= hard_limit ? staging : 0;
-      return need <= auto_limit ? 2 : 1;
-    };
-    P->h_mode = pick(P->kh_smem);
-    P->e_mode = pick(P->ke_smem);
-    if (P->h_mode == 0 || P->e_mode == 0) return fail(IFDTD_ERR_UNSUPPORTED, "staged rows do not fit in shared memory");
+    // pipelined kernels: per-layer rows + n_stages ring stages in dynamic shared memory
+    const int layer_block = pipe::layer_block_bytes(R.layer_reals, (int)sizeof(real));
+    const int budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 256 - layer_block;
+    auto stages = [&](bool ok, int stage) { return ok && stage > 0 ? std::min(pipe::kMaxStages, budget / stage) : 0; };
+    P->kh_stages = stages(P->pipe_h_ok, P->kh_stage);
+    P->ke_stages = stages(P->pipe_e_ok, P->ke_stage);
+    P->kh_smem = (size_t)layer_block + (size_t)P->kh_stages * P->kh_stage;
+    P->ke_smem = (size_t)layer_block + (size_t)P->ke_stages * P->ke_stage;
+    auto pick = [&](int n_stages) { return staging == 1 ? 1 : (n_stages >= 2 ? 2 : (staging >= 2 ? 0 : 1)); };
+    P->h_mode = pick(P->kh_stages);
+    P->e_mode = pick(P->ke_stages);
+    if (P->h_mode == 0 || P->e_mode == 0)
+      return fail(IFDTD_ERR_UNSUPPORTED, "pipelined kernels need at least two patch stages in shared memory");
+    if ((P->h_mode == 1 || P->e_mode == 1) && threads > 256)
+      return fail(IFDTD_ERR_ARGUMENT, "direct kernels take at most 256 threads per CTA");
   }
   {
     void* st = nullptr;
@@ -670,23 +851,25 @@ cudaError_t allow_smem(K kernel, size_t bytes) {
 
 // Persistent grid: SM count x resident CTAs (from the occupancy calculator).
 template <typename K>
-cudaError_t persistent_grid(ifdtd_plan* P, K kernel, size_t smem, int n_patches, int* grid) {
+cudaError_t persistent_grid(ifdtd_plan* P, K kernel, int threads, size_t smem, int n_patches, int* grid) {
   if (*grid > 0) return cudaSuccess;
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, P->threads, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   if (e != cudaSuccess) return e;
-  *grid = std::max(1, std::min(n_patches, P->sm_count * std::max(per_sm, 1)));
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = std::max(1, std::min(n_patches, P->sm_count * per_sm));
   return cudaSuccess;
 }
 
 template <typename real, bool PL>
 cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
-  if (P->h_mode >= 2) {
-    auto k = P->h_mode == 2 ? kh_pipe<real, PL, 0> : kh_pipe<real, PL, 1>;
+  if (P->h_mode == 2) {
+    auto k = P->pipe_copy == 0 ? pipe::kh_tma<real, PL, 0> : pipe::kh_tma<real, PL, 1>;
+    const int threads = P->threads + 32;
     cudaError_t e = allow_smem(k, P->kh_smem);
-    if (e == cudaSuccess) e = persistent_grid(P, k, P->kh_smem, P->n_patches, &P->kh_grid);
+    if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->kh_smem, P->n_patches, &P->kh_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->kh_grid, P->threads, P->kh_smem, st>>>(rec, P->kh_stage);
+    k<<<P->kh_grid, threads, P->kh_smem, st>>>(rec, P->kh_stage, P->kh_stages);
   } else {
     auto k = kh_kernel<real, PL>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
@@ -698,12 +881,13 @@ cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
 
 template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, int istep, cudaStream_t st) {
-  if (P->e_mode >= 2) {
-    auto k = P->e_mode == 2 ? ke_pipe<real, PL, MD, 0> : ke_pipe<real, PL, MD, 1>;
+  if (P->e_mode == 2) {
+    auto k = P->pipe_copy == 0 ? pipe::ke_tma<real, PL, MD, 0> : pipe::ke_tma<real, PL, MD, 1>;
+    const int threads = P->threads + 32;
     cudaError_t e = allow_smem(k, P->ke_smem);
-    if (e == cudaSuccess) e = persistent_grid(P, k, P->ke_smem, P->n_patches_e, &P->ke_grid);
+    if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->ke_smem, P->n_patches_e, &P->ke_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->ke_grid, P->threads, P->ke_smem, st>>>(rec, P->ke_stage, istep);
+    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, istep);
   } else {
     auto k = ke_kernel<real, PL, MD>;
     cudaError_t e = allow_smem(k, P->smem_bytes);

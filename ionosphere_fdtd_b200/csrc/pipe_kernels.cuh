@@ -1,0 +1,395 @@
+// Warp-specialised pipelined step kernels (sm_100a).
+//
+// One persistent CTA per SM walks a contiguous range of patches.  Warp 0 is
+// the producer: for every patch it reads the patch's copy descriptors (built
+// on the host, rows of one source array coalesced into runs) and copies them
+// into the next free stage of an n-stage ring in shared memory, either as one
+// TMA bulk copy (cp.async.bulk global -> shared) per descriptor completing on
+// the stage's "full" mbarrier by transaction count, or as 16-byte cp.async
+// pieces spread over the warp's lanes, completing by one cp.async arrival per
+// lane.  The first descriptor of every patch copies the patch's table blob
+// (local row indices into the stage, metric factors, reconstruction rows, slot
+// tables), so the compute warps make no dependent global loads: they wait on
+// "full", run the same per-run arithmetic as the direct kernels from shared
+// memory, write their outputs straight to global memory and release the stage
+// on its "empty" mbarrier (one arrival per compute warp).
+//
+// Every wait is bounded by the global timer.  A wait that runs out sets bit 0
+// of the device status word and a CTA-wide abort flag; the other waits then
+// return at once, compute is skipped, and the producer waits (again bounded)
+// for the copies it issued before the CTA exits.  Sources are this GPU's
+// global memory only; no copy uses cluster multicast.
+#pragma once
+
+#include "step_kernels.cuh"
+
+namespace ifdtd {
+namespace pipe {
+
+constexpr int kMaxStages = 8;
+constexpr int kDescPerLane = 4;
+constexpr int kMaxDesc = 32 * kDescPerLane;  // copy descriptors per patch
+constexpr int kMaxThreads = 32 + 352;        // producer warp + up to 11 compute warps
+// Registers are granted to warps in groups of four: 12 warps x 32 x 168 <= 65536.
+constexpr int kMaxRegs = 168;
+constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;  // bound of one wait (0.5 s)
+
+// Descriptor sources (int4 {src, first row, stage byte offset, bytes}).
+enum Src : int { kSrcEr = 0, kSrcEt = 1, kSrcHt = 2, kSrcHr = 3, kSrcJsum = 4, kSrcTab = 5, kSrcJ0 = 8 };
+
+// H-phase blob header (ints; offsets are bytes from the stage start).
+enum KhHead : int {
+  kh_ea, kh_ne, kh_fa, kh_nf, kh_o_er, kh_o_et, kh_o_ht, kh_o_hr, kh_o_J,
+  kh_o_eloc, kh_o_einv, kh_o_floc, kh_o_fw, kh_o_fpl, kh_head_ints = 16
+};
+// E-phase blob header.
+enum KeHead : int {
+  ke_nv, ke_ea, ke_ne, ke_o_ht, ke_o_hr, ke_o_J, ke_o_er, ke_o_et, ke_o_vid, ke_o_vh,
+  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_head_ints = 16
+};
+
+// Bytes of per-layer rows at the start of dynamic shared memory (host and
+// device), rounded to 128 so the stages start aligned.
+__host__ __device__ inline int layer_block_bytes(int layer_reals, int real_bytes) {
+  return (layer_reals * real_bytes + 127) / 128 * 128;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16-byte asynchronous copy global -> shared (L2 only), and the arrival on an
+// mbarrier that fires once all of this thread's earlier cp.async copies have
+// landed (.noinc: the arrival is one of the barrier's expected arrivals).
+__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase of `bar` with the given parity.  abort_flag ==
+// nullptr: ignore the CTA abort flag (used while draining).
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* status) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 1; i < (1u << 30); ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 15u) == 0) {
+      if (abort_flag && *abort_flag) return false;
+      if (global_ns() - t0 > kWaitNs) break;
+    }
+  }
+  if (abort_flag) *abort_flag = 1;
+  atomicOr(status, 1);
+  return false;
+}
+
+struct Ring {
+  unsigned char* stages;
+  int stage_bytes, n_stages;
+  uint64_t *full, *empty;
+  volatile int* abort_flag;
+  int* status;
+};
+
+template <typename real>
+__device__ __forceinline__ const void* desc_source(const Rec<real>& R, const unsigned char* tab, int src, int row) {
+  const size_t r = (size_t)row;
+  switch (src) {
+    case kSrcEr: return R.er + r * R.Pn;
+    case kSrcEt: return R.et + r * R.Pm;
+    case kSrcHt: return R.ht + r * R.Pn;
+    case kSrcHr: return R.hr + r * R.Pm;
+    case kSrcJsum: return jsum(R) + r * 3 * R.Pm;
+    case kSrcTab: return tab + r * 16;
+    default: return R.J[(src - kSrcJ0) & (kMaxSpecies - 1)] + r * 3 * R.Pm;
+  }
+}
+
+// Producer warp: fills stage i % n_stages with patch p0 + i.  Descriptor
+// offsets (dptr) are read 32 patches at a time and each patch's descriptors
+// one patch ahead, so their latency overlaps the wait for a free stage.
+// COPY 0: one TMA bulk copy per descriptor (lane-parallel over descriptors),
+// completion by transaction count on the stage's full barrier (1 arrival).
+// COPY 1: 16-byte cp.async pieces, lane-parallel within each descriptor,
+// completion by one cp.async arrival per lane (32 arrivals).
+template <int COPY, typename real>
+__device__ void produce(const Rec<real>& R, const Ring& G, int p0, int p1, int n_patches, const int* dptr,
+                        const int4* desc, const unsigned char* tab) {
+  const int lane = threadIdx.x & 31;
+  int win = p0;
+  int dpw = __ldg(dptr + min(win + lane, n_patches));
+  int4 cur[kDescPerLane], nxt[kDescPerLane];
+  int ncur = 0, nnxt = 0;
+  auto fetch = [&](int p, int4* d, int& n) {
+    if (p + 1 - win >= 32) {
+      win = p;
+      dpw = __ldg(dptr + min(win + lane, n_patches));
+    }
+    const int b = __shfl_sync(0xFFFFFFFFu, dpw, p - win);
+    n = __shfl_sync(0xFFFFFFFFu, dpw, p + 1 - win) - b;
+#pragma unroll
+    for (int k = 0; k < kDescPerLane; ++k) {
+      const int j = lane + 32 * k;
+      d[k] = j < n ? __ldg(desc + b + j) : make_int4(0, 0, 0, 0);
+    }
+  };
+  if (p0 < p1) fetch(p0, cur, ncur);
+  int i = 0;
+  bool ok = true;
+  for (int p = p0; p < p1; ++p, ++i) {
+    if (p + 1 < p1) fetch(p + 1, nxt, nnxt);
+    const int s = i % G.n_stages;
+    const uint32_t ph = (uint32_t)(i / G.n_stages) & 1u;
+    ok = __all_sync(0xFFFFFFFFu, wait_phase(G.empty + s, ph ^ 1u, G.abort_flag, G.status));
+    if (!ok) break;
+    fence_proxy_async();
+    unsigned char* st = G.stages + (size_t)s * G.stage_bytes;
+    if (COPY == 0) {
+      int bytes = 0;
+#pragma unroll
+      for (int k = 0; k < kDescPerLane; ++k)
+        if (lane + 32 * k < ncur) bytes += cur[k].w;
+      bytes = __reduce_add_sync(0xFFFFFFFFu, bytes);
+      if (lane == 0) mbar_expect_tx(G.full + s, (uint32_t)bytes);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < kDescPerLane; ++k)
+        if (lane + 32 * k < ncur)
+          bulk_load(st + cur[k].z, desc_source(R, tab, cur[k].x, cur[k].y), (uint32_t)cur[k].w, G.full + s);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kDescPerLane; ++k) {
+        const int nk = min(32, ncur - 32 * k);
+        for (int j = 0; j < nk; ++j) {
+          const int src = __shfl_sync(0xFFFFFFFFu, cur[k].x, j);
+          const int row = __shfl_sync(0xFFFFFFFFu, cur[k].y, j);
+          const int dst = __shfl_sync(0xFFFFFFFFu, cur[k].z, j);
+          const int bytes = __shfl_sync(0xFFFFFFFFu, cur[k].w, j);
+          const unsigned char* sp = static_cast<const unsigned char*>(desc_source(R, tab, src, row));
+          for (int c = lane * 16; c < bytes; c += 32 * 16) cp16_async(st + dst + c, sp + c);
+        }
+      }
+      cp_async_arrive_noinc(G.full + s);
+    }
+#pragma unroll
+    for (int k = 0; k < kDescPerLane; ++k) cur[k] = nxt[k];
+    ncur = nnxt;
+  }
+  if (!ok) {
+    // patches 0..i-1 were issued; wait (bounded) for the copies of the last
+    // n_stages of them so none lands after the CTA has exited
+    for (int j = max(0, i - G.n_stages); j < i; ++j)
+      wait_phase(G.full + j % G.n_stages, (uint32_t)(j / G.n_stages) & 1u, nullptr, G.status);
+  }
+}
+
+// Compute-warp loop: wait for stage i % n_stages, run `consume` on it, release it.
+template <typename Consume>
+__device__ __forceinline__ void consume_ring(const Ring& G, int p0, int p1, Consume consume) {
+  const int lane = threadIdx.x & 31;
+  int i = 0;
+  for (int p = p0; p < p1; ++p, ++i) {
+    const int s = i % G.n_stages;
+    const uint32_t ph = (uint32_t)(i / G.n_stages) & 1u;
+    if (!__all_sync(0xFFFFFFFFu, wait_phase(G.full + s, ph, G.abort_flag, G.status))) return;
+    consume(G.stages + (size_t)s * G.stage_bytes);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(G.empty + s);
+  }
+}
+
+// H phase of one patch from its stage (same arithmetic as kh_kernel).
+template <typename real, bool PLASMA>
+__device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real>& Ls, const unsigned char* st, int ct,
+                                           int nct) {
+  constexpr int N = Lanes<real>::N;
+  const int* hd = reinterpret_cast<const int*>(st);
+  const int ea = hd[kh_ea], ne = hd[kh_ne], fa = hd[kh_fa], nf = hd[kh_nf];
+  const real* s_er = reinterpret_cast<const real*>(st + hd[kh_o_er]);
+  const real* s_et = reinterpret_cast<const real*>(st + hd[kh_o_et]);
+  const real* s_ht = reinterpret_cast<const real*>(st + hd[kh_o_ht]);
+  const real* s_hr = reinterpret_cast<const real*>(st + hd[kh_o_hr]);
+  const real* s_J = reinterpret_cast<const real*>(st + hd[kh_o_J]);
+  const int4* eloc = reinterpret_cast<const int4*>(st + hd[kh_o_eloc]);
+  const real* einv = reinterpret_cast<const real*>(st + hd[kh_o_einv]);
+  const int4* floc = reinterpret_cast<const int4*>(st + hd[kh_o_floc]);
+  const real* fw = reinterpret_cast<const real*>(st + hd[kh_o_fw]);
+  const real* fpl = reinterpret_cast<const real*>(st + hd[kh_o_fpl]);
+  const int Pn = R.Pn, Pm = R.Pm, cn = Pn / N, cm = Pm / N;
+  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  for (int it = ct; it < ne * cn; it += nct) {
+    const int el = fast_div(it, mag_cn);
+    const int e = ea + el;
+    const int4 loc = eloc[el];
+    h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
+               R.ht + (size_t)e * Pn, einv[el]);
+  }
+  for (int it = ct; it < nf * cm; it += nct) {
+    const int fl = fast_div(it, mag_cm);
+    const int f = fa + fl;
+    const int4 l0 = floc[2 * fl];
+    const int4 l1 = floc[2 * fl + 1];
+    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, s_et + l0.x * Pm, s_et + l0.y * Pm, s_et + l0.z * Pm,
+                             s_hr + fl * Pm, R.hr + (size_t)f * Pm, s_er + l0.w * Pn, s_er + l1.x * Pn,
+                             s_er + l1.y * Pn, s_J + fl * 3 * Pm, nf * 3 * Pm,
+                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr, fw + 4 * fl, fpl + 12 * fl);
+  }
+}
+
+// E phase of one patch from its stage (same arithmetic as ke_kernel).
+template <typename real, bool PLASMA, int MAXDEG>
+__device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, const unsigned char* st, int ct,
+                                           int nct, real current) {
+  constexpr int N = Lanes<real>::N;
+  const int* hd = reinterpret_cast<const int*>(st);
+  const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne];
+  const real* s_ht = reinterpret_cast<const real*>(st + hd[ke_o_ht]);
+  const real* s_hr = reinterpret_cast<const real*>(st + hd[ke_o_hr]);
+  const real* s_J = reinterpret_cast<const real*>(st + hd[ke_o_J]);
+  const real* s_er = reinterpret_cast<const real*>(st + hd[ke_o_er]);
+  const real* s_et = reinterpret_cast<const real*>(st + hd[ke_o_et]);
+  const int* vid = reinterpret_cast<const int*>(st + hd[ke_o_vid]);
+  const int* vh = reinterpret_cast<const int*>(st + hd[ke_o_vh]);
+  const int* vj = reinterpret_cast<const int*>(st + hd[ke_o_vj]);
+  const real* vcoef = reinterpret_cast<const real*>(st + hd[ke_o_vcoef]);
+  const real* vwc = reinterpret_cast<const real*>(st + hd[ke_o_vwc]);
+  const int4* eloc = reinterpret_cast<const int4*>(st + hd[ke_o_eloc]);
+  const real* einv = reinterpret_cast<const real*>(st + hd[ke_o_einv]);
+  const real* etan = reinterpret_cast<const real*>(st + hd[ke_o_etan]);
+  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
+  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  for (int it = ct; it < nv * cn; it += nct) {
+    const int vl = fast_div(it, mag_cn);
+    const int v = vid[vl];
+    const real* hrows[MAXDEG];
+    const real* jrows[MAXDEG];
+#pragma unroll
+    for (int q = 0; q < MAXDEG; ++q) {
+      hrows[q] = s_ht + vh[vl * SW + q] * Pn;
+      jrows[q] = PLASMA ? s_J + vj[vl * SW + q] * 3 * Pm : nullptr;
+    }
+    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, vcoef + vl * SW,
+                                       PLASMA ? vwc + vl * SW * 4 : nullptr, s_er + vl * Pn, R.er + (size_t)v * Pn,
+                                       current);
+  }
+  for (int it = ct; it < ne * cm; it += nct) {
+    const int el = fast_div(it, mag_cm);
+    const int e = ea + el;
+    const int4 loc = eloc[el];
+    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, s_hr + loc.y * Pm, s_hr + loc.z * Pm, s_ht + loc.x * Pn,
+                             PLASMA ? s_J + loc.y * 3 * Pm : nullptr, PLASMA ? s_J + loc.z * 3 * Pm : nullptr,
+                             s_et + el * Pm, R.et + (size_t)e * Pm, current, einv[el],
+                             PLASMA ? etan + el * 8 : nullptr);
+  }
+}
+
+// Shared prologue: barriers, record, per-layer rows, this CTA's patch range.
+template <typename real>
+__device__ __forceinline__ void ring_setup(Rec<real>& R, const Rec<real>* recs, unsigned char* dyn, uint64_t* full,
+                                           uint64_t* empty, int* abort_flag, int stage_bytes, int n_stages,
+                                           int full_arrivals, Layers<real>& Ls, Ring& G) {
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    for (int s = 0; s < n_stages; ++s) {
+      mbar_init(full + s, full_arrivals);
+      mbar_init(empty + s, (blockDim.x - 32) / 32);
+    }
+    fence_mbar_init();
+  }
+  load_rec(R, recs);
+  load_layers(R, reinterpret_cast<real*>(dyn), Ls);
+  G.stages = dyn + layer_block_bytes(R.layer_reals, (int)sizeof(real));
+  G.stage_bytes = stage_bytes;
+  G.n_stages = n_stages;
+  G.full = full;
+  G.empty = empty;
+  G.abort_flag = abort_flag;
+  G.status = R.status;
+}
+
+template <typename real, bool PLASMA, int COPY>
+__global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
+  __shared__ int abort_flag;
+  Layers<real> Ls;
+  Ring G;
+  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? 1 : 32, Ls, G);
+  const int n = R.n_patches_h;
+  const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
+  if (threadIdx.x < 32) {
+    produce<COPY>(R, G, p0, p1, n, R.dptr_h, R.desc_h, R.tab_h);
+  } else {
+    const int ct = threadIdx.x - 32, nct = blockDim.x - 32;
+    consume_ring(G, p0, p1, [&](const unsigned char* st) { kh_consume<real, PLASMA>(R, Ls, st, ct, nct); });
+  }
+}
+
+template <typename real, bool PLASMA, int MAXDEG, int COPY>
+__global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
+                                             int istep) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
+  __shared__ int abort_flag;
+  Layers<real> Ls;
+  Ring G;
+  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? 1 : 32, Ls, G);
+  const int n = R.n_patches_e;
+  const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
+  if (threadIdx.x < 32) {
+    produce<COPY>(R, G, p0, p1, n, R.dptr_e, R.desc_e, R.tab_e);
+  } else {
+    const int ct = threadIdx.x - 32, nct = blockDim.x - 32;
+    const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+    consume_ring(G, p0, p1,
+                 [&](const unsigned char* st) { ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current); });
+  }
+}
+
+}  // namespace pipe
+}  // namespace ifdtd

@@ -69,14 +69,11 @@ struct Rec {
   const real* ps_coef;   // sign * phi_e / A*_v, 0 in padding slots
   const int* ps_face;
   const real* ps_wc;     // (V, slot_width, 4): area weight * face centre, 0 in padding slots
-  // shared-memory staging (per patch row lists and local indices into them)
-  const int *khv_off, *khv_rows, *khe_off, *khe_rows;  // H phase: er rows (vertices), et rows (edges)
-  const int4* kh_edge_loc;                             // per edge: tail, head (er rows), own et row, 0
-  const int4* kh_face_loc;                             // per face, 2 x int4: et rows x3, er rows x3
-  const int *keh_off, *keh_rows, *kef_off, *kef_rows, *kej_off, *kej_rows;  // E phase: ht, hr, J rows
-  const int *ke_slot_h, *ke_slot_j;                    // per vertex slot: local ht row / local J row
-  const int4* ke_edge_loc;                             // per edge: own ht row, left/right hr rows, left J row
-  const int* ke_edge_jr;                               // per edge: right J row
+  // pipelined kernels: per patch copy descriptors (dptr: CSR offsets into desc)
+  // and the per-patch table blobs they copy (16-byte units)
+  const int *dptr_h, *dptr_e;
+  const int4 *desc_h, *desc_e;
+  const unsigned char *tab_h, *tab_e;
   // radial metric rows (padded; staged in shared memory by the kernels)
   const real *invr, *rr, *mid, *invm, *invdr, *invcd;
   real dtmu;             // dt / mu0
@@ -266,73 +263,21 @@ __device__ __forceinline__ void member_patch(const int2* block_map, int n_member
 }
 
 // ---------------------------------------------------------------------------
-// Bulk asynchronous copies (TMA, cp.async.bulk) into shared memory, completed
-// on an mbarrier.  Sources are always this GPU's global memory; no multicast.
-// ---------------------------------------------------------------------------
-constexpr uint32_t kWaitLimit = 1u << 22;  // bounded spin on the staging barrier
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Wait for the staged rows with an iteration limit.  On timeout the CTA flags
-// the status word, waits once more (bounded) for its own copies and reports
-// failure so the caller skips the compute phase.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  if (threadIdx.x == 0) atomicOr(status, 1);
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
-    if (mbar_try_wait(bar, parity)) break;
-  return false;
-}
-
-// Start of the staged-row area after the per-layer rows (16-byte aligned).
-template <typename real>
-__device__ __forceinline__ real* staged_base(const Rec<real>& R, unsigned char* dyn) {
-  return reinterpret_cast<real*>(dyn) + ((R.layer_reals + 3) / 4) * 4;
-}
-
-// ---------------------------------------------------------------------------
-// Per-run arithmetic shared by the direct and the staged kernels.  Input row
-// pointers may address shared or global memory; outputs are global.
+// Per-run arithmetic shared by the direct and the pipelined kernels.  Input
+// row pointers and per-entity table pointers may address shared or global
+// memory; outputs are global.
 // ---------------------------------------------------------------------------
 
 // Ht on nodes k0..k0+N-1 of edge e: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr)/mu0
 // with odd (PEC) Et ghosts (solver.py:877-899, 443-456); the run holding node 0
 // also advances the surface-impedance ADE (surface_impedance.py:225-270).
+// inv_t = 1 / primal edge angle.
 template <typename real>
 __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
-                                           const real* ert, const real* etr, const real* hto, real* htout) {
+                                           const real* ert, const real* etr, const real* hto, real* htout,
+                                           real inv_t) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Lp1 = L + 1, Pm = R.Pm;
-  const real inv_t = __ldg(R.inv_theta + e);
   const real dtmu = R.dtmu;
   const Run<real> vh = ld16(erh + k0);
   const Run<real> vt = ld16(ert + k0);
@@ -377,13 +322,15 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
 }
 
 // Hr and the plasma current on midpoints j0..j0+N-1 of face f
-// (solver.py:915-921; plasma.py:413-442, 489-501).  jin[s] / jout[s] are the
-// face's (3, Pm) current rows of species s.
+// (solver.py:915-921; plasma.py:413-442, 489-501).  The face's (3, Pm) input
+// current rows of species s are at jin0 + s * jin_stride (jin0 == nullptr: the
+// state arrays R.J[s] themselves); outputs go to R.J[s].  fw is the face's
+// circulation row (4 reals) and gp its reconstruction row (12 reals).
 template <typename real, bool PLASMA>
 __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real>& Ls, int f, int j0, const real* et0,
                                            const real* et1, const real* et2, const real* hro, real* hrout,
-                                           const real* pa, const real* pb, const real* pc, const real* const* jin,
-                                           real* const* jout, real* jtot) {
+                                           const real* pa, const real* pb, const real* pc, const real* jin0,
+                                           int jin_stride, real* jtot, const real* fw, const real* gp) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
   const real dtmu = R.dtmu;
@@ -391,8 +338,7 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   const Run<real> a1 = ld16(et1 + j0);
   const Run<real> a2 = ld16(et2 + j0);
   const Run<real> hv = ld16(hro + j0);
-  const real* fw = R.face_w + 4 * (size_t)f;
-  const real w0 = __ldg(fw), w1 = __ldg(fw + 1), w2 = __ldg(fw + 2);
+  const real w0 = fw[0], w1 = fw[1], w2 = fw[2];
   Run<real> hn;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
@@ -409,13 +355,12 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
 #pragma unroll
   for (int r = 0; r < N; ++r) node[r] = (na.x[r] + nb.x[r] + nc.x[r]) * third;
   node[N] = (ta + tb + tc) * third;
-  const real* gp = R.face_pl + 12 * (size_t)f;
   real rc[3][3], cf[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rc[i][c] = __ldg(gp + 4 * i + c);
-    cf[i] = __ldg(gp + 4 * i + 3);
+    for (int c = 0; c < 3; ++c) rc[i][c] = gp[4 * i + c];
+    cf[i] = gp[4 * i + 3];
   }
   real E[N][3];
 #pragma unroll
@@ -428,9 +373,11 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
 #pragma unroll
   for (int r = 0; r < N; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
   for (int s = 0; s < R.n_species; ++s) {
+    real* jo = R.J[s] + (size_t)f * 3 * Pm;
+    const real* ji = jin0 ? jin0 + (size_t)s * jin_stride : jo;
     Run<real> jc[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) jc[c] = ld16(jin[s] + c * Pm + j0);
+    for (int c = 0; c < 3; ++c) jc[c] = ld16(ji + c * Pm + j0);
     Run<real> jn[3];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
@@ -484,7 +431,7 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
       }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) st16(jout[s] + c * Pm + j0, jn[c]);
+    for (int c = 0; c < 3; ++c) st16(jo + c * Pm + j0, jn[c]);
   }
   if (R.n_species > 1) {
 #pragma unroll
@@ -499,23 +446,27 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
 
 // Er on nodes k0..k0+N-1 of vertex v (solver.py:929-962; plasma.py:511-526).
 // hrows[q]: Ht row of slot q's edge; jrows[q]: (3, Pm) summed current rows of
-// slot q's face; slot coefficients come from the slot tables at `slot`.
+// slot q's face; coef[q] = sign * phi_e / A*_v and wcs[4q..4q+2] = area weight *
+// face centre of slot q (zero in padding slots).
 template <typename real, bool PLASMA, int MAXDEG>
-__device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int slot, int k0,
-                                             const real* const* hrows, const real* const* jrows, const real* ero,
-                                             real* erout, real current) {
+__device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int k0,
+                                             const real* const* hrows, const real* const* jrows, const real* coef,
+                                             const real* wcs, const real* ero, real* erout, real current) {
   constexpr int N = Lanes<real>::N;
-  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
+  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm;
   Run<real> hv[MAXDEG];
 #pragma unroll
   for (int q = 0; q < MAXDEG; ++q) hv[q] = ld16(hrows[q] + k0);
   const Run<real> ev = ld16(ero + k0);
+  real cq[MAXDEG];
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) cq[q] = coef[q];
   real acc[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) {
     acc[r] = real(0);
 #pragma unroll
-    for (int q = 0; q < MAXDEG; ++q) acc[r] += __ldg(R.ps_coef + (size_t)slot * SW + q) * hv[q].x[r];
+    for (int q = 0; q < MAXDEG; ++q) acc[r] += cq[q] * hv[q].x[r];
   }
   real jr[N];
 #pragma unroll
@@ -525,10 +476,10 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
     real rav[N + 1];
 #pragma unroll
     for (int r = 0; r <= N; ++r) rav[r] = real(0);
-#pragma unroll 2
+#pragma unroll
     for (int q = 0; q < MAXDEG; ++q) {
-      const real* wc = R.ps_wc + ((size_t)slot * SW + q) * 4;
-      const real c0 = __ldg(wc), c1 = __ldg(wc + 1), c2 = __ldg(wc + 2);
+      const real* wc = wcs + 4 * q;
+      const real c0 = wc[0], c1 = wc[1], c2 = wc[2];
       const real* jf = jrows[q];
       const bool in = k0 < Pm;
       const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
@@ -562,13 +513,13 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
 }
 
 // Et on midpoints j0..j0+N-1 of edge e (solver.py:964-989; plasma.py:503-509).
+// inv_p = 1 / dual edge angle; tp = left tangent, 0, right tangent, 0.
 template <typename real, bool PLASMA>
 __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int j0, const real* hl,
                                            const real* hq, const real* hto, const real* jl, const real* jq,
-                                           const real* eto, real* etout, real current) {
+                                           const real* eto, real* etout, real current, real inv_p, const real* tp) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
-  const real inv_p = __ldg(R.inv_phi + e);
   const Run<real> a = ld16(hl + j0);
   const Run<real> b = ld16(hq + j0);
   const Run<real> hv = ld16(hto + j0);
@@ -578,9 +529,8 @@ __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real
 #pragma unroll
   for (int r = 0; r < N; ++r) jt[r] = real(0);
   if (PLASMA) {
-    const real* tp = R.tan + 8 * (size_t)e;
-    const real l0 = __ldg(tp), l1 = __ldg(tp + 1), l2 = __ldg(tp + 2);
-    const real q0 = __ldg(tp + 4), q1 = __ldg(tp + 5), q2 = __ldg(tp + 6);
+    const real l0 = tp[0], l1 = tp[1], l2 = tp[2];
+    const real q0 = tp[4], q1 = tp[5], q2 = tp[6];
     const Run<real> lx = ld16(jl + j0), ly = ld16(jl + Pm + j0), lz = ld16(jl + 2 * Pm + j0);
     const Run<real> qx = ld16(jq + j0), qy = ld16(jq + Pm + j0), qz = ld16(jq + 2 * Pm + j0);
 #pragma unroll
@@ -635,7 +585,7 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
     const int e = ea + el;
     const int2 th = __ldg(R.edge_th + e);
     h_edge_run(R, Ls, e, (it - el * cn) * N, R.er + (size_t)th.y * Pn, R.er + (size_t)th.x * Pn, R.et + (size_t)e * Pm,
-               R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn);
+               R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn, __ldg(R.inv_theta + e));
   }
   const int fa = patch * R.fpp_h, fb = min(fa + R.fpp_h, R.nF);
   for (int it = threadIdx.x; it < (fb - fa) * cm; it += blockDim.x) {
@@ -643,12 +593,11 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
     const int f = fa + fl;
     const int4 fe = __ldg(R.face_e + f);
     const int4 fv = PLASMA ? __ldg(R.face_v + f) : make_int4(0, 0, 0, 0);
-    real* jrow[kMaxSpecies];
-    for (int s = 0; s < kMaxSpecies; ++s) jrow[s] = s < R.n_species ? R.J[s] + (size_t)f * 3 * Pm : nullptr;
     h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, R.et + (size_t)fe.x * Pm, R.et + (size_t)fe.y * Pm,
                              R.et + (size_t)fe.z * Pm, R.hr + (size_t)f * Pm, R.hr + (size_t)f * Pm,
-                             R.er + (size_t)fv.x * Pn, R.er + (size_t)fv.y * Pn, R.er + (size_t)fv.z * Pn, jrow, jrow,
-                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr);
+                             R.er + (size_t)fv.x * Pn, R.er + (size_t)fv.y * Pn, R.er + (size_t)fv.z * Pn, nullptr, 0,
+                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr, R.face_w + 4 * (size_t)f,
+                             PLASMA ? R.face_pl + 12 * (size_t)f : nullptr);
   }
 }
 
@@ -679,7 +628,8 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
       hrows[q] = R.ht + (size_t)__ldg(R.ps_edge + (size_t)slot * SW + q) * Pn;
       jrows[q] = PLASMA ? Jsum + (size_t)__ldg(R.ps_face + (size_t)slot * SW + q) * 3 * Pm : nullptr;
     }
-    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, slot, (it - vl * cn) * N, hrows, jrows, R.er + (size_t)v * Pn,
+    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, R.ps_coef + (size_t)slot * SW,
+                                       PLASMA ? R.ps_wc + (size_t)slot * SW * 4 : nullptr, R.er + (size_t)v * Pn,
                                        R.er + (size_t)v * Pn, current);
   }
   const int ea = R.eptr_e[patch], eb = R.eptr_e[patch + 1];
@@ -690,292 +640,8 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
     e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, R.hr + (size_t)lr.x * Pm, R.hr + (size_t)lr.y * Pm,
                              R.ht + (size_t)e * Pn, PLASMA ? Jsum + (size_t)lr.x * 3 * Pm : nullptr,
                              PLASMA ? Jsum + (size_t)lr.y * 3 * Pm : nullptr, R.et + (size_t)e * Pm,
-                             R.et + (size_t)e * Pm, current);
+                             R.et + (size_t)e * Pm, current, __ldg(R.inv_phi + e), PLASMA ? R.tan + 8 * (size_t)e : nullptr);
   }
-}
-
-// ---------------------------------------------------------------------------
-// Pipelined staged kernels.  A persistent CTA walks patches p = blockIdx.x,
-// blockIdx.x + gridDim.x, ...; every row a patch reads (gathered neighbour
-// columns and its own contiguous ranges) is copied into one of two shared-
-// memory stages while the CTA computes the previous patch from the other
-// stage, so the copies of the next patch are always in flight.  COPY selects
-// the copy engine: 0 = TMA bulk copies (cp.async.bulk) completing on a per-stage
-// mbarrier, 1 = per-thread 16-byte asynchronous copies (cp.async) completing in
-// commit groups.  Sources are this GPU's memory only; nothing is multicast.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void cp16_async(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// Copies `rows` rows of `len` reals each from global rows src(i) to contiguous
-// shared rows of the same length.  COPY 0: one bulk copy per row from warp 0
-// (lane-strided); COPY 1: 16-byte pieces strided over the whole CTA.
-template <int COPY, typename real, typename SrcRow>
-__device__ __forceinline__ void stage_rows(real* dst, int rows, int len, SrcRow src, uint64_t* bar) {
-  constexpr int V = 16 / sizeof(real);
-  if (rows <= 0 || len <= 0) return;
-  if (COPY == 0) {
-    if (threadIdx.x < 32)
-      for (int i = threadIdx.x; i < rows; i += 32) bulk_load(dst + (size_t)i * len, src(i), len * sizeof(real), bar);
-  } else {
-    const int per = len / V;
-    for (int t = threadIdx.x; t < rows * per; t += blockDim.x) {
-      const int i = t / per, c = t - i * per;
-      cp16_async(dst + (size_t)i * len + c * V, src(i) + c * V);
-    }
-  }
-}
-
-template <typename real, bool PLASMA>
-struct KhPatch {
-  int ea, eb, fa, fb, v0, nv, e0, ne;
-  __device__ __forceinline__ void init(const Rec<real>& R, int p) {
-    ea = R.eptr_h[p];
-    eb = R.eptr_h[p + 1];
-    fa = p * R.fpp_h;
-    fb = min(fa + R.fpp_h, R.nF);
-    v0 = R.khv_off[p];
-    nv = R.khv_off[p + 1] - v0;
-    e0 = R.khe_off[p];
-    ne = R.khe_off[p + 1] - e0;
-  }
-  __device__ __forceinline__ uint32_t reals(const Rec<real>& R) const {
-    const int S = PLASMA ? R.n_species : 0;
-    return (uint32_t)nv * R.Pn + (uint32_t)ne * R.Pm + (uint32_t)(eb - ea) * R.Pn + (uint32_t)(fb - fa) * R.Pm +
-           (uint32_t)S * (fb - fa) * 3 * R.Pm;
-  }
-};
-
-template <int COPY, typename real, bool PLASMA>
-__device__ __forceinline__ void kh_issue(const Rec<real>& R, int p, real* st, uint64_t* bar) {
-  KhPatch<real, PLASMA> P;
-  P.init(R, p);
-  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0, nEo = P.eb - P.ea, nFo = P.fb - P.fa;
-  if (COPY == 0 && threadIdx.x == 0) mbar_expect_tx(bar, P.reals(R) * sizeof(real));
-  if (COPY == 0) __syncwarp();
-  real* s_er = st;
-  real* s_et = s_er + (size_t)P.nv * Pn;
-  real* s_ht = s_et + (size_t)P.ne * Pm;
-  real* s_hr = s_ht + (size_t)nEo * Pn;
-  real* s_J = s_hr + (size_t)nFo * Pm;
-  stage_rows<COPY>(s_er, P.nv, Pn, [&](int i) { return R.er + (size_t)__ldg(R.khv_rows + P.v0 + i) * Pn; }, bar);
-  stage_rows<COPY>(s_et, P.ne, Pm, [&](int i) { return R.et + (size_t)__ldg(R.khe_rows + P.e0 + i) * Pm; }, bar);
-  stage_rows<COPY>(s_ht, 1, nEo * Pn, [&](int) { return R.ht + (size_t)P.ea * Pn; }, bar);
-  stage_rows<COPY>(s_hr, 1, nFo * Pm, [&](int) { return R.hr + (size_t)P.fa * Pm; }, bar);
-  for (int s = 0; s < S; ++s)
-    stage_rows<COPY>(s_J + (size_t)s * nFo * 3 * Pm, 1, nFo * 3 * Pm,
-                     [&](int) { return (const real*)R.J[s] + (size_t)P.fa * 3 * Pm; }, bar);
-}
-
-template <typename real, bool PLASMA>
-__device__ __forceinline__ void kh_compute(const Rec<real>& R, const Layers<real>& Ls, int p, const real* st) {
-  constexpr int N = Lanes<real>::N;
-  KhPatch<real, PLASMA> P;
-  P.init(R, p);
-  const int Pn = R.Pn, Pm = R.Pm, S = PLASMA ? R.n_species : 0, nEo = P.eb - P.ea, nFo = P.fb - P.fa;
-  const real* s_er = st;
-  const real* s_et = s_er + (size_t)P.nv * Pn;
-  const real* s_ht = s_et + (size_t)P.ne * Pm;
-  const real* s_hr = s_ht + (size_t)nEo * Pn;
-  const real* s_J = s_hr + (size_t)nFo * Pm;
-  const int cn = Pn / N, cm = Pm / N;
-  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  for (int it = threadIdx.x; it < nEo * cn; it += blockDim.x) {
-    const int el = fast_div(it, mag_cn);
-    const int e = P.ea + el;
-    const int4 loc = __ldg(R.kh_edge_loc + e);
-    h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + (size_t)loc.y * Pn, s_er + (size_t)loc.x * Pn,
-               s_et + (size_t)loc.z * Pm, s_ht + (size_t)el * Pn, R.ht + (size_t)e * Pn);
-  }
-  for (int it = threadIdx.x; it < nFo * cm; it += blockDim.x) {
-    const int fl = fast_div(it, mag_cm);
-    const int f = P.fa + fl;
-    const int4 l0 = __ldg(R.kh_face_loc + 2 * (size_t)f);
-    const int4 l1 = __ldg(R.kh_face_loc + 2 * (size_t)f + 1);
-    const real* jin[kMaxSpecies];
-    real* jout[kMaxSpecies];
-    for (int s = 0; s < kMaxSpecies; ++s) {
-      jin[s] = s < S ? s_J + ((size_t)s * nFo + fl) * 3 * Pm : nullptr;
-      jout[s] = s < S ? R.J[s] + (size_t)f * 3 * Pm : nullptr;
-    }
-    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, s_et + (size_t)l0.x * Pm, s_et + (size_t)l0.y * Pm,
-                             s_et + (size_t)l0.z * Pm, s_hr + (size_t)fl * Pm, R.hr + (size_t)f * Pm,
-                             s_er + (size_t)l0.w * Pn, s_er + (size_t)l1.x * Pn, s_er + (size_t)l1.y * Pn, jin, jout,
-                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr);
-  }
-}
-
-template <typename real, bool PLASMA>
-struct KePatch {
-  int va, vb, ea, eb, h0, nh, f0, nf, j0, nj;
-  __device__ __forceinline__ void init(const Rec<real>& R, int p) {
-    va = R.vptr[p];
-    vb = R.vptr[p + 1];
-    ea = R.eptr_e[p];
-    eb = R.eptr_e[p + 1];
-    h0 = R.keh_off[p];
-    nh = R.keh_off[p + 1] - h0;
-    f0 = R.kef_off[p];
-    nf = R.kef_off[p + 1] - f0;
-    j0 = PLASMA ? R.kej_off[p] : 0;
-    nj = PLASMA ? R.kej_off[p + 1] - j0 : 0;
-  }
-  __device__ __forceinline__ uint32_t reals(const Rec<real>& R) const {
-    return (uint32_t)nh * R.Pn + (uint32_t)nf * R.Pm + (uint32_t)nj * 3 * R.Pm + (uint32_t)(vb - va) * R.Pn +
-           (uint32_t)(eb - ea) * R.Pm;
-  }
-};
-
-template <int COPY, typename real, bool PLASMA>
-__device__ __forceinline__ void ke_issue(const Rec<real>& R, int p, real* st, uint64_t* bar) {
-  KePatch<real, PLASMA> P;
-  P.init(R, p);
-  const int Pn = R.Pn, Pm = R.Pm;
-  const real* Jsum = PLASMA ? jsum(R) : nullptr;
-  if (COPY == 0 && threadIdx.x == 0) mbar_expect_tx(bar, P.reals(R) * sizeof(real));
-  if (COPY == 0) __syncwarp();
-  real* s_ht = st;
-  real* s_hr = s_ht + (size_t)P.nh * Pn;
-  real* s_J = s_hr + (size_t)P.nf * Pm;
-  real* s_er = s_J + (size_t)P.nj * 3 * Pm;
-  real* s_et = s_er + (size_t)(P.vb - P.va) * Pn;
-  stage_rows<COPY>(s_ht, P.nh, Pn, [&](int i) { return (const real*)R.ht + (size_t)__ldg(R.keh_rows + P.h0 + i) * Pn; }, bar);
-  stage_rows<COPY>(s_hr, P.nf, Pm, [&](int i) { return (const real*)R.hr + (size_t)__ldg(R.kef_rows + P.f0 + i) * Pm; }, bar);
-  if (PLASMA)
-    stage_rows<COPY>(s_J, P.nj, 3 * Pm, [&](int i) { return Jsum + (size_t)__ldg(R.kej_rows + P.j0 + i) * 3 * Pm; }, bar);
-  stage_rows<COPY>(s_er, P.vb - P.va, Pn, [&](int i) { return (const real*)R.er + (size_t)__ldg(R.vlist + P.va + i) * Pn; },
-                   bar);
-  stage_rows<COPY>(s_et, 1, (P.eb - P.ea) * Pm, [&](int) { return (const real*)R.et + (size_t)P.ea * Pm; }, bar);
-}
-
-template <typename real, bool PLASMA, int MAXDEG>
-__device__ __forceinline__ void ke_compute(const Rec<real>& R, const Layers<real>& Ls, int p, const real* st,
-                                           real current) {
-  constexpr int N = Lanes<real>::N;
-  KePatch<real, PLASMA> P;
-  P.init(R, p);
-  const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width;
-  const real* s_ht = st;
-  const real* s_hr = s_ht + (size_t)P.nh * Pn;
-  const real* s_J = s_hr + (size_t)P.nf * Pm;
-  const real* s_er = s_J + (size_t)P.nj * 3 * Pm;
-  const real* s_et = s_er + (size_t)(P.vb - P.va) * Pn;
-  const int cn = Pn / N, cm = Pm / N;
-  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  for (int it = threadIdx.x; it < (P.vb - P.va) * cn; it += blockDim.x) {
-    const int vl = fast_div(it, mag_cn);
-    const int slot = P.va + vl;
-    const int v = __ldg(R.vlist + slot);
-    const real* hrows[MAXDEG];
-    const real* jrows[MAXDEG];
-#pragma unroll
-    for (int q = 0; q < MAXDEG; ++q) {
-      hrows[q] = s_ht + (size_t)__ldg(R.ke_slot_h + (size_t)slot * SW + q) * Pn;
-      jrows[q] = PLASMA ? s_J + (size_t)__ldg(R.ke_slot_j + (size_t)slot * SW + q) * 3 * Pm : nullptr;
-    }
-    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, slot, (it - vl * cn) * N, hrows, jrows, s_er + (size_t)vl * Pn,
-                                       R.er + (size_t)v * Pn, current);
-  }
-  for (int it = threadIdx.x; it < (P.eb - P.ea) * cm; it += blockDim.x) {
-    const int el = fast_div(it, mag_cm);
-    const int e = P.ea + el;
-    const int4 loc = __ldg(R.ke_edge_loc + e);
-    const int jr = PLASMA ? __ldg(R.ke_edge_jr + e) : 0;
-    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, s_hr + (size_t)loc.y * Pm, s_hr + (size_t)loc.z * Pm,
-                             s_ht + (size_t)loc.x * Pn, PLASMA ? s_J + (size_t)loc.w * 3 * Pm : nullptr,
-                             PLASMA ? s_J + (size_t)jr * 3 * Pm : nullptr, s_et + (size_t)el * Pm, R.et + (size_t)e * Pm,
-                             current);
-  }
-}
-
-// The persistent double-buffered loop shared by both phases.  stage_reals is
-// the largest patch's staged size (host-computed, a multiple of 4 reals).
-template <int COPY, typename real, typename Issue, typename Compute>
-__device__ __forceinline__ void pipeline(const Rec<real>& R, int n_patches, int stage_reals, real* stages,
-                                         uint64_t* bars, Issue issue, Compute compute) {
-  const int first = blockIdx.x, step = gridDim.x;
-  // prologue: patches first and first + step into stages 0 and 1
-  for (int s = 0; s < 2; ++s) {
-    const int p = first + s * step;
-    if (p < n_patches) issue(p, stages + (size_t)s * stage_reals, bars + s);
-    if (COPY == 1) cp_async_commit();
-  }
-  int i = 0;
-  for (int p = first; p < n_patches; p += step, ++i) {
-    const int s = i & 1;
-    real* st = stages + (size_t)s * stage_reals;
-    if (COPY == 0) {
-      if (!mbar_wait_bounded(bars + s, (uint32_t)((i >> 1) & 1), R.status)) return;
-    } else {
-      cp_async_wait<1>();
-      __syncthreads();
-    }
-    compute(p, st);
-    __syncthreads();  // the stage is free again
-    const int next = p + 2 * step;
-    if (next < n_patches) {
-      if (COPY == 0) fence_proxy_async();
-      issue(next, st, bars + s);
-    }
-    if (COPY == 1) cp_async_commit();
-  }
-  if (COPY == 1) cp_async_wait<0>();
-}
-
-template <typename real, bool PLASMA, int COPY>
-__global__ void __launch_bounds__(256) kh_pipe(const Rec<real>* __restrict__ recs, int stage_reals) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t bars[2];
-  load_rec(R, recs);
-  if (COPY == 0 && threadIdx.x == 0) {
-    mbar_init(bars, 1);
-    mbar_init(bars + 1, 1);
-  }
-  __syncthreads();
-  Layers<real> Ls;
-  Ls.invr = nullptr;
-  real* stages = staged_base(R, dyn_smem);
-  const int n = R.n_patches_h;
-  // issue the prologue copies before staging the per-layer rows so they overlap
-  pipeline<COPY>(
-      R, n, stage_reals, stages, bars,
-      [&](int p, real* st, uint64_t* bar) { kh_issue<COPY, real, PLASMA>(R, p, st, bar); },
-      [&](int p, const real* st) {
-        if (Ls.invr == nullptr) load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-        kh_compute<real, PLASMA>(R, Ls, p, st);
-      });
-}
-
-template <typename real, bool PLASMA, int MAXDEG, int COPY>
-__global__ void __launch_bounds__(256) ke_pipe(const Rec<real>* __restrict__ recs, int stage_reals, int istep) {
-  extern __shared__ __align__(16) unsigned char dyn_smem[];
-  __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t bars[2];
-  load_rec(R, recs);
-  if (COPY == 0 && threadIdx.x == 0) {
-    mbar_init(bars, 1);
-    mbar_init(bars + 1, 1);
-  }
-  __syncthreads();
-  Layers<real> Ls;
-  Ls.invr = nullptr;
-  real* stages = staged_base(R, dyn_smem);
-  const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
-  pipeline<COPY>(
-      R, R.n_patches_e, stage_reals, stages, bars,
-      [&](int p, real* st, uint64_t* bar) { ke_issue<COPY, real, PLASMA>(R, p, st, bar); },
-      [&](int p, const real* st) {
-        if (Ls.invr == nullptr) load_layers(R, reinterpret_cast<real*>(dyn_smem), Ls);
-        ke_compute<real, PLASMA, MAXDEG>(R, Ls, p, st, current);
-      });
 }
 
 // ---------------------------------------------------------------------------

@@ -36,9 +36,12 @@ class Physics:
 @dataclass
 class Tuning:
     """Launch geometry of a plan: faces per H-phase and E-phase patch, threads
-    per CTA, steps per captured CUDA graph, and the gather mode (0 auto,
-    1 direct global loads, 2 shared-memory pipeline fed by TMA bulk copies,
-    3 shared-memory pipeline fed by 16-byte cp.async copies)."""
+    per CTA (direct kernels, at most 256) or compute threads per CTA besides
+    the producer warp (pipelined kernels, at most 352), steps per captured
+    CUDA graph, and the kernel family (0 auto: the pipeline wherever two patch
+    stages fit in shared memory, 1 direct global gathers, 2 the warp-specialised
+    pipeline fed by TMA bulk copies, 3 the same pipeline fed by 16-byte cp.async
+    copies)."""
 
     faces_per_patch: int = 32
     threads: int = 256
@@ -186,12 +189,12 @@ class Engine:
 
     @property
     def kernel_modes(self) -> tuple[str, str]:
-        """Gather mode of the H and E phases: "direct", "bulk" (TMA bulk-copy
-        pipeline) or "cp.async" (16-byte asynchronous-copy pipeline)."""
+        """Kernel family of the H and E phases: "direct" (global gathers) or
+        "pipeline" (warp-specialised shared-memory pipeline)."""
 
         h, e = C.c_int32(), C.c_int32()
         N.check(N.load().ifdtd_plan_kernels(self.plan, C.byref(h), C.byref(e)), "ifdtd_plan_kernels")
-        name = {1: "direct", 2: "bulk", 3: "cp.async"}
+        name = {1: "direct", 2: "pipeline"}
         return name[h.value], name[e.value]
 
     def status_word(self, reset: bool = False) -> int:

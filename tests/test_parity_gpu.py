@@ -121,19 +121,32 @@ def test_patch_size_does_not_change_results(fpp):
         np.testing.assert_array_equal(ref[f], other[f])
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("staging", [2, 3])
+@pytest.mark.parametrize("fpp", [(16, 8), (32, 16), (4, 4)])
 @pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "tangential_s1", "thin_shell_s1"])
-def test_staged_and_direct_gathers_agree_bitwise(name, mode):
-    """Shared-memory pipelines (TMA bulk copies or cp.async) and direct global
-    gathers run the same per-run arithmetic: results must match bit for bit."""
+def test_pipeline_and_direct_kernels_agree_bitwise(name, fpp, staging):
+    """The pipeline (TMA bulk copies or cp.async) stages every row in shared
+    memory and runs the same per-run arithmetic as the direct global gathers:
+    results match bit for bit."""
 
     from ionosphere_fdtd_b200.engine import Tuning
 
     direct = run_product(C.CASES[name], "float32", tuning=Tuning(staging=1))
-    staged = run_product(C.CASES[name], "float32", tuning=Tuning(staging=mode, faces_per_patch=16, e_faces_per_patch=8))
+    staged = run_product(C.CASES[name], "float32", tuning=Tuning(staging=staging, faces_per_patch=fpp[0], e_faces_per_patch=fpp[1]))
     assert direct["_sim"]._engine.kernel_modes == ("direct", "direct")
-    assert staged["_sim"]._engine.kernel_modes == ({2: ("bulk", "bulk"), 3: ("cp.async", "cp.async")}[mode])
+    assert staged["_sim"]._engine.kernel_modes == ("pipeline", "pipeline")
     for key in ("er", "et", "hr", "ht", "si_memory", "plasma_current_0", "traces"):
         if key in direct:
             np.testing.assert_array_equal(direct[key], staged[key], err_msg=key)
     assert staged["_sim"]._engine.status_word() == 0
+
+
+@pytest.mark.parametrize("threads", [32, 128, 352])
+def test_pipeline_compute_warp_count_does_not_change_results(threads):
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    case = C.CASES["plasma_magnetized_s1"]
+    ref = run_product(case, "float64", tuning=Tuning(staging=2))
+    other = run_product(case, "float64", tuning=Tuning(staging=2, threads=threads))
+    for f in STATE:
+        np.testing.assert_array_equal(ref[f], other[f])
