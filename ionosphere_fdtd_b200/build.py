@@ -16,7 +16,7 @@ from pathlib import Path
 PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
 SOURCES = [PACKAGE / "csrc" / "ifdtd.cu"]
-HEADERS = [PACKAGE / "csrc" / "step_kernels.cuh", ROOT / "include" / "ifdtd.h"]
+HEADERS = [PACKAGE / "csrc" / "step_kernels.cuh", PACKAGE / "csrc" / "pipe_kernels.cuh", ROOT / "include" / "ifdtd.h"]
 LIBRARY = PACKAGE / "libifdtd.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

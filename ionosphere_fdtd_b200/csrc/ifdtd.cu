@@ -88,6 +88,7 @@ struct ifdtd_plan {
   int n_patches = 0, n_patches_e = 0, threads = 256, chunk = 32, maxdeg = 6, Pn = 0, Pm = 0;
   int h_mode = 1, e_mode = 1;  // 1 direct gathers, 2 pipeline
   int pipe_copy = 0;           // pipeline copy engine: 0 TMA bulk copies, 1 cp.async
+  int producers = 2;           // copy-issuing warps per pipelined CTA
   bool pipe_h_ok = false, pipe_e_ok = false;
   int kh_stage = 0, ke_stage = 0, kh_stages = 0, ke_stages = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
@@ -411,8 +412,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int fpp_e = (tune && tune->e_faces_per_patch > 0) ? tune->e_faces_per_patch : 16;
   const int staging = tune ? tune->staging : 0;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
-  if (threads % 32 || threads < 32 || threads > pipe::kMaxThreads - 32)
-    return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 in [32, 352]");
+  const int producers = (tune && tune->producer_warps > 0) ? tune->producer_warps : 2;
+  if (producers > 4) return fail(IFDTD_ERR_ARGUMENT, "producer_warps must be 1 to 4");
+  if (threads % 32 || threads < 32 || threads + 32 * producers > pipe::kMaxThreads)
+    return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 and threads + 32 * producer_warps <= 384");
+  P->producers = producers;
   if (staging < 0 || staging > 3)
     return fail(IFDTD_ERR_ARGUMENT,
                 "staging must be 0 (auto), 1 (direct gathers), 2 (pipeline, TMA bulk copies) or 3 (pipeline, cp.async)");
@@ -574,6 +578,35 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   invcd[0] = (real)(2.0 / (r[1] - r[0]));
   invcd[L] = (real)(2.0 / (r[L] - r[L - 1]));
   for (int k = 1; k < L; ++k) invcd[k] = (real)(1.0 / (m[k] - m[k - 1]));
+  // fused rows (float64 products, zero beyond the last node / midpoint):
+  //   hA = dt/(mu0 r); hU, hD: weights of Et[k] and Et[k-1] in dt/mu0 (1/r) d(m Et)/dr
+  //   (thin shell: d Et / dr) with zero (PEC-odd) ghosts; hC = dt/(mu0 m);
+  //   vwl, vwu: node weights of the midpoints below / above (one-sided at the
+  //   boundary nodes); eU, eD: weights of Ht[j+1] and Ht[j] in (1/m) d(r Ht)/dr
+  //   (thin shell: d Ht / dr).
+  std::vector<real> hA(Pn, 0), hU(Pn, 0), hD(Pn, 0), vwl(Pn, 0), vwu(Pn, 0), hC(Pm, 0), eU(Pm, 0), eD(Pm, 0);
+  {
+    const double dtmu = G->time_step_s / 1.256637062120e-6;
+    const bool full = G->full_spherical != 0;
+    std::vector<double> cd(L + 1);
+    cd[0] = 2.0 / (r[1] - r[0]);
+    cd[L] = 2.0 / (r[L] - r[L - 1]);
+    for (int k = 1; k < L; ++k) cd[k] = 1.0 / (m[k] - m[k - 1]);
+    for (int k = 0; k <= L; ++k) {
+      hA[k] = (real)(dtmu / r[k]);
+      const double w = full ? dtmu * cd[k] / r[k] : dtmu * cd[k];
+      if (k < L) hU[k] = (real)(full ? w * m[k] : w);
+      if (k >= 1) hD[k] = (real)(full ? w * m[k - 1] : w);
+      vwl[k] = (real)(k == 0 ? 0.0 : (k == L ? 1.0 : 0.5));
+      vwu[k] = (real)(k == 0 ? 1.0 : (k == L ? 0.0 : 0.5));
+    }
+    for (int j = 0; j < L; ++j) {
+      const double idr = 1.0 / (r[j + 1] - r[j]);
+      hC[j] = (real)(dtmu / m[j]);
+      eU[j] = (real)(full ? r[j + 1] * idr / m[j] : idr);
+      eD[j] = (real)(full ? r[j] * idr / m[j] : idr);
+    }
+  }
 
   // ---- loss coefficients, rows padded to Pn / Pm ----
   if (!(X->coef_rows_er == 1 || X->coef_rows_er == nV) || !(X->coef_rows_et == 1 || X->coef_rows_et == nE))
@@ -590,23 +623,20 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   // ---- sources ----
   if (X->n_src_er < 0 || X->n_src_er > IFDTD_MAX_SOURCES || X->n_src_et < 0 || X->n_src_et > IFDTD_MAX_SOURCES)
     return fail(IFDTD_ERR_ARGUMENT, "too many source supports");
-  std::vector<int> sv(X->n_src_er), sk(X->n_src_er), se(X->n_src_et), sj(X->n_src_et);
-  int vmin = 1 << 30, vmax = -1, emin = 1 << 30, emax = -1;
+  static_assert(kMaxSources >= IFDTD_MAX_SOURCES, "record source table too small");
   for (int s = 0; s < X->n_src_er; ++s) {
     if (X->src_er_vertex[s] < 0 || X->src_er_vertex[s] >= nV || X->src_er_layer[s] < 0 || X->src_er_layer[s] > L)
       return fail(IFDTD_ERR_ARGUMENT, "vertical source support out of range");
-    sv[s] = (int)X->src_er_vertex[s];
-    sk[s] = (int)X->src_er_layer[s];
-    vmin = std::min(vmin, sv[s]);
-    vmax = std::max(vmax, sv[s]);
+    R.src_er_v[s] = (int)X->src_er_vertex[s];
+    R.src_er_k[s] = (int)X->src_er_layer[s];
+    R.src_er_c[s] = (real)X->src_er_coef[s];
   }
   for (int s = 0; s < X->n_src_et; ++s) {
     if (X->src_et_edge[s] < 0 || X->src_et_edge[s] >= nE || X->src_et_layer[s] < 0 || X->src_et_layer[s] >= L)
       return fail(IFDTD_ERR_ARGUMENT, "tangential source support out of range");
-    se[s] = (int)X->src_et_edge[s];
-    sj[s] = (int)X->src_et_layer[s];
-    emin = std::min(emin, se[s]);
-    emax = std::max(emax, se[s]);
+    R.src_et_e[s] = (int)X->src_et_edge[s];
+    R.src_et_j[s] = (int)X->src_et_layer[s];
+    R.src_et_c[s] = (real)X->src_et_coef[s];
   }
 
   // ---- upload ----
@@ -635,6 +665,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(invm, invm);
   UP(invdr, invdr);
   UP(invcd, invcd);
+  UP(hA, hA);
+  UP(hU, hU);
+  UP(hD, hD);
+  UP(hC, hC);
+  UP(vwl, vwl);
+  UP(vwu, vwu);
+  UP(eU, eU);
+  UP(eD, eD);
   {
     auto ca = pad_rows(X->ca_er, X->coef_rows_er, L + 1, Pn), cb = pad_rows(X->cb_er, X->coef_rows_er, L + 1, Pn);
     auto ct = pad_rows(X->ca_et, X->coef_rows_et, L, Pm), cu = pad_rows(X->cb_et, X->coef_rows_et, L, Pm);
@@ -642,18 +680,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     UP(cb, cb_er);
     UP(ct, ca_et);
     UP(cu, cb_et);
-  }
-  if (X->n_src_er) {
-    auto c = cast<real>(X->src_er_coef, X->n_src_er);
-    UP(sv, src_er_v);
-    UP(sk, src_er_k);
-    UP(c, src_er_c);
-  }
-  if (X->n_src_et) {
-    auto c = cast<real>(X->src_et_coef, X->n_src_et);
-    UP(se, src_et_e);
-    UP(sj, src_et_j);
-    UP(c, src_et_c);
   }
   {
     cudaError_t e1 = A.upload(fsign, &P->face_sign);
@@ -768,10 +794,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.coef_full = X->coef_rows_er != 1 ? 1 : 0;
   R.n_src_er = X->n_src_er;
   R.n_src_et = X->n_src_et;
-  R.src_er_vmin = vmin;
-  R.src_er_vmax = vmax;
-  R.src_et_emin = emin;
-  R.src_et_emax = emax;
   R.maxdeg = MD;
   R.slot_width = SW;
   R.layer_reals = layer_reals(Pn, Pm, R.coef_full, X->plasma_species, R.plasma_full, R.magnetized, X->si_terms);
@@ -865,11 +887,11 @@ template <typename real, bool PL>
 cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
   if (P->h_mode == 2) {
     auto k = P->pipe_copy == 0 ? pipe::kh_tma<real, PL, 0> : pipe::kh_tma<real, PL, 1>;
-    const int threads = P->threads + 32;
+    const int threads = P->threads + 32 * P->producers;
     cudaError_t e = allow_smem(k, P->kh_smem);
     if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->kh_smem, P->n_patches, &P->kh_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->kh_grid, threads, P->kh_smem, st>>>(rec, P->kh_stage, P->kh_stages);
+    k<<<P->kh_grid, threads, P->kh_smem, st>>>(rec, P->kh_stage, P->kh_stages, P->producers);
   } else {
     auto k = kh_kernel<real, PL>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
@@ -883,11 +905,11 @@ template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, int istep, cudaStream_t st) {
   if (P->e_mode == 2) {
     auto k = P->pipe_copy == 0 ? pipe::ke_tma<real, PL, MD, 0> : pipe::ke_tma<real, PL, MD, 1>;
-    const int threads = P->threads + 32;
+    const int threads = P->threads + 32 * P->producers;
     cudaError_t e = allow_smem(k, P->ke_smem);
     if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->ke_smem, P->n_patches_e, &P->ke_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, istep);
+    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, P->producers, istep);
   } else {
     auto k = ke_kernel<real, PL, MD>;
     cudaError_t e = allow_smem(k, P->smem_bytes);

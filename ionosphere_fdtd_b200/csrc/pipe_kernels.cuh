@@ -1,9 +1,9 @@
 // Warp-specialised pipelined step kernels (sm_100a).
 //
-// One persistent CTA per SM walks a contiguous range of patches.  Warp 0 is
-// the producer: for every patch it reads the patch's copy descriptors (built
-// on the host, rows of one source array coalesced into runs) and copies them
-// into the next free stage of an n-stage ring in shared memory, either as one
+// One persistent CTA per SM walks a contiguous range of patches.  The first W
+// warps are producers: for every patch they read the patch's copy descriptors
+// (built on the host, rows of one source array coalesced into runs) and copy
+// them into the next free stage of an n-stage ring in shared memory, either as one
 // TMA bulk copy (cp.async.bulk global -> shared) per descriptor completing on
 // the stage's "full" mbarrier by transaction count, or as 16-byte cp.async
 // pieces spread over the warp's lanes, completing by one cp.async arrival per
@@ -16,8 +16,8 @@
 //
 // Every wait is bounded by the global timer.  A wait that runs out sets bit 0
 // of the device status word and a CTA-wide abort flag; the other waits then
-// return at once, compute is skipped, and the producer waits (again bounded)
-// for the copies it issued before the CTA exits.  Sources are this GPU's
+// return at once, compute is skipped, and the producers wait (again bounded)
+// for the copies they issued before the CTA exits.  Sources are this GPU's
 // global memory only; no copy uses cluster multicast.
 #pragma once
 
@@ -29,7 +29,7 @@ namespace pipe {
 constexpr int kMaxStages = 8;
 constexpr int kDescPerLane = 4;
 constexpr int kMaxDesc = 32 * kDescPerLane;  // copy descriptors per patch
-constexpr int kMaxThreads = 32 + 352;        // producer warp + up to 11 compute warps
+constexpr int kMaxThreads = 384;             // producer warps + compute warps
 // Registers are granted to warps in groups of four: 12 warps x 32 x 168 <= 65536.
 constexpr int kMaxRegs = 168;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;  // bound of one wait (0.5 s)
@@ -148,16 +148,18 @@ __device__ __forceinline__ const void* desc_source(const Rec<real>& R, const uns
   }
 }
 
-// Producer warp: fills stage i % n_stages with patch p0 + i.  Descriptor
+// Producer warp w of W: fills stage i % n_stages with its share (descriptors
+// w, w + W, ...) of patch p0 + i; a single warp issuing lane-parallel bulk
+// copies is issue-bound, so W warps split the descriptor list.  Descriptor
 // offsets (dptr) are read 32 patches at a time and each patch's descriptors
 // one patch ahead, so their latency overlaps the wait for a free stage.
-// COPY 0: one TMA bulk copy per descriptor (lane-parallel over descriptors),
-// completion by transaction count on the stage's full barrier (1 arrival).
+// COPY 0: one TMA bulk copy per descriptor, completion by transaction count
+// on the stage's full barrier (one expect_tx arrival per producer warp).
 // COPY 1: 16-byte cp.async pieces, lane-parallel within each descriptor,
-// completion by one cp.async arrival per lane (32 arrivals).
+// completion by one cp.async arrival per producer lane.
 template <int COPY, typename real>
 __device__ void produce(const Rec<real>& R, const Ring& G, int p0, int p1, int n_patches, const int* dptr,
-                        const int4* desc, const unsigned char* tab) {
+                        const int4* desc, const unsigned char* tab, int w, int W) {
   const int lane = threadIdx.x & 31;
   int win = p0;
   int dpw = __ldg(dptr + min(win + lane, n_patches));
@@ -172,7 +174,7 @@ __device__ void produce(const Rec<real>& R, const Ring& G, int p0, int p1, int n
     n = __shfl_sync(0xFFFFFFFFu, dpw, p + 1 - win) - b;
 #pragma unroll
     for (int k = 0; k < kDescPerLane; ++k) {
-      const int j = lane + 32 * k;
+      const int j = w + W * (lane + 32 * k);
       d[k] = j < n ? __ldg(desc + b + j) : make_int4(0, 0, 0, 0);
     }
   };
@@ -191,18 +193,19 @@ __device__ void produce(const Rec<real>& R, const Ring& G, int p0, int p1, int n
       int bytes = 0;
 #pragma unroll
       for (int k = 0; k < kDescPerLane; ++k)
-        if (lane + 32 * k < ncur) bytes += cur[k].w;
+        if (w + W * (lane + 32 * k) < ncur) bytes += cur[k].w;
       bytes = __reduce_add_sync(0xFFFFFFFFu, bytes);
       if (lane == 0) mbar_expect_tx(G.full + s, (uint32_t)bytes);
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < kDescPerLane; ++k)
-        if (lane + 32 * k < ncur)
+        if (w + W * (lane + 32 * k) < ncur)
           bulk_load(st + cur[k].z, desc_source(R, tab, cur[k].x, cur[k].y), (uint32_t)cur[k].w, G.full + s);
     } else {
 #pragma unroll
       for (int k = 0; k < kDescPerLane; ++k) {
-        const int nk = min(32, ncur - 32 * k);
+        // this warp's descriptors in slot k sit on lanes 0..nk-1
+        const int nk = max(0, min(32, (ncur - w + W - 1) / W - 32 * k));
         for (int j = 0; j < nk; ++j) {
           const int src = __shfl_sync(0xFFFFFFFFu, cur[k].x, j);
           const int row = __shfl_sync(0xFFFFFFFFu, cur[k].y, j);
@@ -330,12 +333,12 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
 template <typename real>
 __device__ __forceinline__ void ring_setup(Rec<real>& R, const Rec<real>* recs, unsigned char* dyn, uint64_t* full,
                                            uint64_t* empty, int* abort_flag, int stage_bytes, int n_stages,
-                                           int full_arrivals, Layers<real>& Ls, Ring& G) {
+                                           int full_arrivals, int producers, Layers<real>& Ls, Ring& G) {
   if (threadIdx.x == 0) {
     *abort_flag = 0;
     for (int s = 0; s < n_stages; ++s) {
       mbar_init(full + s, full_arrivals);
-      mbar_init(empty + s, (blockDim.x - 32) / 32);
+      mbar_init(empty + s, (blockDim.x - 32 * producers) / 32);
     }
     fence_mbar_init();
   }
@@ -351,40 +354,43 @@ __device__ __forceinline__ void ring_setup(Rec<real>& R, const Rec<real>* recs, 
 }
 
 template <typename real, bool PLASMA, int COPY>
-__global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages) {
+__global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
+                                             int producers) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
   __shared__ int abort_flag;
   Layers<real> Ls;
   Ring G;
-  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? 1 : 32, Ls, G);
+  const int W = producers;
+  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? W : 32 * W, W, Ls, G);
   const int n = R.n_patches_h;
   const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
-  if (threadIdx.x < 32) {
-    produce<COPY>(R, G, p0, p1, n, R.dptr_h, R.desc_h, R.tab_h);
+  if (threadIdx.x < 32 * W) {
+    produce<COPY>(R, G, p0, p1, n, R.dptr_h, R.desc_h, R.tab_h, threadIdx.x / 32, W);
   } else {
-    const int ct = threadIdx.x - 32, nct = blockDim.x - 32;
+    const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     consume_ring(G, p0, p1, [&](const unsigned char* st) { kh_consume<real, PLASMA>(R, Ls, st, ct, nct); });
   }
 }
 
 template <typename real, bool PLASMA, int MAXDEG, int COPY>
 __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
-                                             int istep) {
+                                             int producers, int istep) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
   __shared__ int abort_flag;
   Layers<real> Ls;
   Ring G;
-  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? 1 : 32, Ls, G);
+  const int W = producers;
+  ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? W : 32 * W, W, Ls, G);
   const int n = R.n_patches_e;
   const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
-  if (threadIdx.x < 32) {
-    produce<COPY>(R, G, p0, p1, n, R.dptr_e, R.desc_e, R.tab_e);
+  if (threadIdx.x < 32 * W) {
+    produce<COPY>(R, G, p0, p1, n, R.dptr_e, R.desc_e, R.tab_e, threadIdx.x / 32, W);
   } else {
-    const int ct = threadIdx.x - 32, nct = blockDim.x - 32;
+    const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
     consume_ring(G, p0, p1,
                  [&](const unsigned char* st) { ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current); });

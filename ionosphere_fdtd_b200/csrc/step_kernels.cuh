@@ -37,6 +37,7 @@
 namespace ifdtd {
 
 constexpr int kMaxSpecies = 4;
+constexpr int kMaxSources = 16;
 
 template <typename real>
 struct Rec {
@@ -45,7 +46,6 @@ struct Rec {
   int n_patches_h, fpp_h, n_patches_e, fpp_e;
   int full, si_terms, n_species, plasma_full, magnetized, coef_full;
   int n_src_er, n_src_et;
-  int src_er_vmin, src_er_vmax, src_et_emin, src_et_emax;
   int maxdeg, slot_width, layer_reals;
   // state
   real *er, *et, *hr, *ht, *si_mem;
@@ -76,14 +76,15 @@ struct Rec {
   const unsigned char *tab_h, *tab_e;
   // radial metric rows (padded; staged in shared memory by the kernels)
   const real *invr, *rr, *mid, *invm, *invdr, *invcd;
+  // fused per-layer rows: H-edge (hA, hU, hD), H-face (hC), E-vertex current
+  // weights (vwl, vwu), E-edge radial curl (eU, eD); zero beyond the grid
+  const real *hA, *hU, *hD, *hC, *vwl, *vwu, *eU, *eD;
   real dtmu;             // dt / mu0
   // loss coefficients: (rows, Pn) / (rows, Pm), rows = 1 or V / E
   const real *ca_er, *cb_er, *ca_et, *cb_et;
-  // sources
-  const int *src_er_v, *src_er_k;
-  const real* src_er_c;
-  const int *src_et_e, *src_et_j;
-  const real* src_et_c;
+  // sources (supports listed inline: the record lives in shared memory)
+  int src_er_v[kMaxSources], src_er_k[kMaxSources], src_et_e[kMaxSources], src_et_j[kMaxSources];
+  real src_er_c[kMaxSources], src_et_c[kMaxSources];
   // surface impedance
   real si_metric, si_kappa, si_hist_sum;
   const real *si_scale, *si_decay, *si_drive, *si_hist;
@@ -143,12 +144,14 @@ __device__ __forceinline__ Run<real> zero_run() {
   return r;
 }
 
+// 16-byte store to global memory (outputs are always global; the explicit
+// global store also tells the compiler it cannot alias shared memory).
 template <typename real>
 __device__ __forceinline__ void st16(real* p, const Run<real>& r) {
   if constexpr (sizeof(real) == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
+    __stcg(reinterpret_cast<float4*>(p), make_float4(r.x[0], r.x[1], r.x[2], r.x[3]));
   } else {
-    *reinterpret_cast<double2*>(p) = make_double2(r.x[0], r.x[1]);
+    __stcg(reinterpret_cast<double2*>(p), make_double2(r.x[0], r.x[1]));
   }
 }
 
@@ -156,6 +159,7 @@ __device__ __forceinline__ void st16(real* p, const Run<real>& r) {
 template <typename real>
 struct Layers {
   real *invr, *rr, *invcd, *mid, *invm, *invdr;
+  real *hA, *hU, *hD, *vwl, *vwu, *hC, *eU, *eD;
   real *ca_er, *cb_er, *ca_et, *cb_et;  // compressed coefficient rows (else null)
   real *pc, *bd;                        // compressed plasma rows (else null)
   real *si_decay, *si_drive, *si_hist;  // surface-impedance pole rows (else null)
@@ -164,7 +168,7 @@ struct Layers {
 // Number of reals of per-layer data staged in shared memory (host and device).
 __host__ __device__ inline int layer_reals(int Pn, int Pm, int coef_full, int species, int plasma_full, int magnetized,
                                            int si_terms) {
-  int n = 3 * Pn + 3 * Pm;
+  int n = 8 * Pn + 6 * Pm;
   if (!coef_full) n += 2 * Pn + 2 * Pm;
   if (species > 0 && !plasma_full) n += 6 * species * Pm + (magnetized ? 3 * Pm : 0);
   n += 3 * si_terms;
@@ -204,6 +208,22 @@ __device__ __forceinline__ void load_layers(const Rec<real>& R, real* smem, Laye
   copy_row(Ls.mid, R.mid, Pm);
   copy_row(Ls.invm, R.invm, Pm);
   copy_row(Ls.invdr, R.invdr, Pm);
+  Ls.hA = p; p += Pn;
+  Ls.hU = p; p += Pn;
+  Ls.hD = p; p += Pn;
+  Ls.vwl = p; p += Pn;
+  Ls.vwu = p; p += Pn;
+  Ls.hC = p; p += Pm;
+  Ls.eU = p; p += Pm;
+  Ls.eD = p; p += Pm;
+  copy_row(Ls.hA, R.hA, Pn);
+  copy_row(Ls.hU, R.hU, Pn);
+  copy_row(Ls.hD, R.hD, Pn);
+  copy_row(Ls.vwl, R.vwl, Pn);
+  copy_row(Ls.vwu, R.vwu, Pn);
+  copy_row(Ls.hC, R.hC, Pm);
+  copy_row(Ls.eU, R.eU, Pm);
+  copy_row(Ls.eD, R.eD, Pm);
   Ls.ca_er = Ls.cb_er = Ls.ca_et = Ls.cb_et = nullptr;
   if (!R.coef_full) {
     Ls.ca_er = p; p += Pn;
@@ -242,12 +262,6 @@ __device__ __forceinline__ int fast_div(int n, uint32_t m) { return m ? (int)__u
 __device__ __forceinline__ uint32_t div_magic(int d) { return d == 1 ? 0u : 0xFFFFFFFFu / (uint32_t)d + 1u; }
 
 template <typename real>
-__device__ __forceinline__ real pcoef_at(const Rec<real>& R, const Layers<real>& Ls, int s, int c, int f, int j) {
-  if (!R.plasma_full) return Ls.pc[(s * 6 + c) * R.Pm + j];
-  return __ldg(R.pcoef + (((size_t)(s * 6 + c) * R.nF + f) * R.Pm + j));
-}
-
-template <typename real>
 __device__ __forceinline__ const real* jsum(const Rec<real>& R) {
   return R.n_species > 1 ? R.Jtot : R.J[0];
 }
@@ -265,44 +279,42 @@ __device__ __forceinline__ void member_patch(const int2* block_map, int n_member
 // ---------------------------------------------------------------------------
 // Per-run arithmetic shared by the direct and the pipelined kernels.  Input
 // row pointers and per-entity table pointers may address shared or global
-// memory; outputs are global.
+// memory; outputs are global.  Radial factors come from fused per-layer rows
+// (host-computed in float64, zero beyond the last node or midpoint) loaded as
+// 16-byte vectors, so padding lanes come out zero without per-element tests.
 // ---------------------------------------------------------------------------
 
+// Source supports matching entity `id` exist (one pass over the record's list).
+__device__ __forceinline__ bool source_hit(const int* ids, int n, int id) {
+  bool hit = false;
+  for (int s = 0; s < n; ++s) hit |= ids[s] == id;
+  return hit;
+}
+
 // Ht on nodes k0..k0+N-1 of edge e: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr)/mu0
-// with odd (PEC) Et ghosts (solver.py:877-899, 443-456); the run holding node 0
-// also advances the surface-impedance ADE (surface_impedance.py:225-270).
-// inv_t = 1 / primal edge angle.
+// with odd (PEC) Et ghosts (solver.py:877-899, 443-456):
+//   Ht += (Er_head - Er_tail) / theta_e * hA[k] - Et[k] * hU[k] + Et[k-1] * hD[k]
+// (hA = dt/(mu0 r), hU / hD the upper / lower PEC-ghosted radial difference
+// weights).  The run holding node 0 also advances the surface-impedance ADE
+// (surface_impedance.py:225-270).  inv_t = 1 / primal edge angle.
 template <typename real>
 __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
                                            const real* ert, const real* etr, const real* hto, real* htout,
                                            real inv_t) {
   constexpr int N = Lanes<real>::N;
-  const int L = R.L, Lp1 = L + 1, Pm = R.Pm;
-  const real dtmu = R.dtmu;
-  const Run<real> vh = ld16(erh + k0);
-  const Run<real> vt = ld16(ert + k0);
-  const Run<real> vo = ld16(hto + k0);
-  const Run<real> vu = (k0 < Pm) ? ld16(etr + k0) : zero_run<real>();
-  const real vprev = (k0 > 0 && k0 - 1 < L) ? etr[k0 - 1] : real(0);
+  const Run<real> vh = ld16(erh + k0), vt = ld16(ert + k0), vo = ld16(hto + k0);
+  const Run<real> vu = (k0 < R.Pm) ? ld16(etr + k0) : zero_run<real>();
+  const real vprev = k0 > 0 ? etr[k0 - 1] : real(0);
+  const Run<real> fa = ld16(Ls.hA + k0), fu = ld16(Ls.hU + k0), fd = ld16(Ls.hD + k0);
   Run<real> out;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
-    const int k = k0 + r;
-    const real g = (vh.x[r] - vt.x[r]) * inv_t * Ls.invr[k];
-    real up = (k < L) ? vu.x[r] : real(0);
-    real dn = (k >= 1 && k - 1 < L) ? (r == 0 ? vprev : vu.x[r - 1]) : real(0);
-    real d;
-    if (R.full) {
-      up = (k < L) ? up * Ls.mid[k] : real(0);
-      dn = (k >= 1 && k - 1 < L) ? dn * Ls.mid[k - 1] : real(0);
-      d = (up - dn) * Ls.invcd[k] * Ls.invr[k];
-    } else {
-      d = (up - dn) * Ls.invcd[k];
-    }
-    out.x[r] = (k < Lp1) ? vo.x[r] + (g - d) * dtmu : real(0);
+    const real dn = r == 0 ? vprev : vu.x[r - 1];
+    out.x[r] = vo.x[r] + ((vh.x[r] - vt.x[r]) * inv_t) * fa.x[r] - vu.x[r] * fu.x[r] + dn * fd.x[r];
   }
   if (R.si_terms > 0 && k0 == 0) {
     const int T = R.si_terms;
+    const real dtmu = R.dtmu;
     const real h_old = vo.x[0];
     const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
     const real e1 = R.si_metric * vu.x[0];
@@ -322,10 +334,12 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
 }
 
 // Hr and the plasma current on midpoints j0..j0+N-1 of face f
-// (solver.py:915-921; plasma.py:413-442, 489-501).  The face's (3, Pm) input
-// current rows of species s are at jin0 + s * jin_stride (jin0 == nullptr: the
-// state arrays R.J[s] themselves); outputs go to R.J[s].  fw is the face's
-// circulation row (4 reals) and gp its reconstruction row (12 reals).
+// (solver.py:915-921; plasma.py:413-442, 489-501):
+//   Hr -= (sum_i sign_i theta_i Et_i / A_f) * hC[j],  hC = dt / (mu0 m).
+// The face's (3, Pm) input current rows of species s are at jin0 + s *
+// jin_stride (jin0 == nullptr: the state arrays R.J[s] themselves); outputs go
+// to R.J[s].  fw is the face's circulation row (4 reals) and gp its
+// reconstruction row (12 reals).
 template <typename real, bool PLASMA>
 __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real>& Ls, int f, int j0, const real* et0,
                                            const real* et1, const real* et2, const real* hro, real* hrout,
@@ -333,28 +347,22 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
                                            int jin_stride, real* jtot, const real* fw, const real* gp) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
-  const real dtmu = R.dtmu;
-  const Run<real> a0 = ld16(et0 + j0);
-  const Run<real> a1 = ld16(et1 + j0);
-  const Run<real> a2 = ld16(et2 + j0);
-  const Run<real> hv = ld16(hro + j0);
+  const Run<real> a0 = ld16(et0 + j0), a1 = ld16(et1 + j0), a2 = ld16(et2 + j0);
+  const Run<real> hv = ld16(hro + j0), fc = ld16(Ls.hC + j0);
   const real w0 = fw[0], w1 = fw[1], w2 = fw[2];
   Run<real> hn;
 #pragma unroll
-  for (int r = 0; r < N; ++r) {
-    const int j = j0 + r;
-    hn.x[r] = (j < L) ? hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * Ls.invm[j] * dtmu : real(0);
-  }
+  for (int r = 0; r < N; ++r) hn.x[r] = hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * fc.x[r];
   st16(hrout + j0, hn);
   if (!PLASMA) return;
+  // radial E at midpoints: mean of the three vertices' nodes j and j+1
   const Run<real> na = ld16(pa + j0), nb = ld16(pb + j0), nc = ld16(pc + j0);
-  const bool tail = j0 + N < Pn;
-  const real ta = tail ? pa[j0 + N] : real(0), tb = tail ? pb[j0 + N] : real(0), tc = tail ? pc[j0 + N] : real(0);
-  const real third = real(1) / real(3);
-  real node[N + 1];
+  const bool more = j0 + N < Pn;
+  const real ta = more ? pa[j0 + N] : real(0), tb = more ? pb[j0 + N] : real(0), tc = more ? pc[j0 + N] : real(0);
+  real sum[N + 1];
 #pragma unroll
-  for (int r = 0; r < N; ++r) node[r] = (na.x[r] + nb.x[r] + nc.x[r]) * third;
-  node[N] = (ta + tb + tc) * third;
+  for (int r = 0; r < N; ++r) sum[r] = na.x[r] + nb.x[r] + nc.x[r];
+  sum[N] = ta + tb + tc;
   real rc[3][3], cf[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -362,38 +370,39 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
     for (int c = 0; c < 3; ++c) rc[i][c] = gp[4 * i + c];
     cf[i] = gp[4 * i + 3];
   }
+  const real sixth = real(1) / real(6);
   real E[N][3];
 #pragma unroll
   for (int r = 0; r < N; ++r) {
-    const real rad = real(0.5) * (node[r] + node[r + 1]);
+    const real rad = (sum[r] + sum[r + 1]) * sixth;
 #pragma unroll
     for (int c = 0; c < 3; ++c) E[r][c] = a0.x[r] * rc[0][c] + a1.x[r] * rc[1][c] + a2.x[r] * rc[2][c] + rad * cf[c];
   }
   real tot[N][3];
 #pragma unroll
   for (int r = 0; r < N; ++r) tot[r][0] = tot[r][1] = tot[r][2] = real(0);
+  const bool tail = j0 + N > L;  // the run holds padding midpoints
+  const bool full_rows = R.plasma_full != 0, mag = R.magnetized != 0;
   for (int s = 0; s < R.n_species; ++s) {
     real* jo = R.J[s] + (size_t)f * 3 * Pm;
     const real* ji = jin0 ? jin0 + (size_t)s * jin_stride : jo;
     Run<real> jc[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) jc[c] = ld16(ji + c * Pm + j0);
+    // coefficient rows of species s: decay, cos, sin, parallel drive, drive, cross drive
+    auto crow = [&](int c) -> Run<real> {
+      return full_rows ? ldg16(R.pcoef + ((size_t)(s * 6 + c) * R.nF + f) * Pm + j0) : ld16(Ls.pc + (s * 6 + c) * Pm + j0);
+    };
+    const Run<real> decay = crow(0), cs = crow(1), dre = crow(4);
     Run<real> jn[3];
+    if (mag) {
+      const Run<real> sn = crow(2), dpar = crow(3), dim = crow(5);
+      Run<real> bd[3];
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int j = j0 + r;
-      const real decay = pcoef_at(R, Ls, s, 0, f, j);
-      const real cs = pcoef_at(R, Ls, s, 1, f, j);
-      const real dre = pcoef_at(R, Ls, s, 4, f, j);
-      real nj[3];
-      if (R.magnetized) {
-        const real sn = pcoef_at(R, Ls, s, 2, f, j);
-        const real dpar = pcoef_at(R, Ls, s, 3, f, j);
-        const real dim = pcoef_at(R, Ls, s, 5, f, j);
-        real b[3];
+      for (int c = 0; c < 3; ++c) bd[c] = full_rows ? ldg16(R.bdir + ((size_t)f * 3 + c) * Pm + j0) : ld16(Ls.bd + c * Pm + j0);
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-          b[c] = R.plasma_full ? __ldg(R.bdir + ((size_t)f * 3 + c) * Pm + j) : Ls.bd[c * Pm + j];
+      for (int r = 0; r < N; ++r) {
+        const real b[3] = {bd[0].x[r], bd[1].x[r], bd[2].x[r]};
         const real eb = E[r][0] * b[0] + E[r][1] * b[1] + E[r][2] * b[2];
         real Ep[3], Eq[3], Ex[3];
 #pragma unroll
@@ -418,20 +427,26 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
         Jx[2] = Jq[0] * b[1] - Jq[1] * b[0];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          nj[c] = decay * Jp[c] + dpar * Ep[c] + decay * (cs * Jq[c] + sn * Jx[c]) + dre * Eq[c] + dim * Ex[c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) nj[c] = decay * (cs * jc[c].x[r]) + dre * E[r][c];
+          jn[c].x[r] = decay.x[r] * Jp[c] + dpar.x[r] * Ep[c] + decay.x[r] * (cs.x[r] * Jq[c] + sn.x[r] * Jx[c]) +
+                       dre.x[r] * Eq[c] + dim.x[r] * Ex[c];
       }
+    } else {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const real v = (j < L) ? nj[c] : real(0);
-        jn[c].x[r] = v;
-        tot[r][c] += v;
-      }
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) jn[c].x[r] = decay.x[r] * (cs.x[r] * jc[c].x[r]) + dre.x[r] * E[r][c];
+    }
+    if (tail) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+        if (j0 + r >= L) jn[0].x[r] = jn[1].x[r] = jn[2].x[r] = real(0);
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) st16(jo + c * Pm + j0, jn[c]);
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) tot[r][c] += jn[c].x[r];
+      st16(jo + c * Pm + j0, jn[c]);
+    }
   }
   if (R.n_species > 1) {
 #pragma unroll
@@ -444,20 +459,25 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   }
 }
 
-// Er on nodes k0..k0+N-1 of vertex v (solver.py:929-962; plasma.py:511-526).
-// hrows[q]: Ht row of slot q's edge; jrows[q]: (3, Pm) summed current rows of
-// slot q's face; coef[q] = sign * phi_e / A*_v and wcs[4q..4q+2] = area weight *
-// face centre of slot q (zero in padding slots).
+// Er on nodes k0..k0+N-1 of vertex v (solver.py:929-962; plasma.py:511-526):
+//   Er = Ca Er + Cb (circ_v(Ht) / r - J_r) - source,
+// J_r the vertex's area-averaged radial current at the node (weights vwl / vwu
+// of the midpoints below / above).  hrows[q]: Ht row of slot q's edge;
+// jrows[q]: (3, Pm) summed current rows of slot q's face; coef[q] = sign *
+// phi_e / A*_v and wcs[4q..4q+2] = area weight * face centre of slot q (zero in
+// padding slots).
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int k0,
                                              const real* const* hrows, const real* const* jrows, const real* coef,
                                              const real* wcs, const real* ero, real* erout, real current) {
   constexpr int N = Lanes<real>::N;
-  const int L = R.L, Lp1 = L + 1, Pn = R.Pn, Pm = R.Pm;
+  const int L = R.L, Pn = R.Pn, Pm = R.Pm;
   Run<real> hv[MAXDEG];
 #pragma unroll
   for (int q = 0; q < MAXDEG; ++q) hv[q] = ld16(hrows[q] + k0);
-  const Run<real> ev = ld16(ero + k0);
+  const Run<real> ev = ld16(ero + k0), ir = ld16(Ls.invr + k0);
+  const Run<real> ca = R.coef_full ? ldg16(R.ca_er + (size_t)v * Pn + k0) : ld16(Ls.ca_er + k0);
+  const Run<real> cb = R.coef_full ? ldg16(R.cb_er + (size_t)v * Pn + k0) : ld16(Ls.cb_er + k0);
   real cq[MAXDEG];
 #pragma unroll
   for (int q = 0; q < MAXDEG; ++q) cq[q] = coef[q];
@@ -468,66 +488,70 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
 #pragma unroll
     for (int q = 0; q < MAXDEG; ++q) acc[r] += cq[q] * hv[q].x[r];
   }
-  real jr[N];
+  Run<real> out;
 #pragma unroll
-  for (int r = 0; r < N; ++r) jr[r] = real(0);
+  for (int r = 0; r < N; ++r) out.x[r] = ca.x[r] * ev.x[r] + cb.x[r] * (acc[r] * ir.x[r]);
+  if (R.n_src_er > 0 && source_hit(R.src_er_v, R.n_src_er, v)) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      for (int s = 0; s < R.n_src_er; ++s)
+        if (R.src_er_v[s] == v && R.src_er_k[s] == k0 + r) out.x[r] -= R.src_er_c[s] * current;
+  }
   if (PLASMA) {
-    // radial current at faces (J . centre), area-averaged to the vertex, then to nodes
+    // radial current at faces (J . centre), area-averaged to the vertex, at
+    // midpoints k0-1 .. k0+N-1
     real rav[N + 1];
 #pragma unroll
     for (int r = 0; r <= N; ++r) rav[r] = real(0);
+    const bool in = k0 < Pm, below = k0 >= 1 && k0 - 1 < L;
 #pragma unroll
     for (int q = 0; q < MAXDEG; ++q) {
       const real* wc = wcs + 4 * q;
       const real c0 = wc[0], c1 = wc[1], c2 = wc[2];
       const real* jf = jrows[q];
-      const bool in = k0 < Pm;
       const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
       const Run<real> jy = in ? ld16(jf + Pm + k0) : zero_run<real>();
       const Run<real> jz = in ? ld16(jf + 2 * Pm + k0) : zero_run<real>();
-      if (k0 >= 1 && k0 - 1 < L) rav[0] += jf[k0 - 1] * c0 + jf[Pm + k0 - 1] * c1 + jf[2 * Pm + k0 - 1] * c2;
+      if (below) rav[0] += jf[k0 - 1] * c0 + jf[Pm + k0 - 1] * c1 + jf[2 * Pm + k0 - 1] * c2;
 #pragma unroll
       for (int r = 0; r < N; ++r) rav[r + 1] += jx.x[r] * c0 + jy.x[r] * c1 + jz.x[r] * c2;
     }
+    const Run<real> wl = ld16(Ls.vwl + k0), wu = ld16(Ls.vwu + k0);
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      const int k = k0 + r;
-      jr[r] = (k == 0) ? rav[r + 1] : (k == L ? rav[r] : real(0.5) * (rav[r] + rav[r + 1]));
-    }
-  }
-  Run<real> out;
-#pragma unroll
-  for (int r = 0; r < N; ++r) {
-    const int k = k0 + r;
-    const real ca = R.coef_full ? __ldg(R.ca_er + (size_t)v * Pn + k) : Ls.ca_er[k];
-    const real cb = R.coef_full ? __ldg(R.cb_er + (size_t)v * Pn + k) : Ls.cb_er[k];
-    real x = ca * ev.x[r] + cb * (acc[r] * Ls.invr[k]);
-    if (v >= R.src_er_vmin && v <= R.src_er_vmax) {
-      for (int s = 0; s < R.n_src_er; ++s)
-        if (__ldg(R.src_er_v + s) == v && __ldg(R.src_er_k + s) == k) x -= __ldg(R.src_er_c + s) * current;
-    }
-    if (PLASMA) x -= cb * jr[r];
-    out.x[r] = (k < Lp1) ? x : real(0);
+    for (int r = 0; r < N; ++r) out.x[r] -= cb.x[r] * (wl.x[r] * rav[r] + wu.x[r] * rav[r + 1]);
   }
   st16(erout + k0, out);
 }
 
-// Et on midpoints j0..j0+N-1 of edge e (solver.py:964-989; plasma.py:503-509).
-// inv_p = 1 / dual edge angle; tp = left tangent, 0, right tangent, 0.
+// Et on midpoints j0..j0+N-1 of edge e (solver.py:964-989; plasma.py:503-509):
+//   Et = Ca Et + Cb ((Hr_l - Hr_r) / phi_e / m - Ht[j+1] eU + Ht[j] eD - J_t) - source,
+// eU / eD the radial curl weights of the nodes above / below, J_t the mean of
+// the two faces' currents along the edge.  inv_p = 1 / dual edge angle;
+// tp = left tangent, 0, right tangent, 0.
 template <typename real, bool PLASMA>
 __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int j0, const real* hl,
                                            const real* hq, const real* hto, const real* jl, const real* jq,
                                            const real* eto, real* etout, real current, real inv_p, const real* tp) {
   constexpr int N = Lanes<real>::N;
-  const int L = R.L, Pn = R.Pn, Pm = R.Pm;
-  const Run<real> a = ld16(hl + j0);
-  const Run<real> b = ld16(hq + j0);
-  const Run<real> hv = ld16(hto + j0);
+  const int Pn = R.Pn, Pm = R.Pm;
+  const Run<real> a = ld16(hl + j0), b = ld16(hq + j0), hv = ld16(hto + j0), ev = ld16(eto + j0);
   const real htail = (j0 + N < Pn) ? hto[j0 + N] : real(0);
-  const Run<real> ev = ld16(eto + j0);
-  real jt[N];
+  const Run<real> im = ld16(Ls.invm + j0), fu = ld16(Ls.eU + j0), fd = ld16(Ls.eD + j0);
+  const Run<real> ca = R.coef_full ? ldg16(R.ca_et + (size_t)e * Pm + j0) : ld16(Ls.ca_et + j0);
+  const Run<real> cb = R.coef_full ? ldg16(R.cb_et + (size_t)e * Pm + j0) : ld16(Ls.cb_et + j0);
+  Run<real> out;
 #pragma unroll
-  for (int r = 0; r < N; ++r) jt[r] = real(0);
+  for (int r = 0; r < N; ++r) {
+    const real hnext = (r + 1 < N) ? hv.x[r + 1] : htail;
+    const real g = (a.x[r] - b.x[r]) * inv_p * im.x[r] - hnext * fu.x[r] + hv.x[r] * fd.x[r];
+    out.x[r] = ca.x[r] * ev.x[r] + cb.x[r] * g;
+  }
+  if (R.n_src_et > 0 && source_hit(R.src_et_e, R.n_src_et, e)) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+      for (int s = 0; s < R.n_src_et; ++s)
+        if (R.src_et_e[s] == e && R.src_et_j[s] == j0 + r) out.x[r] -= R.src_et_c[s] * current;
+  }
   if (PLASMA) {
     const real l0 = tp[0], l1 = tp[1], l2 = tp[2];
     const real q0 = tp[4], q1 = tp[5], q2 = tp[6];
@@ -537,27 +561,8 @@ __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real
     for (int r = 0; r < N; ++r) {
       const real left = lx.x[r] * l0 + ly.x[r] * l1 + lz.x[r] * l2;
       const real right = qx.x[r] * q0 + qy.x[r] * q1 + qz.x[r] * q2;
-      jt[r] = real(0.5) * (left + right);
+      out.x[r] -= cb.x[r] * (real(0.5) * (left + right));
     }
-  }
-  Run<real> out;
-#pragma unroll
-  for (int r = 0; r < N; ++r) {
-    const int j = j0 + r;
-    const real hnext = (r + 1 < N) ? hv.x[r + 1] : htail;
-    real g = (a.x[r] - b.x[r]) * inv_p * Ls.invm[j];
-    const real d = R.full ? (Ls.rr[j + 1] * hnext - Ls.rr[j] * hv.x[r]) * Ls.invdr[j] * Ls.invm[j]
-                          : (hnext - hv.x[r]) * Ls.invdr[j];
-    g -= d;
-    const real ca = R.coef_full ? __ldg(R.ca_et + (size_t)e * Pm + j) : Ls.ca_et[j];
-    const real cb = R.coef_full ? __ldg(R.cb_et + (size_t)e * Pm + j) : Ls.cb_et[j];
-    real x = ca * ev.x[r] + cb * g;
-    if (e >= R.src_et_emin && e <= R.src_et_emax) {
-      for (int s = 0; s < R.n_src_et; ++s)
-        if (__ldg(R.src_et_e + s) == e && __ldg(R.src_et_j + s) == j) x -= __ldg(R.src_et_c + s) * current;
-    }
-    if (PLASMA) x -= cb * jt[r];
-    out.x[r] = (j < L) ? x : real(0);
   }
   st16(etout + j0, out);
 }

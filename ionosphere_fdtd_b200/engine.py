@@ -41,13 +41,14 @@ class Tuning:
     CUDA graph, and the kernel family (0 auto: the pipeline wherever two patch
     stages fit in shared memory, 1 direct global gathers, 2 the warp-specialised
     pipeline fed by TMA bulk copies, 3 the same pipeline fed by 16-byte cp.async
-    copies)."""
+    copies), and the copy-issuing warps per pipelined CTA (1 to 4)."""
 
     faces_per_patch: int = 32
     threads: int = 256
     graph_chunk: int = 32
     e_faces_per_patch: int = 16
     staging: int = 0
+    producer_warps: int = 2
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -157,7 +158,7 @@ class Engine:
             pd.vertex_faces = i64(p["vertex_faces"])
             pd.vertex_face_weights = f64(p["vertex_face_weights"])
         t = self.tuning
-        td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging)
+        td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(

@@ -141,12 +141,12 @@ def test_pipeline_and_direct_kernels_agree_bitwise(name, fpp, staging):
     assert staged["_sim"]._engine.status_word() == 0
 
 
-@pytest.mark.parametrize("threads", [32, 128, 352])
-def test_pipeline_compute_warp_count_does_not_change_results(threads):
+@pytest.mark.parametrize("threads,producers", [(32, 1), (128, 4), (352, 1), (256, 2), (64, 3)])
+def test_pipeline_warp_counts_do_not_change_results(threads, producers):
     from ionosphere_fdtd_b200.engine import Tuning
 
     case = C.CASES["plasma_magnetized_s1"]
     ref = run_product(case, "float64", tuning=Tuning(staging=2))
-    other = run_product(case, "float64", tuning=Tuning(staging=2, threads=threads))
+    other = run_product(case, "float64", tuning=Tuning(staging=2, threads=threads, producer_warps=producers))
     for f in STATE:
         np.testing.assert_array_equal(ref[f], other[f])
