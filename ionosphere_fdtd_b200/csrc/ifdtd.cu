@@ -408,8 +408,12 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       !in_range(M->face_edges, 3 * (size_t)nF, nE) || !in_range(M->edge_left_faces, nE, nF) ||
       !in_range(M->edge_right_faces, nE, nF))
     return fail(IFDTD_ERR_ARGUMENT, "mesh index table out of range");
-  const int fpp = (tune && tune->faces_per_patch > 0) ? tune->faces_per_patch : 32;
-  const int fpp_e = (tune && tune->e_faces_per_patch > 0) ? tune->e_faces_per_patch : 16;
+  // patch sizes: > 0 as given; 0 (or no tuning) picks, for the pipelined
+  // kernels, the largest candidate whose stage fits twice in shared memory,
+  // and 32 / 16 faces for the direct kernels
+  const bool auto_h = !(tune && tune->faces_per_patch > 0), auto_e = !(tune && tune->e_faces_per_patch > 0);
+  int fpp = auto_h ? 32 : tune->faces_per_patch;
+  int fpp_e = auto_e ? 16 : tune->e_faces_per_patch;
   const int staging = tune ? tune->staging : 0;
   const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
   const int producers = (tune && tune->producer_warps > 0) ? tune->producer_warps : 2;
@@ -512,50 +516,57 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     for (int v = 0; v < nV; ++v) o.vlist[cursor[owner_v[v] / f_per]++] = v;
     return o;
   };
-  const Own oh = ownership(fpp), oe = ownership(fpp_e);
-  const std::vector<int>& vlist = oe.vlist;
-  P->n_patches = oh.n;
-  P->n_patches_e = oe.n;
+  Own oh = ownership(fpp), oe = ownership(fpp_e);
   // ---- fixed-width vertex slots in vlist order (reference slot order, zero-padded) ----
   int maxdeg = 0;
   for (int v = 0; v < nV; ++v) maxdeg = std::max(maxdeg, deg[v]);
   const int MD = maxdeg <= 6 ? 6 : (maxdeg <= 12 ? 12 : 0);
   if (MD == 0) return fail(IFDTD_ERR_UNSUPPORTED, "vertex degree above 12 is not supported");
   const int SW = round4(MD);
-  std::vector<int> ps_edge((size_t)nV * SW, 0);
-  std::vector<real> ps_coef((size_t)nV * SW, real(0));
-  for (int sl = 0; sl < nV; ++sl) {
-    const int v = vlist[sl];
-    const int q0 = v_off[v], n = v_off[v + 1] - q0;
-    for (int q = 0; q < SW; ++q) {
-      ps_edge[(size_t)sl * SW + q] = v_edge[q0 + (q < n ? q : 0)];
-      ps_coef[(size_t)sl * SW + q] = q < n ? (real)v_coef[q0 + q] : real(0);
-    }
-  }
   P->maxdeg = MD;
-  std::vector<int> ps_face;
-  std::vector<real> ps_wc;
-  if (X->plasma_species > 0) {
-    const int W = X->vertex_face_width;
-    ps_face.assign((size_t)nV * SW, 0);
-    ps_wc.assign((size_t)nV * SW * 4, real(0));
+  struct Slots {
+    std::vector<int> edge, face;
+    std::vector<real> coef, wc;
+  };
+  // slot tables of the vertices in the order `vlist` lists them; false on a bad vertex face table
+  auto build_slots = [&](const std::vector<int>& vlist, Slots& out) {
+    out.edge.assign((size_t)nV * SW, 0);
+    out.coef.assign((size_t)nV * SW, real(0));
     for (int sl = 0; sl < nV; ++sl) {
       const int v = vlist[sl];
-      int n = 0, first = -1;
-      for (int q = 0; q < W; ++q) {
-        const double w = X->vertex_face_weights[(size_t)v * W + q];
-        if (w == 0.0) continue;
-        const int64_t f = X->vertex_faces[(size_t)v * W + q];
-        if (f < 0 || f >= nF) return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range");
-        if (n >= MD) return fail(IFDTD_ERR_ARGUMENT, "vertex face table wider than the vertex degree");
-        if (first < 0) first = (int)f;
-        ps_face[(size_t)sl * SW + n] = (int)f;
-        for (int c = 0; c < 3; ++c) ps_wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
-        ++n;
+      const int q0 = v_off[v], n = v_off[v + 1] - q0;
+      for (int q = 0; q < SW; ++q) {
+        out.edge[(size_t)sl * SW + q] = v_edge[q0 + (q < n ? q : 0)];
+        out.coef[(size_t)sl * SW + q] = q < n ? (real)v_coef[q0 + q] : real(0);
       }
-      for (int q = n; q < SW; ++q) ps_face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
     }
-  }
+    out.face.clear();
+    out.wc.clear();
+    if (X->plasma_species > 0) {
+      const int W = X->vertex_face_width;
+      out.face.assign((size_t)nV * SW, 0);
+      out.wc.assign((size_t)nV * SW * 4, real(0));
+      for (int sl = 0; sl < nV; ++sl) {
+        const int v = vlist[sl];
+        int n = 0, first = -1;
+        for (int q = 0; q < W; ++q) {
+          const double w = X->vertex_face_weights[(size_t)v * W + q];
+          if (w == 0.0) continue;
+          const int64_t f = X->vertex_faces[(size_t)v * W + q];
+          if (f < 0 || f >= nF || n >= MD) return false;
+          if (first < 0) first = (int)f;
+          out.face[(size_t)sl * SW + n] = (int)f;
+          for (int c = 0; c < 3; ++c) out.wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
+          ++n;
+        }
+        for (int q = n; q < SW; ++q) out.face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
+      }
+    }
+    return true;
+  };
+  Slots slots;
+  if (!build_slots(oe.vlist, slots))
+    return fail(IFDTD_ERR_ARGUMENT, "vertex face table out of range or wider than the vertex degree");
 
   const int S = std::max(0, X->plasma_species);
   const bool plasma = S > 0;
@@ -646,10 +657,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     if (_e != cudaSuccess)                                                                              \
       return fail(IFDTD_ERR_CUDA, std::string("upload ") + #field + ": " + cudaGetErrorString(_e));     \
   } while (0)
-  UP(oh.eptr, eptr_h);
-  UP(oe.eptr, eptr_e);
-  UP(oe.vptr, vptr);
-  UP(oe.vlist, vlist);
   UP(th, edge_th);
   UP(lr, edge_lr);
   UP(inv_theta, inv_theta);
@@ -657,8 +664,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   UP(fe, face_e);
   UP(fv, face_v);
   UP(fw, face_w);
-  UP(ps_edge, ps_edge);
-  UP(ps_coef, ps_coef);
   UP(invr, invr);
   UP(rr, rr);
   UP(mid, mid);
@@ -743,8 +748,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
           for (int c = 0; c < 3; ++c) bd[((size_t)i * 3 + c) * Pm + j] = (real)X->plasma_bdir[((size_t)i * L + j) * 3 + c];
       UP(bd, bdir);
     }
-    UP(ps_face, ps_face);
-    UP(ps_wc, ps_wc);
     if (S > 1) {
       cudaError_t e = A.alloc((size_t)nF * 3 * Pm * sizeof(real), &P->d_jtot);
       if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of summed plasma current failed");
@@ -753,13 +756,44 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   }
 
   // ---- pipelined kernels: copy descriptors and table blobs per patch ----
+  const int layer_block = pipe::layer_block_bytes(
+      layer_reals(Pn, Pm, X->coef_rows_er != 1, S, X->plasma_rows == nF && nF != 1, X->plasma_magnetized != 0,
+                  X->si_terms),
+      (int)sizeof(real));
+  const int stage_budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 256 - layer_block;
   if (staging != 1) {
     PipeTables th_tab, te_tab;
     std::vector<int> locA(std::max(nV, std::max(nE, nF)), 0), locB(std::max(nE, nF), 0);
-    P->pipe_h_ok = build_pipe_h<real>(th_tab, oh.n, fpp, nF, oh.eptr, th, fe, fv, inv_theta, fw, pl, S, Pn, Pm, locA,
-                                      locB);
-    P->pipe_e_ok = build_pipe_e<real>(te_tab, oe.n, oe.vptr, oe.vlist, oe.eptr, lr, SW, ps_edge, ps_face, ps_coef,
-                                      ps_wc, inv_phi, tn, plasma, Pn, Pm, locA, locB);
+    const std::vector<int> h_cand = auto_h ? std::vector<int>{64, 32, 16, 8} : std::vector<int>{fpp};
+    const std::vector<int> e_cand = auto_e ? std::vector<int>{32, 16, 8} : std::vector<int>{fpp_e};
+    for (const int c : h_cand) {
+      Own o = ownership(c);
+      PipeTables t;
+      const bool ok = build_pipe_h<real>(t, o.n, c, nF, o.eptr, th, fe, fv, inv_theta, fw, pl, S, Pn, Pm, locA, locB);
+      if (ok && 2 * t.stage_bytes <= stage_budget) {
+        P->pipe_h_ok = true;
+        fpp = c;
+        oh = std::move(o);
+        th_tab = std::move(t);
+        break;
+      }
+    }
+    for (const int c : e_cand) {
+      Own o = ownership(c);
+      Slots sl;
+      if (!build_slots(o.vlist, sl)) break;
+      PipeTables t;
+      const bool ok = build_pipe_e<real>(t, o.n, o.vptr, o.vlist, o.eptr, lr, SW, sl.edge, sl.face, sl.coef, sl.wc,
+                                         inv_phi, tn, plasma, Pn, Pm, locA, locB);
+      if (ok && 2 * t.stage_bytes <= stage_budget) {
+        P->pipe_e_ok = true;
+        fpp_e = c;
+        oe = std::move(o);
+        slots = std::move(sl);
+        te_tab = std::move(t);
+        break;
+      }
+    }
     P->kh_stage = th_tab.stage_bytes;
     P->ke_stage = te_tab.stage_bytes;
     if (P->pipe_h_ok) {
@@ -772,6 +806,18 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       UP(te_tab.desc, desc_e);
       UP(te_tab.tab, tab_e);
     }
+  }
+  P->n_patches = oh.n;
+  P->n_patches_e = oe.n;
+  UP(oh.eptr, eptr_h);
+  UP(oe.eptr, eptr_e);
+  UP(oe.vptr, vptr);
+  UP(oe.vlist, vlist);
+  UP(slots.edge, ps_edge);
+  UP(slots.coef, ps_coef);
+  if (plasma) {
+    UP(slots.face, ps_face);
+    UP(slots.wc, ps_wc);
   }
 #undef UP
 
@@ -801,9 +847,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   if (P->smem_bytes > 200 * 1024) return fail(IFDTD_ERR_UNSUPPORTED, "radial grid too fine for the shared per-layer rows");
   {
     // pipelined kernels: per-layer rows + n_stages ring stages in dynamic shared memory
-    const int layer_block = pipe::layer_block_bytes(R.layer_reals, (int)sizeof(real));
-    const int budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 256 - layer_block;
-    auto stages = [&](bool ok, int stage) { return ok && stage > 0 ? std::min(pipe::kMaxStages, budget / stage) : 0; };
+    if (pipe::layer_block_bytes(R.layer_reals, (int)sizeof(real)) != layer_block)
+      return fail(IFDTD_ERR_UNSUPPORTED, "inconsistent shared per-layer rows");
+    auto stages = [&](bool ok, int stage) {
+      return ok && stage > 0 ? std::min(pipe::kMaxStages, stage_budget / stage) : 0;
+    };
     P->kh_stages = stages(P->pipe_h_ok, P->kh_stage);
     P->ke_stages = stages(P->pipe_e_ok, P->ke_stage);
     P->kh_smem = (size_t)layer_block + (size_t)P->kh_stages * P->kh_stage;

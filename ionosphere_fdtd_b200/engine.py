@@ -35,7 +35,8 @@ class Physics:
 
 @dataclass
 class Tuning:
-    """Launch geometry of a plan: faces per H-phase and E-phase patch, threads
+    """Launch geometry of a plan: faces per H-phase and E-phase patch (0: the
+    largest patch whose pipeline stage fits twice in shared memory), threads
     per CTA (direct kernels, at most 256) or compute threads per CTA besides
     the producer warp (pipelined kernels, at most 352), steps per captured
     CUDA graph, and the kernel family (0 auto: the pipeline wherever two patch
@@ -43,10 +44,10 @@ class Tuning:
     pipeline fed by TMA bulk copies, 3 the same pipeline fed by 16-byte cp.async
     copies), and the copy-issuing warps per pipelined CTA (1 to 4)."""
 
-    faces_per_patch: int = 32
+    faces_per_patch: int = 0
     threads: int = 256
     graph_chunk: int = 32
-    e_faces_per_patch: int = 16
+    e_faces_per_patch: int = 0
     staging: int = 0
     producer_warps: int = 2
 
