@@ -110,10 +110,10 @@ typedef struct ifdtd_physics_desc {
 
 /* Tuning of the launch geometry (0 = defaults). */
 typedef struct ifdtd_tuning {
-  int32_t faces_per_patch;   /* faces owned by one H-phase CTA (default 32) */
-  int32_t threads;           /* threads per direct CTA, or compute threads per pipelined CTA (default 256) */
+  int32_t faces_per_patch;   /* faces owned by one H-phase patch (0: fit the pipeline stage to shared memory) */
+  int32_t threads;           /* threads per direct CTA, or compute threads per pipelined CTA (0: automatic) */
   int32_t graph_chunk;       /* steps captured per CUDA graph (default 32; 0 disables) */
-  int32_t e_faces_per_patch; /* faces whose vertices/edges one E-phase CTA owns (default 16) */
+  int32_t e_faces_per_patch; /* faces whose vertices/edges one E-phase patch owns (0: fit the stage to shared memory) */
   int32_t staging;           /* 0 auto, 1 direct global gathers, 2 pipeline (TMA bulk copies), 3 pipeline (cp.async) */
   int32_t producer_warps;    /* copy-issuing warps per pipelined CTA (default 2, at most 4) */
 } ifdtd_tuning;

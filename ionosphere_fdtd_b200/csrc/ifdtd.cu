@@ -415,10 +415,12 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   int fpp = auto_h ? 32 : tune->faces_per_patch;
   int fpp_e = auto_e ? 16 : tune->e_faces_per_patch;
   const int staging = tune ? tune->staging : 0;
-  const int threads = (tune && tune->threads > 0) ? tune->threads : 256;
+  // threads: > 0 as given; 0 picks 320 compute threads for pipelined CTAs and 256 for direct CTAs
+  const bool auto_threads = !(tune && tune->threads > 0);
+  int threads = auto_threads ? 256 : tune->threads;
   const int producers = (tune && tune->producer_warps > 0) ? tune->producer_warps : 2;
   if (producers > 4) return fail(IFDTD_ERR_ARGUMENT, "producer_warps must be 1 to 4");
-  if (threads % 32 || threads < 32 || threads + 32 * producers > pipe::kMaxThreads)
+  if (!auto_threads && (threads % 32 || threads < 32 || threads + 32 * producers > pipe::kMaxThreads))
     return fail(IFDTD_ERR_ARGUMENT, "threads must be a multiple of 32 and threads + 32 * producer_warps <= 384");
   P->producers = producers;
   if (staging < 0 || staging > 3)
@@ -863,6 +865,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       return fail(IFDTD_ERR_UNSUPPORTED, "pipelined kernels need at least two patch stages in shared memory");
     if ((P->h_mode == 1 || P->e_mode == 1) && threads > 256)
       return fail(IFDTD_ERR_ARGUMENT, "direct kernels take at most 256 threads per CTA");
+    if (auto_threads && P->h_mode == 2 && P->e_mode == 2) threads = pipe::kMaxThreads - 32 * producers;
+    P->threads = threads;
   }
   {
     void* st = nullptr;

@@ -38,14 +38,15 @@ class Tuning:
     """Launch geometry of a plan: faces per H-phase and E-phase patch (0: the
     largest patch whose pipeline stage fits twice in shared memory), threads
     per CTA (direct kernels, at most 256) or compute threads per CTA besides
-    the producer warp (pipelined kernels, at most 352), steps per captured
+    the producer warps (pipelined kernels; 0: 256 direct, 384 - 32 x producer
+    warps pipelined), steps per captured
     CUDA graph, and the kernel family (0 auto: the pipeline wherever two patch
     stages fit in shared memory, 1 direct global gathers, 2 the warp-specialised
     pipeline fed by TMA bulk copies, 3 the same pipeline fed by 16-byte cp.async
     copies), and the copy-issuing warps per pipelined CTA (1 to 4)."""
 
     faces_per_patch: int = 0
-    threads: int = 256
+    threads: int = 0
     graph_chunk: int = 32
     e_faces_per_patch: int = 0
     staging: int = 0
