@@ -137,11 +137,12 @@ int32_t ifdtd_plan_create(const ifdtd_mesh_desc* mesh, const ifdtd_grid_desc* gr
 int32_t ifdtd_plan_destroy(ifdtd_plan* plan);
 /* Row pitches (in elements) the plan expects for node and midpoint arrays. */
 int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* mid_pitch);
-/* Device status word: bit 0 set when a staging wait hit its iteration limit
- * (the step's results are then invalid).  Reading it synchronises the plan's
- * device; reset != 0 clears it. */
+/* Device status word: bit 0 set when a wait of the pipelined kernels ran out
+ * its time bound (the step's results are then invalid).  Reading it
+ * synchronises the plan's device; reset != 0 clears it. */
 int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out);
-/* Which step kernels the plan launches: 1 direct, 2 staged (H phase, E phase). */
+/* Which step kernels the plan launches: 1 direct gathers, 2 shared-memory
+ * pipeline (H phase, E phase). */
 int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode);
 /* Bytes of device memory held by the plan (tables, staging, scratch). */
 int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);
