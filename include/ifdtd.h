@@ -155,6 +155,21 @@ int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);
 int32_t ifdtd_step(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
                    int32_t n_steps, void* stream);
 
+/* Same as ifdtd_step, but allocates no device memory in any call.  It has no
+ * counterpart in the reference.  It is for callers that may not call
+ * cudaMalloc while they run: code between the reservations of a custom memory
+ * pool, host callbacks, or processes whose device memory budget is fixed after
+ * start-up.  The scratch that a step with more than one plasma species needs
+ * (the summed current, F x 3 x mid_pitch reals) lives in a 16 MiB static device
+ * array that every GPU loading this library holds until exit; larger meshes
+ * are rejected with IFDTD_ERR_UNSUPPORTED.  currents may be NULL (zero
+ * source).  The first call on a device looks up the static arrays' device
+ * addresses, so make it before any stream capture.  All calls share the
+ * static arrays: calls that overlap on the GPU (other streams, other plans)
+ * race and must be serialised by the caller. */
+int32_t ifdtd_step_static_scratch(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
+                                  int32_t n_steps, void* stream);
+
 /* The two half steps of one leapfrog step, for callers that drive them
  * separately: the magnetic update (solver.py:877-921) and the electric update
  * with source current I (solver.py:923-989).  ifdtd_step is the pair. */

@@ -118,6 +118,7 @@ _SIGNATURES = {
     "ifdtd_status_word": ([_vp, _i32, C.POINTER(_i32)], _i32),
     "ifdtd_plan_kernels": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_step": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
+    "ifdtd_step_static_scratch": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_update_magnetic": ([_vp, C.POINTER(State), _vp], _i32),
     "ifdtd_update_electric": ([_vp, C.POINTER(State), C.c_double, _vp], _i32),
     "ifdtd_probe_create": ([_vp, _i32, _i32, _i32, _i64p, _i64p, _f64p, C.POINTER(_vp)], _i32),

@@ -1348,3 +1348,111 @@ int32_t ifdtd_dual_cell_circulation(ifdtd_plan* plan, const void* in, int32_t co
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free stepping (no counterpart in the reference).
+//
+// Callers that must not allocate device memory while they run (code that runs
+// between a custom allocator's pool reservations, inside host callbacks, or
+// in processes whose memory budget is fixed after start-up) use
+// ifdtd_step_static_scratch.  A multi-species plasma step needs one scratch
+// buffer, the summed species current (F x 3 x mid_pitch reals) that the H
+// kernel writes and the E kernel reads; the plan allocates it with cudaMalloc.
+// Here it lives in a file-scope device array of kStaticScratchBytes instead,
+// together with a device copy of the launch record that points the kernels
+// at it.  Every GPU that loads this library holds both arrays until the
+// process exits.  In host code the arrays' names are host-side stand-ins, so
+// their device addresses are looked up once per device (with that device
+// current) by cudaGetSymbolAddress and passed to the kernels.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;  // summed plasma current
+constexpr int kStaticMaxDevices = 64;
+static_assert(sizeof(Rec<double>) >= sizeof(Rec<float>), "record size");
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+static __device__ __align__(256) unsigned char g_static_record[sizeof(Rec<double>)];
+static __device__ __align__(256) double g_static_zero_current[1];
+
+struct StaticAddresses {
+  bool ready = false;
+  void* scratch = nullptr;
+  void* record = nullptr;
+  void* zero_current = nullptr;
+};
+StaticAddresses g_static_addresses[kStaticMaxDevices];
+
+// Device addresses of the static arrays on `device` (which must be current);
+// looked up on the first call for that device.
+int static_addresses(int device, StaticAddresses** out) {
+  if (device < 0 || device >= kStaticMaxDevices) return fail(IFDTD_ERR_UNSUPPORTED, "device ordinal too large");
+  StaticAddresses& a = g_static_addresses[device];
+  if (!a.ready) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString(e));
+    a.scratch = p;
+    e = cudaGetSymbolAddress(&p, g_static_record);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static record address: ") + cudaGetErrorString(e));
+    a.record = p;
+    e = cudaGetSymbolAddress(&p, g_static_zero_current);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static current address: ") + cudaGetErrorString(e));
+    a.zero_current = p;
+    a.ready = true;
+  }
+  *out = &a;
+  return IFDTD_OK;
+}
+
+template <typename real>
+int step_static(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int n, cudaStream_t stream) {
+  const size_t need = P->S > 1 ? (size_t)P->nF * 3 * P->Pm * sizeof(real) : 0;
+  if (need > kStaticScratchBytes)
+    return fail(IFDTD_ERR_UNSUPPORTED, "ifdtd_step_static_scratch: the summed plasma current needs " +
+                                           std::to_string(need) + " bytes, above the " +
+                                           std::to_string(kStaticScratchBytes) + "-byte static scratch");
+  int rc = bind_state<real>(P, st, stream);
+  if (rc) return rc;
+  if (n <= 0) return IFDTD_OK;
+  StaticAddresses* A = nullptr;
+  rc = static_addresses(P->device, &A);
+  if (rc) return rc;
+  Rec<real> rec;
+  std::memcpy(&rec, P->h_rec.data(), sizeof(rec));
+  rec.Jtot = P->S > 1 ? static_cast<real*>(A->scratch) : nullptr;
+  rec.cur = currents ? currents : static_cast<const double*>(A->zero_current);
+  // the summed current is fully rewritten each step; clearing it keeps a call
+  // independent of what the previous call left behind
+  if (need) CUDA_TRY(cudaMemsetAsync(A->scratch, 0, need, stream));
+  if (!currents) CUDA_TRY(cudaMemsetAsync(A->zero_current, 0, sizeof(double), stream));
+  // pageable source: copied to staging before the call returns
+  CUDA_TRY(cudaMemcpyAsync(A->record, &rec, sizeof(rec), cudaMemcpyHostToDevice, stream));
+  const Rec<real>* drec = static_cast<const Rec<real>*>(A->record);
+  for (int i = 0; i < n; ++i) {
+    cudaError_t e = P->plasma ? launch_kh_t<real, true>(P, drec, stream) : launch_kh_t<real, false>(P, drec, stream);
+    if (e == cudaSuccess) {
+      const int istep = currents ? i : 0;
+      if (P->maxdeg == 6)
+        e = P->plasma ? launch_ke_t<real, true, 6>(P, drec, istep, stream)
+                      : launch_ke_t<real, false, 6>(P, drec, istep, stream);
+      else
+        e = P->plasma ? launch_ke_t<real, true, 12>(P, drec, istep, stream)
+                      : launch_ke_t<real, false, 12>(P, drec, istep, stream);
+    }
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static-scratch step launch: ") + cudaGetErrorString(e));
+  }
+  return IFDTD_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t ifdtd_step_static_scratch(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
+                                             int32_t n_steps, void* stream) {
+  if (!plan) return fail(IFDTD_ERR_ARGUMENT, "null plan");
+  if (n_steps < 0) return fail(IFDTD_ERR_ARGUMENT, "negative step count");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->dtype == 4 ? step_static<float>(plan, state, currents, n_steps, st)
+                          : step_static<double>(plan, state, currents, n_steps, st);
+}
