@@ -310,9 +310,21 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     const real* hrows[MAXDEG];
     const real* jrows[MAXDEG];
 #pragma unroll
-    for (int q = 0; q < MAXDEG; ++q) {
-      hrows[q] = s_ht + vh[vl * SW + q] * Pn;
-      jrows[q] = PLASMA ? s_J + vj[vl * SW + q] * 3 * Pm : nullptr;
+    for (int q = 0; q < MAXDEG; q += 4) {
+      const int4 h4 = *reinterpret_cast<const int4*>(vh + vl * SW + q);
+      hrows[q] = s_ht + h4.x * Pn;
+      hrows[q + 1] = s_ht + h4.y * Pn;
+      if (q + 2 < MAXDEG) hrows[q + 2] = s_ht + h4.z * Pn;
+      if (q + 3 < MAXDEG) hrows[q + 3] = s_ht + h4.w * Pn;
+      if (PLASMA) {
+        const int4 j4 = *reinterpret_cast<const int4*>(vj + vl * SW + q);
+        jrows[q] = s_J + j4.x * 3 * Pm;
+        jrows[q + 1] = s_J + j4.y * 3 * Pm;
+        if (q + 2 < MAXDEG) jrows[q + 2] = s_J + j4.z * 3 * Pm;
+        if (q + 3 < MAXDEG) jrows[q + 3] = s_J + j4.w * 3 * Pm;
+      } else {
+        for (int i = 0; i < 4 && q + i < MAXDEG; ++i) jrows[q + i] = nullptr;
+      }
     }
     e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, vcoef + vl * SW,
                                        PLASMA ? vwc + vl * SW * 4 : nullptr, s_er + vl * Pn, R.er + (size_t)v * Pn,

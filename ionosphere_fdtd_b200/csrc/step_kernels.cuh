@@ -136,6 +136,18 @@ __device__ __forceinline__ Run<real> ldg16(const real* p) {
   return r;
 }
 
+// Four consecutive reals from a 16-byte aligned address (one or two vector loads).
+template <typename real>
+__device__ __forceinline__ void ld4(const real* p, real (&v)[4]) {
+  if constexpr (sizeof(real) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+
 template <typename real>
 __device__ __forceinline__ Run<real> zero_run() {
   Run<real> r;
@@ -349,7 +361,9 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
   const Run<real> a0 = ld16(et0 + j0), a1 = ld16(et1 + j0), a2 = ld16(et2 + j0);
   const Run<real> hv = ld16(hro + j0), fc = ld16(Ls.hC + j0);
-  const real w0 = fw[0], w1 = fw[1], w2 = fw[2];
+  real wv[4];
+  ld4(fw, wv);
+  const real w0 = wv[0], w1 = wv[1], w2 = wv[2];
   Run<real> hn;
 #pragma unroll
   for (int r = 0; r < N; ++r) hn.x[r] = hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * fc.x[r];
@@ -366,9 +380,11 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   real rc[3][3], cf[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
+    real g[4];
+    ld4(gp + 4 * i, g);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rc[i][c] = gp[4 * i + c];
-    cf[i] = gp[4 * i + 3];
+    for (int c = 0; c < 3; ++c) rc[i][c] = g[c];
+    cf[i] = g[3];
   }
   const real sixth = real(1) / real(6);
   real E[N][3];
@@ -478,9 +494,14 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
   const Run<real> ev = ld16(ero + k0), ir = ld16(Ls.invr + k0);
   const Run<real> ca = R.coef_full ? ldg16(R.ca_er + (size_t)v * Pn + k0) : ld16(Ls.ca_er + k0);
   const Run<real> cb = R.coef_full ? ldg16(R.cb_er + (size_t)v * Pn + k0) : ld16(Ls.cb_er + k0);
-  real cq[MAXDEG];
+  real cq[(MAXDEG + 3) / 4 * 4];
 #pragma unroll
-  for (int q = 0; q < MAXDEG; ++q) cq[q] = coef[q];
+  for (int q = 0; q < MAXDEG; q += 4) {
+    real c4[4];
+    ld4(coef + q, c4);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) cq[q + i] = c4[i];
+  }
   real acc[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) {
@@ -506,7 +527,8 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
     const bool in = k0 < Pm, below = k0 >= 1 && k0 - 1 < L;
 #pragma unroll
     for (int q = 0; q < MAXDEG; ++q) {
-      const real* wc = wcs + 4 * q;
+      real wc[4];
+      ld4(wcs + 4 * q, wc);
       const real c0 = wc[0], c1 = wc[1], c2 = wc[2];
       const real* jf = jrows[q];
       const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
@@ -553,8 +575,11 @@ __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real
         if (R.src_et_e[s] == e && R.src_et_j[s] == j0 + r) out.x[r] -= R.src_et_c[s] * current;
   }
   if (PLASMA) {
-    const real l0 = tp[0], l1 = tp[1], l2 = tp[2];
-    const real q0 = tp[4], q1 = tp[5], q2 = tp[6];
+    real tl[4], tq[4];
+    ld4(tp, tl);
+    ld4(tp + 4, tq);
+    const real l0 = tl[0], l1 = tl[1], l2 = tl[2];
+    const real q0 = tq[0], q1 = tq[1], q2 = tq[2];
     const Run<real> lx = ld16(jl + j0), ly = ld16(jl + Pm + j0), lz = ld16(jl + 2 * Pm + j0);
     const Run<real> qx = ld16(jq + j0), qy = ld16(jq + Pm + j0), qz = ld16(jq + 2 * Pm + j0);
 #pragma unroll
