@@ -196,14 +196,16 @@ int round128(int n) { return (n + 127) / 128 * 128; }
 // H phase (patch = faces [q*fpp, ...) and edges eptr[q]..eptr[q+1]).  Stage:
 // blob, er rows (edge ends and, with plasma, face vertices), et rows (face
 // edges, which include the owned edges), own ht rows, own hr rows, own
-// current rows per species.
+// current rows per species, own surface-impedance pole rows (Tsi reals each).
 template <typename real>
 bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>& eptr, const std::vector<int2>& th,
                   const std::vector<int4>& fe, const std::vector<int4>& fv, const std::vector<real>& inv_theta,
-                  const std::vector<real>& fw, const std::vector<real>& pl, int S, int Pn, int Pm,
-                  std::vector<int>& locA, std::vector<int>& locB) {
+                  const std::vector<real>& fw, const std::vector<real>& pl, int S, int Pn, int Pm, int Tsi,
+                  const double* si_scale, std::vector<int>& locA, std::vector<int>& locB, int max_stage) {
   using namespace pipe;
   const int rb = (int)sizeof(real);
+  if (Tsi > 0 && (Tsi * rb) % 16 != 0) return false;  // pole rows must be whole 16-byte units
+  std::vector<real> sis;
   std::vector<int> er_ids, et_ids;
   std::vector<std::pair<int, int>> er_runs, et_runs;
   std::vector<int4> eloc, floc;
@@ -233,7 +235,7 @@ bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>&
     for (;;) {
       n_er = make_runs(er_ids, gap, er_runs, locA);
       n_et = make_runs(et_ids, gap, et_runs, locB);
-      nd = 1 + (int)er_runs.size() + (int)et_runs.size() + (ne > 0) + (nf > 0 ? 1 + S : 0);
+      nd = 1 + (int)er_runs.size() + (int)et_runs.size() + (ne > 0) + (nf > 0 ? 1 + S : 0) + (Tsi > 0 && ne > 0);
       if (nd <= kMaxDesc || gap >= 64) break;
       gap = 2 * gap + 1;
     }
@@ -257,6 +259,13 @@ bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>&
     head[kh_o_floc] = blob_put(T.tab, base, floc.data(), floc.size() * sizeof(int4));
     head[kh_o_fw] = blob_put(T.tab, base, fw.data() + 4 * (size_t)fa, 4 * (size_t)nf * rb);
     head[kh_o_fpl] = S > 0 ? blob_put(T.tab, base, pl.data() + 12 * (size_t)fa, 12 * (size_t)nf * rb) : head[kh_o_fw];
+    if (Tsi > 0) {
+      sis.resize(ne);
+      for (int el = 0; el < ne; ++el) sis[el] = (real)si_scale[ea + el];
+      head[kh_o_esis] = blob_put(T.tab, base, sis.data(), ne * (size_t)rb);
+    } else {
+      head[kh_o_esis] = head[kh_o_fw];
+    }
     const int B = (int)(T.tab.size() - base);
     head[kh_ea] = ea;
     head[kh_ne] = ne;
@@ -267,7 +276,9 @@ bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>&
     head[kh_o_ht] = head[kh_o_et] + n_et * Pm * rb;
     head[kh_o_hr] = head[kh_o_ht] + ne * Pn * rb;
     head[kh_o_J] = head[kh_o_hr] + nf * Pm * rb;
-    const int end = head[kh_o_J] + S * nf * 3 * Pm * rb;
+    head[kh_o_si] = head[kh_o_J] + S * nf * 3 * Pm * rb;
+    const int end = head[kh_o_si] + ne * Tsi * rb;
+    if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
     add_runs(T.desc, kSrcEr, er_runs, head[kh_o_er], Pn * rb);
@@ -278,6 +289,7 @@ bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>&
       for (int s = 0; s < S; ++s)
         T.desc.push_back(make_int4(kSrcJ0 + s, fa, head[kh_o_J] + s * nf * 3 * Pm * rb, nf * 3 * Pm * rb));
     }
+    if (Tsi > 0 && ne > 0) T.desc.push_back(make_int4(kSrcSi, ea, head[kh_o_si], ne * Tsi * rb));
     T.dptr.push_back((int)T.desc.size());
     T.stage_bytes = std::max(T.stage_bytes, round128(end));
     if (T.tab.size() / 16 >= (size_t)1 << 31) return false;
@@ -294,7 +306,7 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
                   const std::vector<int>& eptr, const std::vector<int2>& lr, int SW, const std::vector<int>& ps_edge,
                   const std::vector<int>& ps_face, const std::vector<real>& ps_coef, const std::vector<real>& ps_wc,
                   const std::vector<real>& inv_phi, const std::vector<real>& tn, bool plasma, int Pn, int Pm,
-                  std::vector<int>& locA, std::vector<int>& locB) {
+                  std::vector<int>& locA, std::vector<int>& locB, int max_stage) {
   using namespace pipe;
   const int rb = (int)sizeof(real);
   std::vector<int> h_ids, f_ids, v_ids, vloc;
@@ -380,6 +392,7 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     head[ke_o_er] = head[ke_o_J] + (plasma ? n_f * 3 * Pm * rb : 0);
     head[ke_o_et] = head[ke_o_er] + nv * Pn * rb;
     const int end = head[ke_o_et] + ne * Pm * rb;
+    if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
     add_runs(T.desc, kSrcHt, h_runs, head[ke_o_ht], Pn * rb);
@@ -771,7 +784,9 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     for (const int c : h_cand) {
       Own o = ownership(c);
       PipeTables t;
-      const bool ok = build_pipe_h<real>(t, o.n, c, nF, o.eptr, th, fe, fv, inv_theta, fw, pl, S, Pn, Pm, locA, locB);
+      const bool ok =
+          build_pipe_h<real>(t, o.n, c, nF, o.eptr, th, fe, fv, inv_theta, fw, pl, S, Pn, Pm, X->si_terms,
+                             X->si_scale, locA, locB, stage_budget / 2);
       if (ok && 2 * t.stage_bytes <= stage_budget) {
         P->pipe_h_ok = true;
         fpp = c;
@@ -786,7 +801,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       if (!build_slots(o.vlist, sl)) break;
       PipeTables t;
       const bool ok = build_pipe_e<real>(t, o.n, o.vptr, o.vlist, o.eptr, lr, SW, sl.edge, sl.face, sl.coef, sl.wc,
-                                         inv_phi, tn, plasma, Pn, Pm, locA, locB);
+                                         inv_phi, tn, plasma, Pn, Pm, locA, locB, stage_budget / 2);
       if (ok && 2 * t.stage_bytes <= stage_budget) {
         P->pipe_e_ok = true;
         fpp_e = c;

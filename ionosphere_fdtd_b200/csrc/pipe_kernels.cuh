@@ -35,12 +35,12 @@ constexpr int kMaxRegs = 168;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;  // bound of one wait (0.5 s)
 
 // Descriptor sources (int4 {src, first row, stage byte offset, bytes}).
-enum Src : int { kSrcEr = 0, kSrcEt = 1, kSrcHt = 2, kSrcHr = 3, kSrcJsum = 4, kSrcTab = 5, kSrcJ0 = 8 };
+enum Src : int { kSrcEr = 0, kSrcEt = 1, kSrcHt = 2, kSrcHr = 3, kSrcJsum = 4, kSrcTab = 5, kSrcSi = 6, kSrcJ0 = 8 };
 
 // H-phase blob header (ints; offsets are bytes from the stage start).
 enum KhHead : int {
   kh_ea, kh_ne, kh_fa, kh_nf, kh_o_er, kh_o_et, kh_o_ht, kh_o_hr, kh_o_J,
-  kh_o_eloc, kh_o_einv, kh_o_floc, kh_o_fw, kh_o_fpl, kh_head_ints = 16
+  kh_o_eloc, kh_o_einv, kh_o_floc, kh_o_fw, kh_o_fpl, kh_o_si, kh_o_esis, kh_head_ints = 16
 };
 // E-phase blob header.
 enum KeHead : int {
@@ -144,6 +144,7 @@ __device__ __forceinline__ const void* desc_source(const Rec<real>& R, const uns
     case kSrcHr: return R.hr + r * R.Pm;
     case kSrcJsum: return jsum(R) + r * 3 * R.Pm;
     case kSrcTab: return tab + r * 16;
+    case kSrcSi: return R.si_mem + r * R.si_terms;
     default: return R.J[(src - kSrcJ0) & (kMaxSpecies - 1)] + r * 3 * R.Pm;
   }
 }
@@ -261,6 +262,9 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
   const int4* floc = reinterpret_cast<const int4*>(st + hd[kh_o_floc]);
   const real* fw = reinterpret_cast<const real*>(st + hd[kh_o_fw]);
   const real* fpl = reinterpret_cast<const real*>(st + hd[kh_o_fpl]);
+  const real* s_si = reinterpret_cast<const real*>(st + hd[kh_o_si]);
+  const real* esis = reinterpret_cast<const real*>(st + hd[kh_o_esis]);
+  const int T = R.si_terms;
   const int Pn = R.Pn, Pm = R.Pm, cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
   for (int it = ct; it < ne * cn; it += nct) {
@@ -268,7 +272,7 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
     const int e = ea + el;
     const int4 loc = eloc[el];
     h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
-               R.ht + (size_t)e * Pn, einv[el]);
+               R.ht + (size_t)e * Pn, einv[el], s_si + el * T, R.si_mem + (size_t)e * T, esis + el);
   }
   for (int it = ct; it < nf * cm; it += nct) {
     const int fl = fast_div(it, mag_cm);

@@ -148,6 +148,17 @@ __device__ __forceinline__ void ld4(const real* p, real (&v)[4]) {
   }
 }
 
+// Four consecutive reals to a 16-byte aligned global address.
+template <typename real>
+__device__ __forceinline__ void st4(real* p, const real (&v)[4]) {
+  if constexpr (sizeof(real) == 4) {
+    __stcg(reinterpret_cast<float4*>(p), make_float4(v[0], v[1], v[2], v[3]));
+  } else {
+    __stcg(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
+    __stcg(reinterpret_cast<double2*>(p + 2), make_double2(v[2], v[3]));
+  }
+}
+
 template <typename real>
 __device__ __forceinline__ Run<real> zero_run() {
   Run<real> r;
@@ -308,11 +319,13 @@ __device__ __forceinline__ bool source_hit(const int* ids, int n, int id) {
 //   Ht += (Er_head - Er_tail) / theta_e * hA[k] - Et[k] * hU[k] + Et[k-1] * hD[k]
 // (hA = dt/(mu0 r), hU / hD the upper / lower PEC-ghosted radial difference
 // weights).  The run holding node 0 also advances the surface-impedance ADE
-// (surface_impedance.py:225-270).  inv_t = 1 / primal edge angle.
+// (surface_impedance.py:225-270) from the edge's pole memory si_in (T reals,
+// shared or global) into si_out (global) with the edge's scale *si_sp.
+// inv_t = 1 / primal edge angle.
 template <typename real>
 __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
                                            const real* ert, const real* etr, const real* hto, real* htout,
-                                           real inv_t) {
+                                           real inv_t, const real* si_in, real* si_out, const real* si_sp) {
   constexpr int N = Lanes<real>::N;
   const Run<real> vh = ld16(erh + k0), vt = ld16(ert + k0), vo = ld16(hto + k0);
   const Run<real> vu = (k0 < R.Pm) ? ld16(etr + k0) : zero_run<real>();
@@ -330,16 +343,38 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
     const real h_old = vo.x[0];
     const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
     const real e1 = R.si_metric * vu.x[0];
-    const real s = __ldg(R.si_scale + e);
-    real* mem = R.si_mem + (size_t)e * T;
+    const real s = *si_sp;
+    const bool vec = (T & 3) == 0;  // pole rows are 16-byte aligned: four poles per vector access
     real hist = real(0);
-    for (int p = 0; p < T; ++p) hist += mem[p] * Ls.si_hist[p];
+    if (vec) {
+      for (int p = 0; p < T; p += 4) {
+        real m4[4], w4[4];
+        ld4(si_in + p, m4);
+        ld4(Ls.si_hist + p, w4);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) hist += m4[i] * w4[i];
+      }
+    } else {
+      for (int p = 0; p < T; ++p) hist += si_in[p] * Ls.si_hist[p];
+    }
     hist *= s;
     const real kap = R.si_kappa;
     const real c = kap * (s * R.si_hist_sum);
     const real h_new = ((real(1) - real(0.5) * c) * h_old + dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
     const real hs = h_new + h_old;
-    for (int p = 0; p < T; ++p) mem[p] = mem[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
+    if (vec) {
+      for (int p = 0; p < T; p += 4) {
+        real m4[4], d4[4], r4[4];
+        ld4(si_in + p, m4);
+        ld4(Ls.si_decay + p, d4);
+        ld4(Ls.si_drive + p, r4);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) m4[i] = m4[i] * d4[i] + hs * r4[i];
+        st4(si_out + p, m4);
+      }
+    } else {
+      for (int p = 0; p < T; ++p) si_out[p] = si_in[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
+    }
     out.x[0] = h_new;
   }
   st16(htout + k0, out);
@@ -615,7 +650,8 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
     const int e = ea + el;
     const int2 th = __ldg(R.edge_th + e);
     h_edge_run(R, Ls, e, (it - el * cn) * N, R.er + (size_t)th.y * Pn, R.er + (size_t)th.x * Pn, R.et + (size_t)e * Pm,
-               R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn, __ldg(R.inv_theta + e));
+               R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn, __ldg(R.inv_theta + e), R.si_mem + (size_t)e * R.si_terms,
+               R.si_mem + (size_t)e * R.si_terms, R.si_scale + e);
   }
   const int fa = patch * R.fpp_h, fb = min(fa + R.fpp_h, R.nF);
   for (int it = threadIdx.x; it < (fb - fa) * cm; it += blockDim.x) {
