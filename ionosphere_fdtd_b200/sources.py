@@ -37,16 +37,48 @@ def geographic_tangent_basis(latitude_deg: float, longitude_deg: float):
     return east, north
 
 
+_SEARCH_CACHE: dict[int, tuple[object, float]] = {}
+
+
+def _face_search_cos(mesh) -> float:
+    """Cosine of a cone half-angle that holds every face: 1 % above the largest
+    angle between a face's circumcentre and its corners, plus 1e-6 rad."""
+
+    hit = _SEARCH_CACHE.get(id(mesh))
+    if hit is not None and hit[0] is mesh:
+        return hit[1]
+    cos_min = 1.0
+    for lo in range(0, mesh.n_faces, 1 << 20):
+        corners = mesh.vertices[mesh.faces[lo : lo + (1 << 20)]]
+        centres = mesh.face_centers[lo : lo + (1 << 20)]
+        cos_min = min(cos_min, float(np.min(np.einsum("fkj,fj->fk", corners, centres))))
+    limit = float(np.cos(min(np.pi, 1.01 * float(np.arccos(np.clip(cos_min, -1.0, 1.0))) + 1.0e-6)))
+    if len(_SEARCH_CACHE) >= 4:
+        _SEARCH_CACHE.clear()
+    _SEARCH_CACHE[id(mesh)] = (mesh, limit)
+    return limit
+
+
 def geographic_face_index(simulation, latitude_deg: float, longitude_deg: float) -> int:
-    """Face containing the direction; nearest circumcentre among ties (sources.py:53-85)."""
+    """Face containing the direction; nearest circumcentre among ties (sources.py:53-85).
+
+    The containment test runs only on faces whose circumcentre lies within
+    the search cone of the direction or of its antipode (the test also
+    accepts a face that holds the antipode); every face the test can accept
+    lies in that set, so the candidates, their order and the choice are those
+    of the test over all faces."""
 
     d = geographic_direction(latitude_deg, longitude_deg)
-    tri = simulation.mesh.vertices[simulation.mesh.faces]
+    mesh = simulation.mesh
+    centres = mesh.face_centers
+    proximity = centres @ d
+    limit = _face_search_cos(mesh)
+    near = np.flatnonzero((proximity >= limit) | (-proximity >= limit))
+    tri = mesh.vertices[mesh.faces[near]]
     sides = np.column_stack([np.einsum("ij,j->i", np.cross(tri[:, k], tri[:, (k + 1) % 3]), d) for k in range(3)])
     inside = np.all(sides >= -1.0e-12, axis=1) | np.all(sides <= 1.0e-12, axis=1)
-    cand = np.flatnonzero(inside)
-    centres = simulation.mesh.face_centers
-    return int(cand[np.argmax(centres[cand] @ d)]) if len(cand) else int(np.argmax(centres @ d))
+    cand = near[inside]
+    return int(cand[np.argmax(proximity[cand])]) if len(cand) else int(np.argmax(proximity))
 
 
 def geographic_distribution(simulation, latitude_deg: float, longitude_deg: float, altitude_m: float):

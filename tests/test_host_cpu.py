@@ -223,3 +223,35 @@ def test_kernel_division_by_magic_multiply_is_exact():
         n = np.arange(0, 1 << 16, dtype=np.uint64)
         q = n if m == 0 else (n * np.uint64(m)) >> np.uint64(32)
         assert np.array_equal(q, n // d), d
+
+
+def test_geographic_face_search_equals_the_full_scan():
+    """The cone-filtered face search picks the face the test over all faces
+    picks (sources.py:53-85), random directions, vertices and edge midpoints."""
+
+    from ionosphere_fdtd_b200 import sources as S
+    from ionosphere_fdtd_b200.mesh import build_geodesic_mesh
+
+    class Sim:
+        pass
+
+    def full_scan(sim, lat, lon):
+        d = S.geographic_direction(lat, lon)
+        tri = sim.mesh.vertices[sim.mesh.faces]
+        sides = np.column_stack([np.einsum("ij,j->i", np.cross(tri[:, k], tri[:, (k + 1) % 3]), d) for k in range(3)])
+        inside = np.all(sides >= -1.0e-12, axis=1) | np.all(sides <= 1.0e-12, axis=1)
+        cand = np.flatnonzero(inside)
+        c = sim.mesh.face_centers
+        return int(cand[np.argmax(c[cand] @ d)]) if len(cand) else int(np.argmax(c @ d))
+
+    rng = np.random.default_rng(7)
+    for sub in (1, 3):
+        sim = Sim()
+        sim.mesh = build_geodesic_mesh(sub)
+        v, e = sim.mesh.vertices, sim.mesh.edges
+        dirs = [v[i] for i in range(0, len(v), 7)]
+        dirs += [(v[a] + v[b]) / np.linalg.norm(v[a] + v[b]) for a, b in e[::11]]
+        points = [(float(np.degrees(np.arcsin(np.clip(u[2], -1, 1)))), float(np.degrees(np.arctan2(u[1], u[0])))) for u in dirs]
+        points += [(float(rng.uniform(-90, 90)), float(rng.uniform(-180, 180))) for _ in range(100)]
+        for lat, lon in points:
+            assert S.geographic_face_index(sim, lat, lon) == full_scan(sim, lat, lon), (sub, lat, lon)
