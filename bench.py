@@ -60,17 +60,60 @@ def measured_peak() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_from_profile(workload: str) -> float | None:
-    """DRAM bytes per leapfrog step from the committed ncu summary, if any."""
+def traffic_from_profile(workload: str) -> dict[str, float]:
+    """DRAM bytes per launch of each step kernel from the committed ncu summary
+    (lines ``dram_bytes_per_launch <kernel>: <bytes>``), if any."""
 
+    out = {}
     path = ROOT / "profiles" / f"fdtd_step_{workload}_traffic.txt"
     try:
         for line in path.read_text().splitlines():
-            if line.startswith("dram_bytes_per_step:"):
-                return float(line.split(":", 1)[1])
+            if line.startswith("dram_bytes_per_launch "):
+                name, value = line[len("dram_bytes_per_launch ") :].split(":", 1)
+                out[name.strip()] = float(value)
     except OSError:
         pass
-    return None
+    return out
+
+
+def kernel_bytes(sim) -> dict[str, int]:
+    """Algorithmic bytes of one launch of each phase kernel: every array it
+    needs read once and every array it updates written once.  H phase: reads
+    Er, Et; reads and writes Hr, Ht, the plasma currents and the surface-
+    impedance memory.  E phase: reads Hr, Ht and the plasma currents; reads and
+    writes Er, Et."""
+
+    item = sim.backend.itemsize
+    e = sum(int(getattr(sim, f).numel()) for f in ("er", "et"))
+    h = sum(int(getattr(sim, f).numel()) for f in ("hr", "ht"))
+    j = sum(int(x.numel()) for x in sim._plasma_coupler.ade.current_density) if sim._plasma_coupler is not None else 0
+    si = int(sim._surface_impedance_ade.memory.numel()) if sim._surface_impedance_ade is not None else 0
+    return {"h_phase": item * (e + 2 * (h + j + si)), "e_phase": item * (h + j + 2 * e)}
+
+
+def phase_times_ms(sim, reps: int, stream) -> dict[str, float]:
+    """Median device time of each phase kernel, CUDA events on the launching stream."""
+
+    import torch
+
+    eng = sim._engine
+    state = sim._state()
+    marks = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(reps)]
+    for _ in range(3):
+        eng.update_magnetic(state)
+        eng.update_electric(state, 0.0)
+    torch.cuda.synchronize()
+    for m in marks:
+        m[0].record(stream)
+        eng.update_magnetic(state)
+        m[1].record(stream)
+        eng.update_electric(state, 0.0)
+        m[2].record(stream)
+    torch.cuda.synchronize()
+    return {
+        "h_phase": statistics.median(m[0].elapsed_time(m[1]) for m in marks),
+        "e_phase": statistics.median(m[1].elapsed_time(m[2]) for m in marks),
+    }
 
 
 class ClockSampler:
@@ -284,17 +327,36 @@ def main() -> None:
     peak, peak_kind = measured_peak()
     step_ms = statistics.median(per_step_ms) / T
     achieved = wl.bytes_per_step / (step_ms / 1e3) / 1e9
+    # per-kernel roofline: each phase kernel timed alone after the timed region
+    phase_ms = phase_times_ms(sim, 50, stream)
+    nbytes = kernel_bytes(sim)
+    modes = sim._engine.kernel_modes
+    names = {"h_phase": "kh_tma" if modes[0] == "pipeline" else "kh_kernel", "e_phase": "ke_tma" if modes[1] == "pipeline" else "ke_kernel"}
     traffic = traffic_from_profile(args.workload)
+    kernels = {
+        phase: {
+            "kernel": names[phase],
+            "launch_ms": phase_ms[phase],
+            "algorithmic_bytes_per_launch": nbytes[phase],
+            "achieved": nbytes[phase] / (phase_ms[phase] / 1e3) / 1e9,
+            "frac": nbytes[phase] / (phase_ms[phase] / 1e3) / 1e9 / peak,
+            "traffic": traffic.get(names[phase]),
+        }
+        for phase in ("h_phase", "e_phase")
+    }
+    top = max(kernels, key=lambda k: kernels[k]["launch_ms"])
     roofline = {
         "bound": "hbm",
-        "kernel": "one leapfrog step (kh_kernel + ke_kernel, CUDA graph)",
-        "achieved": achieved,
+        "kernel": f"{kernels[top]['kernel']} ({top.replace('_', ' ')}, dominant)",
+        "achieved": kernels[top]["achieved"],
         "peak": peak,
-        "peak_source": f"{peak_kind} hbm_gbs",
+        "peak_source": f"{peak_kind} hbm_gbs (burst copy; kernels timed alone)",
         "unit": "GB/s",
-        "frac": achieved / peak,
-        "algorithmic_bytes_per_step": wl.bytes_per_step,
-        "traffic": traffic,
+        "frac": kernels[top]["frac"],
+        "traffic": kernels[top]["traffic"],
+        "algorithmic_bytes_per_launch": kernels[top]["algorithmic_bytes_per_launch"],
+        "kernels": kernels,
+        "step": {"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": wl.bytes_per_step, "ms": step_ms},
     }
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -333,6 +395,7 @@ def main() -> None:
                 "parallelism": f"replicas x{world}",
             },
             "hbm_gbs": achieved,
+            "kernel_modes": list(modes),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -775,7 +775,9 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       layer_reals(Pn, Pm, X->coef_rows_er != 1, S, X->plasma_rows == nF && nF != 1, X->plasma_magnetized != 0,
                   X->si_terms),
       (int)sizeof(real));
-  const int stage_budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 256 - layer_block;
+  // static shared memory of the pipelined kernels: the record, 2 x 8 barriers
+  // and the abort flag, well inside 1 KiB besides the record
+  const int stage_budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 1024 - layer_block;
   if (staging != 1) {
     PipeTables th_tab, te_tab;
     std::vector<int> locA(std::max(nV, std::max(nE, nF)), 0), locB(std::max(nE, nF), 0);
