@@ -531,6 +531,29 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     for (int v = 0; v < nV; ++v) o.vlist[cursor[owner_v[v] / f_per]++] = v;
     return o;
   };
+  // ownership with arbitrary patch boundaries: patch q owns faces [bounds[q], bounds[q+1])
+  // and the edges and vertices whose lowest adjacent / incident face lies there
+  auto ownership_bounds = [&](const std::vector<int>& bounds) {
+    Own o;
+    o.fpp = 0;
+    o.n = (int)bounds.size() - 1;
+    o.eptr.assign(o.n + 1, nE);
+    int e = 0;
+    for (int q = 0; q < o.n; ++q) {
+      while (e < nE && owner_e[e] < bounds[q]) ++e;
+      o.eptr[q] = e;
+    }
+    std::vector<int> patch_of_face(nF);
+    for (int q = 0; q < o.n; ++q)
+      for (int f = bounds[q]; f < bounds[q + 1]; ++f) patch_of_face[f] = q;
+    o.vptr.assign(o.n + 1, 0);
+    o.vlist.assign(nV, 0);
+    for (int v = 0; v < nV; ++v) o.vptr[patch_of_face[owner_v[v]] + 1]++;
+    for (int q = 0; q < o.n; ++q) o.vptr[q + 1] += o.vptr[q];
+    std::vector<int> cursor(o.vptr.begin(), o.vptr.end() - 1);
+    for (int v = 0; v < nV; ++v) o.vlist[cursor[patch_of_face[owner_v[v]]]++] = v;
+    return o;
+  };
   Own oh = ownership(fpp), oe = ownership(fpp_e);
   // ---- fixed-width vertex slots in vlist order (reference slot order, zero-padded) ----
   int maxdeg = 0;
@@ -578,6 +601,92 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       }
     }
     return true;
+  };
+  // E-phase patch boundaries whose staged bytes (the pipelined E stage layout,
+  // before 16-byte run bridging) stay within `cap`: faces are scanned in order
+  // and a patch closes before the face whose owned vertices and edges would
+  // overflow it.
+  std::vector<int> vtx_by_owner_off(nF + 1, 0), vtx_by_owner;
+  for (int v = 0; v < nV; ++v) vtx_by_owner_off[owner_v[v] + 1]++;
+  for (int f = 0; f < nF; ++f) vtx_by_owner_off[f + 1] += vtx_by_owner_off[f];
+  vtx_by_owner.assign(nV, 0);
+  {
+    std::vector<int> cur(vtx_by_owner_off.begin(), vtx_by_owner_off.end() - 1);
+    for (int v = 0; v < nV; ++v) vtx_by_owner[cur[owner_v[v]]++] = v;
+  }
+  auto balanced_e_bounds = [&](int cap, bool with_plasma, int rb) {
+    std::vector<int> bounds{0};
+    std::vector<int> stamp_e(nE, -1), stamp_f(nF, -1);
+    int patch = 0, n_ht = 0, n_f = 0, nv = 0, ne = 0;
+    const int W = X->vertex_face_width;
+    auto a16 = [](long b) { return (b + 15) / 16 * 16; };
+    auto bytes = [&](int h, int fcount, int v, int e) {
+      long blob = 64 + a16(4L * v) + a16(4L * v * SW) * (with_plasma ? 2 : 1) + a16((long)rb * v * SW) +
+                  (with_plasma ? a16(4L * rb * v * SW) : 0) + a16(16L * e) + a16((long)rb * e) +
+                  (with_plasma ? a16(8L * rb * e) : 0);
+      long rows = (long)rb * ((long)h * Pn + (long)fcount * Pm * (with_plasma ? 4 : 1) + (long)v * Pn + (long)e * Pm);
+      return (blob + rows + 127) / 128 * 128;
+    };
+    int e_cursor = 0;
+    std::vector<int> touched_e, touched_f;
+    for (int f = 0; f < nF; ++f) {
+      const int e0 = e_cursor;
+      while (e_cursor < nE && owner_e[e_cursor] == f) ++e_cursor;
+      for (int pass = 0; pass < 2; ++pass) {
+        // pass 0: count what face f's entities add; pass 1: commit them
+        int dh = 0, df = 0;
+        const int mark = pass == 0 ? -2 - patch : patch;  // pass-0 marks are undone below
+        touched_e.clear();
+        touched_f.clear();
+        auto add_e = [&](int id) {
+          if (stamp_e[id] != patch && stamp_e[id] != -2 - patch) {
+            stamp_e[id] = mark;
+            ++dh;
+            if (pass == 0) touched_e.push_back(id);
+          } else if (pass == 1 && stamp_e[id] != patch) {
+            stamp_e[id] = patch;
+          }
+        };
+        auto add_f = [&](int id) {
+          if (stamp_f[id] != patch && stamp_f[id] != -2 - patch) {
+            stamp_f[id] = mark;
+            ++df;
+            if (pass == 0) touched_f.push_back(id);
+          } else if (pass == 1 && stamp_f[id] != patch) {
+            stamp_f[id] = patch;
+          }
+        };
+        for (int k = vtx_by_owner_off[f]; k < vtx_by_owner_off[f + 1]; ++k) {
+          const int v = vtx_by_owner[k];
+          for (int q = v_off[v]; q < v_off[v + 1]; ++q) add_e(v_edge[q]);
+          if (with_plasma)
+            for (int q = 0; q < W; ++q)
+              if (X->vertex_face_weights[(size_t)v * W + q] != 0.0) add_f((int)X->vertex_faces[(size_t)v * W + q]);
+        }
+        for (int e = e0; e < e_cursor; ++e) {
+          add_e(e);
+          add_f(lr[e].x);
+          add_f(lr[e].y);
+        }
+        const int dv = vtx_by_owner_off[f + 1] - vtx_by_owner_off[f], de = e_cursor - e0;
+        if (pass == 0) {
+          for (int id : touched_e) stamp_e[id] = -1;
+          for (int id : touched_f) stamp_f[id] = -1;
+          if ((nv + ne) > 0 && bytes(n_ht + dh, n_f + df, nv + dv, ne + de) > cap) {
+            bounds.push_back(f);  // close the patch before face f
+            ++patch;
+            n_ht = n_f = nv = ne = 0;
+          }
+        } else {
+          n_ht += dh;
+          n_f += df;
+          nv += dv;
+          ne += de;
+        }
+      }
+    }
+    bounds.push_back(nF);
+    return bounds;
   };
   Slots slots;
   if (!build_slots(oe.vlist, slots))
@@ -782,7 +891,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     PipeTables th_tab, te_tab;
     std::vector<int> locA(std::max(nV, std::max(nE, nF)), 0), locB(std::max(nE, nF), 0);
     const std::vector<int> h_cand = auto_h ? std::vector<int>{64, 32, 16, 8} : std::vector<int>{fpp};
-    const std::vector<int> e_cand = auto_e ? std::vector<int>{32, 16, 8} : std::vector<int>{fpp_e};
     for (const int c : h_cand) {
       Own o = ownership(c);
       PipeTables t;
@@ -797,16 +905,22 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
         break;
       }
     }
-    for (const int c : e_cand) {
-      Own o = ownership(c);
+    // E phase: balanced patches for two, then three stages; then fixed face counts
+    std::vector<int> e_try;  // > 0: faces per patch; < 0: balanced for -n stages
+    if (auto_e) e_try = {-2, -3, 32, 16, 8};
+    else e_try = {fpp_e};
+    for (const int c : e_try) {
+      const int stages_wanted = c < 0 ? -c : 2;
+      Own o = c < 0 ? ownership_bounds(balanced_e_bounds(stage_budget / stages_wanted * 97 / 100, plasma, (int)sizeof(real)))
+                    : ownership(c);
       Slots sl;
       if (!build_slots(o.vlist, sl)) break;
       PipeTables t;
       const bool ok = build_pipe_e<real>(t, o.n, o.vptr, o.vlist, o.eptr, lr, SW, sl.edge, sl.face, sl.coef, sl.wc,
-                                         inv_phi, tn, plasma, Pn, Pm, locA, locB, stage_budget / 2);
-      if (ok && 2 * t.stage_bytes <= stage_budget) {
+                                         inv_phi, tn, plasma, Pn, Pm, locA, locB, stage_budget / stages_wanted);
+      if (ok && stages_wanted * t.stage_bytes <= stage_budget) {
         P->pipe_e_ok = true;
-        fpp_e = c;
+        fpp_e = c > 0 ? c : 0;
         oe = std::move(o);
         slots = std::move(sl);
         te_tab = std::move(t);
