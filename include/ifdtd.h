@@ -141,6 +141,12 @@ int32_t ifdtd_plan_layout(const ifdtd_plan* plan, int32_t* node_pitch, int32_t* 
  * its time bound (the step's results are then invalid).  Reading it
  * synchronises the plan's device; reset != 0 clears it. */
 int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out);
+/* Test hook for failure detection (no counterpart in the reference): runs one
+ * bounded wait of the pipelined kernels on an mbarrier that nothing completes.
+ * The wait gives up after its time bound (0.5 s), sets bit 0 of the plan's
+ * status word and returns; waited_seconds receives the time it waited.
+ * Synchronises the stream. */
+int32_t ifdtd_wait_selftest(ifdtd_plan* plan, double* waited_seconds, void* stream);
 /* Which step kernels the plan launches: 1 direct gathers, 2 shared-memory
  * pipeline (H phase, E phase). */
 int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode);

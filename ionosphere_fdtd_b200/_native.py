@@ -117,6 +117,7 @@ _SIGNATURES = {
     "ifdtd_plan_layout": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_status_word": ([_vp, _i32, C.POINTER(_i32)], _i32),
     "ifdtd_plan_kernels": ([_vp, C.POINTER(_i32), C.POINTER(_i32)], _i32),
+    "ifdtd_wait_selftest": ([_vp, C.POINTER(C.c_double), _vp], _i32),
     "ifdtd_step": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_step_static_scratch": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_update_magnetic": ([_vp, C.POINTER(State), _vp], _i32),

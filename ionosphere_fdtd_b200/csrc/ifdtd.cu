@@ -193,6 +193,41 @@ void add_runs(std::vector<int4>& desc, int src, const std::vector<std::pair<int,
 
 int round128(int n) { return (n + 127) / 128 * 128; }
 
+// Check every copy descriptor before upload: a positive multiple of 16 bytes
+// of whole rows, a 16-byte aligned destination inside the patch's stage, source
+// rows inside their array, the blob first and inside the table, and at most
+// 2^20 - 1 bytes per patch (the mbarrier transaction limit).
+bool descriptors_valid(const PipeTables& T, int rb, int Pn, int Pm, int Tsi, int nV, int nE, int nF, int S) {
+  using namespace pipe;
+  for (size_t q = 0; q + 1 < T.dptr.size(); ++q) {
+    long total = 0;
+    for (int d = T.dptr[q]; d < T.dptr[q + 1]; ++d) {
+      const int4 x = T.desc[d];
+      int row = 0;
+      long rows = 0;
+      switch (x.x) {
+        case kSrcEr: row = Pn * rb; rows = nV; break;
+        case kSrcEt: row = Pm * rb; rows = nE; break;
+        case kSrcHt: row = Pn * rb; rows = nE; break;
+        case kSrcHr: row = Pm * rb; rows = nF; break;
+        case kSrcJsum: row = 3 * Pm * rb; rows = S > 0 ? nF : 0; break;
+        case kSrcSi: row = Tsi * rb; rows = Tsi > 0 ? nE : 0; break;
+        case kSrcTab: row = 16; rows = (long)(T.tab.size() / 16); break;
+        default:
+          if (x.x < kSrcJ0 || x.x >= kSrcJ0 + S) return false;
+          row = 3 * Pm * rb;
+          rows = nF;
+      }
+      if (row <= 0 || x.w <= 0 || x.w % 16 || x.w % row || x.z % 16 || x.z < 0 || x.z + x.w > T.stage_bytes) return false;
+      if (x.y < 0 || (long)x.y + x.w / row > rows) return false;
+      if ((x.x == kSrcTab) != (d == T.dptr[q]) || (x.x == kSrcTab && x.z != 0)) return false;
+      total += x.w;
+    }
+    if (total >= (1 << 20)) return false;
+  }
+  return true;
+}
+
 // H phase (patch = faces [q*fpp, ...) and edges eptr[q]..eptr[q+1]).  Stage:
 // blob, er rows (edge ends and, with plasma, face vertices), et rows (face
 // edges, which include the owned edges), own ht rows, own hr rows, own
@@ -927,6 +962,10 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
         break;
       }
     }
+    if (P->pipe_h_ok && !descriptors_valid(th_tab, (int)sizeof(real), Pn, Pm, X->si_terms, nV, nE, nF, S))
+      P->pipe_h_ok = false;
+    if (P->pipe_e_ok && !descriptors_valid(te_tab, (int)sizeof(real), Pn, Pm, 0, nV, nE, nF, plasma ? 1 : 0))
+      P->pipe_e_ok = false;
     P->kh_stage = th_tab.stage_bytes;
     P->ke_stage = te_tab.stage_bytes;
     if (P->pipe_h_ok) {
@@ -1262,6 +1301,23 @@ int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out) {
   CUDA_TRY(cudaMemcpy(&value, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost));
   if (reset) CUDA_TRY(cudaMemset(plan->d_status, 0, sizeof(int)));
   *out = value;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_wait_selftest(ifdtd_plan* plan, double* waited_seconds, void* stream) {
+  if (!plan || !waited_seconds) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* d_ns = nullptr;
+  CUDA_TRY(cudaMalloc(&d_ns, sizeof(unsigned long long)));
+  pipe::wait_selftest_kernel<<<1, 32, 0, st>>>(plan->d_status, d_ns);
+  cudaError_t e = cudaGetLastError();
+  unsigned long long ns = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&ns, d_ns, sizeof(ns), cudaMemcpyDeviceToHost);
+  cudaFree(d_ns);
+  if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("wait self-test: ") + cudaGetErrorString(e));
+  *waited_seconds = (double)ns * 1e-9;
   return IFDTD_OK;
 }
 

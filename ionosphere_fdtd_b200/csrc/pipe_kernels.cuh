@@ -413,5 +413,23 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
   }
 }
 
+// Self-test of the bounded wait: one warp waits, with the kernels' own
+// wait_phase, for a phase of an mbarrier that nothing arrives on.  The wait
+// gives up after kWaitNs, sets bit 0 of *status and the kernel returns; the
+// time waited goes to *waited_ns.
+__global__ void wait_selftest_kernel(int* status, unsigned long long* waited_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    abort_flag = 0;
+  }
+  __syncthreads();
+  const uint64_t t0 = global_ns();
+  const bool ok = __all_sync(0xFFFFFFFFu, wait_phase(&bar, 0u, &abort_flag, status));
+  if (threadIdx.x == 0) *waited_ns = ok ? 0ull : global_ns() - t0;
+}
+
 }  // namespace pipe
 }  // namespace ifdtd

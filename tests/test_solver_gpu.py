@@ -204,3 +204,32 @@ def test_surface_impedance_solver_remains_bounded():
     e1 = max(float(s.er.abs().max()), float(s.et.abs().max()))
     h1 = max(float(s.hr.abs().max()), float(s.ht.abs().max()))
     assert np.isfinite(e1) and np.isfinite(h1) and e1 < 2 * e0 and h1 < 2 * h0
+
+
+def test_bounded_wait_gives_up_reports_and_keeps_the_context():
+    """Failure detection without a fault: a wait of the pipelined kernels on a
+    barrier that nothing completes gives up after its bound (0.5 s), sets bit 0
+    of the status word, and the same context then steps and matches the
+    reference fixture."""
+
+    import ctypes
+
+    import cases as CS
+    from casebuild import golden, grouped_rel_l2, run_product
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    s = sim(small_config(), dtype="float32")
+    eng = s._engine
+    assert eng.kernel_modes == ("pipeline", "pipeline")
+    assert eng.status_word(reset=True) == 0
+    waited = ctypes.c_double()
+    N.check(N.load().ifdtd_wait_selftest(eng.plan, ctypes.byref(waited), eng.backend.stream_handle()), "ifdtd_wait_selftest")
+    assert 0.45 < waited.value < 5.0
+    assert eng.status_word(reset=True) & 1
+    assert eng.status_word() == 0
+    s.step(3)
+    assert eng.status_word() == 0
+    out = run_product(CS.CASES["config4_mini_s2"], "float32")
+    assert max(grouped_rel_l2(out, golden("case_config4_mini_s2")).values()) < 2.0e-5
+    assert out["_sim"]._engine.status_word() == 0
