@@ -30,13 +30,41 @@ CHECKPOINT_VERSION = 4
 SUPPORTED_CHECKPOINT_VERSIONS = (1, 2, 3, CHECKPOINT_VERSION)
 
 
-def save_checkpoint(simulation: Any, path: str | Path) -> Path:
-    """Atomically write the NPZ (checkpoint.py:32-93)."""
+def _device_arrays_to_host(tensors: dict[str, Any]) -> dict[str, np.ndarray]:
+    """Copy device tensors into pinned host buffers with asynchronous copies on
+    the current stream and one synchronisation (instead of a blocking copy per
+    array)."""
+
+    import torch
+
+    hosts = {}
+    for name, t in tensors.items():
+        host = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+        host.copy_(t, non_blocking=True)
+        hosts[name] = host
+    torch.cuda.current_stream().synchronize()
+    return {name: h.numpy() for name, h in hosts.items()}
+
+
+def save_checkpoint(simulation: Any, path: str | Path, *, compress: bool = True) -> Path:
+    """Atomically write the NPZ (checkpoint.py:32-93).
+
+    ``compress=False`` writes the same keys, shapes and dtypes without zlib
+    compression (a stored zip that ``np.load`` reads like the compressed one),
+    for large meshes where compression dominates the save time.  Device arrays
+    come to the host through pinned buffers with one synchronisation."""
 
     destination = Path(path)
     metadata = _metadata(simulation)
     destination.parent.mkdir(parents=True, exist_ok=True)
     ade = simulation._surface_impedance_ade
+    device = {f: getattr(simulation, f) for f in ("er", "et", "hr", "ht")}
+    if ade is not None:
+        device["surface_impedance_memory"] = ade.memory
+    if simulation.plasma is not None:
+        for i, v in enumerate(simulation._plasma_coupler.ade.current_density):
+            device[f"plasma_current_{i}"] = v
+    host = _device_arrays_to_host(device)
     arrays = {
         "metadata": np.asarray(json.dumps(metadata, default=_json_default, sort_keys=True)),
         "mesh_vertices": np.asarray(simulation.mesh.vertices, dtype=np.float64),
@@ -44,23 +72,21 @@ def save_checkpoint(simulation: Any, path: str | Path) -> Path:
         "mesh_face_levels": (
             np.asarray(simulation.mesh.face_levels, dtype=np.int64) if simulation.mesh.face_levels is not None else np.empty(0, dtype=np.int64)
         ),
-        "er": simulation.to_numpy(simulation.er),
-        "et": simulation.to_numpy(simulation.et),
-        "hr": simulation.to_numpy(simulation.hr),
-        "ht": simulation.to_numpy(simulation.ht),
-        "surface_impedance_memory": simulation.to_numpy(ade.memory) if ade is not None else np.empty((0, 0), dtype=np.float64),
+        "er": host["er"],
+        "et": host["et"],
+        "hr": host["hr"],
+        "ht": host["ht"],
+        "surface_impedance_memory": host["surface_impedance_memory"] if ade is not None else np.empty((0, 0), dtype=np.float64),
     }
     if simulation.plasma is not None:
         _, plasma_arrays = simulation.plasma.archive_payload()
         arrays.update({f"plasma_model_{n}": v for n, v in plasma_arrays.items()})
-        arrays.update(
-            {f"plasma_current_{i}": simulation.to_numpy(v) for i, v in enumerate(simulation._plasma_coupler.ade.current_density)}
-        )
+        arrays.update({k: v for k, v in host.items() if k.startswith("plasma_current_")})
     temporary = None
     try:
         with tempfile.NamedTemporaryFile(mode="wb", dir=destination.parent, prefix=f".{destination.name}.", delete=False) as handle:
             temporary = handle.name
-            np.savez_compressed(handle, **arrays)
+            (np.savez_compressed if compress else np.savez)(handle, **arrays)
             handle.flush()
             os.fsync(handle.fileno())
         os.replace(temporary, destination)

@@ -492,10 +492,10 @@ class GeodesicFDTD:
 
     # -- checkpoints -----------------------------------------------------------------
 
-    def save_checkpoint(self, path: str | Path) -> Path:
+    def save_checkpoint(self, path: str | Path, *, compress: bool = True) -> Path:
         from .checkpoint import save_checkpoint
 
-        return save_checkpoint(self, path)
+        return save_checkpoint(self, path, compress=compress)
 
     @classmethod
     def load_checkpoint(

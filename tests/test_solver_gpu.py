@@ -233,3 +233,34 @@ def test_bounded_wait_gives_up_reports_and_keeps_the_context():
     out = run_product(CS.CASES["config4_mini_s2"], "float32")
     assert max(grouped_rel_l2(out, golden("case_config4_mini_s2")).values()) < 2.0e-5
     assert out["_sim"]._engine.status_word() == 0
+
+
+def test_uncompressed_checkpoint_has_the_same_arrays_and_resumes(tmp_path):
+    """save_checkpoint(compress=False): same keys, shapes, dtypes and values as
+    the compressed file (plasma and surface-impedance state included), a stored
+    zip, and a bitwise continuation after loading."""
+
+    import zipfile
+
+    import cases as CS
+    from casebuild import build_product
+
+    case = dict(CS.CASES["config4_mini_s2"], steps=4, material="default")  # checkpoints need the stock material
+    whole = build_product(case, "float32")
+    part = build_product(case, "float32")
+    whole.step(9)
+    part.step(4)
+    packed = part.save_checkpoint(tmp_path / "packed.npz")
+    stored = part.save_checkpoint(tmp_path / "stored.npz", compress=False)
+    with zipfile.ZipFile(stored) as z:
+        assert all(i.compress_type == zipfile.ZIP_STORED for i in z.infolist())
+    with np.load(packed) as a, np.load(stored) as b:
+        assert sorted(a.files) == sorted(b.files)
+        assert any(k.startswith("plasma_current_") for k in a.files) and "surface_impedance_memory" in a.files
+        for k in a.files:
+            assert a[k].dtype == b[k].dtype and a[k].shape == b[k].shape, k
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    resumed = GeodesicFDTD.load_checkpoint(stored, device="cuda")
+    resumed.step(5)
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(resumed.to_numpy(getattr(resumed, f)), whole.to_numpy(getattr(whole, f)))
