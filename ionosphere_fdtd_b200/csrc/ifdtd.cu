@@ -2,6 +2,7 @@
 // launches or CUDA-graph chunks), observation probes, reductions and the
 // ArrayBackend primitives.  Declarations and reference citations: include/ifdtd.h.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -426,7 +427,8 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     head[ke_o_J] = head[ke_o_hr] + n_f * Pm * rb;
     head[ke_o_er] = head[ke_o_J] + (plasma ? n_f * 3 * Pm * rb : 0);
     head[ke_o_et] = head[ke_o_er] + nv * Pn * rb;
-    const int end = head[ke_o_et] + ne * Pm * rb;
+    head[ke_o_rav] = head[ke_o_et] + ne * Pm * rb;  // scratch: radial current per own vertex (not copied)
+    const int end = head[ke_o_rav] + (plasma ? nv * Pm * rb : 0);
     if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
@@ -656,10 +658,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     const int W = X->vertex_face_width;
     auto a16 = [](long b) { return (b + 15) / 16 * 16; };
     auto bytes = [&](int h, int fcount, int v, int e) {
-      long blob = 64 + a16(4L * v) + a16(4L * v * SW) * (with_plasma ? 2 : 1) + a16((long)rb * v * SW) +
+      long blob = 16L * ((pipe::ke_head_ints * 4 + 15) / 16) + a16(4L * v) + a16(4L * v * SW) * (with_plasma ? 2 : 1) + a16((long)rb * v * SW) +
                   (with_plasma ? a16(4L * rb * v * SW) : 0) + a16(16L * e) + a16((long)rb * e) +
                   (with_plasma ? a16(8L * rb * e) : 0);
-      long rows = (long)rb * ((long)h * Pn + (long)fcount * Pm * (with_plasma ? 4 : 1) + (long)v * Pn + (long)e * Pm);
+      long rows = (long)rb * ((long)h * Pn + (long)fcount * Pm * (with_plasma ? 4 : 1) + (long)v * Pn + (long)e * Pm +
+                              (with_plasma ? (long)v * Pm : 0));
       return (blob + rows + 127) / 128 * 128;
     };
     int e_cursor = 0;
@@ -1177,6 +1180,11 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
   int rc = bind_state<real>(P, st, stream);
   if (rc) return rc;
   if (n <= 0) return IFDTD_OK;
+  // NVTX range over the host-side enqueue of these steps (visible to profilers)
+  struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+  } range(probe ? "ifdtd_step_sampled" : "ifdtd_step");
   const int cap = std::max(P->chunk, 1);
   for (int s0 = 0; s0 < n; s0 += cap) {
     const int c = std::min(cap, n - s0);

@@ -45,7 +45,7 @@ enum KhHead : int {
 // E-phase blob header.
 enum KeHead : int {
   ke_nv, ke_ea, ke_ne, ke_o_ht, ke_o_hr, ke_o_J, ke_o_er, ke_o_et, ke_o_vid, ke_o_vh,
-  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_head_ints = 16
+  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_o_rav, ke_head_ints = 20
 };
 
 // Bytes of per-layer rows at the start of dynamic shared memory (host and
@@ -239,7 +239,7 @@ __device__ __forceinline__ void consume_ring(const Ring& G, int p0, int p1, Cons
     const int s = i % G.n_stages;
     const uint32_t ph = (uint32_t)(i / G.n_stages) & 1u;
     if (!__all_sync(0xFFFFFFFFu, wait_phase(G.full + s, ph, G.abort_flag, G.status))) return;
-    consume(G.stages + (size_t)s * G.stage_bytes);
+    consume(G.stages + (size_t)s * G.stage_bytes, s, ph);
     __syncwarp();
     if (lane == 0) mbar_arrive(G.empty + s);
   }
@@ -288,8 +288,8 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
 
 // E phase of one patch from its stage (same arithmetic as ke_kernel).
 template <typename real, bool PLASMA, int MAXDEG>
-__device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, const unsigned char* st, int ct,
-                                           int nct, real current) {
+__device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
+                                           int nct, real current, uint64_t* group, uint32_t ph, const Ring& G) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
   const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne];
@@ -306,13 +306,10 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
   const int4* eloc = reinterpret_cast<const int4*>(st + hd[ke_o_eloc]);
   const real* einv = reinterpret_cast<const real*>(st + hd[ke_o_einv]);
   const real* etan = reinterpret_cast<const real*>(st + hd[ke_o_etan]);
+  real* s_rav = reinterpret_cast<real*>(st + hd[ke_o_rav]);
   const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
-  for (int it = ct; it < nv * cn; it += nct) {
-    const int vl = fast_div(it, mag_cn);
-    const int v = vid[vl];
-    const real* hrows[MAXDEG];
-    const real* jrows[MAXDEG];
+  auto slot_rows = [&](int vl, const real** hrows, const real** jrows) {
 #pragma unroll
     for (int q = 0; q < MAXDEG; q += 4) {
       const int4 h4 = *reinterpret_cast<const int4*>(vh + vl * SW + q);
@@ -330,9 +327,37 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
         for (int i = 0; i < 4 && q + i < MAXDEG; ++i) jrows[q + i] = nullptr;
       }
     }
+  };
+  if (PLASMA) {
+    // pass 1: each owned vertex's radial current at every midpoint, into the
+    // stage's scratch rows; then all compute warps meet on the slot's group
+    // barrier (bounded) before the vertex runs read them
+    for (int it = ct; it < nv * cm; it += nct) {
+      const int vl = fast_div(it, mag_cm);
+      const real* hrows[MAXDEG];
+      const real* jrows[MAXDEG];
+      slot_rows(vl, hrows, jrows);
+      const int j0 = (it - vl * cm) * N;
+      const Run<real> r = vertex_radial_current<real, MAXDEG>(jrows, vwc + vl * SW * 4, j0, Pm);
+      if constexpr (sizeof(real) == 4) {
+        *reinterpret_cast<float4*>(s_rav + vl * Pm + j0) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
+      } else {
+        *reinterpret_cast<double2*>(s_rav + vl * Pm + j0) = make_double2(r.x[0], r.x[1]);
+      }
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(group);
+    if (!__all_sync(0xFFFFFFFFu, wait_phase(group, ph, G.abort_flag, G.status))) return;
+  }
+  for (int it = ct; it < nv * cn; it += nct) {
+    const int vl = fast_div(it, mag_cn);
+    const int v = vid[vl];
+    const real* hrows[MAXDEG];
+    const real* jrows[MAXDEG];
+    slot_rows(vl, hrows, jrows);
     e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, vcoef + vl * SW,
                                        PLASMA ? vwc + vl * SW * 4 : nullptr, s_er + vl * Pn, R.er + (size_t)v * Pn,
-                                       current);
+                                       current, PLASMA ? s_rav + vl * Pm : nullptr);
   }
   for (int it = ct; it < ne * cm; it += nct) {
     const int el = fast_div(it, mag_cm);
@@ -386,7 +411,7 @@ __global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs,
     produce<COPY>(R, G, p0, p1, n, R.dptr_h, R.desc_h, R.tab_h, threadIdx.x / 32, W);
   } else {
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
-    consume_ring(G, p0, p1, [&](const unsigned char* st) { kh_consume<real, PLASMA>(R, Ls, st, ct, nct); });
+    consume_ring(G, p0, p1, [&](const unsigned char* st, int, uint32_t) { kh_consume<real, PLASMA>(R, Ls, st, ct, nct); });
   }
 }
 
@@ -395,11 +420,13 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
                                              int producers, int istep) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
   __shared__ int abort_flag;
   Layers<real> Ls;
   Ring G;
   const int W = producers;
+  if (threadIdx.x == 0)
+    for (int s = 0; s < n_stages; ++s) mbar_init(group + s, (blockDim.x - 32 * W) / 32);  // made visible by ring_setup
   ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? W : 32 * W, W, Ls, G);
   const int n = R.n_patches_e;
   const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
@@ -408,8 +435,9 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
   } else {
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
-    consume_ring(G, p0, p1,
-                 [&](const unsigned char* st) { ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current); });
+    consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
+      ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, group + s, ph, G);
+    });
   }
 }
 

@@ -307,6 +307,39 @@ __device__ __forceinline__ void member_patch(const int2* block_map, int n_member
 // 16-byte vectors, so padding lanes come out zero without per-element tests.
 // ---------------------------------------------------------------------------
 
+// acc + (x*c0 + y*c1 + z*c2) with explicit roundings, so every kernel that
+// accumulates a vertex's radial current gets the same bits.
+__device__ __forceinline__ float rav_term(float acc, float x, float y, float z, float c0, float c1, float c2) {
+  float t = __fmul_rn(x, c0);
+  t = __fmaf_rn(y, c1, t);
+  t = __fmaf_rn(z, c2, t);
+  return __fadd_rn(acc, t);
+}
+__device__ __forceinline__ double rav_term(double acc, double x, double y, double z, double c0, double c1, double c2) {
+  double t = __dmul_rn(x, c0);
+  t = __fma_rn(y, c1, t);
+  t = __fma_rn(z, c2, t);
+  return __dadd_rn(acc, t);
+}
+
+// Radial current of one vertex at midpoints j0..j0+N-1: sum over its face
+// slots of (area weight * face centre) . J (plasma.py:511-526).
+template <typename real, int MAXDEG>
+__device__ __forceinline__ Run<real> vertex_radial_current(const real* const* jrows, const real* wcs, int j0, int Pm) {
+  constexpr int N = Lanes<real>::N;
+  Run<real> acc = zero_run<real>();
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) {
+    real wc[4];
+    ld4(wcs + 4 * q, wc);
+    const real* jf = jrows[q];
+    const Run<real> jx = ld16(jf + j0), jy = ld16(jf + Pm + j0), jz = ld16(jf + 2 * Pm + j0);
+#pragma unroll
+    for (int r = 0; r < N; ++r) acc.x[r] = rav_term(acc.x[r], jx.x[r], jy.x[r], jz.x[r], wc[0], wc[1], wc[2]);
+  }
+  return acc;
+}
+
 // Source supports matching entity `id` exist (one pass over the record's list).
 __device__ __forceinline__ bool source_hit(const int* ids, int n, int id) {
   bool hit = false;
@@ -516,11 +549,13 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
 // of the midpoints below / above).  hrows[q]: Ht row of slot q's edge;
 // jrows[q]: (3, Pm) summed current rows of slot q's face; coef[q] = sign *
 // phi_e / A*_v and wcs[4q..4q+2] = area weight * face centre of slot q (zero in
-// padding slots).
+// padding slots).  rav_row: the vertex's radial current at every midpoint
+// (Pm reals, from vertex_radial_current), or nullptr to accumulate it here.
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int k0,
                                              const real* const* hrows, const real* const* jrows, const real* coef,
-                                             const real* wcs, const real* ero, real* erout, real current) {
+                                             const real* wcs, const real* ero, real* erout, real current,
+                                             const real* rav_row = nullptr) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
   Run<real> hv[MAXDEG];
@@ -560,18 +595,27 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
 #pragma unroll
     for (int r = 0; r <= N; ++r) rav[r] = real(0);
     const bool in = k0 < Pm, below = k0 >= 1 && k0 - 1 < L;
+    if (rav_row) {
+      if (below) rav[0] = rav_row[k0 - 1];
+      if (in) {
+        const Run<real> up = ld16(rav_row + k0);
 #pragma unroll
-    for (int q = 0; q < MAXDEG; ++q) {
-      real wc[4];
-      ld4(wcs + 4 * q, wc);
-      const real c0 = wc[0], c1 = wc[1], c2 = wc[2];
-      const real* jf = jrows[q];
-      const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
-      const Run<real> jy = in ? ld16(jf + Pm + k0) : zero_run<real>();
-      const Run<real> jz = in ? ld16(jf + 2 * Pm + k0) : zero_run<real>();
-      if (below) rav[0] += jf[k0 - 1] * c0 + jf[Pm + k0 - 1] * c1 + jf[2 * Pm + k0 - 1] * c2;
+        for (int r = 0; r < N; ++r) rav[r + 1] = up.x[r];
+      }
+    } else {
 #pragma unroll
-      for (int r = 0; r < N; ++r) rav[r + 1] += jx.x[r] * c0 + jy.x[r] * c1 + jz.x[r] * c2;
+      for (int q = 0; q < MAXDEG; ++q) {
+        real wc[4];
+        ld4(wcs + 4 * q, wc);
+        const real c0 = wc[0], c1 = wc[1], c2 = wc[2];
+        const real* jf = jrows[q];
+        const Run<real> jx = in ? ld16(jf + k0) : zero_run<real>();
+        const Run<real> jy = in ? ld16(jf + Pm + k0) : zero_run<real>();
+        const Run<real> jz = in ? ld16(jf + 2 * Pm + k0) : zero_run<real>();
+        if (below) rav[0] = rav_term(rav[0], jf[k0 - 1], jf[Pm + k0 - 1], jf[2 * Pm + k0 - 1], c0, c1, c2);
+#pragma unroll
+        for (int r = 0; r < N; ++r) rav[r + 1] = rav_term(rav[r + 1], jx.x[r], jy.x[r], jz.x[r], c0, c1, c2);
+      }
     }
     const Run<real> wl = ld16(Ls.vwl + k0), wu = ld16(Ls.vwu + k0);
 #pragma unroll
