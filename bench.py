@@ -168,6 +168,18 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest value over all ranks (every rank gets it); ``dist`` None = one rank."""
+
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def build(workload: str, device: str):
     from ionosphere_fdtd_b200 import workloads as W
 
@@ -295,9 +307,7 @@ def main() -> None:
     elapsed_ms = start.elapsed_time(stop)
     per_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
     if dist:
-        t = torch.tensor([elapsed_ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+        elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
         dist.barrier()
     total_cells = wl.cells * T * args.steps * world
     value = total_cells / (elapsed_ms / 1e3) / 1e9
@@ -313,9 +323,7 @@ def main() -> None:
         t1 = time.perf_counter()
         wall = t1 - t0
         if dist:
-            t = torch.tensor([wall], device=device, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+            wall = max_over_ranks(wall, dist, device)
         e2e = {
             "value": wl.cells * T * args.steps * world / wall / 1e9,
             "unit": UNIT,

@@ -1,0 +1,68 @@
+"""Multi-rank plumbing of bench.py on CPU (gloo, world size 2): the timing
+reduction gives every rank the maximum over ranks, and the reference arm does
+its work on rank 0 only."""
+
+import os
+import socket
+import sys
+from pathlib import Path
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, out) -> None:
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        out[rank] = bench.max_over_ranks(10.0 * (rank + 1), dist, "cpu")
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_timing_is_the_maximum_over_ranks():
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as manager:
+        out = manager.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        assert dict(out) == {0: 20.0, 1: 20.0}
+
+
+def test_single_rank_reduction_is_the_value():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+
+
+def test_reference_arm_works_on_rank_zero_only(capsys):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    class Args:
+        workload, steps, warmup, gpus = "config2", 1, 0, 2
+
+    bench.reference_arm(Args, world=2, rank=1)  # returns at once: no oracle run, no output
+    assert capsys.readouterr().out == ""
