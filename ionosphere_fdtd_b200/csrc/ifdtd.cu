@@ -313,7 +313,8 @@ bool build_pipe_h(PipeTables& T, int n, int fpp, int nF, const std::vector<int>&
     head[kh_o_hr] = head[kh_o_ht] + ne * Pn * rb;
     head[kh_o_J] = head[kh_o_hr] + nf * Pm * rb;
     head[kh_o_si] = head[kh_o_J] + S * nf * 3 * Pm * rb;
-    const int end = head[kh_o_si] + ne * Tsi * rb;
+    head[kh_o_hnew] = head[kh_o_si] + ne * Tsi * rb;  // scratch: node-0 Ht of the owned edges (not copied)
+    const int end = head[kh_o_hnew] + (pipe::si_lane_groups(Tsi) ? (ne * rb + 15) / 16 * 16 : 0);
     if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));

@@ -40,7 +40,7 @@ enum Src : int { kSrcEr = 0, kSrcEt = 1, kSrcHt = 2, kSrcHr = 3, kSrcJsum = 4, k
 // H-phase blob header (ints; offsets are bytes from the stage start).
 enum KhHead : int {
   kh_ea, kh_ne, kh_fa, kh_nf, kh_o_er, kh_o_et, kh_o_ht, kh_o_hr, kh_o_J,
-  kh_o_eloc, kh_o_einv, kh_o_floc, kh_o_fw, kh_o_fpl, kh_o_si, kh_o_esis, kh_head_ints = 16
+  kh_o_eloc, kh_o_einv, kh_o_floc, kh_o_fw, kh_o_fpl, kh_o_si, kh_o_esis, kh_o_hnew, kh_head_ints = 20
 };
 // E-phase blob header.
 enum KeHead : int {
@@ -246,9 +246,16 @@ __device__ __forceinline__ void consume_ring(const Ring& G, int p0, int p1, Cons
 }
 
 // H phase of one patch from its stage (same arithmetic as kh_kernel).
+// Surface-impedance poles are handled by groups of T/4 lanes when T/4 is a
+// power of two up to 32 (so a group never straddles a warp).
+__host__ __device__ inline bool si_lane_groups(int T) {
+  const int q = T / 4;
+  return T > 0 && (T & 3) == 0 && q <= 32 && (q & (q - 1)) == 0;
+}
+
 template <typename real, bool PLASMA>
-__device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real>& Ls, const unsigned char* st, int ct,
-                                           int nct) {
+__device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
+                                           int nct, uint64_t* group, uint32_t ph, const Ring& G) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
   const int ea = hd[kh_ea], ne = hd[kh_ne], fa = hd[kh_fa], nf = hd[kh_nf];
@@ -264,15 +271,46 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
   const real* fpl = reinterpret_cast<const real*>(st + hd[kh_o_fpl]);
   const real* s_si = reinterpret_cast<const real*>(st + hd[kh_o_si]);
   const real* esis = reinterpret_cast<const real*>(st + hd[kh_o_esis]);
+  real* s_hnew = reinterpret_cast<real*>(st + hd[kh_o_hnew]);
   const int T = R.si_terms;
+  const bool si_pass = si_lane_groups(T);
   const int Pn = R.Pn, Pm = R.Pm, cn = Pn / N, cm = Pm / N;
   const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  if (si_pass) {
+    // each owned edge's surface-impedance ADE on T/4 lanes (four poles each):
+    // partial history sums gathered in pole order, the node-0 Ht into the
+    // stage's scratch, then all compute warps meet on the slot's group barrier
+    const int Q = T / 4, lane = threadIdx.x & 31, n_it = ne * Q;
+    for (int base = ct - lane; base < n_it; base += nct) {
+      const int it = min(base + lane, n_it - 1);
+      const int el = it / Q, qd = it - el * Q;
+      const int e = ea + el;
+      const int4 loc = eloc[el];
+      const real* mem = s_si + el * T;
+      const real part = si_quad(mem + 4 * qd, Ls.si_hist + 4 * qd);
+      const int first = lane - qd;
+      real hist = __shfl_sync(0xFFFFFFFFu, part, first);
+      for (int q = 1; q < Q; ++q) hist = add_rn(hist, __shfl_sync(0xFFFFFFFFu, part, first + q));
+      const real h_old = s_ht[el * Pn];
+      const real g0 = (s_er[loc.y * Pn] - s_er[loc.x * Pn]) * einv[el] * Ls.invr[0];
+      const real e1 = R.si_metric * s_et[loc.z * Pm];
+      const real h_new = si_boundary(R, h_old, g0, e1, esis[el], hist);
+      if (base + lane < n_it) {
+        si_update_quad(mem + 4 * qd, R.si_mem + (size_t)e * T + 4 * qd, Ls, 4 * qd, h_new + h_old);
+        if (qd == 0) s_hnew[el] = h_new;
+      }
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(group);
+    if (!__all_sync(0xFFFFFFFFu, wait_phase(group, ph, G.abort_flag, G.status))) return;
+  }
   for (int it = ct; it < ne * cn; it += nct) {
     const int el = fast_div(it, mag_cn);
     const int e = ea + el;
     const int4 loc = eloc[el];
     h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
-               R.ht + (size_t)e * Pn, einv[el], s_si + el * T, R.si_mem + (size_t)e * T, esis + el);
+               R.ht + (size_t)e * Pn, einv[el], s_si + el * T, R.si_mem + (size_t)e * T, esis + el,
+               si_pass ? s_hnew + el : nullptr);
   }
   for (int it = ct; it < nf * cm; it += nct) {
     const int fl = fast_div(it, mag_cm);
@@ -399,11 +437,13 @@ __global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs,
                                              int producers) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
   __shared__ int abort_flag;
   Layers<real> Ls;
   Ring G;
   const int W = producers;
+  if (threadIdx.x == 0)
+    for (int s = 0; s < n_stages; ++s) mbar_init(group + s, (blockDim.x - 32 * W) / 32);  // made visible by ring_setup
   ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? W : 32 * W, W, Ls, G);
   const int n = R.n_patches_h;
   const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
@@ -411,7 +451,9 @@ __global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs,
     produce<COPY>(R, G, p0, p1, n, R.dptr_h, R.desc_h, R.tab_h, threadIdx.x / 32, W);
   } else {
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
-    consume_ring(G, p0, p1, [&](const unsigned char* st, int, uint32_t) { kh_consume<real, PLASMA>(R, Ls, st, ct, nct); });
+    consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
+      kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G);
+    });
   }
 }
 

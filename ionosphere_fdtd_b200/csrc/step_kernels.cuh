@@ -347,18 +347,79 @@ __device__ __forceinline__ bool source_hit(const int* ids, int n, int id) {
   return hit;
 }
 
+// ---- surface-impedance ADE pieces (surface_impedance.py:225-270) ----
+// History sum of four poles: explicit fused multiply-adds in pole order.
+__device__ __forceinline__ float si_quad(const float* m, const float* w) {
+  float m4[4], w4[4];
+  ld4(m, m4);
+  ld4(w, w4);
+  float a = __fmul_rn(m4[0], w4[0]);
+  a = __fmaf_rn(m4[1], w4[1], a);
+  a = __fmaf_rn(m4[2], w4[2], a);
+  return __fmaf_rn(m4[3], w4[3], a);
+}
+__device__ __forceinline__ double si_quad(const double* m, const double* w) {
+  double m4[4], w4[4];
+  ld4(m, m4);
+  ld4(w, w4);
+  double a = __dmul_rn(m4[0], w4[0]);
+  a = __fma_rn(m4[1], w4[1], a);
+  a = __fma_rn(m4[2], w4[2], a);
+  return __fma_rn(m4[3], w4[3], a);
+}
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// Pole history sum: quads of four poles, added in pole order (the order the
+// four-lane pass reproduces); poles one by one when T is not a multiple of 4.
+template <typename real>
+__device__ __forceinline__ real si_history(const real* mem, const real* w, int T) {
+  if ((T & 3) == 0) {
+    real h = si_quad(mem, w);
+    for (int p = 4; p < T; p += 4) h = add_rn(h, si_quad(mem + p, w + p));
+    return h;
+  }
+  real h = real(0);
+  for (int p = 0; p < T; ++p) h += mem[p] * w[p];
+  return h;
+}
+
+// New node-0 Ht from the old value, the surface gradient term g0, the Et term
+// e1, the edge's scale s and the pole history sum.
+template <typename real>
+__device__ __forceinline__ real si_boundary(const Rec<real>& R, real h_old, real g0, real e1, real s, real hist) {
+  hist *= s;
+  const real kap = R.si_kappa;
+  const real c = kap * (s * R.si_hist_sum);
+  return ((real(1) - real(0.5) * c) * h_old + R.dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
+}
+
+// Poles p..p+3 of the memory: mem = mem * decay + (h_new + h_old) * drive.
+template <typename real>
+__device__ __forceinline__ void si_update_quad(const real* in, real* out, const Layers<real>& Ls, int p, real hs) {
+  real m4[4], d4[4], r4[4];
+  ld4(in, m4);
+  ld4(Ls.si_decay + p, d4);
+  ld4(Ls.si_drive + p, r4);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) m4[i] = m4[i] * d4[i] + hs * r4[i];
+  st4(out, m4);
+}
+
 // Ht on nodes k0..k0+N-1 of edge e: d/dt Ht = (grad_s Er - (1/r) d(m Et)/dr)/mu0
 // with odd (PEC) Et ghosts (solver.py:877-899, 443-456):
 //   Ht += (Er_head - Er_tail) / theta_e * hA[k] - Et[k] * hU[k] + Et[k-1] * hD[k]
 // (hA = dt/(mu0 r), hU / hD the upper / lower PEC-ghosted radial difference
 // weights).  The run holding node 0 also advances the surface-impedance ADE
 // (surface_impedance.py:225-270) from the edge's pole memory si_in (T reals,
-// shared or global) into si_out (global) with the edge's scale *si_sp.
+// shared or global) into si_out (global) with the edge's scale *si_sp, unless
+// hnew points at the node-0 value a separate pass already advanced.
 // inv_t = 1 / primal edge angle.
 template <typename real>
 __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
                                            const real* ert, const real* etr, const real* hto, real* htout,
-                                           real inv_t, const real* si_in, real* si_out, const real* si_sp) {
+                                           real inv_t, const real* si_in, real* si_out, const real* si_sp,
+                                           const real* hnew = nullptr) {
   constexpr int N = Lanes<real>::N;
   const Run<real> vh = ld16(erh + k0), vt = ld16(ert + k0), vo = ld16(hto + k0);
   const Run<real> vu = (k0 < R.Pm) ? ld16(etr + k0) : zero_run<real>();
@@ -371,44 +432,23 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
     out.x[r] = vo.x[r] + ((vh.x[r] - vt.x[r]) * inv_t) * fa.x[r] - vu.x[r] * fu.x[r] + dn * fd.x[r];
   }
   if (R.si_terms > 0 && k0 == 0) {
-    const int T = R.si_terms;
-    const real dtmu = R.dtmu;
-    const real h_old = vo.x[0];
-    const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
-    const real e1 = R.si_metric * vu.x[0];
-    const real s = *si_sp;
-    const bool vec = (T & 3) == 0;  // pole rows are 16-byte aligned: four poles per vector access
-    real hist = real(0);
-    if (vec) {
-      for (int p = 0; p < T; p += 4) {
-        real m4[4], w4[4];
-        ld4(si_in + p, m4);
-        ld4(Ls.si_hist + p, w4);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) hist += m4[i] * w4[i];
-      }
+    if (hnew) {
+      out.x[0] = *hnew;  // advanced by the patch's surface-impedance pass
     } else {
-      for (int p = 0; p < T; ++p) hist += si_in[p] * Ls.si_hist[p];
-    }
-    hist *= s;
-    const real kap = R.si_kappa;
-    const real c = kap * (s * R.si_hist_sum);
-    const real h_new = ((real(1) - real(0.5) * c) * h_old + dtmu * g0 - kap * e1 + kap * hist) / (real(1) + real(0.5) * c);
-    const real hs = h_new + h_old;
-    if (vec) {
-      for (int p = 0; p < T; p += 4) {
-        real m4[4], d4[4], r4[4];
-        ld4(si_in + p, m4);
-        ld4(Ls.si_decay + p, d4);
-        ld4(Ls.si_drive + p, r4);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) m4[i] = m4[i] * d4[i] + hs * r4[i];
-        st4(si_out + p, m4);
+      const int T = R.si_terms;
+      const real h_old = vo.x[0];
+      const real g0 = (vh.x[0] - vt.x[0]) * inv_t * Ls.invr[0];
+      const real e1 = R.si_metric * vu.x[0];
+      const real s = *si_sp;
+      const real h_new = si_boundary(R, h_old, g0, e1, s, si_history(si_in, Ls.si_hist, T));
+      const real hs = h_new + h_old;
+      if ((T & 3) == 0) {
+        for (int p = 0; p < T; p += 4) si_update_quad(si_in + p, si_out + p, Ls, p, hs);
+      } else {
+        for (int p = 0; p < T; ++p) si_out[p] = si_in[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
       }
-    } else {
-      for (int p = 0; p < T; ++p) si_out[p] = si_in[p] * Ls.si_decay[p] + hs * Ls.si_drive[p];
+      out.x[0] = h_new;
     }
-    out.x[0] = h_new;
   }
   st16(htout + k0, out);
 }
