@@ -49,6 +49,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-drift", action="store_true", help="skip the float32-vs-float64 drift run")
     return p.parse_args()
 
 
@@ -180,15 +181,37 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
-def build(workload: str, device: str):
+def build(workload: str, device: str, dtype: str = "float32"):
     from ionosphere_fdtd_b200 import workloads as W
 
     if workload == "config4":
-        wl = W.config4(device=device)
+        wl = W.config4(device=device, dtype=dtype)
     else:
-        wl = W.config2(device=device)
+        wl = W.config2(device=device, dtype=dtype)
     W.seed_fields(wl.simulation)
     return wl
+
+
+def fp32_drift(workload: str, device: str, steps: int) -> dict:
+    """Relative L2 per (E, H) group between float32 and float64 runs of the
+    engine from the same seeded state (the float64 run stands in for the
+    float64 NumPy path, far too slow at these sizes) after ``steps`` steps."""
+
+    import torch
+
+    out = {}
+    sims = {}
+    for dtype in ("float64", "float32"):
+        sim = build(workload, device, dtype).simulation
+        sim.step(steps)
+        sims[dtype] = {f: getattr(sim, f).to(torch.float64) for f in ("er", "et", "hr", "ht")}
+        del sim
+        torch.cuda.empty_cache()
+    for name, group in (("E", ("er", "et")), ("H", ("hr", "ht"))):
+        a = torch.cat([sims["float32"][f].flatten() for f in group])
+        b = torch.cat([sims["float64"][f].flatten() for f in group])
+        out[f"rel_l2_{name}"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    return {"steps": steps, **out, "against": "float64 engine from the same seeded state"}
 
 
 def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
@@ -366,6 +389,23 @@ def main() -> None:
         "kernels": kernels,
         "step": {"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": wl.bytes_per_step, "ms": step_ms},
     }
+    config = {
+        "workload": args.workload,
+        "subdivision": sim.config.subdivision,
+        "radial_cells": sim.config.radial_cells,
+        "cells": wl.cells,
+        "time_steps_per_step": T,
+        "plasma": "drude (1 species)",
+        "surface_impedance": sim._surface_impedance_ade is not None,
+        "receivers": int(wl.receivers[0].shape[0]),
+        "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
+        "parallelism": f"replicas x{world}",
+    }
+    drift = None
+    if rank == 0 and world == 1 and not args.no_drift:
+        del wl, sim
+        torch.cuda.empty_cache()
+        drift = fp32_drift(args.workload, device, T)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = oracle_sample(args.workload, 3)
@@ -390,23 +430,13 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {
-                "workload": args.workload,
-                "subdivision": sim.config.subdivision,
-                "radial_cells": sim.config.radial_cells,
-                "cells": wl.cells,
-                "time_steps_per_step": T,
-                "plasma": "drude (1 species)",
-                "surface_impedance": sim._surface_impedance_ade is not None,
-                "receivers": int(wl.receivers[0].shape[0]),
-                "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
-                "parallelism": f"replicas x{world}",
-            },
+            "config": config,
             "hbm_gbs": achieved,
             "kernel_modes": list(modes),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "fp32_drift": drift,
             "gpu_launches": 2 * T * args.steps,
             "clocks": clocks,
         }

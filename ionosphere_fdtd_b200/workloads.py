@@ -175,4 +175,5 @@ def seed_fields(sim, seed: int = 20260814, amplitude: float = 1.0e-6) -> None:
     g.manual_seed(seed)
     for f in ("er", "et", "hr", "ht"):
         t = getattr(sim, f)
-        t.copy_(torch.randn(t.shape, generator=g, device=t.device, dtype=t.dtype) * amplitude)
+        # drawn in float64 and rounded, so float32 and float64 runs start from the same state
+        t.copy_((torch.randn(t.shape, generator=g, device=t.device, dtype=torch.float64) * amplitude).to(t.dtype))
