@@ -50,6 +50,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-drift", action="store_true", help="skip the float32-vs-float64 drift run")
+    p.add_argument("--subdivision", type=int, default=None, help="override the workload's subdivision (small profiling cases)")
     return p.parse_args()
 
 
@@ -181,18 +182,19 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
-def build(workload: str, device: str, dtype: str = "float32"):
+def build(workload: str, device: str, dtype: str = "float32", subdivision: int | None = None):
     from ionosphere_fdtd_b200 import workloads as W
 
+    extra = {} if subdivision is None else {"subdivision": subdivision}
     if workload == "config4":
-        wl = W.config4(device=device, dtype=dtype)
+        wl = W.config4(device=device, dtype=dtype, **extra)
     else:
-        wl = W.config2(device=device, dtype=dtype)
+        wl = W.config2(device=device, dtype=dtype, **extra)
     W.seed_fields(wl.simulation)
     return wl
 
 
-def fp32_drift(workload: str, device: str, steps: int) -> dict:
+def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None = None) -> dict:
     """Relative L2 per (E, H) group between float32 and float64 runs of the
     engine from the same seeded state (the float64 run stands in for the
     float64 NumPy path, far too slow at these sizes) after ``steps`` steps."""
@@ -202,7 +204,7 @@ def fp32_drift(workload: str, device: str, steps: int) -> dict:
     out = {}
     sims = {}
     for dtype in ("float64", "float32"):
-        sim = build(workload, device, dtype).simulation
+        sim = build(workload, device, dtype, subdivision).simulation
         sim.step(steps)
         sims[dtype] = {f: getattr(sim, f).to(torch.float64) for f in ("er", "et", "hr", "ht")}
         del sim
@@ -303,7 +305,7 @@ def main() -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
     device = f"cuda:{local}"
-    wl = build(args.workload, device)
+    wl = build(args.workload, device, subdivision=args.subdivision)
     sim = wl.simulation
     T = args.time_steps or (1000 if args.workload == "config2" else 100)
     stream = torch.cuda.current_stream()
@@ -363,7 +365,7 @@ def main() -> None:
     nbytes = kernel_bytes(sim)
     modes = sim._engine.kernel_modes
     names = {"h_phase": "kh_tma" if modes[0] == "pipeline" else "kh_kernel", "e_phase": "ke_tma" if modes[1] == "pipeline" else "ke_kernel"}
-    traffic = traffic_from_profile(args.workload)
+    traffic = traffic_from_profile(args.workload) if args.subdivision is None else {}
     kernels = {
         phase: {
             "kernel": names[phase],
@@ -405,7 +407,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_drift:
         del wl, sim
         torch.cuda.empty_cache()
-        drift = fp32_drift(args.workload, device, T)
+        drift = fp32_drift(args.workload, device, T, args.subdivision)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = oracle_sample(args.workload, 3)
