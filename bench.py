@@ -216,8 +216,8 @@ def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None =
     return {"steps": steps, **out, "against": "float64 engine from the same seeded state"}
 
 
-def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
-    """Time the CPU oracle on ``steps`` leapfrog steps of the same workload (float32)."""
+def oracle_build(workload: str):
+    """The CPU oracle on the same workload (float32), fields seeded as the engine's."""
 
     import oracle.fdtd as O
     from ionosphere_fdtd_b200 import workloads as W
@@ -244,23 +244,34 @@ def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
     rng = np.random.default_rng(20260814)
     for f in ("er", "et", "hr", "ht"):
         getattr(sim, f)[:] = (1.0e-6 * rng.standard_normal(getattr(sim, f).shape)).astype(np.float32)
-    sim.step(warm)
+    return sim, {"cells": mesh.n_vertices * L, "sub": sub, "L": L}
+
+
+def oracle_time(sim, info: dict, steps: int) -> dict:
     t0 = time.perf_counter()
     sim.step(steps)
     dt = time.perf_counter() - t0
-    cells = mesh.n_vertices * L
-    return {"gcells": cells * steps / dt / 1e9, "seconds": dt, "steps": steps, "cells": cells, "sub": sub, "L": L}
+    return {"gcells": info["cells"] * steps / dt / 1e9, "seconds": dt, "steps": steps, **info}
+
+
+def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
+    """Time the CPU oracle on ``steps`` leapfrog steps of the same workload (float32)."""
+
+    sim, info = oracle_build(workload)
+    sim.step(warm)
+    return oracle_time(sim, info, steps)
 
 
 def reference_arm(args, world: int, rank: int) -> None:
     if rank != 0:
         return
     per_step = 1
+    sim, info = oracle_build(args.workload)
     for _ in range(args.warmup):
-        oracle_sample(args.workload, per_step, warm=0)
+        oracle_time(sim, info, per_step)
     rates, secs = [], 0.0
     for _ in range(args.steps):
-        r = oracle_sample(args.workload, per_step, warm=0)
+        r = oracle_time(sim, info, per_step)
         rates.append(r["gcells"])
         secs += r["seconds"]
     value = statistics.median(rates)
