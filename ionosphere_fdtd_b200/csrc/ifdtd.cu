@@ -343,7 +343,8 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
                   const std::vector<int>& eptr, const std::vector<int2>& lr, int SW, const std::vector<int>& ps_edge,
                   const std::vector<int>& ps_face, const std::vector<real>& ps_coef, const std::vector<real>& ps_wc,
                   const std::vector<real>& inv_phi, const std::vector<real>& tn, bool plasma, int Pn, int Pm,
-                  std::vector<int>& locA, std::vector<int>& locB, int max_stage) {
+                  const std::vector<char>& v_src, const std::vector<char>& e_src, std::vector<int>& locA,
+                  std::vector<int>& locB, int max_stage) {
   using namespace pipe;
   const int rb = (int)sizeof(real);
   std::vector<int> h_ids, f_ids, v_ids, vloc;
@@ -423,6 +424,8 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     head[ke_nv] = nv;
     head[ke_ea] = ea;
     head[ke_ne] = ne;
+    for (const auto& o : own) head[ke_src] |= v_src[o.first] ? 1 : 0;
+    for (int e = ea; e < eb; ++e) head[ke_src] |= e_src[e] ? 2 : 0;
     head[ke_o_ht] = B;
     head[ke_o_hr] = head[ke_o_ht] + n_h * Pn * rb;
     head[ke_o_J] = head[ke_o_hr] + n_f * Pm * rb;
@@ -948,6 +951,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     std::vector<int> e_try;  // > 0: faces per patch; < 0: balanced for -n stages
     if (auto_e) e_try = {-2, -3, 32, 16, 8};
     else e_try = {fpp_e};
+    // the pipelined E consumer gives every compute thread a fixed radial quad,
+    // so no row may have more quads than the CTA has compute threads (at least
+    // 256 when the count is automatic)
+    const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
+    if (row_quads > (auto_threads ? 256 : threads)) e_try.clear();
+    std::vector<char> v_src(nV, 0), e_src(nE, 0);
+    for (int s = 0; s < X->n_src_er; ++s) v_src[X->src_er_vertex[s]] = 1;
+    for (int s = 0; s < X->n_src_et; ++s) e_src[X->src_et_edge[s]] = 1;
     for (const int c : e_try) {
       const int stages_wanted = c < 0 ? -c : 2;
       Own o = c < 0 ? ownership_bounds(balanced_e_bounds(stage_budget / stages_wanted * 97 / 100, plasma, (int)sizeof(real)))
@@ -956,7 +967,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       if (!build_slots(o.vlist, sl)) break;
       PipeTables t;
       const bool ok = build_pipe_e<real>(t, o.n, o.vptr, o.vlist, o.eptr, lr, SW, sl.edge, sl.face, sl.coef, sl.wc,
-                                         inv_phi, tn, plasma, Pn, Pm, locA, locB, stage_budget / stages_wanted);
+                                         inv_phi, tn, plasma, Pn, Pm, v_src, e_src, locA, locB,
+                                         stage_budget / stages_wanted);
       if (ok && stages_wanted * t.stage_bytes <= stage_budget) {
         P->pipe_e_ok = true;
         fpp_e = c > 0 ? c : 0;

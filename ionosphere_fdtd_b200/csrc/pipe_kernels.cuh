@@ -45,8 +45,10 @@ enum KhHead : int {
 // E-phase blob header.
 enum KeHead : int {
   ke_nv, ke_ea, ke_ne, ke_o_ht, ke_o_hr, ke_o_J, ke_o_er, ke_o_et, ke_o_vid, ke_o_vh,
-  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_o_rav, ke_head_ints = 20
+  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_o_rav, ke_src, ke_head_ints = 20
 };
+// ke_src: bit 0 = an owned vertex carries a vertical source support, bit 1 =
+// an owned edge carries a tangential one (other patches skip the search).
 
 // Bytes of per-layer rows at the start of dynamic shared memory (host and
 // device), rounded to 128 so the stages start aligned.
@@ -324,13 +326,17 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
   }
 }
 
-// E phase of one patch from its stage (same arithmetic as ke_kernel).
+// E phase of one patch from its stage (same arithmetic as ke_kernel).  Each
+// loop gives every thread a fixed radial quad: thread ct takes quad ct % c of
+// entities ct / c, ct / c + per, ... (c quads per row, per = nct / c entities
+// per sweep; threads from per * c on sit the loop out), so the per-layer
+// factors of its quad load once per patch instead of once per run.
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
                                            int nct, real current, uint64_t* group, uint32_t ph, const Ring& G) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
-  const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne];
+  const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne], src = hd[ke_src];
   const real* s_ht = reinterpret_cast<const real*>(st + hd[ke_o_ht]);
   const real* s_hr = reinterpret_cast<const real*>(st + hd[ke_o_hr]);
   const real* s_J = reinterpret_cast<const real*>(st + hd[ke_o_J]);
@@ -346,7 +352,7 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
   const real* etan = reinterpret_cast<const real*>(st + hd[ke_o_etan]);
   real* s_rav = reinterpret_cast<real*>(st + hd[ke_o_rav]);
   const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
-  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
+  const bool full = R.coef_full != 0;
   auto slot_rows = [&](int vl, const real** hrows, const real** jrows) {
 #pragma unroll
     for (int q = 0; q < MAXDEG; q += 4) {
@@ -370,41 +376,57 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     // pass 1: each owned vertex's radial current at every midpoint, into the
     // stage's scratch rows; then all compute warps meet on the slot's group
     // barrier (bounded) before the vertex runs read them
-    for (int it = ct; it < nv * cm; it += nct) {
-      const int vl = fast_div(it, mag_cm);
-      const real* hrows[MAXDEG];
-      const real* jrows[MAXDEG];
-      slot_rows(vl, hrows, jrows);
-      const int j0 = (it - vl * cm) * N;
-      const Run<real> r = vertex_radial_current<real, MAXDEG>(jrows, vwc + vl * SW * 4, j0, Pm);
-      if constexpr (sizeof(real) == 4) {
-        *reinterpret_cast<float4*>(s_rav + vl * Pm + j0) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
-      } else {
-        *reinterpret_cast<double2*>(s_rav + vl * Pm + j0) = make_double2(r.x[0], r.x[1]);
+    const int per = nct / cm;
+    if (ct < per * cm) {
+      const int j0 = (ct % cm) * N;
+      for (int vl = ct / cm; vl < nv; vl += per) {
+        const real* hrows[MAXDEG];
+        const real* jrows[MAXDEG];
+        slot_rows(vl, hrows, jrows);
+        const Run<real> r = vertex_radial_current<real, MAXDEG>(jrows, vwc + vl * SW * 4, j0, Pm);
+        if constexpr (sizeof(real) == 4) {
+          *reinterpret_cast<float4*>(s_rav + vl * Pm + j0) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
+        } else {
+          *reinterpret_cast<double2*>(s_rav + vl * Pm + j0) = make_double2(r.x[0], r.x[1]);
+        }
       }
     }
     __syncwarp();
     if ((threadIdx.x & 31) == 0) mbar_arrive(group);
     if (!__all_sync(0xFFFFFFFFu, wait_phase(group, ph, G.abort_flag, G.status))) return;
   }
-  for (int it = ct; it < nv * cn; it += nct) {
-    const int vl = fast_div(it, mag_cn);
-    const int v = vid[vl];
-    const real* hrows[MAXDEG];
-    const real* jrows[MAXDEG];
-    slot_rows(vl, hrows, jrows);
-    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, vcoef + vl * SW,
-                                       PLASMA ? vwc + vl * SW * 4 : nullptr, s_er + vl * Pn, R.er + (size_t)v * Pn,
-                                       current, PLASMA ? s_rav + vl * Pm : nullptr);
+  {
+    const int per = nct / cn;
+    if (ct < per * cn) {
+      const int k0 = (ct % cn) * N;
+      const VertexLayer<real> fixed = vertex_layer(R, Ls, 0, k0);
+      for (int vl = ct / cn; vl < nv; vl += per) {
+        const int v = vid[vl];
+        const real* hrows[MAXDEG];
+        const real* jrows[MAXDEG];
+        slot_rows(vl, hrows, jrows);
+        e_vertex_run<real, PLASMA, MAXDEG>(R, full ? vertex_layer(R, Ls, v, k0) : fixed, (src & 1) != 0, v, k0, hrows,
+                                           jrows, vcoef + vl * SW, PLASMA ? vwc + vl * SW * 4 : nullptr,
+                                           s_er + vl * Pn, R.er + (size_t)v * Pn, current,
+                                           PLASMA ? s_rav + vl * Pm : nullptr);
+      }
+    }
   }
-  for (int it = ct; it < ne * cm; it += nct) {
-    const int el = fast_div(it, mag_cm);
-    const int e = ea + el;
-    const int4 loc = eloc[el];
-    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, s_hr + loc.y * Pm, s_hr + loc.z * Pm, s_ht + loc.x * Pn,
-                             PLASMA ? s_J + loc.y * 3 * Pm : nullptr, PLASMA ? s_J + loc.z * 3 * Pm : nullptr,
-                             s_et + el * Pm, R.et + (size_t)e * Pm, current, einv[el],
-                             PLASMA ? etan + el * 8 : nullptr);
+  {
+    const int per = nct / cm;
+    if (ct < per * cm) {
+      const int j0 = (ct % cm) * N;
+      const EdgeLayer<real> fixed = edge_layer(R, Ls, ea, j0);
+      for (int el = ct / cm; el < ne; el += per) {
+        const int e = ea + el;
+        const int4 loc = eloc[el];
+        e_edge_run<real, PLASMA>(R, full ? edge_layer(R, Ls, e, j0) : fixed, (src & 2) != 0, e, j0,
+                                 s_hr + loc.y * Pm, s_hr + loc.z * Pm, s_ht + loc.x * Pn,
+                                 PLASMA ? s_J + loc.y * 3 * Pm : nullptr, PLASMA ? s_J + loc.z * 3 * Pm : nullptr,
+                                 s_et + el * Pm, R.et + (size_t)e * Pm, current, einv[el],
+                                 PLASMA ? etan + el * 8 : nullptr);
+      }
+    }
   }
 }
 

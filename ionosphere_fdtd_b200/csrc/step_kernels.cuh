@@ -583,27 +583,70 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   }
 }
 
+// Per-layer factors of a vertex run at nodes k0..k0+N-1: 1/r, the loss
+// coefficients (shared rows, or vertex v's own rows when the material varies
+// horizontally), the node weights of the midpoints below / above, and whether
+// midpoints k0-1 (below) and k0 (in) exist.
+template <typename real>
+struct VertexLayer {
+  Run<real> ir, ca, cb, wl, wu;
+  bool in, below;
+};
+template <typename real>
+__device__ __forceinline__ VertexLayer<real> vertex_layer(const Rec<real>& R, const Layers<real>& Ls, int v, int k0) {
+  VertexLayer<real> y;
+  y.ir = ld16(Ls.invr + k0);
+  y.ca = R.coef_full ? ldg16(R.ca_er + (size_t)v * R.Pn + k0) : ld16(Ls.ca_er + k0);
+  y.cb = R.coef_full ? ldg16(R.cb_er + (size_t)v * R.Pn + k0) : ld16(Ls.cb_er + k0);
+  y.wl = ld16(Ls.vwl + k0);
+  y.wu = ld16(Ls.vwu + k0);
+  y.in = k0 < R.Pm;
+  y.below = k0 >= 1 && k0 - 1 < R.L;
+  return y;
+}
+
+// Per-layer factors of an edge run at midpoints j0..j0+N-1: 1/m, the radial
+// curl weights, the loss coefficients (shared rows or edge e's own rows) and
+// whether node j0+N exists.
+template <typename real>
+struct EdgeLayer {
+  Run<real> im, fu, fd, ca, cb;
+  bool tail;
+};
+template <typename real>
+__device__ __forceinline__ EdgeLayer<real> edge_layer(const Rec<real>& R, const Layers<real>& Ls, int e, int j0) {
+  EdgeLayer<real> y;
+  y.im = ld16(Ls.invm + j0);
+  y.fu = ld16(Ls.eU + j0);
+  y.fd = ld16(Ls.eD + j0);
+  y.ca = R.coef_full ? ldg16(R.ca_et + (size_t)e * R.Pm + j0) : ld16(Ls.ca_et + j0);
+  y.cb = R.coef_full ? ldg16(R.cb_et + (size_t)e * R.Pm + j0) : ld16(Ls.cb_et + j0);
+  y.tail = j0 + Lanes<real>::N < R.Pn;
+  return y;
+}
+
 // Er on nodes k0..k0+N-1 of vertex v (solver.py:929-962; plasma.py:511-526):
 //   Er = Ca Er + Cb (circ_v(Ht) / r - J_r) - source,
 // J_r the vertex's area-averaged radial current at the node (weights vwl / vwu
-// of the midpoints below / above).  hrows[q]: Ht row of slot q's edge;
-// jrows[q]: (3, Pm) summed current rows of slot q's face; coef[q] = sign *
-// phi_e / A*_v and wcs[4q..4q+2] = area weight * face centre of slot q (zero in
-// padding slots).  rav_row: the vertex's radial current at every midpoint
-// (Pm reals, from vertex_radial_current), or nullptr to accumulate it here.
+// of the midpoints below / above).  y: the run's layer factors; src: whether v
+// may carry a vertical source support (else the source list is not searched).
+// hrows[q]: Ht row of slot q's edge; jrows[q]: (3, Pm) summed current rows of
+// slot q's face; coef[q] = sign * phi_e / A*_v and wcs[4q..4q+2] = area weight
+// * face centre of slot q (zero in padding slots).  rav_row: the vertex's
+// radial current at every midpoint (Pm reals, from vertex_radial_current), or
+// nullptr to accumulate it here.
 template <typename real, bool PLASMA, int MAXDEG>
-__device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<real>& Ls, int v, int k0,
+__device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const VertexLayer<real>& y, bool src, int v, int k0,
                                              const real* const* hrows, const real* const* jrows, const real* coef,
                                              const real* wcs, const real* ero, real* erout, real current,
                                              const real* rav_row = nullptr) {
   constexpr int N = Lanes<real>::N;
-  const int L = R.L, Pn = R.Pn, Pm = R.Pm;
+  const int Pm = R.Pm;
   Run<real> hv[MAXDEG];
 #pragma unroll
   for (int q = 0; q < MAXDEG; ++q) hv[q] = ld16(hrows[q] + k0);
-  const Run<real> ev = ld16(ero + k0), ir = ld16(Ls.invr + k0);
-  const Run<real> ca = R.coef_full ? ldg16(R.ca_er + (size_t)v * Pn + k0) : ld16(Ls.ca_er + k0);
-  const Run<real> cb = R.coef_full ? ldg16(R.cb_er + (size_t)v * Pn + k0) : ld16(Ls.cb_er + k0);
+  const Run<real> ev = ld16(ero + k0);
+  const Run<real>&ir = y.ir, &ca = y.ca, &cb = y.cb;
   real cq[(MAXDEG + 3) / 4 * 4];
 #pragma unroll
   for (int q = 0; q < MAXDEG; q += 4) {
@@ -622,7 +665,7 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
   Run<real> out;
 #pragma unroll
   for (int r = 0; r < N; ++r) out.x[r] = ca.x[r] * ev.x[r] + cb.x[r] * (acc[r] * ir.x[r]);
-  if (R.n_src_er > 0 && source_hit(R.src_er_v, R.n_src_er, v)) {
+  if (src && source_hit(R.src_er_v, R.n_src_er, v)) {
 #pragma unroll
     for (int r = 0; r < N; ++r)
       for (int s = 0; s < R.n_src_er; ++s)
@@ -634,7 +677,7 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
     real rav[N + 1];
 #pragma unroll
     for (int r = 0; r <= N; ++r) rav[r] = real(0);
-    const bool in = k0 < Pm, below = k0 >= 1 && k0 - 1 < L;
+    const bool in = y.in, below = y.below;
     if (rav_row) {
       if (below) rav[0] = rav_row[k0 - 1];
       if (in) {
@@ -657,9 +700,8 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
         for (int r = 0; r < N; ++r) rav[r + 1] = rav_term(rav[r + 1], jx.x[r], jy.x[r], jz.x[r], c0, c1, c2);
       }
     }
-    const Run<real> wl = ld16(Ls.vwl + k0), wu = ld16(Ls.vwu + k0);
 #pragma unroll
-    for (int r = 0; r < N; ++r) out.x[r] -= cb.x[r] * (wl.x[r] * rav[r] + wu.x[r] * rav[r + 1]);
+    for (int r = 0; r < N; ++r) out.x[r] -= cb.x[r] * (y.wl.x[r] * rav[r] + y.wu.x[r] * rav[r + 1]);
   }
   st16(erout + k0, out);
 }
@@ -667,19 +709,19 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const Layers<re
 // Et on midpoints j0..j0+N-1 of edge e (solver.py:964-989; plasma.py:503-509):
 //   Et = Ca Et + Cb ((Hr_l - Hr_r) / phi_e / m - Ht[j+1] eU + Ht[j] eD - J_t) - source,
 // eU / eD the radial curl weights of the nodes above / below, J_t the mean of
-// the two faces' currents along the edge.  inv_p = 1 / dual edge angle;
-// tp = left tangent, 0, right tangent, 0.
+// the two faces' currents along the edge.  y: the run's layer factors; src:
+// whether e may carry a tangential source support.  inv_p = 1 / dual edge
+// angle; tp = left tangent, 0, right tangent, 0.
 template <typename real, bool PLASMA>
-__device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int j0, const real* hl,
-                                           const real* hq, const real* hto, const real* jl, const real* jq,
-                                           const real* eto, real* etout, real current, real inv_p, const real* tp) {
+__device__ __forceinline__ void e_edge_run(const Rec<real>& R, const EdgeLayer<real>& y, bool src, int e, int j0,
+                                           const real* hl, const real* hq, const real* hto, const real* jl,
+                                           const real* jq, const real* eto, real* etout, real current, real inv_p,
+                                           const real* tp) {
   constexpr int N = Lanes<real>::N;
-  const int Pn = R.Pn, Pm = R.Pm;
+  const int Pm = R.Pm;
   const Run<real> a = ld16(hl + j0), b = ld16(hq + j0), hv = ld16(hto + j0), ev = ld16(eto + j0);
-  const real htail = (j0 + N < Pn) ? hto[j0 + N] : real(0);
-  const Run<real> im = ld16(Ls.invm + j0), fu = ld16(Ls.eU + j0), fd = ld16(Ls.eD + j0);
-  const Run<real> ca = R.coef_full ? ldg16(R.ca_et + (size_t)e * Pm + j0) : ld16(Ls.ca_et + j0);
-  const Run<real> cb = R.coef_full ? ldg16(R.cb_et + (size_t)e * Pm + j0) : ld16(Ls.cb_et + j0);
+  const real htail = y.tail ? hto[j0 + N] : real(0);
+  const Run<real>&im = y.im, &fu = y.fu, &fd = y.fd, &ca = y.ca, &cb = y.cb;
   Run<real> out;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
@@ -687,7 +729,7 @@ __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const Layers<real
     const real g = (a.x[r] - b.x[r]) * inv_p * im.x[r] - hnext * fu.x[r] + hv.x[r] * fd.x[r];
     out.x[r] = ca.x[r] * ev.x[r] + cb.x[r] * g;
   }
-  if (R.n_src_et > 0 && source_hit(R.src_et_e, R.n_src_et, e)) {
+  if (src && source_hit(R.src_et_e, R.n_src_et, e)) {
 #pragma unroll
     for (int r = 0; r < N; ++r)
       for (int s = 0; s < R.n_src_et; ++s)
@@ -778,7 +820,9 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
       hrows[q] = R.ht + (size_t)__ldg(R.ps_edge + (size_t)slot * SW + q) * Pn;
       jrows[q] = PLASMA ? Jsum + (size_t)__ldg(R.ps_face + (size_t)slot * SW + q) * 3 * Pm : nullptr;
     }
-    e_vertex_run<real, PLASMA, MAXDEG>(R, Ls, v, (it - vl * cn) * N, hrows, jrows, R.ps_coef + (size_t)slot * SW,
+    const int k0 = (it - vl * cn) * N;
+    e_vertex_run<real, PLASMA, MAXDEG>(R, vertex_layer(R, Ls, v, k0), R.n_src_er > 0, v, k0, hrows, jrows,
+                                       R.ps_coef + (size_t)slot * SW,
                                        PLASMA ? R.ps_wc + (size_t)slot * SW * 4 : nullptr, R.er + (size_t)v * Pn,
                                        R.er + (size_t)v * Pn, current);
   }
@@ -787,7 +831,9 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
     const int el = fast_div(it, mag_cm);
     const int e = ea + el;
     const int2 lr = __ldg(R.edge_lr + e);
-    e_edge_run<real, PLASMA>(R, Ls, e, (it - el * cm) * N, R.hr + (size_t)lr.x * Pm, R.hr + (size_t)lr.y * Pm,
+    const int j0 = (it - el * cm) * N;
+    e_edge_run<real, PLASMA>(R, edge_layer(R, Ls, e, j0), R.n_src_et > 0, e, j0, R.hr + (size_t)lr.x * Pm,
+                             R.hr + (size_t)lr.y * Pm,
                              R.ht + (size_t)e * Pn, PLASMA ? Jsum + (size_t)lr.x * 3 * Pm : nullptr,
                              PLASMA ? Jsum + (size_t)lr.y * 3 * Pm : nullptr, R.et + (size_t)e * Pm,
                              R.et + (size_t)e * Pm, current, __ldg(R.inv_phi + e), PLASMA ? R.tan + 8 * (size_t)e : nullptr);
