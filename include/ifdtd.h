@@ -46,6 +46,7 @@ typedef enum ifdtd_status {
 
 typedef struct ifdtd_plan ifdtd_plan;
 typedef struct ifdtd_probe ifdtd_probe;
+typedef struct ifdtd_batch ifdtd_batch;
 
 /* Mesh tables as GeodesicMesh holds them (src/ionosphere_fdtd/mesh.py:21-41). */
 typedef struct ifdtd_mesh_desc {
@@ -196,6 +197,30 @@ int32_t ifdtd_sample(ifdtd_plan* plan, const ifdtd_state* state, const ifdtd_pro
  * (record_er_observations' inner loop, solver.py:1126-1135). */
 int32_t ifdtd_step_sampled(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
                            int32_t n_steps, const ifdtd_probe* probe, double* out_rows, void* stream);
+
+/* Ensembles.  The reference runs an ensemble as a loop over GeodesicFDTD
+ * objects, each calling step() / record_er_observations (solver.py:789-816,
+ * 1080-1136); it has no batched runner.  A batch advances all its member plans
+ * by the same number of steps: one launch per phase for every group of
+ * members whose plans run both phases on the pipeline (grouped by plasma,
+ * vertex slot width, copy engine, threads and producer warps), the other
+ * members launched on their own within the step, and one launch per step that
+ * samples every member's receivers.  Each member's fields come out as from its
+ * own ifdtd_step.  All plans share one device and one precision and must
+ * outlive the batch; chunk (>= 1) is the steps per captured CUDA graph, capped
+ * at the graph_chunk of members launched on their own. */
+int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t chunk, ifdtd_batch** out);
+int32_t ifdtd_batch_destroy(ifdtd_batch* batch);
+/* states: n_members states.  currents: device float64 (n_members, n_steps),
+ * row i member i's source currents I((n+1/2)dt) (NULL: zero).  probes: NULL or
+ * n_members probe handles (entries may be NULL) created on the members' plans;
+ * out_rows[i]: device float64 (n_steps, rows_i) for member i's samples. */
+int32_t ifdtd_batch_step(ifdtd_batch* batch, const ifdtd_state* states, const double* currents, int32_t n_steps,
+                         ifdtd_probe* const* probes, double* const* out_rows, void* stream);
+/* Launch layout: batched groups, members launched on their own, and the CTAs
+ * of the first group's H and E launches (0 when there is no group). */
+int32_t ifdtd_batch_info(const ifdtd_batch* batch, int32_t* groups, int32_t* solo, int32_t* kh_grid,
+                         int32_t* ke_grid);
 
 /* max |field| of er, et, hr, ht into out4 (device, float64); the four
  * reductions of diagnostics() (solver.py:1027-1030, torch_backend.py:218-219). */

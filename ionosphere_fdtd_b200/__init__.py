@@ -7,6 +7,7 @@ written against its PyTorch CUDA backend switches by changing the import.
 from .backend import CudaBackend, create_backend
 from .checkpoint import load_checkpoint, save_checkpoint
 from .constants import C_0, EARTH_RADIUS_M, EPSILON_0, MU_0
+from .ensemble import Ensemble
 from .errors import BackendUnavailableError, CheckpointError
 from .materials import EarthIonosphereMaterial, SphericalAnomaly
 from .mesh import (
@@ -38,6 +39,7 @@ from .surface_impedance import ConductiveHalfSpaceSurface, SurfaceImpedanceADE
 __version__ = "0.1.0"
 
 __all__ = [
+    "Ensemble",
     "BackendUnavailableError",
     "C_0",
     "CheckpointError",

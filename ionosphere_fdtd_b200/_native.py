@@ -126,6 +126,10 @@ _SIGNATURES = {
     "ifdtd_probe_destroy": ([_vp], _i32),
     "ifdtd_sample": ([_vp, C.POINTER(State), _vp, _vp, _vp], _i32),
     "ifdtd_step_sampled": ([_vp, C.POINTER(State), _vp, _i32, _vp, _vp, _vp], _i32),
+    "ifdtd_batch_create": ([C.POINTER(_vp), _i32, _i32, C.POINTER(_vp)], _i32),
+    "ifdtd_batch_destroy": ([_vp], _i32),
+    "ifdtd_batch_step": ([_vp, C.POINTER(State), _vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp], _i32),
+    "ifdtd_batch_info": ([_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_max_abs": ([_vp, C.POINTER(State), _vp, _vp], _i32),
     "ifdtd_edge_difference": ([_vp, _vp, _i32, _vp, _vp], _i32),
     "ifdtd_dual_edge_difference": ([_vp, _vp, _i32, _vp, _vp], _i32),

@@ -113,6 +113,7 @@ struct ifdtd_plan {
   cudaStream_t capture_stream = nullptr;
   std::vector<GraphEntry> graphs;
   std::vector<ifdtd_probe*> probes;
+  std::vector<float> kh_cost, ke_cost;  // staged bytes per pipelined patch (balances batched launches)
   ~ifdtd_plan() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     if (capture_stream) cudaStreamDestroy(capture_stream);
@@ -984,6 +985,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       P->pipe_e_ok = false;
     P->kh_stage = th_tab.stage_bytes;
     P->ke_stage = te_tab.stage_bytes;
+    auto patch_costs = [](const PipeTables& t) {
+      std::vector<float> c(t.dptr.size() - 1, 0.f);
+      for (size_t q = 0; q + 1 < t.dptr.size(); ++q)
+        for (int d = t.dptr[q]; d < t.dptr[q + 1]; ++d) c[q] += (float)t.desc[d].w;
+      return c;
+    };
+    if (P->pipe_h_ok) P->kh_cost = patch_costs(th_tab);
+    if (P->pipe_e_ok) P->ke_cost = patch_costs(te_tab);
     if (P->pipe_h_ok) {
       UP(th_tab.dptr, dptr_h);
       UP(th_tab.desc, desc_h);
@@ -1254,6 +1263,360 @@ int grid_for(size_t n) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Ensembles: member plans advanced together.  Members whose two phases both
+// run on the pipeline are grouped by kernel template (precision is the
+// batch's; plasma, vertex slot width, copy engine, threads and producer warps
+// per group) and every group takes one batched launch per phase: CTAs walk
+// cost-balanced ranges of the members' concatenated patch lists.  Other
+// members launch on their own inside the same step.  Receivers of all members
+// are sampled by one launch per step.
+// ---------------------------------------------------------------------------
+struct BatchGroup {
+  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2;
+  std::vector<int> members;
+  size_t kh_smem = 0, ke_smem = 0;
+  int kh_grid = 0, ke_grid = 0;
+  const int4* segs_h = nullptr;
+  const int* sptr_h = nullptr;
+  const int4* segs_e = nullptr;
+  const int* sptr_e = nullptr;
+};
+
+struct ifdtd_batch {
+  int device = 0, dtype = 4, n = 0, chunk = 32;
+  std::vector<ifdtd_plan*> plans;
+  std::vector<int> solo;  // members with a direct-kernel phase
+  std::vector<BatchGroup> groups;
+  DeviceArena arena;
+  void* d_recs = nullptr;  // one record per member: bound fields, currents from d_cur
+  std::vector<unsigned char> h_recs;
+  size_t rec_bytes = 0;
+  double* d_cur = nullptr;  // (n, chunk) step currents
+  const int2* d_ring_h = nullptr;
+  const int2* d_ring_e = nullptr;
+  // sampled steps: probe table, row map and (chunk, rows) staging; they grow
+  // on demand and every captured graph is dropped when they move
+  void* d_refs = nullptr;
+  void* d_rowmap = nullptr;
+  double* d_stage = nullptr;
+  int cap_refs = 0, cap_rows = 0;
+  std::vector<ifdtd_state> last;
+  bool have_state = false;
+  cudaStream_t capture_stream = nullptr;
+  struct Graph {
+    int chunk, rows;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Graph> graphs;
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
+  ~ifdtd_batch() {
+    drop_graphs();
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    cudaFree(d_refs);
+    cudaFree(d_rowmap);
+    cudaFree(d_stage);
+  }
+};
+
+namespace {
+
+// Cost-balanced contiguous ranges of the members' concatenated patch lists,
+// one per CTA, cut at member boundaries into segments {member, first patch,
+// end patch, 0}; CTA b owns segs[sptr[b]] .. segs[sptr[b + 1] - 1].  A patch
+// goes to the CTA in whose share its cost midpoint falls; the last CTA takes
+// the rest.
+void split_patches(const std::vector<int>& members, const std::vector<const std::vector<float>*>& cost, int grid,
+                   std::vector<int4>& segs, std::vector<int>& sptr) {
+  double total = 0.0;
+  for (const auto* c : cost)
+    for (const float x : *c) total += std::max(x, 1.0f);
+  segs.clear();
+  sptr.assign(1, 0);
+  size_t mi = 0;
+  int p = 0;
+  double acc = 0.0;
+  for (int b = 0; b < grid; ++b) {
+    const double end = total * (b + 1) / grid;
+    while (mi < members.size()) {
+      const std::vector<float>& cv = *cost[mi];
+      if (p >= (int)cv.size()) {
+        ++mi;
+        p = 0;
+        continue;
+      }
+      const double w = std::max(cv[p], 1.0f);
+      if (b + 1 < grid && acc + 0.5 * w > end) break;
+      if ((int)segs.size() > sptr.back() && segs.back().x == members[mi] && segs.back().z == p)
+        segs.back().z = p + 1;
+      else
+        segs.push_back(make_int4(members[mi], p, p + 1, 0));
+      acc += w;
+      ++p;
+    }
+    sptr.push_back((int)segs.size());
+  }
+}
+
+template <typename real>
+auto batch_kh_kernel(const BatchGroup& g) {
+  using namespace pipe;
+  if (g.plasma) return g.copy ? kh_tma_batch<real, true, 1> : kh_tma_batch<real, true, 0>;
+  return g.copy ? kh_tma_batch<real, false, 1> : kh_tma_batch<real, false, 0>;
+}
+
+template <typename real>
+auto batch_ke_kernel(const BatchGroup& g) {
+  using namespace pipe;
+  if (g.plasma) {
+    if (g.maxdeg == 6) return g.copy ? ke_tma_batch<real, true, 6, 1> : ke_tma_batch<real, true, 6, 0>;
+    return g.copy ? ke_tma_batch<real, true, 12, 1> : ke_tma_batch<real, true, 12, 0>;
+  }
+  if (g.maxdeg == 6) return g.copy ? ke_tma_batch<real, false, 6, 1> : ke_tma_batch<real, false, 6, 0>;
+  return g.copy ? ke_tma_batch<real, false, 12, 1> : ke_tma_batch<real, false, 12, 0>;
+}
+
+template <typename K>
+cudaError_t batch_grid(K kernel, int threads, size_t smem, int sm_count, int n_patches, int* grid) {
+  cudaError_t e = allow_smem(kernel, smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = std::max(1, std::min(n_patches, sm_count * per_sm));
+  return cudaSuccess;
+}
+
+template <typename real>
+int batch_build(ifdtd_batch* B) {
+  B->rec_bytes = sizeof(Rec<real>);
+  for (int i = 0; i < B->n; ++i) {
+    ifdtd_plan* P = B->plans[i];
+    if (P->h_mode != 2 || P->e_mode != 2) {
+      B->solo.push_back(i);
+      continue;
+    }
+    BatchGroup key;
+    key.plasma = P->plasma ? 1 : 0;
+    key.maxdeg = P->maxdeg;
+    key.copy = P->pipe_copy;
+    key.threads = P->threads;
+    key.producers = P->producers;
+    BatchGroup* g = nullptr;
+    for (auto& x : B->groups)
+      if (x.plasma == key.plasma && x.maxdeg == key.maxdeg && x.copy == key.copy && x.threads == key.threads &&
+          x.producers == key.producers)
+        g = &x;
+    if (!g) {
+      B->groups.push_back(key);
+      g = &B->groups.back();
+    }
+    g->members.push_back(i);
+  }
+  std::vector<int2> ring_h(B->n, make_int2(0, 0)), ring_e(B->n, make_int2(0, 0));
+  for (const auto& g : B->groups)
+    for (const int i : g.members) {
+      const ifdtd_plan* P = B->plans[i];
+      ring_h[i] = make_int2(P->kh_stage, P->kh_stages);
+      ring_e[i] = make_int2(P->ke_stage, P->ke_stages);
+    }
+  if (B->arena.upload(ring_h, &B->d_ring_h) != cudaSuccess || B->arena.upload(ring_e, &B->d_ring_e) != cudaSuccess)
+    return fail(IFDTD_ERR_CUDA, "upload of batch ring table failed");
+  const int sm_count = B->plans[0]->sm_count;
+  for (auto& g : B->groups) {
+    int nh = 0, ne = 0;
+    std::vector<const std::vector<float>*> ch, ce;
+    for (const int i : g.members) {
+      const ifdtd_plan* P = B->plans[i];
+      g.kh_smem = std::max(g.kh_smem, P->kh_smem);
+      g.ke_smem = std::max(g.ke_smem, P->ke_smem);
+      nh += P->n_patches;
+      ne += P->n_patches_e;
+      ch.push_back(&P->kh_cost);
+      ce.push_back(&P->ke_cost);
+    }
+    const int threads = g.threads + 32 * g.producers;
+    cudaError_t e = batch_grid(batch_kh_kernel<real>(g), threads, g.kh_smem, sm_count, nh, &g.kh_grid);
+    if (e == cudaSuccess) e = batch_grid(batch_ke_kernel<real>(g), threads, g.ke_smem, sm_count, ne, &g.ke_grid);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batched launch shape: ") + cudaGetErrorString(e));
+    std::vector<int4> segs;
+    std::vector<int> sptr;
+    split_patches(g.members, ch, g.kh_grid, segs, sptr);
+    if (B->arena.upload(segs, &g.segs_h) != cudaSuccess || B->arena.upload(sptr, &g.sptr_h) != cudaSuccess)
+      return fail(IFDTD_ERR_CUDA, "upload of batch segments failed");
+    split_patches(g.members, ce, g.ke_grid, segs, sptr);
+    if (B->arena.upload(segs, &g.segs_e) != cudaSuccess || B->arena.upload(sptr, &g.sptr_e) != cudaSuccess)
+      return fail(IFDTD_ERR_CUDA, "upload of batch segments failed");
+  }
+  void* cur = nullptr;
+  void* recs = nullptr;
+  if (B->arena.alloc((size_t)B->n * B->chunk * sizeof(double), &cur) != cudaSuccess ||
+      B->arena.alloc((size_t)B->n * B->rec_bytes, &recs) != cudaSuccess)
+    return fail(IFDTD_ERR_CUDA, "allocation of batch records failed");
+  B->d_cur = (double*)cur;
+  B->d_recs = recs;
+  B->h_recs.assign((size_t)B->n * B->rec_bytes, 0);
+  for (int i = 0; i < B->n; ++i) {
+    std::memcpy(B->h_recs.data() + (size_t)i * B->rec_bytes, B->plans[i]->h_rec.data(), B->rec_bytes);
+    reinterpret_cast<Rec<real>*>(B->h_recs.data() + (size_t)i * B->rec_bytes)->cur = B->d_cur + (size_t)i * B->chunk;
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&B->capture_stream, cudaStreamNonBlocking));
+  return IFDTD_OK;
+}
+
+template <typename real>
+cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row, cudaStream_t st) {
+  const Rec<real>* recs = (const Rec<real>*)B->d_recs;
+  for (const auto& g : B->groups) {
+    auto k = batch_kh_kernel<real>(g);
+    k<<<g.kh_grid, g.threads + 32 * g.producers, g.kh_smem, st>>>(recs, g.segs_h, g.sptr_h, B->d_ring_h, g.producers);
+  }
+  for (const int i : B->solo) {
+    cudaError_t e = launch_kh<real>(B->plans[i], st);
+    if (e != cudaSuccess) return e;
+  }
+  for (const auto& g : B->groups) {
+    auto k = batch_ke_kernel<real>(g);
+    k<<<g.ke_grid, g.threads + 32 * g.producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.producers,
+                                                                   istep);
+  }
+  for (const int i : B->solo) {
+    cudaError_t e = launch_ke<real>(B->plans[i], istep, st);
+    if (e != cudaSuccess) return e;
+  }
+  if (rows > 0)
+    sample_batch_kernel<real><<<(rows * 32 + 255) / 256, 256, 0, st>>>(recs, (const ProbeRef*)B->d_refs,
+                                                                         (const int2*)B->d_rowmap, rows, step_row);
+  return cudaGetLastError();
+}
+
+template <typename real>
+int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents, int n, ifdtd_probe* const* probes,
+              double* const* out_rows, cudaStream_t stream) {
+  for (int i = 0; i < B->n; ++i) {
+    const ifdtd_plan* P = B->plans[i];
+    const ifdtd_state& s = states[i];
+    if (!s.er || !s.et || !s.hr || !s.ht) return fail(IFDTD_ERR_ARGUMENT, "state pointers missing");
+    if (P->T > 0 && !s.si_memory) return fail(IFDTD_ERR_ARGUMENT, "surface impedance memory missing");
+    for (int k = 0; k < P->S; ++k)
+      if (!s.plasma_current[k]) return fail(IFDTD_ERR_ARGUMENT, "plasma current missing");
+  }
+  for (const int i : B->solo) {
+    const int rc = bind_state<real>(B->plans[i], &states[i], stream);
+    if (rc) return rc;
+  }
+  if (!B->have_state || std::memcmp(B->last.data(), states, (size_t)B->n * sizeof(ifdtd_state)) != 0) {
+    for (int i = 0; i < B->n; ++i) {
+      Rec<real>* R = reinterpret_cast<Rec<real>*>(B->h_recs.data() + (size_t)i * B->rec_bytes);
+      const ifdtd_state& s = states[i];
+      R->er = (real*)s.er;
+      R->et = (real*)s.et;
+      R->hr = (real*)s.hr;
+      R->ht = (real*)s.ht;
+      R->si_mem = (real*)s.si_memory;
+      for (int k = 0; k < kMaxSpecies; ++k) R->J[k] = (real*)s.plasma_current[k];
+    }
+    // pageable source: the runtime stages it before returning
+    CUDA_TRY(cudaMemcpyAsync(B->d_recs, B->h_recs.data(), B->h_recs.size(), cudaMemcpyHostToDevice, stream));
+    B->last.assign(states, states + B->n);
+    B->have_state = true;
+  }
+  // receiver rows of every probed member, in member order
+  int rows = 0;
+  std::vector<ProbeRef> refs;
+  std::vector<int2> rowmap;
+  std::vector<int> offset(B->n, -1);
+  if (probes)
+    for (int i = 0; i < B->n; ++i) {
+      const ifdtd_probe* p = probes[i];
+      if (!p) continue;
+      if (p->plan != B->plans[i]) return fail(IFDTD_ERR_ARGUMENT, "probe belongs to another plan");
+      if (!out_rows || !out_rows[i]) return fail(IFDTD_ERR_ARGUMENT, "output rows missing for a probed member");
+      offset[i] = rows;
+      for (int r = 0; r < p->rows; ++r) rowmap.push_back(make_int2((int)refs.size(), r));
+      refs.push_back(ProbeRef{i, p->kind, p->rows, p->width, p->index, p->layer, p->weight, nullptr});
+      rows += p->rows;
+    }
+  if (n <= 0) return IFDTD_OK;
+  if (rows > 0) {
+    if ((int)refs.size() > B->cap_refs || rows > B->cap_rows) {
+      CUDA_TRY(cudaStreamSynchronize(stream));
+      B->drop_graphs();
+      cudaFree(B->d_refs);
+      cudaFree(B->d_rowmap);
+      cudaFree(B->d_stage);
+      B->d_refs = B->d_rowmap = nullptr;
+      B->d_stage = nullptr;
+      B->cap_refs = B->cap_rows = 0;
+      CUDA_TRY(cudaMalloc(&B->d_refs, refs.size() * sizeof(ProbeRef)));
+      CUDA_TRY(cudaMalloc(&B->d_rowmap, (size_t)rows * sizeof(int2)));
+      CUDA_TRY(cudaMalloc((void**)&B->d_stage, (size_t)B->chunk * rows * sizeof(double)));
+      B->cap_refs = (int)refs.size();
+      B->cap_rows = rows;
+    }
+    for (auto& r : refs) r.staging = B->d_stage + offset[r.member];
+    CUDA_TRY(cudaMemcpyAsync(B->d_refs, refs.data(), refs.size() * sizeof(ProbeRef), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(B->d_rowmap, rowmap.data(), rowmap.size() * sizeof(int2), cudaMemcpyHostToDevice, stream));
+  }
+  struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+  } range("ifdtd_batch_step");
+  const int cap = std::max(B->chunk, 1);
+  for (int s0 = 0; s0 < n; s0 += cap) {
+    const int c = std::min(cap, n - s0);
+    if (currents) {
+      CUDA_TRY(cudaMemcpy2DAsync(B->d_cur, (size_t)B->chunk * sizeof(double), currents + s0, (size_t)n * sizeof(double),
+                                 (size_t)c * sizeof(double), B->n, cudaMemcpyDeviceToDevice, stream));
+      for (const int i : B->solo)
+        CUDA_TRY(cudaMemcpyAsync(B->plans[i]->d_cur, currents + (size_t)i * n + s0, c * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, stream));
+    } else {
+      CUDA_TRY(cudaMemsetAsync(B->d_cur, 0, (size_t)B->n * B->chunk * sizeof(double), stream));
+      for (const int i : B->solo) CUDA_TRY(cudaMemsetAsync(B->plans[i]->d_cur, 0, c * sizeof(double), stream));
+    }
+    if (c == B->chunk) {
+      cudaGraphExec_t exec = nullptr;
+      for (auto& g : B->graphs)
+        if (g.chunk == c && g.rows == rows) exec = g.exec;
+      if (!exec) {
+        cudaGraph_t graph;
+        CUDA_TRY(cudaStreamBeginCapture(B->capture_stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t le = cudaSuccess;
+        for (int i = 0; i < c && le == cudaSuccess; ++i) le = batch_launch_step<real>(B, i, rows, i, B->capture_stream);
+        cudaError_t ce = cudaStreamEndCapture(B->capture_stream, &graph);
+        if (le != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(le));
+        if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess)
+          return fail(IFDTD_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+        B->graphs.push_back({c, rows, exec});
+      }
+      CUDA_TRY(cudaGraphLaunch(exec, stream));
+    } else {
+      for (int i = 0; i < c; ++i) {
+        cudaError_t e = batch_launch_step<real>(B, i, rows, i, stream);
+        if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch step launch: ") + cudaGetErrorString(e));
+      }
+    }
+    for (int i = 0; i < B->n; ++i) {
+      if (offset[i] < 0) continue;
+      const int r = probes[i]->rows;
+      CUDA_TRY(cudaMemcpy2DAsync(out_rows[i] + (size_t)s0 * r, (size_t)r * sizeof(double), B->d_stage + offset[i],
+                                 (size_t)rows * sizeof(double), (size_t)r * sizeof(double), c, cudaMemcpyDeviceToDevice,
+                                 stream));
+    }
+  }
+  return IFDTD_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int32_t ifdtd_version(void) { return 10000; }
@@ -1478,6 +1841,62 @@ int32_t ifdtd_step_sampled(ifdtd_plan* plan, const ifdtd_state* state, const dou
   cudaStream_t st = (cudaStream_t)stream;
   return plan->dtype == 4 ? run_steps<float>(plan, state, currents, n_steps, probe, out_rows, st)
                           : run_steps<double>(plan, state, currents, n_steps, probe, out_rows, st);
+}
+
+int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t chunk, ifdtd_batch** out) {
+  if (!plans || !out || n_members <= 0 || chunk < 1) return fail(IFDTD_ERR_ARGUMENT, "bad batch arguments");
+  *out = nullptr;
+  for (int i = 0; i < n_members; ++i) {
+    if (!plans[i]) return fail(IFDTD_ERR_ARGUMENT, "null member plan");
+    if (plans[i]->device != plans[0]->device || plans[i]->dtype != plans[0]->dtype)
+      return fail(IFDTD_ERR_ARGUMENT, "batch members must share one device and one precision");
+    for (int j = 0; j < i; ++j)
+      if (plans[j] == plans[i]) return fail(IFDTD_ERR_ARGUMENT, "a plan appears twice in the batch");
+  }
+  DeviceGuard guard(plans[0]->device);
+  ifdtd_batch* B = new ifdtd_batch();
+  B->device = plans[0]->device;
+  B->dtype = plans[0]->dtype;
+  B->n = n_members;
+  B->plans.assign(plans, plans + n_members);
+  B->chunk = chunk;
+  for (int i = 0; i < n_members; ++i)
+    if (plans[i]->h_mode != 2 || plans[i]->e_mode != 2) B->chunk = std::min(B->chunk, std::max(plans[i]->chunk, 1));
+  const int rc = B->dtype == 4 ? batch_build<float>(B) : batch_build<double>(B);
+  if (rc) {
+    delete B;
+    return rc;
+  }
+  *out = B;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_batch_destroy(ifdtd_batch* batch) {
+  if (!batch) return IFDTD_OK;
+  DeviceGuard guard(batch->device);
+  cudaDeviceSynchronize();
+  delete batch;
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_batch_step(ifdtd_batch* batch, const ifdtd_state* states, const double* currents, int32_t n_steps,
+                         ifdtd_probe* const* probes, double* const* out_rows, void* stream) {
+  if (!batch || !states) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  if (n_steps < 0) return fail(IFDTD_ERR_ARGUMENT, "negative step count");
+  DeviceGuard guard(batch->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  return batch->dtype == 4 ? run_batch<float>(batch, states, currents, n_steps, probes, out_rows, st)
+                           : run_batch<double>(batch, states, currents, n_steps, probes, out_rows, st);
+}
+
+int32_t ifdtd_batch_info(const ifdtd_batch* batch, int32_t* groups, int32_t* solo, int32_t* kh_grid,
+                         int32_t* ke_grid) {
+  if (!batch || !groups || !solo || !kh_grid || !ke_grid) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  *groups = (int32_t)batch->groups.size();
+  *solo = (int32_t)batch->solo.size();
+  *kh_grid = batch->groups.empty() ? 0 : batch->groups[0].kh_grid;
+  *ke_grid = batch->groups.empty() ? 0 : batch->groups[0].ke_grid;
+  return IFDTD_OK;
 }
 
 int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, void* stream) {

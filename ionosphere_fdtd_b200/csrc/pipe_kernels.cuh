@@ -64,6 +64,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -502,6 +506,94 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
     consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
       ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, group + s, ph, G);
     });
+  }
+}
+
+// Batched launches over the members of an ensemble (one launch per phase for
+// all members that share the template arguments).  CTA b walks the segments
+// segs[sptr[b]] .. segs[sptr[b + 1] - 1], each int4 {member, first patch, end
+// patch, 0}, in order; rings[member] = {stage bytes, stages} of that member's
+// plan.  Every segment starts from a fresh ring: all threads meet, the
+// barriers of the previous segment (all of whose copies have landed and been
+// consumed) are invalidated and initialised again, and the member's record
+// and per-layer rows are loaded.  The per-patch work is kh_consume /
+// ke_consume, so a member's result is the same as its own launch.  A wait that
+// runs out ends the CTA's walk after the segment it happened in.
+template <typename real>
+__device__ __forceinline__ void batch_segment_start(uint64_t* full, uint64_t* empty, uint64_t* group, int prev_stages,
+                                                    int n_stages, int compute_warps) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < prev_stages; ++s) {
+      mbar_inval(full + s);
+      mbar_inval(empty + s);
+      mbar_inval(group + s);
+    }
+    for (int s = 0; s < n_stages; ++s) mbar_init(group + s, compute_warps);  // made visible by ring_setup
+  }
+}
+
+template <typename real, bool PLASMA, int COPY>
+__global__ void __maxnreg__(kMaxRegs) kh_tma_batch(const Rec<real>* __restrict__ recs, const int4* __restrict__ segs,
+                                                   const int* __restrict__ sptr, const int2* __restrict__ rings,
+                                                   int producers) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
+  __shared__ int abort_flag;
+  const int W = producers;
+  if (threadIdx.x == 0) abort_flag = 0;
+  int prev = 0;
+  for (int k = sptr[blockIdx.x]; k < sptr[blockIdx.x + 1]; ++k) {
+    __syncthreads();
+    if (abort_flag) break;
+    const int4 sg = segs[k];
+    const int2 rg = rings[sg.x];
+    batch_segment_start<real>(full, empty, group, prev, rg.y, (blockDim.x - 32 * W) / 32);
+    prev = rg.y;
+    Layers<real> Ls;
+    Ring G;
+    ring_setup(R, recs + sg.x, dyn_smem, full, empty, &abort_flag, rg.x, rg.y, COPY == 0 ? W : 32 * W, W, Ls, G);
+    if (threadIdx.x < 32 * W) {
+      produce<COPY>(R, G, sg.y, sg.z, R.n_patches_h, R.dptr_h, R.desc_h, R.tab_h, threadIdx.x / 32, W);
+    } else {
+      const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
+      consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
+        kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G);
+      });
+    }
+  }
+}
+
+template <typename real, bool PLASMA, int MAXDEG, int COPY>
+__global__ void __maxnreg__(kMaxRegs) ke_tma_batch(const Rec<real>* __restrict__ recs, const int4* __restrict__ segs,
+                                                   const int* __restrict__ sptr, const int2* __restrict__ rings,
+                                                   int producers, int istep) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
+  __shared__ int abort_flag;
+  const int W = producers;
+  if (threadIdx.x == 0) abort_flag = 0;
+  int prev = 0;
+  for (int k = sptr[blockIdx.x]; k < sptr[blockIdx.x + 1]; ++k) {
+    __syncthreads();
+    if (abort_flag) break;
+    const int4 sg = segs[k];
+    const int2 rg = rings[sg.x];
+    batch_segment_start<real>(full, empty, group, prev, rg.y, (blockDim.x - 32 * W) / 32);
+    prev = rg.y;
+    Layers<real> Ls;
+    Ring G;
+    ring_setup(R, recs + sg.x, dyn_smem, full, empty, &abort_flag, rg.x, rg.y, COPY == 0 ? W : 32 * W, W, Ls, G);
+    if (threadIdx.x < 32 * W) {
+      produce<COPY>(R, G, sg.y, sg.z, R.n_patches_e, R.dptr_e, R.desc_e, R.tab_e, threadIdx.x / 32, W);
+    } else {
+      const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
+      const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+      consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
+        ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, group + s, ph, G);
+      });
+    }
   }
 }
 

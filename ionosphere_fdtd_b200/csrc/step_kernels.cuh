@@ -882,6 +882,42 @@ __global__ void sample_rec_kernel(const Rec<real>* __restrict__ rec, int kind, i
   if (lane == 0) out[warp] = acc;
 }
 
+// One member's probe in a batched sampling launch: the member's record,
+// field kind, rows, support width, the probe's device tables and the row of
+// its staging buffer that this step writes.
+struct ProbeRef {
+  int member, kind, rows, width;
+  const int* index;
+  const int* layer;
+  const double* weight;
+  double* staging;  // column 0 of this probe's rows in the (chunk, total rows) staging
+};
+
+// Receiver rows of every member of an ensemble in one launch: warp w samples
+// global row w; rowmap[w] = {probe, row within that probe}.  Same arithmetic
+// as sample_rec_kernel; step `step_row` of the chunk goes to row step_row of
+// the (chunk, total_rows) staging.
+template <typename real>
+__global__ void sample_batch_kernel(const Rec<real>* __restrict__ recs, const ProbeRef* __restrict__ refs,
+                                    const int2* __restrict__ rowmap, int total_rows, int step_row) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= total_rows) return;
+  const int2 rm = rowmap[warp];
+  const ProbeRef pr = refs[rm.x];
+  const Rec<real>* rec = recs + pr.member;
+  const real* field = pr.kind == 0 ? rec->er : pr.kind == 1 ? rec->et : pr.kind == 2 ? rec->hr : rec->ht;
+  const int pitch = (pr.kind == 0 || pr.kind == 3) ? rec->Pn : rec->Pm;
+  double acc = 0.0;
+  for (int q = lane; q < pr.width; q += 32) {
+    const int o = rm.y * pr.width + q;
+    acc += pr.weight[o] * (double)field[(size_t)pr.index[o] * pitch + pr.layer[o]];
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, s);
+  if (lane == 0) pr.staging[(size_t)step_row * total_rows + rm.y] = acc;
+}
+
 // max |x| of up to four arrays; results combined with an order-independent
 // atomic max on the bit pattern of non-negative doubles (NaN sorts above +Inf,
 // so a non-finite field reports NaN or Inf).  Row padding is zero and does not

@@ -601,18 +601,7 @@ class GeodesicFDTD:
         w = np.asarray(weights, dtype=np.float64)
         steps = self._validated_count(steps, "step count", minimum=0)
         self._validated_count(synchronize_every, "synchronize_every", minimum=1)
-        if vertices.ndim != 2 or w.shape != vertices.shape:
-            raise ValueError("vertex_indices and weights must have matching 2-D shapes")
-        if layers.shape != (vertices.shape[0],):
-            raise ValueError("radial_layers must contain one layer per observation")
-        if np.any(vertices < 0) or np.any(vertices >= self.mesh.n_vertices):
-            raise ValueError("observation vertex index is out of range")
-        if np.any(layers < 0) or np.any(layers >= len(self.radii_m)):
-            raise ValueError("observation radial layer is out of range")
-        if not np.all(np.isfinite(w)):
-            raise ValueError("observation weights must be finite")
-        if not np.allclose(w.sum(axis=1), 1.0):
-            raise ValueError("observation weights must sum to one")
+        self._check_er_observation(vertices, layers, w)
         torch = self.backend.torch
         traces = torch.zeros((steps + 1, vertices.shape[0]), dtype=torch.float64, device=self.backend.torch_device)
         probe = self._engine.probe("er", vertices, np.broadcast_to(layers[:, None], vertices.shape), w)
@@ -627,6 +616,24 @@ class GeodesicFDTD:
         finally:
             probe.close()
         return self.to_numpy(traces)
+
+    def _check_er_observation(self, vertices, layers, w) -> None:
+        """Shape, range and weight checks of an Er observation set (vertices
+        (R, K), layers (R,), weights (R, K)) with the reference's messages
+        (solver.py:1104-1115)."""
+
+        if vertices.ndim != 2 or w.shape != vertices.shape:
+            raise ValueError("vertex_indices and weights must have matching 2-D shapes")
+        if layers.shape != (vertices.shape[0],):
+            raise ValueError("radial_layers must contain one layer per observation")
+        if np.any(vertices < 0) or np.any(vertices >= self.mesh.n_vertices):
+            raise ValueError("observation vertex index is out of range")
+        if np.any(layers < 0) or np.any(layers >= len(self.radii_m)):
+            raise ValueError("observation radial layer is out of range")
+        if not np.all(np.isfinite(w)):
+            raise ValueError("observation weights must be finite")
+        if not np.allclose(w.sum(axis=1), 1.0):
+            raise ValueError("observation weights must sum to one")
 
     def record_h_observations(
         self,

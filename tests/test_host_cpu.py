@@ -255,3 +255,14 @@ def test_geographic_face_search_equals_the_full_scan():
         points += [(float(rng.uniform(-90, 90)), float(rng.uniform(-180, 180))) for _ in range(100)]
         for lat, lon in points:
             assert S.geographic_face_index(sim, lat, lon) == full_scan(sim, lat, lon), (sub, lat, lon)
+
+
+def test_ensemble_rejects_empty_member_lists_and_bad_chunks():
+    from ionosphere_fdtd_b200 import Ensemble
+
+    with pytest.raises(ValueError, match="at least one member"):
+        Ensemble([])
+    with pytest.raises(ValueError, match="graph_chunk"):
+        Ensemble([object()], graph_chunk=0)
+    with pytest.raises(TypeError, match="GeodesicFDTD"):
+        Ensemble([object()])
