@@ -12,6 +12,12 @@ HBM; ``e2e`` is the same metric through the public API
 (``GeodesicFDTD.record_er_observations``) with host-computed source currents
 copied in and receiver traces copied out every bench step.
 
+``--workload config3`` measures ensemble runs/s instead: 64 seeded members
+of uneven size (s5-s7, 24-60 radial cells, exponential ionospheres, 16
+receivers each), each run being 5000 leapfrog steps; ``value`` is the batched
+``Ensemble`` step (all members per launch) and ``sequential`` the same members
+stepped one after another, both with the receivers sampled on the device.
+
 ``--impl reference`` times the CPU oracle (a NumPy restatement of the
 reference's own NumPy path, the reference being pure Python) on a bounded
 sample of the same workload.  Under torchrun every rank runs an independent
@@ -45,7 +51,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("engine", "reference"), default="engine")
-    p.add_argument("--workload", choices=("config2", "config4"), default="config2")
+    p.add_argument("--workload", choices=("config2", "config3", "config4"), default="config2")
+    p.add_argument("--members", type=int, default=64, help="config3: ensemble members")
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -262,8 +269,222 @@ def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
     return oracle_time(sim, info, steps)
 
 
+ENSEMBLE_METRIC = "ensemble runs/s"
+RUN_STEPS = 5000  # leapfrog steps per ensemble run
+
+
+def oracle_ensemble_rate(steps: int = 1) -> dict:
+    """CPU oracle rate (Gcell/s) on a mid-size ensemble member: s6 / 40 cells,
+    exponential ionosphere, float32, one Gaussian source."""
+
+    import oracle.fdtd as O
+
+    sim = O.OracleFDTD(subdivision=6, radial_cells=40, material=O.EarthIonosphereParams(lithosphere_conductivity_s_m=1.0e-2),
+                       dtype=np.float32, source=O.OracleSource(peak_current_a=1.0, carrier_frequency_hz=30.0))
+    info = {"cells": sim.mesh.n_vertices * 40, "sub": 6, "L": 40}
+    sim.step(1)
+    return oracle_time(sim, info, steps)
+
+
+def ensemble_reference_arm(args) -> None:
+    from ionosphere_fdtd_b200 import workloads as W
+
+    cells = ensemble_cells(args.members)
+    mean_cells = statistics.mean(cells)
+    rates, secs = [], 0.0
+    for _ in range(args.warmup):
+        oracle_ensemble_rate()
+    for _ in range(args.steps):
+        r = oracle_ensemble_rate()
+        rates.append(r["gcells"])
+        secs += r["seconds"]
+    gcells = statistics.median(rates)
+    value = gcells * 1e9 / (RUN_STEPS * mean_cells)
+    sample = (f"1 leapfrog step of an s6/L40 float32 member per bench step ({r['cells']} cells), NumPy oracle; runs/s = "
+              f"rate / ({RUN_STEPS} steps x mean member cells {mean_cells:.0f})")
+    line = {
+        "impl": "reference", "metric": ENSEMBLE_METRIC, "value": value, "unit": "runs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config3", "members": args.members, "run_steps": RUN_STEPS, "device": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "runs/s", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ensemble_cells(members: int) -> list[int]:
+    """Cells (vertices x radial cells) of the config3 members."""
+
+    from ionosphere_fdtd_b200 import workloads as W
+
+    return [(10 * 4 ** d["subdivision"] + 2) * d["radial_cells"] for d in W.config3_draws(members=members)]
+
+
+def ensemble_main(args, world: int, rank: int, local: int) -> None:
+    import torch
+
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    device = f"cuda:{local}"
+    t_setup = time.perf_counter()
+    wls = W.config3_members(device=device, members=args.members)
+    setup_s = time.perf_counter() - t_setup
+    sims = [w.simulation for w in wls]
+    for sim in sims:
+        W.seed_fields(sim)
+    T = args.time_steps or 100
+    stream = torch.cuda.current_stream()
+    probes = [sim._engine.probe("er", w.receivers[0], np.broadcast_to(w.receivers[1][:, None], w.receivers[0].shape), w.receivers[2])
+              for sim, w in zip(sims, wls)]
+    outs = [torch.zeros((T, w.receivers[0].shape[0]), dtype=torch.float64, device=device) for w in wls]
+    ens = Ensemble(sims)
+    layout = ens.launch_layout()
+
+    def batched():
+        ens._run(T, probes, outs)
+        ens._advance_clocks(T)
+
+    def sequential():
+        for sim, probe, out in zip(sims, probes, outs):
+            sim._engine.step_sampled(sim._state(), sim._source_currents(T), T, probe, out)
+            sim.steps += T
+            sim.time_s = sim.steps * sim.time_step_s
+
+    def timed(fn, reps):
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        marks[0].record(stream)
+        for i in range(reps):
+            fn()
+            marks[i + 1].record(stream)
+        torch.cuda.synchronize()
+        return [marks[i].elapsed_time(marks[i + 1]) for i in range(reps)]
+
+    for _ in range(max(args.warmup, 3)):
+        batched()
+        sequential()
+    uuid = getattr(torch.cuda.get_device_properties(local), "uuid", None)
+    sampler = ClockSampler(f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None))
+    b_ms = timed(batched, args.steps)
+    clocks = sampler.stop()
+    s_ms = timed(sequential, args.steps)
+    b_total, s_total = sum(b_ms), sum(s_ms)
+    if dist:
+        b_total = max_over_ranks(b_total, dist, device)
+        s_total = max_over_ranks(s_total, dist, device)
+    n = len(sims)
+    b_step = b_total / args.steps / T  # ms per leapfrog step of the whole ensemble
+    s_step = s_total / args.steps / T
+    value = world * n / (RUN_STEPS * b_step / 1e3)
+    seq_value = world * n / (RUN_STEPS * s_step / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        obs = [w.receivers for w in wls]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            traces = ens.record_er_observations(obs, T)
+        wall = time.perf_counter() - t0
+        if dist:
+            wall = max_over_ranks(wall, dist, device)
+        e2e = {
+            "value": world * n / (RUN_STEPS * wall / args.steps / T),
+            "unit": "runs/s",
+            "h2d_bytes_per_step": 8 * T * n,
+            "d2h_bytes_per_step": int(sum(t.nbytes for t in traces)),
+            "api": "Ensemble.record_er_observations",
+        }
+    peak, peak_kind = measured_peak()
+    step_bytes = sum(w.bytes_per_step for w in wls)
+    achieved = step_bytes / (b_step / 1e3) / 1e9
+    seq_achieved = step_bytes / (s_step / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm",
+        "kernel": "kh_tma_batch + ke_tma_batch + sample_batch_kernel (one batched leapfrog step of all members)",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "traffic": None,
+        "algorithmic_bytes_per_step": step_bytes,
+    }
+    cells = [w.cells for w in wls]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = oracle_ensemble_rate()
+        cpu = {
+            "value": r["gcells"] * 1e9 / (RUN_STEPS * statistics.mean(cells)),
+            "unit": "runs/s",
+            "cores": 1,
+            "kind": "port",
+            "sample": f"1 leapfrog step of an s6/L40 float32 member ({r['seconds']:.1f} s), NumPy oracle; runs/s = rate / ({RUN_STEPS} x mean member cells)",
+        }
+    for p in probes:
+        p.close()
+    if rank == 0:
+        line = {
+            "metric": ENSEMBLE_METRIC,
+            "value": value,
+            "unit": "runs/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": b_total / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": "config3",
+                "members": n,
+                "subdivisions": sorted({s.config.subdivision for s in sims}),
+                "radial_cells": [min(s.config.radial_cells for s in sims), max(s.config.radial_cells for s in sims)],
+                "cells_total": int(sum(cells)),
+                "receivers_per_member": int(wls[0].receivers[0].shape[0]),
+                "run_steps": RUN_STEPS,
+                "time_steps_per_step": T,
+                "setup_s": setup_s,
+                "launch_layout": layout,
+                "l2": f"ensemble state {step_bytes // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
+                "parallelism": f"replicas x{world}",
+            },
+            "sequential": {"value": seq_value, "unit": "runs/s", "ms_per_step": s_total / args.steps, "achieved_gbs": seq_achieved,
+                           "api": "each member's own ifdtd_step_sampled, one member after another"},
+            "speedup_vs_sequential": value / seq_value,
+            "gcell_updates_per_s": sum(cells) / (b_step / 1e3) / 1e9,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * T * (2 * layout["groups"] + 2 * layout["solo"] + 1),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ens.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def reference_arm(args, world: int, rank: int) -> None:
     if rank != 0:
+        return
+    if args.workload == "config3":
+        ensemble_reference_arm(args)
         return
     per_step = 1
     sim, info = oracle_build(args.workload)
@@ -304,6 +525,9 @@ def main() -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, world, rank)
+        return
+    if args.workload == "config3":
+        ensemble_main(args, world, rank, local)
         return
     import torch
 

@@ -10,6 +10,12 @@ setup (material profile, plasma profile, source, receivers) built from a seed.
   electron plasma n_e(h) = 1e6 exp((h - 85 km)/3 km) m^-3,
   nu(h) = 1e7 exp(-(h - 70 km)/6 km) s^-1, a 50 Hz source and 64 receivers at
   seed-uniform sphere points with barycentric weights.
+* ``config3``: an ensemble of 64 independent runs of uneven size: subdivision
+  uniform in {5, 6, 7}, radial cells uniform in 24-60, an exponential
+  ionosphere sigma(h) = sigma0 exp((h - h0)/zeta) with sigma0 log-uniform in
+  1e-8-1e-6 S/m, h0 uniform in 55-70 km and zeta uniform in 3-6 km, ground
+  sigma log-uniform in 1e-3-1e-1 S/m, a seed-uniform source vertex with a
+  carrier uniform in 10-60 Hz and 16 receivers at seed-uniform sphere points.
 * ``config4``: s9 / 80 cells over 0-100 km with the surface-impedance lower
   boundary over a seeded smooth log-normal ground-conductivity map (median
   1e-2 S/m), the config-2 plasma, a 20 Hz source and 256 receivers.
@@ -164,6 +170,56 @@ def config4(device: str = "cuda", dtype: str = "float32", seed: int = 20260814, 
     )
     rec = uniform_receivers(sim, receivers, seed)
     return Workload("config4", sim, rec, mesh.n_vertices * radial_cells, algorithmic_bytes_per_step(sim))
+
+
+def config3_draws(seed: int = 20260803, members: int = 64) -> list[dict]:
+    """The seeded per-member parameters of the ensemble configuration."""
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(members):
+        d = {"subdivision": int(rng.integers(5, 8)), "radial_cells": int(rng.integers(24, 61))}
+        d["sigma0"] = 10.0 ** rng.uniform(-8.0, -6.0)
+        d["h0"] = rng.uniform(55_000.0, 70_000.0)
+        d["zeta"] = rng.uniform(3_000.0, 6_000.0)
+        d["ground"] = 10.0 ** rng.uniform(-3.0, -1.0)
+        d["carrier"] = rng.uniform(10.0, 60.0)
+        d["source_draw"] = int(rng.integers(1 << 31))
+        d["receiver_seed"] = int(rng.integers(1 << 31))
+        out.append(d)
+    return out
+
+
+def config3_members(device: str = "cuda", dtype: str = "float32", seed: int = 20260803, members: int = 64, receivers: int = 16, **kwargs) -> list[Workload]:
+    """The ensemble configuration: ``members`` seeded runs of uneven size and
+    physics (one mesh per subdivision level, shared by its members)."""
+
+    from .constants import EPSILON_0
+    from .materials import EarthIonosphereMaterial
+    from .mesh import build_geodesic_mesh
+    from .solver import GeodesicFDTD, SimulationConfig
+
+    meshes: dict[int, object] = {}
+    out = []
+    for i, d in enumerate(config3_draws(seed, members)):
+        sub, L, ground, h0, zeta, sigma0, carrier = (d[k] for k in ("subdivision", "radial_cells", "ground", "h0", "zeta", "sigma0", "carrier"))
+        src_draw, rec_seed = d["source_draw"], d["receiver_seed"]
+        mesh = meshes.get(sub)
+        if mesh is None:
+            mesh = meshes[sub] = build_geodesic_mesh(sub)
+        material = EarthIonosphereMaterial(
+            lithosphere_conductivity_s_m=ground,
+            ionosphere_reference_height_m=h0,
+            ionosphere_scale_height_m=zeta,
+            ionosphere_prefactor_hz=sigma0 / EPSILON_0,
+        )
+        lat, lon = vertex_lat_lon(mesh.vertices, src_draw % mesh.n_vertices)
+        source = GaussianCurrent(latitude_deg=lat, longitude_deg=lon, peak_current_a=1.0, carrier_frequency_hz=carrier)
+        sim = GeodesicFDTD(SimulationConfig(subdivision=sub, radial_cells=L), material=material, source=source, mesh=mesh,
+                           device=device, dtype=dtype, **kwargs)
+        rec = uniform_receivers(sim, receivers, rec_seed)
+        out.append(Workload(f"config3[{i}]", sim, rec, mesh.n_vertices * L, algorithmic_bytes_per_step(sim)))
+    return out
 
 
 def seed_fields(sim, seed: int = 20260814, amplitude: float = 1.0e-6) -> None:
