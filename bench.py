@@ -53,6 +53,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--impl", choices=("engine", "reference"), default="engine")
     p.add_argument("--workload", choices=("config2", "config3", "config4"), default="config2")
     p.add_argument("--members", type=int, default=64, help="config3: ensemble members")
+    p.add_argument("--no-autotune", action="store_true", help="config3: keep the automatic launch geometry")
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -342,6 +343,19 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
     sims = [w.simulation for w in wls]
     for sim in sims:
         W.seed_fields(sim)
+    tuning = None
+    if not args.no_autotune:
+        from ionosphere_fdtd_b200.autotune import SHAPE_FREE_CANDIDATES, autotune_ensemble
+
+        t_tune = time.perf_counter()
+        tuned = autotune_ensemble(sims, SHAPE_FREE_CANDIDATES, steps=32, repeats=3,
+                                  key=lambda m: (m.config.subdivision, m.backend.itemsize))
+        tuning = {
+            "seconds": time.perf_counter() - t_tune,
+            "candidates": len(SHAPE_FREE_CANDIDATES),
+            "classes": {f"s{k[0]}": {"producer_warps": r.best.producer_warps, "staging": r.best.staging, "ms_per_step": r.best_ms}
+                        for k, r in tuned.items()},
+        }
     T = args.time_steps or 100
     stream = torch.cuda.current_stream()
     probes = [sim._engine.probe("er", w.receivers[0], np.broadcast_to(w.receivers[1][:, None], w.receivers[0].shape), w.receivers[2])
@@ -460,6 +474,7 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
                 "time_steps_per_step": T,
                 "setup_s": setup_s,
                 "launch_layout": layout,
+                "autotune": tuning,
                 "l2": f"ensemble state {step_bytes // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
                 "parallelism": f"replicas x{world}",
             },

@@ -266,3 +266,12 @@ def test_ensemble_rejects_empty_member_lists_and_bad_chunks():
         Ensemble([object()], graph_chunk=0)
     with pytest.raises(TypeError, match="GeodesicFDTD"):
         Ensemble([object()])
+
+
+def test_autotune_rejects_bad_arguments_before_touching_the_device():
+    from ionosphere_fdtd_b200.autotune import autotune
+
+    with pytest.raises(ValueError, match="positive"):
+        autotune(object(), steps=0)
+    with pytest.raises(ValueError, match="candidate"):
+        autotune(object(), candidates=())
