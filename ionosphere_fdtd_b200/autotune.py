@@ -8,9 +8,9 @@ for every candidate from the simulation's own mesh and physics, times
 graph-captured steps of each on the simulation's own state with CUDA events,
 restores that state, and installs the fastest plan.  Every candidate computes
 the same bits (patch size and kernel family do not change any result), so
-tuning changes speed only.  ``autotune_ensemble`` tunes one representative
-member per (mesh level, radial cells, physics) class and gives the winner to
-the whole class.
+tuning changes speed only.  ``autotune_ensemble`` tunes the largest member
+of each class (by default: mesh level, radial cells, precision and physics)
+and gives the winner to the whole class.
 """
 
 from __future__ import annotations
@@ -164,9 +164,9 @@ def autotune_ensemble(members: Sequence, candidates: Sequence[Tuning] = DEFAULT_
     for group in classes.values():
         group.sort(key=lambda m: -m.mesh.n_vertices * m.config.radial_cells)
     out = {}
-    for key, group in classes.items():
+    for cls, group in classes.items():
         res = autotune(group[0], candidates, steps=steps, repeats=repeats)
-        out[key] = res
+        out[cls] = res
         for m in group[1:]:
             if m._engine.tuning != res.best:
                 engine = _engine_for(m, res.best)
