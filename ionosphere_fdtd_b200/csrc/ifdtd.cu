@@ -1112,9 +1112,16 @@ int bind_state(ifdtd_plan* P, const ifdtd_state* st, cudaStream_t stream) {
   return IFDTD_OK;
 }
 
+// Dynamic shared memory above 48 KiB is opted into per kernel function.  The
+// limit is only ever raised: plans and batch groups that launch the same
+// instantiation with smaller stages (and graphs captured for them) stay valid.
 template <typename K>
 cudaError_t allow_smem(K kernel, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
+  cudaFuncAttributes attr;
+  cudaError_t e = cudaFuncGetAttributes(&attr, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)attr.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
@@ -1309,6 +1316,7 @@ struct ifdtd_batch {
     cudaGraphExec_t exec;
   };
   std::vector<Graph> graphs;
+  std::string failed;  // the launch that failed last (error messages)
   void drop_graphs() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     graphs.clear();
@@ -1471,27 +1479,39 @@ int batch_build(ifdtd_batch* B) {
 template <typename real>
 cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row, cudaStream_t st) {
   const Rec<real>* recs = (const Rec<real>*)B->d_recs;
-  for (const auto& g : B->groups) {
+  cudaError_t e = cudaSuccess;
+  // every launch is checked at once, so a failure reports its own error
+  // rather than the invalidated capture it leaves behind
+  for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
+    const BatchGroup& g = B->groups[q];
     auto k = batch_kh_kernel<real>(g);
     k<<<g.kh_grid, g.threads + 32 * g.producers, g.kh_smem, st>>>(recs, g.segs_h, g.sptr_h, B->d_ring_h, g.producers);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) B->failed = "kh_tma_batch of group " + std::to_string(q);
   }
-  for (const int i : B->solo) {
-    cudaError_t e = launch_kh<real>(B->plans[i], st);
-    if (e != cudaSuccess) return e;
+  for (size_t q = 0; q < B->solo.size() && e == cudaSuccess; ++q) {
+    e = launch_kh<real>(B->plans[B->solo[q]], st);
+    if (e != cudaSuccess) B->failed = "H phase of member " + std::to_string(B->solo[q]);
   }
-  for (const auto& g : B->groups) {
+  for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
+    const BatchGroup& g = B->groups[q];
     auto k = batch_ke_kernel<real>(g);
     k<<<g.ke_grid, g.threads + 32 * g.producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.producers,
                                                                    istep);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) B->failed = "ke_tma_batch of group " + std::to_string(q);
   }
-  for (const int i : B->solo) {
-    cudaError_t e = launch_ke<real>(B->plans[i], istep, st);
-    if (e != cudaSuccess) return e;
+  for (size_t q = 0; q < B->solo.size() && e == cudaSuccess; ++q) {
+    e = launch_ke<real>(B->plans[B->solo[q]], istep, st);
+    if (e != cudaSuccess) B->failed = "E phase of member " + std::to_string(B->solo[q]);
   }
-  if (rows > 0)
+  if (rows > 0 && e == cudaSuccess) {
     sample_batch_kernel<real><<<(rows * 32 + 255) / 256, 256, 0, st>>>(recs, (const ProbeRef*)B->d_refs,
                                                                          (const int2*)B->d_rowmap, rows, step_row);
-  return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) B->failed = "sample_batch_kernel";
+  }
+  return e;
 }
 
 template <typename real>
@@ -1589,7 +1609,8 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
         cudaError_t le = cudaSuccess;
         for (int i = 0; i < c && le == cudaSuccess; ++i) le = batch_launch_step<real>(B, i, rows, i, B->capture_stream);
         cudaError_t ce = cudaStreamEndCapture(B->capture_stream, &graph);
-        if (le != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(le));
+        if (le != cudaSuccess)
+          return fail(IFDTD_ERR_CUDA, "batch graph capture: " + B->failed + ": " + cudaGetErrorString(le));
         if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
         cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
@@ -1601,7 +1622,7 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
     } else {
       for (int i = 0; i < c; ++i) {
         cudaError_t e = batch_launch_step<real>(B, i, rows, i, stream);
-        if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch step launch: ") + cudaGetErrorString(e));
+        if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "batch step launch: " + B->failed + ": " + cudaGetErrorString(e));
       }
     }
     for (int i = 0; i < B->n; ++i) {

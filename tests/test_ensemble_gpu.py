@@ -109,3 +109,27 @@ def test_batched_receiver_traces_match_each_members_own_recording():
             assert traces[i].shape == expected.shape
             assert np.array_equal(traces[i], expected), names[i]
         _assert_same(together[i], sim, names[i])
+
+
+def test_members_with_different_launch_tunings_form_groups_and_match_their_own_runs():
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    # producer warps 1 / 2 / 3 and the cp.async copy engine: four groups, two of
+    # which share a kernel instantiation with different shared-memory sizes
+    spec = [
+        ("config1_s2", Tuning(producer_warps=1)),
+        ("plasma_drude_s2", Tuning()),
+        ("source_s1", Tuning(producer_warps=3)),
+        ("config4_mini_s2", Tuning(staging=3)),
+        ("surface_s1", Tuning(producer_warps=1)),
+    ]
+    together = [build_product(CS.CASES[n], "float32", tuning=t) for n, t in spec]
+    alone = [build_product(CS.CASES[n], "float32", tuning=t) for n, t in spec]
+    with Ensemble(together) as ens:
+        assert ens.launch_layout()["groups"] == 4
+        ens.step(34)
+    for sim in alone:
+        sim.step(34)
+    for (name, _), a, b in zip(spec, together, alone):
+        _assert_same(a, b, name)
