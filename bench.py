@@ -555,7 +555,9 @@ def main() -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
     device = f"cuda:{local}"
+    t_setup = time.perf_counter()
     wl = build(args.workload, device, subdivision=args.subdivision)
+    setup_s = time.perf_counter() - t_setup
     sim = wl.simulation
     T = args.time_steps or (1000 if args.workload == "config2" else 100)
     stream = torch.cuda.current_stream()
@@ -652,6 +654,7 @@ def main() -> None:
         "receivers": int(wl.receivers[0].shape[0]),
         "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
         "parallelism": f"replicas x{world}",
+        "setup_s": setup_s,
     }
     drift = None
     if rank == 0 and world == 1 and not args.no_drift:

@@ -20,6 +20,7 @@ import hashlib
 import json
 import os
 import tempfile
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import asdict, dataclass
 from pathlib import Path
 from typing import Any
@@ -327,9 +328,21 @@ def face_reconstruction(mesh) -> tuple[NDArray[np.float64], NDArray[np.float64]]
     tangents = np.cross(normals[mesh.face_edges], mesh.face_centers[:, None, :])
     tangents /= np.linalg.norm(tangents, axis=2, keepdims=True)
     recon = np.empty_like(tangents)
-    step = 1 << 18
-    for start in range(0, mesh.n_faces, step):
+    step = 1 << 15
+
+    # LAPACK works on each 3 x 3 matrix alone, so the chunks may run on
+    # threads (numpy releases the GIL in them) and the bits do not change
+    def chunk(start: int) -> None:
         recon[start : start + step] = np.swapaxes(np.linalg.pinv(tangents[start : start + step]), 1, 2)
+
+    starts = range(0, mesh.n_faces, step)
+    workers = min(len(starts), os.cpu_count() or 1)
+    if workers > 1:
+        with ThreadPoolExecutor(workers) as pool:
+            list(pool.map(chunk, starts))
+    else:
+        for start in starts:
+            chunk(start)
     return recon, tangents
 
 
