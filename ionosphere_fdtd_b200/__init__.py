@@ -4,6 +4,12 @@ Public names follow the reference package (``ionosphere_fdtd``) so that code
 written against its PyTorch CUDA backend switches by changing the import.
 """
 
+from .adaptive_mesh import (
+    AdaptiveMeshValidation,
+    SphericalRefinementRegion,
+    build_adaptive_geodesic_mesh,
+    validate_adaptive_mesh,
+)
 from .backend import CudaBackend, create_backend
 from .checkpoint import load_checkpoint, save_checkpoint
 from .constants import C_0, EARTH_RADIUS_M, EPSILON_0, MU_0
@@ -39,6 +45,10 @@ from .surface_impedance import ConductiveHalfSpaceSurface, SurfaceImpedanceADE
 __version__ = "0.1.0"
 
 __all__ = [
+    "AdaptiveMeshValidation",
+    "SphericalRefinementRegion",
+    "build_adaptive_geodesic_mesh",
+    "validate_adaptive_mesh",
     "Ensemble",
     "BackendUnavailableError",
     "C_0",

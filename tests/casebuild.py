@@ -54,11 +54,27 @@ def plasma_arrays(spec: dict, n_faces: int, cfg: dict):
     return mids, magnetic, species
 
 
+def adaptive_mesh(case: dict):
+    """The package's locally refined mesh of an adaptive case."""
+
+    import ionosphere_fdtd_b200 as P
+    from ionosphere_fdtd_b200.adaptive_mesh import SphericalRefinementRegion, build_adaptive_geodesic_mesh
+
+    base, regions = case["adaptive"]
+    return build_adaptive_geodesic_mesh(base, tuple(SphericalRefinementRegion(*r) for r in regions))
+
+
 def build_oracle(case: dict, dtype=np.float64):
     import oracle.fdtd as O
 
     cfg = dict(case["config"])
-    mesh = O.build_mesh(cfg["subdivision"])
+    if "adaptive" in case:
+        # the refined vertices and faces come from the package's builder, pinned
+        # bit for bit to the reference's by tests/test_adaptive_cpu.py
+        m = adaptive_mesh(case)
+        mesh = O.assemble_mesh(np.array(m.vertices), np.array(m.faces), m.subdivision)
+    else:
+        mesh = O.build_mesh(cfg["subdivision"])
     kwargs = dict(
         subdivision=cfg["subdivision"],
         radial_cells=cfg["radial_cells"],
@@ -164,7 +180,7 @@ def build_product(case: dict, dtype: str = "float64", **kwargs):
     import ionosphere_fdtd_b200 as P
 
     cfg = P.SimulationConfig(**case["config"])
-    mesh = P.build_geodesic_mesh(cfg.subdivision)
+    mesh = adaptive_mesh(case) if "adaptive" in case else P.build_geodesic_mesh(cfg.subdivision)
     mat = case.get("material", "default")
     if mat == "default":
         material = None

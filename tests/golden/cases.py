@@ -216,6 +216,26 @@ CASES: dict[str, dict] = {
         receivers=dict(seed=20260805, count=8),
         steps=1000,
     ),
+    # locally refined meshes (adaptive_mesh.py): base level, refinement regions
+    # (lat, lon, radius, target level, transition width, label); vertex degree 7-8
+    "adaptive_s1": dict(
+        config=dict(subdivision=1, radial_cells=6, courant_factor=0.2),
+        adaptive=(1, ((35.0, 126.0, 8.0, 3, 8.0, "source"),)),
+        material="default",
+        source=dict(kind="vertical", peak_current_a=1.0e6, seed_vertex=20260806),
+        init=(20260807, 1.0e-6),
+        steps=12,
+    ),
+    "adaptive_plasma_si_s1": dict(
+        config=dict(subdivision=1, radial_cells=5, minimum_altitude_m=0.0, maximum_altitude_m=100_000.0, courant_factor=0.25,
+                    radial_boundary_condition="surface-impedance"),
+        adaptive=(1, ((46.5, -90.9, 8.0, 3, 8.0, "source"), (69.0, -156.0, 8.0, 3, 8.0, "oil"))),
+        material="default",
+        surface=dict(conductivity="scalar", value=1.0e-2),
+        plasma=dict(kind="uniform", magnetic_t=40.0e-6, density_m3=1.0e6, collision_hz=1.0e4, two_species=True),
+        init=(13, 1.0e-9),
+        steps=8,
+    ),
 }
 
 

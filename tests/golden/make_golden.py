@@ -67,7 +67,13 @@ def _provenance(rdata):
 def build_reference(case: dict, mods, dtype: str = "float64"):
     rmesh, rsolver, rsources, rsi, rplasma, rmat, rdata, _ = mods
     cfg = rsolver.SimulationConfig(**case["config"])
-    mesh = rmesh.build_geodesic_mesh(cfg.subdivision)
+    if "adaptive" in case:
+        from ionosphere_fdtd import adaptive_mesh as ram
+
+        base, regions = case["adaptive"]
+        mesh = ram.build_adaptive_geodesic_mesh(base, tuple(ram.SphericalRefinementRegion(*r) for r in regions))
+    else:
+        mesh = rmesh.build_geodesic_mesh(cfg.subdivision)
     mat = case.get("material", "default")
     if mat == "default":
         material = None
@@ -194,6 +200,13 @@ def main(src: str) -> None:
     mods = _import_reference(src)
     if "--checkpoint-only" in sys.argv:
         checkpoint_fixture(mods)
+        return
+    only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--cases=")]
+    if only:
+        # regenerate the named cases only: --cases=name1,name2
+        for name in only[0].split(","):
+            np.savez_compressed(HERE / f"case_{name}.npz", **run_case(name, C.CASES[name], mods))
+            print("wrote", name)
         return
     checkpoint_fixture(mods)
     mesh_fixtures(mods)
