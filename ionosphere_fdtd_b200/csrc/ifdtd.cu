@@ -933,7 +933,13 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   if (staging != 1) {
     PipeTables th_tab, te_tab;
     std::vector<int> locA(std::max(nV, std::max(nE, nF)), 0), locB(std::max(nE, nF), 0);
-    const std::vector<int> h_cand = auto_h ? std::vector<int>{64, 32, 16, 8} : std::vector<int>{fpp};
+    // the pipelined consumers give every compute thread a fixed radial quad,
+    // so no row may have more quads than the CTA has compute threads (at least
+    // 256 when the count is automatic)
+    const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
+    const bool quads_fit = row_quads <= (auto_threads ? 256 : threads);
+    std::vector<int> h_cand = auto_h ? std::vector<int>{64, 32, 16, 8} : std::vector<int>{fpp};
+    if (!quads_fit) h_cand.clear();
     for (const int c : h_cand) {
       Own o = ownership(c);
       PipeTables t;
@@ -952,11 +958,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     std::vector<int> e_try;  // > 0: faces per patch; < 0: balanced for -n stages
     if (auto_e) e_try = {-2, -3, 32, 16, 8};
     else e_try = {fpp_e};
-    // the pipelined E consumer gives every compute thread a fixed radial quad,
-    // so no row may have more quads than the CTA has compute threads (at least
-    // 256 when the count is automatic)
-    const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
-    if (row_quads > (auto_threads ? 256 : threads)) e_try.clear();
+    if (!quads_fit) e_try.clear();
     std::vector<char> v_src(nV, 0), e_src(nE, 0);
     for (int s = 0; s < X->n_src_er; ++s) v_src[X->src_er_vertex[s]] = 1;
     for (int s = 0; s < X->n_src_et; ++s) e_src[X->src_et_edge[s]] = 1;

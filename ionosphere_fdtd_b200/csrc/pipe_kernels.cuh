@@ -281,7 +281,6 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
   const int T = R.si_terms;
   const bool si_pass = si_lane_groups(T);
   const int Pn = R.Pn, Pm = R.Pm, cn = Pn / N, cm = Pm / N;
-  const uint32_t mag_cn = div_magic(cn), mag_cm = div_magic(cm);
   if (si_pass) {
     // each owned edge's surface-impedance ADE on T/4 lanes (four poles each):
     // partial history sums gathered in pole order, the node-0 Ht into the
@@ -310,23 +309,37 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
     if ((threadIdx.x & 31) == 0) mbar_arrive(group);
     if (!__all_sync(0xFFFFFFFFu, wait_phase(group, ph, G.abort_flag, G.status))) return;
   }
-  for (int it = ct; it < ne * cn; it += nct) {
-    const int el = fast_div(it, mag_cn);
-    const int e = ea + el;
-    const int4 loc = eloc[el];
-    h_edge_run(R, Ls, e, (it - el * cn) * N, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
-               R.ht + (size_t)e * Pn, einv[el], s_si + el * T, R.si_mem + (size_t)e * T, esis + el,
-               si_pass ? s_hnew + el : nullptr);
+  // edge runs (nodes) and face runs (midpoints), each thread on a fixed
+  // radial quad (layer factors loaded once per patch; see ke_consume)
+  {
+    const int per = nct / cn;
+    if (ct < per * cn) {
+      const int k0 = (ct % cn) * N;
+      const HEdgeLayer<real> y = h_edge_layer(R, Ls, k0);
+      for (int el = ct / cn; el < ne; el += per) {
+        const int e = ea + el;
+        const int4 loc = eloc[el];
+        h_edge_run(R, Ls, y, e, k0, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
+                   R.ht + (size_t)e * Pn, einv[el], s_si + el * T, R.si_mem + (size_t)e * T, esis + el,
+                   si_pass ? s_hnew + el : nullptr);
+      }
+    }
   }
-  for (int it = ct; it < nf * cm; it += nct) {
-    const int fl = fast_div(it, mag_cm);
-    const int f = fa + fl;
-    const int4 l0 = floc[2 * fl];
-    const int4 l1 = floc[2 * fl + 1];
-    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, s_et + l0.x * Pm, s_et + l0.y * Pm, s_et + l0.z * Pm,
-                             s_hr + fl * Pm, R.hr + (size_t)f * Pm, s_er + l0.w * Pn, s_er + l1.x * Pn,
-                             s_er + l1.y * Pn, s_J + fl * 3 * Pm, nf * 3 * Pm,
-                             R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr, fw + 4 * fl, fpl + 12 * fl);
+  {
+    const int per = nct / cm;
+    if (ct < per * cm) {
+      const int j0 = (ct % cm) * N;
+      const Run<real> fc = ld16(Ls.hC + j0);
+      for (int fl = ct / cm; fl < nf; fl += per) {
+        const int f = fa + fl;
+        const int4 l0 = floc[2 * fl];
+        const int4 l1 = floc[2 * fl + 1];
+        h_face_run<real, PLASMA>(R, Ls, fc, f, j0, s_et + l0.x * Pm, s_et + l0.y * Pm, s_et + l0.z * Pm,
+                                 s_hr + fl * Pm, R.hr + (size_t)f * Pm, s_er + l0.w * Pn, s_er + l1.x * Pn,
+                                 s_er + l1.y * Pn, s_J + fl * 3 * Pm, nf * 3 * Pm,
+                                 R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr, fw + 4 * fl, fpl + 12 * fl);
+      }
+    }
   }
 }
 

@@ -410,21 +410,39 @@ __device__ __forceinline__ void si_update_quad(const real* in, real* out, const 
 // with odd (PEC) Et ghosts (solver.py:877-899, 443-456):
 //   Ht += (Er_head - Er_tail) / theta_e * hA[k] - Et[k] * hU[k] + Et[k-1] * hD[k]
 // (hA = dt/(mu0 r), hU / hD the upper / lower PEC-ghosted radial difference
-// weights).  The run holding node 0 also advances the surface-impedance ADE
+// weights; y holds them for the run's nodes).  The run holding node 0 also
+// advances the surface-impedance ADE
 // (surface_impedance.py:225-270) from the edge's pole memory si_in (T reals,
 // shared or global) into si_out (global) with the edge's scale *si_sp, unless
 // hnew points at the node-0 value a separate pass already advanced.
 // inv_t = 1 / primal edge angle.
+// Per-layer factors of an edge's H run at nodes k0..k0+N-1: hA, hU, hD and
+// whether midpoint k0 exists (the run's upper Et).
 template <typename real>
-__device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, int e, int k0, const real* erh,
-                                           const real* ert, const real* etr, const real* hto, real* htout,
-                                           real inv_t, const real* si_in, real* si_out, const real* si_sp,
+struct HEdgeLayer {
+  Run<real> fa, fu, fd;
+  bool up;
+};
+template <typename real>
+__device__ __forceinline__ HEdgeLayer<real> h_edge_layer(const Rec<real>& R, const Layers<real>& Ls, int k0) {
+  HEdgeLayer<real> y;
+  y.fa = ld16(Ls.hA + k0);
+  y.fu = ld16(Ls.hU + k0);
+  y.fd = ld16(Ls.hD + k0);
+  y.up = k0 < R.Pm;
+  return y;
+}
+
+template <typename real>
+__device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, const HEdgeLayer<real>& y, int e,
+                                           int k0, const real* erh, const real* ert, const real* etr, const real* hto,
+                                           real* htout, real inv_t, const real* si_in, real* si_out, const real* si_sp,
                                            const real* hnew = nullptr) {
   constexpr int N = Lanes<real>::N;
   const Run<real> vh = ld16(erh + k0), vt = ld16(ert + k0), vo = ld16(hto + k0);
-  const Run<real> vu = (k0 < R.Pm) ? ld16(etr + k0) : zero_run<real>();
+  const Run<real> vu = y.up ? ld16(etr + k0) : zero_run<real>();
   const real vprev = k0 > 0 ? etr[k0 - 1] : real(0);
-  const Run<real> fa = ld16(Ls.hA + k0), fu = ld16(Ls.hU + k0), fd = ld16(Ls.hD + k0);
+  const Run<real>&fa = y.fa, &fu = y.fu, &fd = y.fd;
   Run<real> out;
 #pragma unroll
   for (int r = 0; r < N; ++r) {
@@ -459,16 +477,17 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
 // The face's (3, Pm) input current rows of species s are at jin0 + s *
 // jin_stride (jin0 == nullptr: the state arrays R.J[s] themselves); outputs go
 // to R.J[s].  fw is the face's circulation row (4 reals) and gp its
-// reconstruction row (12 reals).
+// reconstruction row (12 reals); fc is hC at the run's midpoints.
 template <typename real, bool PLASMA>
-__device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real>& Ls, int f, int j0, const real* et0,
-                                           const real* et1, const real* et2, const real* hro, real* hrout,
-                                           const real* pa, const real* pb, const real* pc, const real* jin0,
-                                           int jin_stride, real* jtot, const real* fw, const real* gp) {
+__device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real>& Ls, const Run<real>& fc, int f,
+                                           int j0, const real* et0, const real* et1, const real* et2, const real* hro,
+                                           real* hrout, const real* pa, const real* pb, const real* pc,
+                                           const real* jin0, int jin_stride, real* jtot, const real* fw,
+                                           const real* gp) {
   constexpr int N = Lanes<real>::N;
   const int L = R.L, Pn = R.Pn, Pm = R.Pm;
   const Run<real> a0 = ld16(et0 + j0), a1 = ld16(et1 + j0), a2 = ld16(et2 + j0);
-  const Run<real> hv = ld16(hro + j0), fc = ld16(Ls.hC + j0);
+  const Run<real> hv = ld16(hro + j0);
   real wv[4];
   ld4(fw, wv);
   const real w0 = wv[0], w1 = wv[1], w2 = wv[2];
@@ -775,7 +794,8 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
     const int el = fast_div(it, mag_cn);
     const int e = ea + el;
     const int2 th = __ldg(R.edge_th + e);
-    h_edge_run(R, Ls, e, (it - el * cn) * N, R.er + (size_t)th.y * Pn, R.er + (size_t)th.x * Pn, R.et + (size_t)e * Pm,
+    const int k0 = (it - el * cn) * N;
+    h_edge_run(R, Ls, h_edge_layer(R, Ls, k0), e, k0, R.er + (size_t)th.y * Pn, R.er + (size_t)th.x * Pn, R.et + (size_t)e * Pm,
                R.ht + (size_t)e * Pn, R.ht + (size_t)e * Pn, __ldg(R.inv_theta + e), R.si_mem + (size_t)e * R.si_terms,
                R.si_mem + (size_t)e * R.si_terms, R.si_scale + e);
   }
@@ -785,7 +805,8 @@ __global__ void __launch_bounds__(256) kh_kernel(const Rec<real>* __restrict__ r
     const int f = fa + fl;
     const int4 fe = __ldg(R.face_e + f);
     const int4 fv = PLASMA ? __ldg(R.face_v + f) : make_int4(0, 0, 0, 0);
-    h_face_run<real, PLASMA>(R, Ls, f, (it - fl * cm) * N, R.et + (size_t)fe.x * Pm, R.et + (size_t)fe.y * Pm,
+    const int j0 = (it - fl * cm) * N;
+    h_face_run<real, PLASMA>(R, Ls, ld16(Ls.hC + j0), f, j0, R.et + (size_t)fe.x * Pm, R.et + (size_t)fe.y * Pm,
                              R.et + (size_t)fe.z * Pm, R.hr + (size_t)f * Pm, R.hr + (size_t)f * Pm,
                              R.er + (size_t)fv.x * Pn, R.er + (size_t)fv.y * Pn, R.er + (size_t)fv.z * Pn, nullptr, 0,
                              R.n_species > 1 ? R.Jtot + (size_t)f * 3 * Pm : nullptr, R.face_w + 4 * (size_t)f,
