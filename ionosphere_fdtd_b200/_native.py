@@ -131,6 +131,13 @@ _SIGNATURES = {
     "ifdtd_batch_step": ([_vp, C.POINTER(State), _vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp], _i32),
     "ifdtd_batch_info": ([_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_max_abs": ([_vp, C.POINTER(State), _vp, _vp], _i32),
+    "ifdtd_nn_gemm": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp], _i32),
+    "ifdtd_nn_bias_act": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp], _i32),
+    "ifdtd_nn_act_grad": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp, _vp], _i32),
+    "ifdtd_nn_col_sum": ([_i32, _i32, _vp, _vp, _vp], _i32),
+    "ifdtd_nn_mse": ([_i32, _vp, _vp, _vp, _vp, _vp], _i32),
+    "ifdtd_nn_adam": ([_i32, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, _i32, _vp, _vp], _i32),
+    "ifdtd_nn_to_bf16": ([C.c_int64, _vp, _vp, _vp], _i32),
     "ifdtd_edge_difference": ([_vp, _vp, _i32, _vp, _vp], _i32),
     "ifdtd_dual_edge_difference": ([_vp, _vp, _i32, _vp, _vp], _i32),
     "ifdtd_face_circulation": ([_vp, _vp, _i32, _vp, _vp], _i32),

@@ -15,8 +15,14 @@ from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
-SOURCES = [PACKAGE / "csrc" / "ifdtd.cu"]
-HEADERS = [PACKAGE / "csrc" / "step_kernels.cuh", PACKAGE / "csrc" / "pipe_kernels.cuh", ROOT / "include" / "ifdtd.h"]
+SOURCES = [PACKAGE / "csrc" / "ifdtd.cu", PACKAGE / "csrc" / "surrogate.cu"]
+HEADERS = [
+    PACKAGE / "csrc" / "step_kernels.cuh",
+    PACKAGE / "csrc" / "pipe_kernels.cuh",
+    PACKAGE / "csrc" / "errors.cuh",
+    ROOT / "include" / "ifdtd.h",
+    ROOT / "include" / "ifdtd_surrogate.h",
+]
 LIBRARY = PACKAGE / "libifdtd.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

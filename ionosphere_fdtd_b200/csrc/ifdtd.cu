@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/ifdtd.h"
+#include "errors.cuh"
 #include "pipe_kernels.cuh"
 #include "step_kernels.cuh"
 
@@ -26,6 +27,12 @@ int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+
+}  // namespace
+
+int ifdtd::record_error(int code, const std::string& msg) { return fail(code, msg); }
+
+namespace {
 
 #define CUDA_TRY(expr)                                                                          \
   do {                                                                                          \

@@ -180,8 +180,12 @@ def test_plasma_artifact_round_trip_and_corruption(tmp_path):
 
 
 def _declared_symbols() -> set[str]:
-    text = (ROOT / "include" / "ifdtd.h").read_text()
-    return set(re.findall(r"^\s*int32_t\s+(ifdtd_\w+)\s*\(", text, flags=re.M))
+    """Every entry point declared in the public headers (include/*.h)."""
+
+    names: set[str] = set()
+    for header in sorted((ROOT / "include").glob("*.h")):
+        names |= set(re.findall(r"^\s*int32_t\s+(ifdtd_\w+)\s*\(", header.read_text(), flags=re.M))
+    return names
 
 
 def test_c_abi_library_exports_every_declared_symbol():

@@ -1,0 +1,89 @@
+"""The trace surrogate on the GPU: the BF16 tensor-core GEMM against a float32
+product of the same bf16 inputs, forward and backward passes against the CPU
+oracle, and training on traces the engine generates, against the method
+without the network (the mean trace of the training set)."""
+
+import numpy as np
+import pytest
+
+import oracle.surrogate as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(t):
+    import torch
+
+    return t.to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("m,n,k", [(70, 45, 37), (1, 130, 8), (300, 4, 520), (64, 64, 64)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb):
+    import torch
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    g = torch.Generator(device="cuda").manual_seed(m * 7 + n + k)
+    a = _bf16(torch.randn((k, m) if ta else (m, k), device="cuda", generator=g))
+    b = _bf16(torch.randn((n, k) if tb else (k, n), device="cuda", generator=g))
+    c0 = torch.randn((m, n), device="cuda", generator=g)
+    c = c0.clone()
+    stream = torch.cuda.current_stream().cuda_stream
+    N.check(N.load().ifdtd_nn_gemm(m, n, k, a.data_ptr(), a.shape[1], ta, b.data_ptr(), b.shape[1], tb, 0.5, 2.0,
+                                   c.data_ptr(), n, stream), "ifdtd_nn_gemm")
+    A = (a.float().T if ta else a.float()).double()
+    B = (b.float().T if tb else b.float()).double()
+    expected = 0.5 * (A @ B) + 2.0 * c0.double()
+    err = (c.double() - expected).norm() / expected.norm()
+    assert float(err) < 1e-6
+
+
+def test_forward_and_backward_match_the_cpu_oracle():
+    import torch
+
+    from ionosphere_fdtd_b200.surrogate import TraceSurrogate, architecture
+
+    layers = architecture(inputs=8, width=48, depth=3, samples=64, t0=4, c0=8, channels=(4, 1), stride=4)
+    net = TraceSurrogate(layers, seed=5)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((6, 8))
+    t = rng.standard_normal((6, 64)) * 0.1
+    pred = net.forward(torch.tensor(x, dtype=torch.bfloat16, device="cuda"))
+    _, grad = net.loss_and_grad(pred, torch.tensor(t, dtype=torch.float32, device="cuda"))
+    net.backward(grad)
+    spec = [(L.fan_in, L.fan_out, L.act, L.expand) for L in layers]
+    w = [p.double().cpu().numpy() for p in net.w]
+    b = [p.double().cpu().numpy() for p in net.b]
+    opred, acts = O.forward(spec, w, b, x)
+    _, ograd = O.mse(opred, t)
+    gw, gb = O.backward(spec, w, acts, ograd)
+    rel = lambda a, e: float(np.linalg.norm(a - e) / max(np.linalg.norm(e), 1e-30))  # noqa: E731
+    assert rel(pred.double().cpu().numpy(), opred) < 5e-3
+    for i in range(len(layers)):
+        assert rel(net.gw[i].double().cpu().numpy(), gw[i]) < 2e-2, i
+        assert rel(net.gb[i].double().cpu().numpy(), gb[i]) < 2e-2, i
+
+
+def test_training_on_engine_traces_beats_the_mean_trace():
+    import torch
+
+    from ionosphere_fdtd_b200.surrogate import TraceSurrogate, architecture, encode_features, generate_traces, relative_l2
+
+    params, traces = generate_traces(48, subdivision=3, radial_cells=16, steps=256, receivers=8, distance_deg=(2.0, 10.0),
+                                     batch_members=24, seed=7)
+    assert traces.shape == (384, 256) and np.all(np.isfinite(traces))
+    scale = float(np.sqrt(np.mean(traces**2)))
+    assert scale > 0.0
+    x = torch.tensor(encode_features(params), dtype=torch.bfloat16, device="cuda")
+    y = torch.tensor(traces / scale, dtype=torch.float32, device="cuda")
+    train, test = slice(0, 288), slice(288, 384)  # whole runs held out
+    net = TraceSurrogate(architecture(inputs=8, width=64, depth=3, samples=256, t0=16, c0=16, channels=(8, 1), stride=4), seed=1)
+    losses = net.fit(x[train], y[train], iterations=1500, batch=64, lr=3e-3, lr_final=2e-4, seed=3)
+    assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:10])
+    pred = net.predict(x[test])
+    mean_trace = y[train].mean(dim=0, keepdim=True).expand_as(y[test])
+    keep = y[test].norm(dim=1) > 1e-3 * y[test].norm(dim=1).max()
+    err_net = float(relative_l2(pred, y[test])[keep].median())
+    err_mean = float(relative_l2(mean_trace, y[test])[keep].median())
+    assert err_net < err_mean, (err_net, err_mean)
