@@ -51,7 +51,10 @@ def parse() -> argparse.Namespace:
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("engine", "reference"), default="engine")
-    p.add_argument("--workload", choices=("config2", "config3", "config4"), default="config2")
+    p.add_argument("--workload", choices=("config2", "config3", "config4", "config5"), default="config2")
+    p.add_argument("--runs", type=int, default=256, help="config5: training runs generated by the engine")
+    p.add_argument("--eval-runs", type=int, default=32, help="config5: held-out runs (16 receivers each)")
+    p.add_argument("--iterations", type=int, default=3000, help="config5: training iterations per network")
     p.add_argument("--members", type=int, default=64, help="config3: ensemble members")
     p.add_argument("--no-autotune", action="store_true", help="config3: keep the automatic launch geometry")
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
@@ -495,8 +498,110 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
         dist.destroy_process_group()
 
 
+SURROGATE_METRIC = "surrogate traces/s"
+
+
+def surrogate_main(args, world: int, rank: int, local: int) -> None:
+    """Config 5: train the trace surrogate on engine-generated runs (s6 / 40
+    cells, 1024 samples, 16 receivers per run), judge it on held-out runs with
+    the engine, and compare traces/s of the surrogate with the batched engine
+    that generated them.  One replica per rank; rank 0 prints the line."""
+
+    import torch
+
+    from ionosphere_fdtd_b200.surrogate import SurrogateEnsemble, architecture, encode_features, generate_traces, relative_l2
+
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    steps, receivers = 1024, 16
+    n_runs = args.runs + args.eval_runs
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    # receivers 1-6 degrees from the source: the pulse (centred at 35 % of the
+    # 1024-step window) reaches all of them inside the window
+    params, traces = generate_traces(n_runs, subdivision=6, radial_cells=40, steps=steps, receivers=receivers, seed=20260805 + rank,
+                                     distance_deg=(1.0, 6.0), batch_members=32, device=device)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    scale = float(np.sqrt(np.mean(traces**2)))
+    x = torch.tensor(encode_features(params), dtype=torch.bfloat16, device=device)
+    y = torch.tensor(traces / scale, dtype=torch.float32, device=device)
+    n_train = args.runs * receivers
+    layers = architecture()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens, hist = SurrogateEnsemble.train(layers, x[:n_train], y[:n_train], k=4, iterations=args.iterations, batch=256,
+                                        lr=1e-3, lr_final=5e-5, device=device, seed=11)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    xe, ye = x[n_train:], y[n_train:]
+    # inference rate: the 4-member ensemble over the held-out cases, CUDA events
+    for _ in range(3):
+        ens.predict(xe)
+    reps = max(args.steps, 3)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        mean, spread = ens.predict(xe)
+    b.record()
+    torch.cuda.synchronize()
+    infer_ms = a.elapsed_time(b) / reps
+    # per-trace relative L2 over traces above 1 % of the median trace norm (a
+    # near-empty trace makes the per-trace ratio meaningless), and the global
+    # relative L2 over all held-out traces
+    norms = ye.norm(dim=1)
+    live = norms > 0.01 * norms.median()
+    err = relative_l2(mean, ye)[live]
+    mean_trace = y[:n_train].mean(dim=0, keepdim=True).expand_as(ye)
+    baseline = relative_l2(mean_trace, ye)[live]
+    tau = float(torch.quantile(spread, 0.8))  # the most uncertain 20 % go back to the engine
+    fallback = spread > tau
+    hybrid_pred = torch.where(fallback[:, None], ye, mean)
+    hybrid = relative_l2(hybrid_pred, ye)[live]
+    glob = lambda p: float((p - ye).norm() / ye.norm())  # noqa: E731
+    n_eval = int(ye.shape[0])
+    value = world * n_eval / (infer_ms / 1e3)
+    engine_traces_s = world * n_runs * receivers / gen_s
+    line = {
+        "metric": SURROGATE_METRIC,
+        "value": value,
+        "unit": "traces/s",
+        "n_gpus": world,
+        "steps": reps,
+        "warmup": 3,
+        "ms_per_step": infer_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16",
+        "data": "synthetic (engine-generated traces)",
+        "config": {
+            "workload": "config5", "subdivision": 6, "radial_cells": 40, "samples": steps, "receivers_per_run": receivers,
+            "train_runs": args.runs, "eval_runs": args.eval_runs, "network": "MLP 8-512x4 + transposed-conv decoder (16x64 -> 1024)",
+            "ensemble": 4, "iterations": args.iterations, "batch": 256, "parallelism": f"replicas x{world}",
+        },
+        "engine": {"traces_per_s": engine_traces_s, "generation_s": gen_s, "api": "Ensemble.record_er_observations (setup included)"},
+        "speedup_vs_engine": value / engine_traces_s,
+        "train_s": train_s,
+        "final_loss": [float(np.mean(h[-50:])) for h in hist],
+        "rel_l2": {"global": glob(mean), "median": float(err.median()), "p90": float(torch.quantile(err, 0.9)),
+                   "traces_scored": int(live.sum()), "traces": n_eval,
+                   "mean_trace_baseline": {"global": glob(mean_trace), "median": float(baseline.median())}},
+        "fallback": {"spread_threshold": tau, "fraction": float(fallback.float().mean()), "global": glob(hybrid_pred),
+                     "median": float(hybrid.median()), "p90": float(torch.quantile(hybrid, 0.9))},
+        "e2e": None,
+        "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def reference_arm(args, world: int, rank: int) -> None:
     if rank != 0:
+        return
+    if args.workload == "config5":
+        print(json.dumps({"impl": "reference", "metric": SURROGATE_METRIC,
+                          "unavailable": "the reference has no learned surrogate"}), flush=True)
         return
     if args.workload == "config3":
         ensemble_reference_arm(args)
@@ -543,6 +648,9 @@ def main() -> None:
         return
     if args.workload == "config3":
         ensemble_main(args, world, rank, local)
+        return
+    if args.workload == "config5":
+        surrogate_main(args, world, rank, local)
         return
     import torch
 
