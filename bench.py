@@ -530,8 +530,10 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
     layers = architecture()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    # each trace weighted by the inverse of its mean square: the loss is the
+    # mean squared relative error, the metric the engine judges
     ens, hist = SurrogateEnsemble.train(layers, x[:n_train], y[:n_train], k=4, iterations=args.iterations, batch=256,
-                                        lr=1e-3, lr_final=5e-5, device=device, seed=11)
+                                        lr=1e-3, lr_final=5e-5, device=device, seed=11, relative=True)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     xe, ye = x[n_train:], y[n_train:]
@@ -578,7 +580,8 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
         "config": {
             "workload": "config5", "subdivision": 6, "radial_cells": 40, "samples": steps, "receivers_per_run": receivers,
             "train_runs": args.runs, "eval_runs": args.eval_runs, "network": "MLP 8-512x4 + transposed-conv decoder (16x64 -> 1024)",
-            "ensemble": 4, "iterations": args.iterations, "batch": 256, "parallelism": f"replicas x{world}",
+            "ensemble": 4, "iterations": args.iterations, "batch": 256, "loss": "per-trace relative squared error",
+            "parallelism": f"replicas x{world}",
         },
         "engine": {"traces_per_s": engine_traces_s, "generation_s": gen_s, "api": "Ensemble.record_er_observations (setup included)"},
         "speedup_vs_engine": value / engine_traces_s,

@@ -35,6 +35,10 @@ int32_t ifdtd_nn_act_grad(int32_t rows, int32_t cols, const float* z, const floa
 int32_t ifdtd_nn_col_sum(int32_t rows, int32_t cols, const float* x, float* out, void* stream);
 /* grad = 2 (pred - target) / n; *loss += mean squared error (loss must start at 0). */
 int32_t ifdtd_nn_mse(int32_t n, const float* pred, const float* target, float* grad, float* loss, void* stream);
+/* Row-weighted squared error over a rows x cols array: *loss += sum_r row_weight[r] * sum_c (pred - target)^2
+ * / (rows * cols), grad = 2 row_weight[r] (pred - target) / (rows * cols) (loss must start at 0). */
+int32_t ifdtd_nn_wmse(int32_t rows, int32_t cols, const float* pred, const float* target, const float* row_weight,
+                      float* grad, float* loss, void* stream);
 /* One Adam step (bias-corrected, step >= 1) on fp32 weights w; w_bf16 (may be NULL) receives the bf16 copy. */
 int32_t ifdtd_nn_adam(int32_t n, float* w, const float* g, float* m, float* v, float lr, float beta1, float beta2,
                       float eps, int32_t step, void* w_bf16, void* stream);

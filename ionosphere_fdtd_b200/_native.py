@@ -136,6 +136,7 @@ _SIGNATURES = {
     "ifdtd_nn_act_grad": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp, _vp], _i32),
     "ifdtd_nn_col_sum": ([_i32, _i32, _vp, _vp, _vp], _i32),
     "ifdtd_nn_mse": ([_i32, _vp, _vp, _vp, _vp, _vp], _i32),
+    "ifdtd_nn_wmse": ([_i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp], _i32),
     "ifdtd_nn_adam": ([_i32, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float, _i32, _vp, _vp], _i32),
     "ifdtd_nn_to_bf16": ([C.c_int64, _vp, _vp, _vp], _i32),
     "ifdtd_edge_difference": ([_vp, _vp, _i32, _vp, _vp], _i32),

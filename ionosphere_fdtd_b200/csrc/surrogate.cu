@@ -165,6 +165,28 @@ __global__ void mse(int n, const float* __restrict__ p, const float* __restrict_
   if (threadIdx.x == 0) atomicAdd(loss, part[0] / (float)n);
 }
 
+// Row-weighted squared error: loss += sum_r w[r] sum_c (p - t)^2 / (rows * cols),
+// grad = 2 w[r] (p - t) / (rows * cols) (w[r] = 1 / mean square of target row
+// r makes every trace count by its relative error)
+__global__ void wmse(int rows, int cols, const float* __restrict__ p, const float* __restrict__ t,
+                     const float* __restrict__ w, float* __restrict__ grad, float* __restrict__ loss) {
+  __shared__ float part[256];
+  const int n = rows * cols;
+  float s = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float d = p[i] - t[i], wr = w[i / cols];
+    grad[i] = 2.f * wr * d / (float)n;
+    s += wr * d * d;
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) part[threadIdx.x] += part[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss, part[0] / (float)n);
+}
+
 // Adam on fp32 master weights; the bf16 copy the GEMMs read is refreshed
 __global__ void adam(int n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                      float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2,
@@ -244,6 +266,14 @@ int32_t ifdtd_nn_mse(int32_t n, const float* pred, const float* target, float* g
   if (n <= 0 || !pred || !target || !grad || !loss) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad mse arguments");
   mse<<<grid1d((size_t)n), 256, 0, (cudaStream_t)stream>>>(n, pred, target, grad, loss);
   return launched("mse");
+}
+
+int32_t ifdtd_nn_wmse(int32_t rows, int32_t cols, const float* pred, const float* target, const float* row_weight,
+                      float* grad, float* loss, void* stream) {
+  if (rows <= 0 || cols <= 0 || (int64_t)rows * cols >= (int64_t)1 << 31 || !pred || !target || !row_weight || !grad || !loss)
+    return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad wmse arguments");
+  wmse<<<grid1d((size_t)rows * cols), 256, 0, (cudaStream_t)stream>>>(rows, cols, pred, target, row_weight, grad, loss);
+  return launched("wmse");
 }
 
 int32_t ifdtd_nn_adam(int32_t n, float* w, const float* g, float* m, float* v, float lr, float beta1, float beta2,

@@ -147,6 +147,17 @@ class TraceSurrogate:
                "ifdtd_nn_mse")
         return loss, grad
 
+    def weighted_loss_and_grad(self, pred, target, row_weight):
+        """Squared error with one weight per case (row)."""
+
+        torch = self.torch
+        grad = torch.empty_like(pred)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        rows, cols = int(pred.shape[0]), int(pred.shape[1])
+        _check(_lib().ifdtd_nn_wmse(rows, cols, pred.data_ptr(), target.data_ptr(), row_weight.data_ptr(), grad.data_ptr(), loss.data_ptr(),
+                                    self._stream()), "ifdtd_nn_wmse")
+        return loss, grad
+
     def adam_step(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
         lib, s = _lib(), self._stream()
         self.step_count += 1
@@ -156,19 +167,28 @@ class TraceSurrogate:
             _check(lib.ifdtd_nn_adam(int(self.b[i].numel()), self.b[i].data_ptr(), self.gb[i].data_ptr(), self.mb[i].data_ptr(),
                                      self.vb[i].data_ptr(), lr, beta1, beta2, eps, self.step_count, None, s), "ifdtd_nn_adam")
 
-    def fit(self, x, y, *, iterations: int, batch: int, lr: float = 1e-3, seed: int = 0, lr_final: float | None = None) -> list[float]:
+    def fit(self, x, y, *, iterations: int, batch: int, lr: float = 1e-3, seed: int = 0, lr_final: float | None = None,
+            relative: bool = False) -> list[float]:
         """Train on device tensors x (N, inputs) bf16 and y (N, samples) fp32;
-        returns the loss of every iteration (one host read at the end)."""
+        returns the loss of every iteration (one host read at the end).
+        relative: weight each case by the inverse mean square of its target, so
+        the loss is the cases' mean squared relative error."""
 
         torch = self.torch
         gen = torch.Generator(device=self.device)
         gen.manual_seed(seed)
         n = int(x.shape[0])
+        weight = None
+        if relative:
+            weight = 1.0 / y.pow(2).mean(dim=1).clamp_min(1e-12 * float(y.pow(2).mean()))
         losses = []
         for it in range(iterations):
             idx = torch.randint(0, n, (min(batch, n),), device=self.device, generator=gen)
             pred = self.forward(x[idx].contiguous())
-            loss, grad = self.loss_and_grad(pred, y[idx].contiguous())
+            if weight is None:
+                loss, grad = self.loss_and_grad(pred, y[idx].contiguous())
+            else:
+                loss, grad = self.weighted_loss_and_grad(pred, y[idx].contiguous(), weight[idx].contiguous())
             self.backward(grad)
             frac = it / max(iterations - 1, 1)
             rate = lr if lr_final is None else lr * (lr_final / lr) ** frac
@@ -191,12 +211,13 @@ class SurrogateEnsemble:
 
     @classmethod
     def train(cls, layers: list[Layer], x, y, *, k: int = 4, iterations: int = 1000, batch: int = 256, lr: float = 1e-3,
-              lr_final: float | None = 1e-4, device: str = "cuda", seed: int = 0):
+              lr_final: float | None = 1e-4, device: str = "cuda", seed: int = 0, relative: bool = False):
         ens = cls()
         histories = []
         for m in range(k):
             net = TraceSurrogate(layers, seed=seed + 1000 * m, device=device)
-            histories.append(net.fit(x, y, iterations=iterations, batch=batch, lr=lr, lr_final=lr_final, seed=seed + m))
+            histories.append(net.fit(x, y, iterations=iterations, batch=batch, lr=lr, lr_final=lr_final, seed=seed + m,
+                                     relative=relative))
             ens.members.append(net)
         return ens, histories
 

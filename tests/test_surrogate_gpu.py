@@ -87,3 +87,20 @@ def test_training_on_engine_traces_beats_the_mean_trace():
     err_net = float(relative_l2(pred, y[test])[keep].median())
     err_mean = float(relative_l2(mean_trace, y[test])[keep].median())
     assert err_net < err_mean, (err_net, err_mean)
+
+
+def test_weighted_squared_error_matches_a_float64_reference():
+    import torch
+
+    from ionosphere_fdtd_b200.surrogate import TraceSurrogate, architecture
+
+    net = TraceSurrogate(architecture(inputs=8, width=16, depth=1, samples=16, t0=1, c0=4, channels=(4, 1), stride=4))
+    g = torch.Generator(device="cuda").manual_seed(4)
+    p = torch.randn((37, 53), device="cuda", generator=g)
+    t = torch.randn((37, 53), device="cuda", generator=g)
+    w = torch.rand(37, device="cuda", generator=g) + 0.5
+    loss, grad = net.weighted_loss_and_grad(p, t, w)
+    d = (p - t).double()
+    expected = float((w.double()[:, None] * d * d).sum() / d.numel())
+    assert float(loss) == pytest.approx(expected, rel=1e-5)
+    torch.testing.assert_close(grad.double(), 2.0 * w.double()[:, None] * d / d.numel(), rtol=1e-6, atol=1e-9)
