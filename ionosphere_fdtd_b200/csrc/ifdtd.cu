@@ -439,8 +439,8 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     head[ke_o_J] = head[ke_o_hr] + n_f * Pm * rb;
     head[ke_o_er] = head[ke_o_J] + (plasma ? n_f * 3 * Pm * rb : 0);
     head[ke_o_et] = head[ke_o_er] + nv * Pn * rb;
-    head[ke_o_rav] = head[ke_o_et] + ne * Pm * rb;  // scratch: radial current per own vertex (not copied)
-    const int end = head[ke_o_rav] + (plasma ? nv * Pm * rb : 0);
+    head[ke_o_rav] = head[ke_o_et] + ne * Pm * rb;  // end of the staged rows (no scratch follows)
+    const int end = head[ke_o_rav];
     if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
@@ -673,8 +673,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       long blob = 16L * ((pipe::ke_head_ints * 4 + 15) / 16) + a16(4L * v) + a16(4L * v * SW) * (with_plasma ? 2 : 1) + a16((long)rb * v * SW) +
                   (with_plasma ? a16(4L * rb * v * SW) : 0) + a16(16L * e) + a16((long)rb * e) +
                   (with_plasma ? a16(8L * rb * e) : 0);
-      long rows = (long)rb * ((long)h * Pn + (long)fcount * Pm * (with_plasma ? 4 : 1) + (long)v * Pn + (long)e * Pm +
-                              (with_plasma ? (long)v * Pm : 0));
+      long rows = (long)rb * ((long)h * Pn + (long)fcount * Pm * (with_plasma ? 4 : 1) + (long)v * Pn + (long)e * Pm);
       return (blob + rows + 127) / 128 * 128;
     };
     int e_cursor = 0;

@@ -350,7 +350,7 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
 // factors of its quad load once per patch instead of once per run.
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
-                                           int nct, real current, uint64_t* group, uint32_t ph, const Ring& G) {
+                                           int nct, real current) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
   const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne], src = hd[ke_src];
@@ -367,7 +367,6 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
   const int4* eloc = reinterpret_cast<const int4*>(st + hd[ke_o_eloc]);
   const real* einv = reinterpret_cast<const real*>(st + hd[ke_o_einv]);
   const real* etan = reinterpret_cast<const real*>(st + hd[ke_o_etan]);
-  real* s_rav = reinterpret_cast<real*>(st + hd[ke_o_rav]);
   const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
   const bool full = R.coef_full != 0;
   auto slot_rows = [&](int vl, const real** hrows, const real** jrows) {
@@ -389,43 +388,40 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
       }
     }
   };
-  if (PLASMA) {
-    // pass 1: each owned vertex's radial current at every midpoint, into the
-    // stage's scratch rows; then all compute warps meet on the slot's group
-    // barrier (bounded) before the vertex runs read them
-    const int per = nct / cm;
-    if (ct < per * cm) {
-      const int j0 = (ct % cm) * N;
-      for (int vl = ct / cm; vl < nv; vl += per) {
-        const real* hrows[MAXDEG];
-        const real* jrows[MAXDEG];
-        slot_rows(vl, hrows, jrows);
-        const Run<real> r = vertex_radial_current<real, MAXDEG>(jrows, vwc + vl * SW * 4, j0, Pm);
-        if constexpr (sizeof(real) == 4) {
-          *reinterpret_cast<float4*>(s_rav + vl * Pm + j0) = make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
-        } else {
-          *reinterpret_cast<double2*>(s_rav + vl * Pm + j0) = make_double2(r.x[0], r.x[1]);
-        }
-      }
-    }
-    __syncwarp();
-    if ((threadIdx.x & 31) == 0) mbar_arrive(group);
-    if (!__all_sync(0xFFFFFFFFu, wait_phase(group, ph, G.abort_flag, G.status))) return;
-  }
   {
+    // vertex runs: thread ct holds node quad q of its vertices.  With plasma
+    // it computes the vertex's radial current on midpoint quad q itself
+    // (midpoints k0 .. k0+N-1) and takes the one below, k0-1, from lane - 1,
+    // which holds quad q-1 of the same vertex; a lane whose quad q-1 sits in
+    // the previous warp (lane 0) computes that value directly
     const int per = nct / cn;
     if (ct < per * cn) {
-      const int k0 = (ct % cn) * N;
+      const int q = ct % cn, k0 = q * N;
+      const int lane = threadIdx.x & 31, wbase = ct - lane;
       const VertexLayer<real> fixed = vertex_layer(R, Ls, 0, k0);
-      for (int vl = ct / cn; vl < nv; vl += per) {
+      for (int k = 0;; ++k) {
+        const int vl = ct / cn + k * per;
+        if (vl >= nv) break;
+        // lanes in this iteration: those whose thread index is below limit
+        const int cnt = min(per, nv - k * per) * cn - wbase;
+        const unsigned mask = cnt >= 32 ? 0xFFFFFFFFu : ((1u << cnt) - 1u);
         const int v = vid[vl];
         const real* hrows[MAXDEG];
         const real* jrows[MAXDEG];
         slot_rows(vl, hrows, jrows);
+        real rav[N + 1];
+        if (PLASMA) {
+          const real* wcs = vwc + vl * SW * 4;
+          const Run<real> own =
+              k0 < Pm ? vertex_radial_current<real, MAXDEG>(jrows, wcs, k0, Pm) : zero_run<real>();
+          const real below = __shfl_up_sync(mask, own.x[N - 1], 1);
+          rav[0] = q == 0 ? real(0) : (lane > 0 ? below : vertex_radial_current_at<real, MAXDEG>(jrows, wcs, k0 - 1, Pm));
+#pragma unroll
+          for (int r = 0; r < N; ++r) rav[r + 1] = own.x[r];
+        }
         e_vertex_run<real, PLASMA, MAXDEG>(R, full ? vertex_layer(R, Ls, v, k0) : fixed, (src & 1) != 0, v, k0, hrows,
                                            jrows, vcoef + vl * SW, PLASMA ? vwc + vl * SW * 4 : nullptr,
-                                           s_er + vl * Pn, R.er + (size_t)v * Pn, current,
-                                           PLASMA ? s_rav + vl * Pm : nullptr);
+                                           s_er + vl * Pn, R.er + (size_t)v * Pn, current, PLASMA ? rav : nullptr);
       }
     }
   }
@@ -501,13 +497,11 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
                                              int producers, int istep) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
-  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
   __shared__ int abort_flag;
   Layers<real> Ls;
   Ring G;
   const int W = producers;
-  if (threadIdx.x == 0)
-    for (int s = 0; s < n_stages; ++s) mbar_init(group + s, (blockDim.x - 32 * W) / 32);  // made visible by ring_setup
   ring_setup(R, recs, dyn_smem, full, empty, &abort_flag, stage_bytes, n_stages, COPY == 0 ? W : 32 * W, W, Ls, G);
   const int n = R.n_patches_e;
   const int p0 = (int)((long long)n * blockIdx.x / gridDim.x), p1 = (int)((long long)n * (blockIdx.x + 1) / gridDim.x);
@@ -517,7 +511,7 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
     consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
-      ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, group + s, ph, G);
+      ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current);
     });
   }
 }
@@ -604,7 +598,7 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma_batch(const Rec<real>* __restrict__
       const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
       const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
       consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
-        ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, group + s, ph, G);
+        ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current);
       });
     }
   }

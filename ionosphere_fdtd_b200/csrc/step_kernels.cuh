@@ -340,6 +340,21 @@ __device__ __forceinline__ Run<real> vertex_radial_current(const real* const* jr
   return acc;
 }
 
+// Radial current of one vertex at the single midpoint j (the same rav_term
+// sequence over the slots as vertex_radial_current, so the same bits).
+template <typename real, int MAXDEG>
+__device__ __forceinline__ real vertex_radial_current_at(const real* const* jrows, const real* wcs, int j, int Pm) {
+  real acc = real(0);
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) {
+    real wc[4];
+    ld4(wcs + 4 * q, wc);
+    const real* jf = jrows[q];
+    acc = rav_term(acc, jf[j], jf[Pm + j], jf[2 * Pm + j], wc[0], wc[1], wc[2]);
+  }
+  return acc;
+}
+
 // Source supports matching entity `id` exist (one pass over the record's list).
 __device__ __forceinline__ bool source_hit(const int* ids, int n, int id) {
   bool hit = false;
@@ -651,14 +666,15 @@ __device__ __forceinline__ EdgeLayer<real> edge_layer(const Rec<real>& R, const 
 // may carry a vertical source support (else the source list is not searched).
 // hrows[q]: Ht row of slot q's edge; jrows[q]: (3, Pm) summed current rows of
 // slot q's face; coef[q] = sign * phi_e / A*_v and wcs[4q..4q+2] = area weight
-// * face centre of slot q (zero in padding slots).  rav_row: the vertex's
-// radial current at every midpoint (Pm reals, from vertex_radial_current), or
-// nullptr to accumulate it here.
+// * face centre of slot q (zero in padding slots).  rav_in: the vertex's
+// radial current at midpoints k0-1 .. k0+N-1 (N+1 values, zero where a
+// midpoint does not exist), computed by the caller with rav_term in slot order
+// (the same bits as accumulating it here), or nullptr to accumulate it here.
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const VertexLayer<real>& y, bool src, int v, int k0,
                                              const real* const* hrows, const real* const* jrows, const real* coef,
                                              const real* wcs, const real* ero, real* erout, real current,
-                                             const real* rav_row = nullptr) {
+                                             const real* rav_in = nullptr) {
   constexpr int N = Lanes<real>::N;
   const int Pm = R.Pm;
   Run<real> hv[MAXDEG];
@@ -697,13 +713,9 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const VertexLay
 #pragma unroll
     for (int r = 0; r <= N; ++r) rav[r] = real(0);
     const bool in = y.in, below = y.below;
-    if (rav_row) {
-      if (below) rav[0] = rav_row[k0 - 1];
-      if (in) {
-        const Run<real> up = ld16(rav_row + k0);
+    if (rav_in) {
 #pragma unroll
-        for (int r = 0; r < N; ++r) rav[r + 1] = up.x[r];
-      }
+      for (int r = 0; r <= N; ++r) rav[r] = rav_in[r];
     } else {
 #pragma unroll
       for (int q = 0; q < MAXDEG; ++q) {
