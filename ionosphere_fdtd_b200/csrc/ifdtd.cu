@@ -439,8 +439,8 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     head[ke_o_J] = head[ke_o_hr] + n_f * Pm * rb;
     head[ke_o_er] = head[ke_o_J] + (plasma ? n_f * 3 * Pm * rb : 0);
     head[ke_o_et] = head[ke_o_er] + nv * Pn * rb;
-    head[ke_o_rav] = head[ke_o_et] + ne * Pm * rb;  // end of the staged rows (no scratch follows)
-    const int end = head[ke_o_rav];
+    head[ke_o_end] = head[ke_o_et] + ne * Pm * rb;
+    const int end = head[ke_o_end];
     if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
     std::memcpy(T.tab.data() + base, head, sizeof(head));
     T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));

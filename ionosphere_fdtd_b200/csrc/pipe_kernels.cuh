@@ -45,8 +45,9 @@ enum KhHead : int {
 // E-phase blob header.
 enum KeHead : int {
   ke_nv, ke_ea, ke_ne, ke_o_ht, ke_o_hr, ke_o_J, ke_o_er, ke_o_et, ke_o_vid, ke_o_vh,
-  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_o_rav, ke_src, ke_head_ints = 20
+  ke_o_vj, ke_o_vcoef, ke_o_vwc, ke_o_eloc, ke_o_einv, ke_o_etan, ke_o_end, ke_src, ke_head_ints = 20
 };
+// ke_o_end: the end of the staged rows (the stage holds nothing after them).
 // ke_src: bit 0 = an owned vertex carries a vertical source support, bit 1 =
 // an owned edge carries a tangential one (other patches skip the search).
 
