@@ -47,7 +47,8 @@ class Ensemble:
                 raise ValueError("ensemble members must share one CUDA device and one dtype")
         self._members = members
         self._backend = first
-        plans = (C.c_void_p * len(members))(*[m._engine.plan for m in members])
+        self._plans = [m._engine.plan.value for m in members]
+        plans = (C.c_void_p * len(members))(*self._plans)
         handle = C.c_void_p()
         N.check(N.load().ifdtd_batch_create(plans, len(members), int(graph_chunk), C.byref(handle)), "ifdtd_batch_create")
         self._handle = handle
@@ -141,6 +142,10 @@ class Ensemble:
     def _live(self) -> C.c_void_p:
         if not self._handle:
             raise ValueError("the ensemble is closed")
+        # the batch holds the members' plans: a member whose engine was replaced
+        # (autotuning, for instance) must not be stepped through a stale plan
+        if any(m._engine.plan.value != p for m, p in zip(self._members, self._plans)):
+            raise ValueError("a member's plan changed after the ensemble was built; build a new Ensemble")
         return self._handle
 
     def _advance_clocks(self, count: int) -> None:

@@ -133,3 +133,15 @@ def test_members_with_different_launch_tunings_form_groups_and_match_their_own_r
         sim.step(34)
     for (name, _), a, b in zip(spec, together, alone):
         _assert_same(a, b, name)
+
+
+def test_ensemble_refuses_members_whose_plan_changed():
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200.autotune import SHAPE_FREE_CANDIDATES, autotune
+
+    sims = [build_product(CS.CASES["source_s1"], "float32"), build_product(CS.CASES["plasma_drude_s2"], "float32")]
+    with Ensemble(sims) as ens:
+        ens.step(2)
+        autotune(sims[1], SHAPE_FREE_CANDIDATES[1:2], steps=4, repeats=1)  # installs a new plan
+        with pytest.raises(ValueError, match="plan changed"):
+            ens.step(1)
