@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(THREADS) gemm_bf16(int M, int N, int K, const 
                                                      float alpha, float beta, float* __restrict__ C, int ldc) {
   __shared__ __align__(16) __nv_bfloat16 As[BM][BK + PAD];
   __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + PAD];
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;  // row tiles on x (up to 2^31 - 1 of them)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
   const int g = lane >> 2, t = lane & 3;
@@ -231,7 +231,8 @@ int32_t ifdtd_nn_gemm(int32_t m, int32_t n, int32_t k, const void* a, int32_t ld
   if (m <= 0 || n <= 0 || k <= 0 || !a || !b || !c) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad gemm shape");
   if (lda < (trans_a ? m : k) || ldb < (trans_b ? k : n) || ldc < n)
     return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm leading dimension too small");
-  const dim3 grid((n + BN - 1) / BN, (m + BM - 1) / BM);
+  if ((n + BN - 1) / BN > 65535) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm has too many columns");
+  const dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
   gemm_bf16<<<grid, THREADS, 0, (cudaStream_t)stream>>>(m, n, k, (const __nv_bfloat16*)a, lda, trans_a != 0,
                                                           (const __nv_bfloat16*)b, ldb, trans_b != 0, alpha, beta, c,
                                                           ldc);
