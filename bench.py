@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--runs", type=int, default=256, help="config5: training runs generated by the engine")
     p.add_argument("--eval-runs", type=int, default=32, help="config5: held-out runs (16 receivers each)")
     p.add_argument("--iterations", type=int, default=3000, help="config5: training iterations per network")
+    p.add_argument("--decoder", default="16x64:4:32,16,1",
+                   help="config5: decoder shape t0 x c0 : stride : channels (t0 * stride ** len(channels) = 1024)")
     p.add_argument("--members", type=int, default=64, help="config3: ensemble members")
     p.add_argument("--no-autotune", action="store_true", help="config3: keep the automatic launch geometry")
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
@@ -527,7 +529,9 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
     x = torch.tensor(encode_features(params), dtype=torch.bfloat16, device=device)
     y = torch.tensor(traces / scale, dtype=torch.float32, device=device)
     n_train = args.runs * receivers
-    layers = architecture()
+    shape, stride, chans = args.decoder.split(":")
+    t0, c0 = (int(v) for v in shape.split("x"))
+    layers = architecture(samples=steps, t0=t0, c0=c0, channels=tuple(int(c) for c in chans.split(",")), stride=int(stride))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     # each trace weighted by the inverse of its mean square: the loss is the
@@ -579,7 +583,7 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
         "data": "synthetic (engine-generated traces)",
         "config": {
             "workload": "config5", "subdivision": 6, "radial_cells": 40, "samples": steps, "receivers_per_run": receivers,
-            "train_runs": args.runs, "eval_runs": args.eval_runs, "network": "MLP 8-512x4 + transposed-conv decoder (16x64 -> 1024)",
+            "train_runs": args.runs, "eval_runs": args.eval_runs, "network": f"MLP 8-512x4 + transposed-conv decoder ({t0}x{c0}, stride {stride}, channels {chans} -> 1024)",
             "ensemble": 4, "iterations": args.iterations, "batch": 256, "loss": "per-trace relative squared error",
             "parallelism": f"replicas x{world}",
         },
