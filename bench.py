@@ -505,8 +505,8 @@ SURROGATE_METRIC = "surrogate traces/s"
 
 def surrogate_main(args, world: int, rank: int, local: int) -> None:
     """Config 5: train the trace surrogate on engine-generated runs (s6 / 40
-    cells, 1024 samples, 16 receivers per run), judge it on held-out runs with
-    the engine, and compare traces/s of the surrogate with the batched engine
+    cells, 1024 samples, 16 receivers per run), score it on held-out runs
+    against the engine, and compare traces/s of the surrogate with the batched engine
     that generated them.  One replica per rank; rank 0 prints the line."""
 
     import torch
@@ -535,7 +535,7 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     # each trace weighted by the inverse of its mean square: the loss is the
-    # mean squared relative error, the metric the engine judges
+    # mean squared relative error, the metric the held-out traces are scored by
     ens, hist = SurrogateEnsemble.train(layers, x[:n_train], y[:n_train], k=4, iterations=args.iterations, batch=256,
                                         lr=1e-3, lr_final=5e-5, device=device, seed=11, relative=True)
     torch.cuda.synchronize()

@@ -1,7 +1,6 @@
 """Learned receiver-trace surrogate, trained on traces the engine generates.
 
-The reference has no surrogate; this module is the north star's "pattern 4":
-a small network maps eight scalars of a run (ionosphere prefactor sigma0,
+The reference has no surrogate.  A small network maps eight scalars of a run (ionosphere prefactor sigma0,
 reference height h0, scale height zeta, ground conductivity, source latitude
 and longitude, receiver latitude and longitude) to the receiver's Er trace.
 
@@ -16,7 +15,7 @@ Training uses the library's own kernels for every step (GEMMs, bias + SiLU,
 its derivative, bias sums, mean-squared error, Adam); PyTorch only holds the
 device buffers.
 
-The solver is the judge and the fallback: ``SurrogateEnsemble`` trains k
+The engine scores the surrogate and is its fallback: ``SurrogateEnsemble`` trains k
 networks from different seeds; a case whose members disagree by more than a
 threshold (relative spread of their traces) is handed back to the solver.
 """

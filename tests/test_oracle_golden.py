@@ -16,7 +16,7 @@ STATE = ("er", "et", "hr", "ht")
 def group_scale(ref, key):
     """Absolute scale for a compared array: the largest magnitude in its
     (E or H) field group, so pure round-off fields such as Hr under a
-    vertical source are judged against the physical scale."""
+    vertical source are compared against the physical scale."""
 
     groups = {"er": ("er", "et"), "et": ("er", "et"), "hr": ("hr", "ht"), "ht": ("hr", "ht")}
     names = groups.get(key, (key,))

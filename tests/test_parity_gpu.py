@@ -1,6 +1,6 @@
 """Parity of the CUDA engine with the reference (golden fixtures) and the oracle.
 
-Tolerances (stated per the north-star parity bar):
+Tolerances:
 * float64 engine vs reference float64: per (E, H) group relative L2 < 1e-11
   and elementwise rtol 1e-8 against the group scale (operation order differs
   from NumPy's, so results agree to accumulated rounding, not bitwise);
