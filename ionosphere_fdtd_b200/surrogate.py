@@ -1,8 +1,9 @@
 """Learned receiver-trace surrogate, trained on traces the engine generates.
 
-The reference has no surrogate.  A small network maps eight scalars of a run (ionosphere prefactor sigma0,
-reference height h0, scale height zeta, ground conductivity, source latitude
-and longitude, receiver latitude and longitude) to the receiver's Er trace.
+The reference has no surrogate.  A small network maps eight scalars of a run
+(ionosphere prefactor sigma0, reference height h0, scale height zeta, ground
+conductivity, source latitude and longitude, receiver latitude and longitude)
+to the receiver's Er trace.
 
 Network: an MLP (``depth`` SiLU layers of ``width``) and a projection to a
 ``t0`` x ``c0`` sequence, then non-overlapping 1-D transposed convolutions
