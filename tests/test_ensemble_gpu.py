@@ -25,6 +25,8 @@ MIXED = [
     "config1_s2",
     "thin_shell_s1",
     "trapezoidal_s1",
+    "adaptive_s1",  # vertex degree 7-8: the 12-slot kernels, a group of their own
+    "adaptive_plasma_si_s1",
 ]
 
 
