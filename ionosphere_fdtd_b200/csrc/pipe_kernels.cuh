@@ -399,7 +399,8 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     if (ct < per * cn) {
       const int q = ct % cn, k0 = q * N;
       const int lane = threadIdx.x & 31, wbase = ct - lane;
-      const VertexLayer<real> fixed = vertex_layer(R, Ls, 0, k0);
+      // the vertex layer factors are re-read per run here: hoisting them too
+      // would push this kernel past its register budget into local memory
       for (int k = 0;; ++k) {
         const int vl = ct / cn + k * per;
         if (vl >= nv) break;
@@ -420,7 +421,7 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
 #pragma unroll
           for (int r = 0; r < N; ++r) rav[r + 1] = own.x[r];
         }
-        e_vertex_run<real, PLASMA, MAXDEG>(R, full ? vertex_layer(R, Ls, v, k0) : fixed, (src & 1) != 0, v, k0, hrows,
+        e_vertex_run<real, PLASMA, MAXDEG>(R, vertex_layer(R, Ls, v, k0), (src & 1) != 0, v, k0, hrows,
                                            jrows, vcoef + vl * SW, PLASMA ? vwc + vl * SW * 4 : nullptr,
                                            s_er + vl * Pn, R.er + (size_t)v * Pn, current, PLASMA ? rav : nullptr);
       }
