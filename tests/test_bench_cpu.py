@@ -66,3 +66,33 @@ def test_reference_arm_works_on_rank_zero_only(capsys):
 
     bench.reference_arm(Args, world=2, rank=1)  # returns at once: no oracle run, no output
     assert capsys.readouterr().out == ""
+
+
+def test_surrogate_reference_arm_reports_unavailable(capsys):
+    import json
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    class Args:
+        workload, steps, warmup, gpus = "config5", 1, 0, 1
+
+    bench.reference_arm(Args, world=1, rank=0)
+    line = json.loads(capsys.readouterr().out)
+    assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_ensemble_cells_follow_the_member_generator():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    from ionosphere_fdtd_b200 import workloads as W
+
+    draws = W.config3_draws(members=64)
+    cells = bench.ensemble_cells(64)
+    assert len(cells) == 64
+    assert cells == [(10 * 4 ** d["subdivision"] + 2) * d["radial_cells"] for d in draws]
+    assert {d["subdivision"] for d in draws} == {5, 6, 7}
+    assert all(24 <= d["radial_cells"] <= 60 for d in draws)
+    assert all(1e-8 <= d["sigma0"] <= 1e-6 and 1e-3 <= d["ground"] <= 1e-1 for d in draws)
+    assert all(55e3 <= d["h0"] <= 70e3 and 3e3 <= d["zeta"] <= 6e3 and 10.0 <= d["carrier"] <= 60.0 for d in draws)
