@@ -11,6 +11,8 @@ order (mesh.py:569-593, 674-708); the golden tests check the tables bitwise.
 from __future__ import annotations
 
 import json
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 from typing import Any, Mapping
 
@@ -149,6 +151,24 @@ class GeodesicMesh:
 
 def _unit(values: FloatArray) -> FloatArray:
     return values / np.linalg.norm(values, axis=-1, keepdims=True)
+
+
+_ROWS_PER_CHUNK = 1 << 16
+
+
+def _rowwise(fn, *arrays):
+    """fn(*arrays) for functions that treat every row on its own: large inputs
+    are cut into row chunks run on threads (NumPy releases the GIL in them),
+    which gives the same bits as one call."""
+
+    n = len(arrays[0])
+    workers = min(os.cpu_count() or 1, n // _ROWS_PER_CHUNK)
+    if workers < 2:
+        return fn(*arrays)
+    starts = range(0, n, _ROWS_PER_CHUNK)
+    with ThreadPoolExecutor(workers) as pool:
+        parts = list(pool.map(lambda a: fn(*(x[a : a + _ROWS_PER_CHUNK] for x in arrays)), starts))
+    return np.concatenate(parts)
 
 
 # The 12-vertex / 20-face seed of every level (the reference's table,
@@ -297,16 +317,19 @@ def _assemble(
 ) -> GeodesicMesh:
     """Orient, number and measure a closed triangulation (mesh.py:397-468)."""
 
-    faces = _orient_outward(vertices, faces)
-    centres = _circumcentres(vertices, faces)
+    # every measure below is row-wise, so large meshes compute it in threaded
+    # row chunks with the same bits (_rowwise)
+    faces = _rowwise(lambda f: _orient_outward(vertices, f), faces)
+    centres = _rowwise(lambda f: _circumcentres(vertices, f), faces)
     edges, face_edges, signs, left, right = _edge_tables(faces, len(vertices))
-    primal = _arc(vertices[edges[:, 0]], vertices[edges[:, 1]])
-    dual = _arc(centres[left], centres[right])
-    face_area = np.abs(_signed_triangle(vertices[faces[:, 0]], vertices[faces[:, 1]], vertices[faces[:, 2]]))
+    primal = _rowwise(lambda e: _arc(vertices[e[:, 0]], vertices[e[:, 1]]), edges)
+    cl, cr = centres[left], centres[right]
+    dual = _rowwise(_arc, cl, cr)
+    face_area = np.abs(_rowwise(lambda f: _signed_triangle(vertices[f[:, 0]], vertices[f[:, 1]], vertices[f[:, 2]]), faces))
     # dual areas: the tail wedges (negated) of every edge in edge order, then the
     # head wedges, accumulated per vertex in that order (mesh.py:768-789)
-    tail_w = -_signed_triangle(vertices[edges[:, 0]], centres[left], centres[right])
-    head_w = _signed_triangle(vertices[edges[:, 1]], centres[left], centres[right])
+    tail_w = -_rowwise(lambda e, a, b: _signed_triangle(vertices[e], a, b), edges[:, 0], cl, cr)
+    head_w = _rowwise(lambda e, a, b: _signed_triangle(vertices[e], a, b), edges[:, 1], cl, cr)
     dual_area = np.bincount(
         np.concatenate((edges[:, 0], edges[:, 1])), weights=np.concatenate((tail_w, head_w)), minlength=len(vertices)
     )

@@ -279,3 +279,14 @@ def test_autotune_rejects_bad_arguments_before_touching_the_device():
         autotune(object(), steps=0)
     with pytest.raises(ValueError, match="candidate"):
         autotune(object(), candidates=())
+
+
+def test_threaded_row_chunks_give_the_same_mesh_bits(monkeypatch):
+    import ionosphere_fdtd_b200.mesh as M
+
+    serial = M.build_geodesic_mesh(3)
+    monkeypatch.setattr(M, "_ROWS_PER_CHUNK", 97)  # many uneven chunks on several threads
+    chunked = M.build_geodesic_mesh(3)
+    for name in ("faces", "edges", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles",
+                 "dual_cell_solid_angles", "vertex_degree"):
+        np.testing.assert_array_equal(getattr(chunked, name), getattr(serial, name), err_msg=name)
