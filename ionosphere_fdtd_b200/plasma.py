@@ -323,26 +323,35 @@ def ade_coefficients(model: MeshPlasmaModel, time_step_s: float):
 def face_reconstruction(mesh) -> tuple[NDArray[np.float64], NDArray[np.float64]]:
     """Per-face ``pinv(tangents).T`` and the unit edge tangents (plasma.py:548-559)."""
 
-    normals = np.cross(mesh.vertices[mesh.edges[:, 0]], mesh.vertices[mesh.edges[:, 1]])
-    normals /= np.linalg.norm(normals, axis=1, keepdims=True)
-    tangents = np.cross(normals[mesh.face_edges], mesh.face_centers[:, None, :])
-    tangents /= np.linalg.norm(tangents, axis=2, keepdims=True)
+    edges, face_edges, centres = mesh.edges, mesh.face_edges, mesh.face_centers
+    tangents = np.empty((mesh.n_faces, 3, 3))
     recon = np.empty_like(tangents)
+    normals = np.empty((mesh.n_edges, 3))
     step = 1 << 15
 
-    # LAPACK works on each 3 x 3 matrix alone, so the chunks may run on
-    # threads (numpy releases the GIL in them) and the bits do not change
-    def chunk(start: int) -> None:
-        recon[start : start + step] = np.swapaxes(np.linalg.pinv(tangents[start : start + step]), 1, 2)
+    # every step is row-wise (an edge's normal, a face's tangents and its 3 x 3
+    # pseudo-inverse), so the chunks may run on threads (NumPy and LAPACK
+    # release the GIL in them) and the bits do not change
+    def edge_chunk(start: int) -> None:
+        e = edges[start : start + step]
+        n = np.cross(mesh.vertices[e[:, 0]], mesh.vertices[e[:, 1]])
+        normals[start : start + step] = n / np.linalg.norm(n, axis=1, keepdims=True)
 
-    starts = range(0, mesh.n_faces, step)
-    workers = min(len(starts), os.cpu_count() or 1)
-    if workers > 1:
-        with ThreadPoolExecutor(workers) as pool:
-            list(pool.map(chunk, starts))
-    else:
-        for start in starts:
-            chunk(start)
+    def face_chunk(start: int) -> None:
+        t = np.cross(normals[face_edges[start : start + step]], centres[start : start + step, None, :])
+        t /= np.linalg.norm(t, axis=2, keepdims=True)
+        tangents[start : start + step] = t
+        recon[start : start + step] = np.swapaxes(np.linalg.pinv(t), 1, 2)
+
+    for job, n in ((edge_chunk, mesh.n_edges), (face_chunk, mesh.n_faces)):
+        starts = range(0, n, step)
+        workers = min(len(starts), os.cpu_count() or 1)
+        if workers > 1:
+            with ThreadPoolExecutor(workers) as pool:
+                list(pool.map(job, starts))
+        else:
+            for start in starts:
+                job(start)
     return recon, tangents
 
 
