@@ -222,6 +222,15 @@ int32_t ifdtd_batch_step(ifdtd_batch* batch, const ifdtd_state* states, const do
 int32_t ifdtd_batch_info(const ifdtd_batch* batch, int32_t* groups, int32_t* solo, int32_t* kh_grid,
                          int32_t* ke_grid);
 
+/* Host-side mesh numbering (no device needed): number the distinct pairs
+ * (lo[i], hi[i]), 0 <= lo, hi < n_vertices, in order of first appearance, as
+ * the reference numbers midpoints and edges while scanning faces in order
+ * (mesh.py:569-593, 674-708: a dict assigning len(dict) on first insertion).
+ * rank[i] is the number of pair i; first[r] (room for n entries) the position
+ * of number r's first appearance; *n_distinct the count of numbers. */
+int32_t ifdtd_first_use_numbering(const int64_t* lo, const int64_t* hi, int64_t n, int64_t n_vertices, int64_t* rank,
+                                  int64_t* first, int64_t* n_distinct);
+
 /* max |field| of er, et, hr, ht into out4 (device, float64); the four
  * reductions of diagnostics() (solver.py:1027-1030, torch_backend.py:218-219). */
 int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, void* stream);

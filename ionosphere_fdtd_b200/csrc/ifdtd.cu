@@ -1872,6 +1872,37 @@ int32_t ifdtd_step_sampled(ifdtd_plan* plan, const ifdtd_state* state, const dou
                           : run_steps<double>(plan, state, currents, n_steps, probe, out_rows, st);
 }
 
+int32_t ifdtd_first_use_numbering(const int64_t* lo, const int64_t* hi, int64_t n, int64_t n_vertices, int64_t* rank,
+                                  int64_t* first, int64_t* n_distinct) {
+  if (!n_distinct || n < 0 || n_vertices <= 0 || n_vertices >= ((int64_t)1 << 31) ||
+      (n > 0 && (!lo || !hi || !rank || !first)))
+    return fail(IFDTD_ERR_ARGUMENT, "bad first-use numbering arguments");
+  // open addressing on key = lo * n_vertices + hi, table at least twice the pairs
+  int shift = 64 - 4;
+  size_t cap = 16;
+  while (cap < 2 * (size_t)n) {
+    cap <<= 1;
+    --shift;
+  }
+  std::vector<int64_t> keys(cap, -1), ranks(cap, 0);
+  int64_t count = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (lo[i] < 0 || hi[i] < 0 || lo[i] >= n_vertices || hi[i] >= n_vertices)
+      return fail(IFDTD_ERR_ARGUMENT, "vertex index out of range in first-use numbering");
+    const int64_t key = lo[i] * n_vertices + hi[i];
+    size_t h = (size_t)(((uint64_t)key * 0x9E3779B97F4A7C15ull) >> shift);
+    while (keys[h] != -1 && keys[h] != key) h = (h + 1) & (cap - 1);
+    if (keys[h] == -1) {
+      keys[h] = key;
+      ranks[h] = count;
+      first[count++] = i;
+    }
+    rank[i] = ranks[h];
+  }
+  *n_distinct = count;
+  return IFDTD_OK;
+}
+
 int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t chunk, ifdtd_batch** out) {
   if (!plans || !out || n_members <= 0 || chunk < 1) return fail(IFDTD_ERR_ARGUMENT, "bad batch arguments");
   *out = nullptr;

@@ -230,12 +230,22 @@ def _first_use_numbering(lo: IntArray, hi: IntArray, n_vertices: int) -> tuple[I
     to assigning ``len(dict)`` on first insertion during a sequential scan.
     """
 
-    key = lo * np.int64(n_vertices) + hi
-    _, first, inverse = np.unique(key, return_index=True, return_inverse=True)
-    order = np.argsort(first, kind="stable")
-    rank = np.empty_like(order)
-    rank[order] = np.arange(len(order))
-    return rank[inverse.ravel()], first[order]
+    import ctypes
+
+    from . import _native as N
+
+    lo = np.ascontiguousarray(lo, dtype=np.int64).ravel()
+    hi = np.ascontiguousarray(hi, dtype=np.int64).ravel()
+    rank = np.empty(len(lo), dtype=np.int64)
+    first = np.empty(len(lo), dtype=np.int64)
+    count = ctypes.c_int64()
+    # one pass with a hash table in the library (host code, no device needed)
+    N.check(
+        N.load().ifdtd_first_use_numbering(N.ptr_i64(lo), N.ptr_i64(hi), len(lo), int(n_vertices), N.ptr_i64(rank),
+                                           N.ptr_i64(first), ctypes.byref(count)),
+        "ifdtd_first_use_numbering",
+    )
+    return rank, first[: count.value].copy()
 
 
 def _quarter(vertices: FloatArray, faces: IntArray) -> tuple[FloatArray, IntArray]:

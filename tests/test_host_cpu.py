@@ -290,3 +290,22 @@ def test_threaded_row_chunks_give_the_same_mesh_bits(monkeypatch):
     for name in ("faces", "edges", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles",
                  "dual_cell_solid_angles", "vertex_degree"):
         np.testing.assert_array_equal(getattr(chunked, name), getattr(serial, name), err_msg=name)
+
+
+def test_first_use_numbering_matches_a_sequential_dict():
+    import ionosphere_fdtd_b200.mesh as M
+
+    rng = np.random.default_rng(5)
+    for n, nv in ((0, 5), (1, 3), (1000, 40), (20000, 3000)):
+        lo = rng.integers(0, nv, n)
+        hi = rng.integers(0, nv, n)
+        seen: dict = {}
+        rank_ref, first_ref = [], []
+        for i, key in enumerate(zip(lo.tolist(), hi.tolist())):
+            if key not in seen:
+                seen[key] = len(seen)
+                first_ref.append(i)
+            rank_ref.append(seen[key])
+        rank, first = M._first_use_numbering(lo, hi, nv)
+        np.testing.assert_array_equal(rank, np.asarray(rank_ref, dtype=np.int64).reshape(rank.shape))
+        np.testing.assert_array_equal(first, np.asarray(first_ref, dtype=np.int64).reshape(first.shape))
