@@ -309,3 +309,33 @@ def test_first_use_numbering_matches_a_sequential_dict():
         rank, first = M._first_use_numbering(lo, hi, nv)
         np.testing.assert_array_equal(rank, np.asarray(rank_ref, dtype=np.int64).reshape(rank.shape))
         np.testing.assert_array_equal(first, np.asarray(first_ref, dtype=np.int64).reshape(first.shape))
+
+
+def test_new_entry_points_reject_bad_arguments_before_any_device_work():
+    import ctypes
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    lib = N.load()
+    out = ctypes.c_void_p()
+    assert lib.ifdtd_batch_create(None, 0, 32, ctypes.byref(out)) == 1  # IFDTD_ERR_ARGUMENT
+    plans = (ctypes.c_void_p * 1)(None)
+    assert lib.ifdtd_batch_create(plans, 1, 32, ctypes.byref(out)) == 1
+    assert lib.ifdtd_batch_create(plans, 1, 0, ctypes.byref(out)) == 1
+    assert lib.ifdtd_batch_step(None, None, None, 1, None, None, None) == 1
+    # surrogate kernels: shapes and leading dimensions are checked on the host
+    assert lib.ifdtd_nn_gemm(0, 4, 4, 1, 4, 0, 1, 4, 0, 1.0, 0.0, 1, 4, None) == 1
+    assert lib.ifdtd_nn_gemm(4, 4, 8, 1, 4, 0, 1, 4, 0, 1.0, 0.0, 1, 4, None) == 1  # lda < k
+    assert lib.ifdtd_nn_gemm(4, 4, 4, 1, 4, 0, 1, 4, 0, 1.0, 0.0, 1, 2, None) == 1  # ldc < n
+    assert lib.ifdtd_nn_adam(4, 1, 1, 1, 1, 1e-3, 0.9, 0.999, 1e-8, 0, None, None) == 1  # step must be >= 1
+    assert lib.ifdtd_nn_bias_act(4, 4, 1, 1, 2, None, None) == 1  # act must be 0 or 1
+    buf = ctypes.create_string_buffer(64)
+    lib.ifdtd_last_error(buf, 64)
+    assert b"bias_act" in buf.value
+    # host numbering: indices outside [0, n_vertices) are refused
+    lo = np.asarray([0, 5], dtype=np.int64)
+    hi = np.asarray([1, 2], dtype=np.int64)
+    rank = np.empty(2, dtype=np.int64)
+    first = np.empty(2, dtype=np.int64)
+    count = ctypes.c_int64()
+    assert lib.ifdtd_first_use_numbering(N.ptr_i64(lo), N.ptr_i64(hi), 2, 4, N.ptr_i64(rank), N.ptr_i64(first), ctypes.byref(count)) == 1
