@@ -944,7 +944,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     // 256 when the count is automatic)
     const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
     const bool quads_fit = row_quads <= (auto_threads ? 256 : threads);
-    std::vector<int> h_cand = auto_h ? std::vector<int>{64, 32, 16, 8} : std::vector<int>{fpp};
+    std::vector<int> h_cand = auto_h ? std::vector<int>{256, 128, 64, 32, 16, 8} : std::vector<int>{fpp};
     if (!quads_fit) h_cand.clear();
     for (const int c : h_cand) {
       Own o = ownership(c);
