@@ -229,12 +229,21 @@ def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None =
     return {"steps": steps, **out, "against": "float64 engine from the same seeded state"}
 
 
-# Subdivision of the CPU oracle's sample per workload. A full s9 / 80-cell step takes the NumPy
-# oracle about 2.5 minutes, so the s9 workload is sampled on the same 80-cell column with the
-# same plasma and surface impedance at s6 (40,962 vertices): the oracle's rate per cell is
-# nearly size-independent (0.00098 Gcell/s at s6 against 0.00092 at s7 on one core), and the
-# smaller sample gives the CPU the slightly higher rate.
-ORACLE_SAMPLE_SUB = {"config2": 7, "config4": 6}
+# Subdivision of the CPU oracle's sample per workload. A full s9 / 80-cell step takes the
+# oracle tens of seconds even on every host thread, so the s9 workload is sampled on the same
+# 80-cell column with the same plasma and surface impedance at s7 (163,842 vertices): the
+# oracle's rate per cell hardly depends on the mesh level (on 8 threads 0.0039 Gcell/s at s6
+# against 0.0037 at s7).
+ORACLE_SAMPLE_SUB = {"config2": 7, "config4": 7}
+
+
+def host_threads() -> int:
+    """Host threads this process may run on (its CPU affinity set)."""
+
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def oracle_build(workload: str, sub: int | None = None):
@@ -272,19 +281,29 @@ def oracle_build(workload: str, sub: int | None = None):
     return sim, {"cells": mesh.n_vertices * L, "sub": sub, "L": L, "note": note}
 
 
-def oracle_time(sim, info: dict, steps: int) -> dict:
+def oracle_stepper(sim):
+    """The oracle's step on PyTorch CPU tensors over every host thread: the reference's
+    multi-threaded CPU path (its Torch backend on the CPU with ``torch_threads``)."""
+
+    from oracle.threaded import ThreadedOracleStep
+
+    return ThreadedOracleStep(sim, host_threads())
+
+
+def oracle_time(stepper, info: dict, steps: int) -> dict:
     t0 = time.perf_counter()
-    sim.step(steps)
+    stepper.step(steps)
     dt = time.perf_counter() - t0
-    return {"gcells": info["cells"] * steps / dt / 1e9, "seconds": dt, "steps": steps, **info}
+    return {"gcells": info["cells"] * steps / dt / 1e9, "seconds": dt, "steps": steps, "cores": stepper.threads, **info}
 
 
 def oracle_sample(workload: str, steps: int, warm: int = 1) -> dict:
     """Time the CPU oracle on ``steps`` leapfrog steps of the same workload (float32)."""
 
     sim, info = oracle_build(workload)
-    sim.step(warm)
-    return oracle_time(sim, info, steps)
+    stepper = oracle_stepper(sim)
+    stepper.step(warm)
+    return oracle_time(stepper, info, steps)
 
 
 ENSEMBLE_METRIC = "ensemble runs/s"
@@ -300,8 +319,9 @@ def oracle_ensemble_rate(steps: int = 1) -> dict:
     sim = O.OracleFDTD(subdivision=6, radial_cells=40, material=O.EarthIonosphereParams(lithosphere_conductivity_s_m=1.0e-2),
                        dtype=np.float32, source=O.OracleSource(peak_current_a=1.0, carrier_frequency_hz=30.0))
     info = {"cells": sim.mesh.n_vertices * 40, "sub": 6, "L": 40}
-    sim.step(1)
-    return oracle_time(sim, info, steps)
+    stepper = oracle_stepper(sim)
+    stepper.step(1)
+    return oracle_time(stepper, info, steps)
 
 
 def ensemble_reference_arm(args) -> None:
@@ -318,14 +338,14 @@ def ensemble_reference_arm(args) -> None:
         secs += r["seconds"]
     gcells = statistics.median(rates)
     value = gcells * 1e9 / (RUN_STEPS * mean_cells)
-    sample = (f"1 leapfrog step of an s6/L40 float32 member per bench step ({r['cells']} cells), NumPy oracle; runs/s = "
-              f"rate / ({RUN_STEPS} steps x mean member cells {mean_cells:.0f})")
+    sample = (f"1 leapfrog step of an s6/L40 float32 member per bench step ({r['cells']} cells), oracle on PyTorch CPU "
+              f"tensors over {r['cores']} threads; runs/s = rate / ({RUN_STEPS} steps x mean member cells {mean_cells:.0f})")
     line = {
         "impl": "reference", "metric": ENSEMBLE_METRIC, "value": value, "unit": "runs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "config3", "members": args.members, "run_steps": RUN_STEPS, "device": "cpu"},
-        "cpu_baseline": {"value": value, "unit": "runs/s", "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "runs/s", "cores": r["cores"], "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -460,9 +480,10 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
         cpu = {
             "value": r["gcells"] * 1e9 / (RUN_STEPS * statistics.mean(cells)),
             "unit": "runs/s",
-            "cores": 1,
+            "cores": r["cores"],
             "kind": "port",
-            "sample": f"1 leapfrog step of an s6/L40 float32 member ({r['seconds']:.1f} s), NumPy oracle; runs/s = rate / ({RUN_STEPS} x mean member cells)",
+            "sample": (f"1 leapfrog step of an s6/L40 float32 member ({r['seconds']:.1f} s), oracle on PyTorch CPU tensors over "
+                       f"{r['cores']} threads; runs/s = rate / ({RUN_STEPS} x mean member cells)"),
         }
     for p in probes:
         p.close()
@@ -627,16 +648,17 @@ def reference_arm(args, world: int, rank: int) -> None:
         return
     per_step = 1
     sim, info = oracle_build(args.workload)
+    stepper = oracle_stepper(sim)
     for _ in range(args.warmup):
-        oracle_time(sim, info, per_step)
+        oracle_time(stepper, info, per_step)
     rates, secs = [], 0.0
     for _ in range(args.steps):
-        r = oracle_time(sim, info, per_step)
+        r = oracle_time(stepper, info, per_step)
         rates.append(r["gcells"])
         secs += r["seconds"]
     value = statistics.median(rates)
-    sample = (f"{per_step} leapfrog step(s) of s{r['sub']}/L{r['L']} float32 per bench step{r['note']}, NumPy oracle "
-              "restating the reference NumPy backend, single-threaded gathers")
+    sample = (f"{per_step} leapfrog step(s) of s{r['sub']}/L{r['L']} float32 per bench step{r['note']}, the oracle's "
+              f"step on PyTorch CPU tensors over {r['cores']} threads (the reference's Torch-on-CPU path)")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -652,7 +674,7 @@ def reference_arm(args, world: int, rank: int) -> None:
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": args.workload, "cells": r["cells"], "time_steps_per_step": per_step, "device": "cpu"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -791,14 +813,14 @@ def main() -> None:
         drift = fp32_drift(args.workload, device, T, args.subdivision)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = oracle_sample(args.workload, 6 if args.workload == "config4" else 3)
+        r = oracle_sample(args.workload, 3)
         cpu = {
             "value": r["gcells"],
             "unit": UNIT,
-            "cores": 1,
+            "cores": r["cores"],
             "kind": "port",
             "sample": (f"{r['steps']} leapfrog steps of s{r['sub']}/L{r['L']} float32{r['note']} after 1 warm-up step "
-                       f"({r['seconds']:.1f} s), NumPy oracle"),
+                       f"({r['seconds']:.1f} s), the oracle's step on PyTorch CPU tensors over {r['cores']} threads"),
         }
     if rank == 0:
         line = {

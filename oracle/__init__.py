@@ -12,6 +12,10 @@ Parity is pinned: ``tests/golden/make_golden.py`` runs the reference itself
 (imported from its source tree in the build container) and commits its mesh
 tables, fields, ADE states and receiver traces as fixtures;
 ``tests/test_oracle_golden.py`` checks this oracle against them.
+
+``oracle.threaded`` runs the same step on PyTorch CPU tensors over every host
+thread (the reference's Torch-on-CPU path); it is the timed CPU baseline and is
+checked against the same fixtures.
 """
 
 from .fdtd import (  # noqa: F401

@@ -89,3 +89,31 @@ def test_oracle_h_observations_match_reference():
     )
     np.testing.assert_allclose(hr, ref["hr"], rtol=1e-11, atol=1e-30)
     np.testing.assert_allclose(ht, ref["ht"], rtol=1e-11, atol=1e-30)
+
+
+@pytest.mark.parametrize("name", sorted(C.CASES))
+def test_threaded_oracle_float64_matches_reference(name):
+    """The all-threads CPU baseline (PyTorch CPU tensors, ``oracle.threaded``)
+    advances every golden case to the reference's own state."""
+
+    import torch
+
+    from casebuild import build_oracle
+    from oracle.threaded import ThreadedOracleStep
+
+    case = C.CASES[name]
+    ref = golden(f"case_{name}")
+    sim = build_oracle(case)
+    threads = torch.get_num_threads()
+    try:
+        ThreadedOracleStep(sim, 2).step(case["steps"])
+    finally:
+        torch.set_num_threads(threads)
+    assert sim.steps == case["steps"]
+    out = {f: getattr(sim, f) for f in STATE}
+    if sim.surface is not None:
+        out["si_memory"] = sim.si_memory
+    if sim.plasma is not None:
+        out.update({f"plasma_current_{i}": j for i, j in enumerate(sim.p_current)})
+    for key, value in out.items():
+        np.testing.assert_allclose(value, ref[key], rtol=1e-11, atol=1e-12 * group_scale(ref, key), err_msg=key)
