@@ -47,8 +47,10 @@ class Ensemble:
                 raise ValueError("ensemble members must share one CUDA device and one dtype")
         self._members = members
         self._backend = first
-        self._plans = [m._engine.plan.value for m in members]
-        plans = (C.c_void_p * len(members))(*self._plans)
+        # the engines themselves, not their plan addresses: a replaced engine's plan is freed,
+        # and a new plan may be allocated at the same address
+        self._engines = [m._engine for m in members]
+        plans = (C.c_void_p * len(members))(*[e.plan.value for e in self._engines])
         handle = C.c_void_p()
         N.check(N.load().ifdtd_batch_create(plans, len(members), int(graph_chunk), C.byref(handle)), "ifdtd_batch_create")
         self._handle = handle
@@ -144,7 +146,7 @@ class Ensemble:
             raise ValueError("the ensemble is closed")
         # the batch holds the members' plans: a member whose engine was replaced
         # (autotuning, for instance) must not be stepped through a stale plan
-        if any(m._engine.plan.value != p for m, p in zip(self._members, self._plans)):
+        if any(m._engine is not e or not e.plan for m, e in zip(self._members, self._engines)):
             raise ValueError("a member's plan changed after the ensemble was built; build a new Ensemble")
         return self._handle
 

@@ -272,6 +272,40 @@ def test_ensemble_rejects_empty_member_lists_and_bad_chunks():
         Ensemble([object()])
 
 
+def test_ensemble_refuses_a_replaced_engine_even_at_the_same_plan_address():
+    """A freed plan's address can be handed to the next plan; the batch must still
+    refuse a member whose engine was replaced (host logic only, no device)."""
+
+    import ctypes
+
+    from ionosphere_fdtd_b200 import Ensemble
+
+    class FakeEngine:
+        def __init__(self, address):
+            self.plan = ctypes.c_void_p(address)
+
+    class FakeMember:
+        def __init__(self, engine):
+            self._engine = engine
+
+    members = [FakeMember(FakeEngine(0x1000)), FakeMember(FakeEngine(0x2000))]
+    ens = Ensemble.__new__(Ensemble)
+    ens._members = members
+    ens._engines = [m._engine for m in members]
+    ens._handle = ctypes.c_void_p(0x3000)
+    assert ens._live().value == 0x3000
+    members[1]._engine = FakeEngine(0x2000)  # a new engine whose plan reuses the freed address
+    with pytest.raises(ValueError, match="plan changed"):
+        ens._live()
+    members[1]._engine = ens._engines[1]
+    ens._engines[1].plan = ctypes.c_void_p()  # the original engine closed in place
+    with pytest.raises(ValueError, match="plan changed"):
+        ens._live()
+    ens._handle = ctypes.c_void_p()  # nothing to destroy on the fake handle
+    with pytest.raises(ValueError, match="closed"):
+        ens._live()
+
+
 def test_autotune_rejects_bad_arguments_before_touching_the_device():
     from ionosphere_fdtd_b200.autotune import autotune
 
