@@ -109,7 +109,11 @@ def autotune(sim, candidates: Sequence[Tuning] = DEFAULT_CANDIDATES, *, steps: i
             except (ValueError, RuntimeError, BackendUnavailableError) as err:
                 result.timings.append((tuning, None, str(err)))
                 continue
-            ms = _time_engine(sim, engine, steps, repeats)
+            try:
+                ms = _time_engine(sim, engine, steps, repeats)
+            except BaseException:
+                engine.close()
+                raise
             _restore(sim, saved)
             result.timings.append((tuning, ms, None))
             if ms < result.best_ms:
@@ -118,6 +122,10 @@ def autotune(sim, candidates: Sequence[Tuning] = DEFAULT_CANDIDATES, *, steps: i
                 best_engine, result.best, result.best_ms = engine, tuning, ms
             else:
                 engine.close()
+    except BaseException:
+        if best_engine is not None:
+            best_engine.close()
+        raise
     finally:
         _restore(sim, saved)
         sim.backend.synchronize()
