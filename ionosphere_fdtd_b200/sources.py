@@ -37,26 +37,55 @@ def geographic_tangent_basis(latitude_deg: float, longitude_deg: float):
     return east, north
 
 
-_SEARCH_CACHE: dict[int, tuple[object, float]] = {}
+@dataclass(frozen=True)
+class _FaceSearch:
+    """Per-mesh search structure: the search cone and the faces sorted by the z
+    coordinate of their circumcentre."""
+
+    mesh: object
+    half_angle: float  # of the search cone, radians
+    cos_limit: float  # its cosine
+    order: NDArray[np.int64]  # face indices by ascending circumcentre z
+    z: NDArray[np.float64]  # those z values
 
 
-def _face_search_cos(mesh) -> float:
-    """Cosine of a cone half-angle that holds every face: 1 % above the largest
+_SEARCH_CACHE: dict[int, _FaceSearch] = {}
+_BAND_MARGIN = 1.0e-6  # radians and z units added to each band; the band only needs to hold the cone
+
+
+def _face_search(mesh) -> _FaceSearch:
+    """The search cone holds every face: its half-angle is 1 % above the largest
     angle between a face's circumcentre and its corners, plus 1e-6 rad."""
 
     hit = _SEARCH_CACHE.get(id(mesh))
-    if hit is not None and hit[0] is mesh:
-        return hit[1]
+    if hit is not None and hit.mesh is mesh:
+        return hit
     cos_min = 1.0
     for lo in range(0, mesh.n_faces, 1 << 20):
         corners = mesh.vertices[mesh.faces[lo : lo + (1 << 20)]]
         centres = mesh.face_centers[lo : lo + (1 << 20)]
         cos_min = min(cos_min, float(np.min(np.einsum("fkj,fj->fk", corners, centres))))
-    limit = float(np.cos(min(np.pi, 1.01 * float(np.arccos(np.clip(cos_min, -1.0, 1.0))) + 1.0e-6)))
+    half = min(np.pi, 1.01 * float(np.arccos(np.clip(cos_min, -1.0, 1.0))) + 1.0e-6)
+    z = np.ascontiguousarray(mesh.face_centers[:, 2])
+    order = np.argsort(z, kind="stable")
+    out = _FaceSearch(mesh, half, float(np.cos(half)), order, z[order])
     if len(_SEARCH_CACHE) >= 4:
         _SEARCH_CACHE.clear()
-    _SEARCH_CACHE[id(mesh)] = (mesh, limit)
-    return limit
+    _SEARCH_CACHE[id(mesh)] = out
+    return out
+
+
+def _cone_band(search: _FaceSearch, u: NDArray[np.float64]) -> NDArray[np.int64]:
+    """Faces whose circumcentre z lies in the band that any direction within the
+    search cone around the unit vector ``u`` can reach (a superset of the cone)."""
+
+    theta = float(np.arccos(np.clip(u[2], -1.0, 1.0)))
+    a = search.half_angle + _BAND_MARGIN
+    z_lo = float(np.cos(min(np.pi, theta + a))) - _BAND_MARGIN
+    z_hi = float(np.cos(max(0.0, theta - a))) + _BAND_MARGIN
+    lo = int(np.searchsorted(search.z, z_lo, side="left"))
+    hi = int(np.searchsorted(search.z, z_hi, side="right"))
+    return search.order[lo:hi]
 
 
 def geographic_face_index(simulation, latitude_deg: float, longitude_deg: float) -> int:
@@ -65,20 +94,24 @@ def geographic_face_index(simulation, latitude_deg: float, longitude_deg: float)
     The containment test runs only on faces whose circumcentre lies within
     the search cone of the direction or of its antipode (the test also
     accepts a face that holds the antipode); every face the test can accept
-    lies in that set, so the candidates, their order and the choice are those
-    of the test over all faces."""
+    lies in that set.  The cone's faces are found in two z bands of the
+    faces sorted by circumcentre z, and are tested in index order, so the
+    candidates, their order and the choice (the reference's own product
+    ``face_centers[candidates] @ direction``) are those of the test over all
+    faces."""
 
     d = geographic_direction(latitude_deg, longitude_deg)
     mesh = simulation.mesh
     centres = mesh.face_centers
-    proximity = centres @ d
-    limit = _face_search_cos(mesh)
-    near = np.flatnonzero((proximity >= limit) | (-proximity >= limit))
+    search = _face_search(mesh)
+    pool = np.unique(np.concatenate((_cone_band(search, d), _cone_band(search, -d))))
+    proximity = centres[pool] @ d
+    near = pool[(proximity >= search.cos_limit) | (-proximity >= search.cos_limit)]
     tri = mesh.vertices[mesh.faces[near]]
     sides = np.column_stack([np.einsum("ij,j->i", np.cross(tri[:, k], tri[:, (k + 1) % 3]), d) for k in range(3)])
     inside = np.all(sides >= -1.0e-12, axis=1) | np.all(sides <= 1.0e-12, axis=1)
     cand = near[inside]
-    return int(cand[np.argmax(proximity[cand])]) if len(cand) else int(np.argmax(proximity))
+    return int(cand[np.argmax(centres[cand] @ d)]) if len(cand) else int(np.argmax(centres @ d))
 
 
 def geographic_distribution(simulation, latitude_deg: float, longitude_deg: float, altitude_m: float):
