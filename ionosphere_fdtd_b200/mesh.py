@@ -87,7 +87,7 @@ class GeodesicMesh:
         return value
 
     def edge_midpoints(self) -> FloatArray:
-        return _unit(self.vertices[self.edges].sum(axis=1))
+        return _rowwise(lambda e: _unit(self.vertices[e].sum(axis=1)), self.edges)
 
     def edge_diamond_solid_angles(self) -> FloatArray:
         tail = self.vertices[self.edges[:, 0]]

@@ -134,13 +134,21 @@ def _validated_material_sample(values, expected_shape, label):
     eps = np.asarray(epsilon_values, dtype=np.float64)
     if sigma.shape != expected_shape or eps.shape != expected_shape:
         raise ValueError(f"{label} material arrays must have shape {expected_shape}")
-    if not np.all(np.isfinite(sigma)) or not np.all(np.isfinite(eps)):
+    # every element is checked once: a broadcast (zero-stride) axis repeats the same values
+    s_core, e_core = _distinct_elements(sigma), _distinct_elements(eps)
+    if not np.all(np.isfinite(s_core)) or not np.all(np.isfinite(e_core)):
         raise ValueError(f"{label} material arrays must be finite")
-    if np.any(sigma < 0.0):
+    if np.any(s_core < 0.0):
         raise ValueError(f"{label} conductivity cannot be negative")
-    if np.any(eps <= 0.0):
+    if np.any(e_core <= 0.0):
         raise ValueError(f"{label} relative permittivity must be positive")
     return sigma, eps
+
+
+def _distinct_elements(a: NDArray[np.float64]) -> NDArray[np.float64]:
+    """``a`` restricted to index 0 along its zero-stride axes: the same set of values."""
+
+    return a[tuple(slice(0, 1) if st == 0 else slice(None) for st in a.strides)]
 
 
 def _uniform_rows(values: NDArray[np.float64]) -> bool:

@@ -375,3 +375,19 @@ def test_new_entry_points_reject_bad_arguments_before_any_device_work():
     first = np.empty(2, dtype=np.int64)
     count = ctypes.c_int64()
     assert lib.ifdtd_first_use_numbering(N.ptr_i64(lo), N.ptr_i64(hi), 2, 4, N.ptr_i64(rank), N.ptr_i64(first), ctypes.byref(count)) == 1
+
+
+def test_material_validation_checks_broadcast_samples_once_with_the_same_messages():
+    from ionosphere_fdtd_b200.solver import _validated_material_sample as validate
+
+    ones = np.ones((5, 2))
+    with pytest.raises(ValueError, match="must be finite"):
+        validate((np.broadcast_to(np.array([1.0, np.nan]), (5, 2)), ones), (5, 2), "node")
+    with pytest.raises(ValueError, match="conductivity cannot be negative"):
+        validate((np.broadcast_to(np.array([[1.0], [-1.0]]), (2, 5)), np.ones((2, 5))), (2, 5), "node")
+    with pytest.raises(ValueError, match="permittivity must be positive"):
+        validate((ones, np.broadcast_to(0.0, (5, 2))), (5, 2), "edge")
+    with pytest.raises(ValueError, match="must have shape"):
+        validate((np.broadcast_to(1.0, (5, 3)), ones), (5, 2), "node")
+    sigma, eps = validate((np.broadcast_to(np.array([0.0, 1e-3]), (5, 2)), ones), (5, 2), "node")
+    assert sigma.shape == (5, 2) and sigma.strides[0] == 0
