@@ -32,6 +32,7 @@ from .provenance import (
     DatasetProvenance,
     VariableProvenance,
     array_sha256,
+    distinct_elements,
     mesh_faces_sha256,
     mesh_vertices_sha256,
 )
@@ -85,7 +86,8 @@ class ColdPlasmaSpecies:
         collision = np.asarray(self.collision_frequency_hz, dtype=np.float64)
         if density.ndim != 2 or collision.shape != density.shape:
             raise ValueError("plasma density and collision grids must have one shape")
-        if not np.all(np.isfinite(density)) or np.any(density < 0.0) or not np.all(np.isfinite(collision)) or np.any(collision <= 0.0):
+        d_core, c_core = distinct_elements(density), distinct_elements(collision)
+        if not np.all(np.isfinite(d_core)) or np.any(d_core < 0.0) or not np.all(np.isfinite(c_core)) or np.any(c_core <= 0.0):
             raise ValueError("plasma density/collision values are invalid")
         object.__setattr__(self, "number_density_m3", _readonly(density))
         object.__setattr__(self, "collision_frequency_hz", _readonly(collision))
@@ -111,7 +113,7 @@ class MeshPlasmaModel:
             raise ValueError("plasma radial midpoints must be finite and increasing")
         if magnetic.ndim != 3 or magnetic.shape[1:] != (len(alt), 3):
             raise ValueError("magnetic field must have shape (face, radial, 3)")
-        if not np.all(np.isfinite(magnetic)):
+        if not np.all(np.isfinite(distinct_elements(magnetic))):
             raise ValueError("magnetic field must be finite")
         if not species or not all(isinstance(s, ColdPlasmaSpecies) for s in species):
             raise ValueError("plasma model requires charged species")

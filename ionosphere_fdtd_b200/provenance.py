@@ -16,6 +16,7 @@ from pathlib import Path
 from typing import Any
 
 import numpy as np
+from numpy.typing import NDArray
 
 _SHA256 = re.compile(r"[0-9a-f]{64}")
 
@@ -91,17 +92,34 @@ def file_sha256(path: str | Path) -> str:
         raise DataArtifactError(f"cannot hash source file {path}: {error}") from error
 
 
+def distinct_elements(a: Any) -> NDArray:
+    """``a`` restricted to index 0 along its zero-stride (broadcast) axes: the
+    same set of values, each stored element once, for validity checks."""
+
+    a = np.asarray(a)
+    return a[tuple(slice(0, 1) if st == 0 else slice(None) for st in a.strides)]
+
+
 def array_sha256(values: Any) -> str:
     """SHA-256 of the array in little-endian C order, floats as <f8 and integers as <i8."""
 
     array = np.asarray(values)
     if np.issubdtype(array.dtype, np.floating):
-        canonical = np.asarray(array, dtype="<f8", order="C")
+        dtype = "<f8"
     elif np.issubdtype(array.dtype, np.integer):
-        canonical = np.asarray(array, dtype="<i8", order="C")
+        dtype = "<i8"
     else:
         raise DataArtifactError("only numeric arrays can be checksummed")
-    return hashlib.sha256(canonical.tobytes()).hexdigest()
+    digest = hashlib.sha256()
+    if array.ndim == 0:
+        digest.update(np.asarray(array, dtype=dtype).tobytes())
+        return digest.hexdigest()
+    # leading-axis chunks of about 16 MiB, hashed in order: the same bytes as the whole
+    # array in C order, without materialising broadcast or converted arrays in full
+    rows = max(1, (1 << 24) // max(1, 8 * int(np.prod(array.shape[1:]))))
+    for lo in range(0, array.shape[0], rows):
+        digest.update(np.ascontiguousarray(array[lo : lo + rows], dtype=dtype).data)
+    return digest.hexdigest()
 
 
 def mesh_vertices_sha256(mesh: Any) -> str:

@@ -27,6 +27,7 @@ from .engine import Engine, Physics, Tuning, plasma_inputs, surface_inputs
 from .materials import EarthIonosphereMaterial
 from .mesh import GeodesicMesh, build_geodesic_mesh
 from .plasma import GeodesicPlasmaCoupler, MeshPlasmaModel
+from .provenance import distinct_elements
 from .sources import GaussianCurrent, TangentialGaussianCurrent
 from .surface_impedance import ConductiveHalfSpaceSurface, SurfaceImpedanceADE
 
@@ -135,7 +136,7 @@ def _validated_material_sample(values, expected_shape, label):
     if sigma.shape != expected_shape or eps.shape != expected_shape:
         raise ValueError(f"{label} material arrays must have shape {expected_shape}")
     # every element is checked once: a broadcast (zero-stride) axis repeats the same values
-    s_core, e_core = _distinct_elements(sigma), _distinct_elements(eps)
+    s_core, e_core = distinct_elements(sigma), distinct_elements(eps)
     if not np.all(np.isfinite(s_core)) or not np.all(np.isfinite(e_core)):
         raise ValueError(f"{label} material arrays must be finite")
     if np.any(s_core < 0.0):
@@ -143,12 +144,6 @@ def _validated_material_sample(values, expected_shape, label):
     if np.any(e_core <= 0.0):
         raise ValueError(f"{label} relative permittivity must be positive")
     return sigma, eps
-
-
-def _distinct_elements(a: NDArray[np.float64]) -> NDArray[np.float64]:
-    """``a`` restricted to index 0 along its zero-stride axes: the same set of values."""
-
-    return a[tuple(slice(0, 1) if st == 0 else slice(None) for st in a.strides)]
 
 
 def _uniform_rows(values: NDArray[np.float64]) -> bool:

@@ -85,9 +85,16 @@ def smooth_log_normal(directions, seed: int, median: float = 1.0e-2, spread: flo
 
     d = np.asarray(directions, dtype=np.float64)
     rng = np.random.default_rng(seed)
-    x, y, z = d[:, 0], d[:, 1], d[:, 2]
-    basis = np.stack([x, y, z, x * y, y * z, z * x, x * x - y * y, 3 * z * z - 1, x * y * z, x**3 - 3 * x * y * y, z**3], axis=1)
-    field = basis @ rng.standard_normal(basis.shape[1])
+    x, y, z = (np.ascontiguousarray(d[:, k]) for k in range(3))
+    terms = (
+        lambda: x, lambda: y, lambda: z, lambda: x * y, lambda: y * z, lambda: z * x, lambda: x * x - y * y,
+        lambda: 3 * z * z - 1, lambda: x * y * z, lambda: x**3 - 3 * x * y * y, lambda: z**3,
+    )
+    weights = rng.standard_normal(len(terms))
+    # the weighted sum of the monomials, one term at a time (no (n, 11) basis matrix)
+    field = np.zeros(len(d))
+    for w, term in zip(weights, terms):
+        field += w * term()
     field = (field - field.mean()) / max(field.std(), 1e-30)
     return median * np.exp(spread * field)
 

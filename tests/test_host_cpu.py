@@ -391,3 +391,50 @@ def test_material_validation_checks_broadcast_samples_once_with_the_same_message
         validate((np.broadcast_to(1.0, (5, 3)), ones), (5, 2), "node")
     sigma, eps = validate((np.broadcast_to(np.array([0.0, 1e-3]), (5, 2)), ones), (5, 2), "node")
     assert sigma.shape == (5, 2) and sigma.strides[0] == 0
+
+
+def test_array_digest_is_the_digest_of_the_canonical_bytes():
+    """Chunked hashing gives the SHA-256 of the whole array's little-endian C-order
+    bytes (floats as <f8, integers as <i8), for any layout."""
+
+    from ionosphere_fdtd_b200.provenance import array_sha256
+
+    def whole(a):
+        a = np.asarray(a)
+        dtype = "<f8" if np.issubdtype(a.dtype, np.floating) else "<i8"
+        return hashlib.sha256(np.asarray(a, dtype=dtype, order="C").tobytes()).hexdigest()
+
+    rng = np.random.default_rng(3)
+    cases = [
+        rng.standard_normal((3000, 80, 3)),
+        np.broadcast_to(rng.standard_normal((1, 40, 3)), (70_000, 40, 3)),
+        rng.standard_normal((500, 7)).T,
+        rng.integers(0, 1 << 30, (9000, 3)).astype(np.int32),
+        rng.standard_normal(100).astype(">f8"),
+        rng.standard_normal((4, 5)).astype(np.float32),
+        np.float64(2.5),
+        np.zeros((0, 3)),
+        np.arange(17),
+    ]
+    for a in cases:
+        assert array_sha256(a) == whole(a)
+
+
+def test_plasma_validation_sees_bad_values_in_broadcast_profiles():
+    from casebuild import product_provenance
+
+    mesh = P.build_geodesic_mesh(0)
+    h = np.array([60_000.0, 80_000.0])
+    shape = (mesh.n_faces, 2)
+    good = np.broadcast_to(np.array([1e6, 1e8]), shape)
+    with pytest.raises(ValueError, match="density/collision"):
+        P.ColdPlasmaSpecies("e", -P.ELEMENTARY_CHARGE_C, P.ELECTRON_MASS_KG, np.broadcast_to(np.array([1e6, -1.0]), shape), good)
+    with pytest.raises(ValueError, match="density/collision"):
+        P.ColdPlasmaSpecies("e", -P.ELEMENTARY_CHARGE_C, P.ELECTRON_MASS_KG, good, np.broadcast_to(np.array([0.0, 1e3]), shape))
+    sp = P.ColdPlasmaSpecies("e", -P.ELEMENTARY_CHARGE_C, P.ELECTRON_MASS_KG, good, good)
+    bad_b = np.broadcast_to(np.array([[[0.0, 0.0, 5e-5], [0.0, np.inf, 0.0]]]), (*shape, 3))
+    with pytest.raises(ValueError, match="magnetic field must be finite"):
+        P.MeshPlasmaModel.from_mesh(mesh, h, bad_b, (sp,), provenance=(product_provenance(),), interpolation="profile")
+    ok_b = np.broadcast_to(np.zeros((1, 2, 3)), (*shape, 3))
+    model = P.MeshPlasmaModel.from_mesh(mesh, h, ok_b, (sp,), provenance=(product_provenance(),), interpolation="profile")
+    assert model.magnetic_field_t.shape == (*shape, 3)
