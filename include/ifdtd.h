@@ -231,6 +231,14 @@ int32_t ifdtd_batch_info(const ifdtd_batch* batch, int32_t* groups, int32_t* sol
 int32_t ifdtd_first_use_numbering(const int64_t* lo, const int64_t* hi, int64_t n, int64_t n_vertices, int64_t* rank,
                                   int64_t* first, int64_t* n_distinct);
 
+/* Host-side grouping (no device needed): order[] receives the permutation that
+ * a stable sort of keys[0..n) gives (positions grouped by key, ascending, each
+ * group in position order) and counts[k] (room for n_keys entries) the size of
+ * group k; every key must lie in [0, n_keys).  It replaces the stable argsort
+ * of face corners by vertex behind the plasma coupler's incident-face tables
+ * (plasma.py:572-588, a per-vertex list filled while scanning faces in order). */
+int32_t ifdtd_stable_group(const int64_t* keys, int64_t n, int64_t n_keys, int64_t* order, int64_t* counts);
+
 /* max |field| of er, et, hr, ht into out4 (device, float64); the four
  * reductions of diagnostics() (solver.py:1027-1030, torch_backend.py:218-219). */
 int32_t ifdtd_max_abs(ifdtd_plan* plan, const ifdtd_state* state, double* out4, void* stream);

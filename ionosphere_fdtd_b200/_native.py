@@ -127,6 +127,7 @@ _SIGNATURES = {
     "ifdtd_sample": ([_vp, C.POINTER(State), _vp, _vp, _vp], _i32),
     "ifdtd_step_sampled": ([_vp, C.POINTER(State), _vp, _i32, _vp, _vp, _vp], _i32),
     "ifdtd_first_use_numbering": ([_i64p, _i64p, C.c_int64, C.c_int64, _i64p, _i64p, C.POINTER(C.c_int64)], _i32),
+    "ifdtd_stable_group": ([_i64p, C.c_int64, C.c_int64, _i64p, _i64p], _i32),
     "ifdtd_batch_create": ([C.POINTER(_vp), _i32, _i32, C.POINTER(_vp)], _i32),
     "ifdtd_batch_destroy": ([_vp], _i32),
     "ifdtd_batch_step": ([_vp, C.POINTER(State), _vp, _i32, C.POINTER(_vp), C.POINTER(_vp), _vp], _i32),

@@ -1903,6 +1903,25 @@ int32_t ifdtd_first_use_numbering(const int64_t* lo, const int64_t* hi, int64_t 
   return IFDTD_OK;
 }
 
+int32_t ifdtd_stable_group(const int64_t* keys, int64_t n, int64_t n_keys, int64_t* order, int64_t* counts) {
+  if (n < 0 || n_keys <= 0 || !counts || (n > 0 && (!keys || !order)))
+    return fail(IFDTD_ERR_ARGUMENT, "bad stable grouping arguments");
+  std::fill(counts, counts + n_keys, (int64_t)0);
+  for (int64_t i = 0; i < n; ++i) {
+    if (keys[i] < 0 || keys[i] >= n_keys) return fail(IFDTD_ERR_ARGUMENT, "key out of range in stable grouping");
+    ++counts[keys[i]];
+  }
+  // counting sort: each group's first free position, filled in position order
+  std::vector<int64_t> next((size_t)n_keys);
+  int64_t at = 0;
+  for (int64_t k = 0; k < n_keys; ++k) {
+    next[(size_t)k] = at;
+    at += counts[k];
+  }
+  for (int64_t i = 0; i < n; ++i) order[next[(size_t)keys[i]]++] = i;
+  return IFDTD_OK;
+}
+
 int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t chunk, ifdtd_batch** out) {
   if (!plans || !out || n_members <= 0 || chunk < 1) return fail(IFDTD_ERR_ARGUMENT, "bad batch arguments");
   *out = nullptr;

@@ -360,20 +360,31 @@ def face_reconstruction(mesh) -> tuple[NDArray[np.float64], NDArray[np.float64]]
 def edge_face_slots(mesh, faces) -> NDArray[np.int64]:
     """Position of each edge inside its left (or right) face (plasma.py:562-569)."""
 
-    matches = mesh.face_edges[faces] == np.arange(mesh.n_edges)[:, None]
-    if not np.all(np.sum(matches, axis=1) == 1):
+    slots = mesh.face_edges[faces]
+    edge = np.arange(mesh.n_edges)
+    m0, m1, m2 = (slots[:, k] == edge for k in range(3))
+    if not np.all(m0.astype(np.int8) + m1 + m2 == 1):
         raise RuntimeError("edge is absent from an adjacent face")
-    return np.argmax(matches, axis=1)
+    return np.where(m0, 0, np.where(m1, 1, 2))
 
 
 def vertex_face_average(mesh) -> tuple[NDArray[np.int64], NDArray[np.float64]]:
     """Incident faces per vertex in face order with area weights (plasma.py:572-588)."""
 
-    owners = mesh.faces.ravel()
-    face_of = np.repeat(np.arange(mesh.n_faces, dtype=np.int64), 3)
-    order = np.argsort(owners, kind="stable")
-    owners, face_of = owners[order], face_of[order]
-    counts = np.bincount(owners, minlength=mesh.n_vertices)
+    import ctypes
+
+    from . import _native as N
+
+    owners = np.ascontiguousarray(mesh.faces, dtype=np.int64).ravel()
+    # face corners grouped by vertex, each group in face order (a stable counting sort
+    # in the library's host code)
+    order = np.empty(len(owners), dtype=np.int64)
+    counts = np.empty(mesh.n_vertices, dtype=np.int64)
+    N.check(
+        N.load().ifdtd_stable_group(N.ptr_i64(owners), len(owners), mesh.n_vertices, N.ptr_i64(order), N.ptr_i64(counts)),
+        "ifdtd_stable_group",
+    )
+    owners, face_of = owners[order], order // 3
     width = int(counts.max())
     starts = np.concatenate(([0], np.cumsum(counts)[:-1]))
     slot = np.arange(len(owners)) - np.repeat(starts, counts)

@@ -438,3 +438,41 @@ def test_plasma_validation_sees_bad_values_in_broadcast_profiles():
     ok_b = np.broadcast_to(np.zeros((1, 2, 3)), (*shape, 3))
     model = P.MeshPlasmaModel.from_mesh(mesh, h, ok_b, (sp,), provenance=(product_provenance(),), interpolation="profile")
     assert model.magnetic_field_t.shape == (*shape, 3)
+
+
+def test_stable_grouping_is_the_stable_argsort():
+    from ionosphere_fdtd_b200 import _native as N
+
+    rng = np.random.default_rng(11)
+    for n, n_keys in ((0, 3), (1, 1), (1000, 7), (200_000, 5000), (50_000, 100_000)):
+        keys = rng.integers(0, n_keys, n).astype(np.int64)
+        order = np.empty(n, dtype=np.int64)
+        counts = np.empty(n_keys, dtype=np.int64)
+        assert N.load().ifdtd_stable_group(N.ptr_i64(keys), n, n_keys, N.ptr_i64(order), N.ptr_i64(counts)) == 0
+        np.testing.assert_array_equal(order, np.argsort(keys, kind="stable"))
+        np.testing.assert_array_equal(counts, np.bincount(keys, minlength=n_keys))
+    bad = np.array([0, 3, 1], dtype=np.int64)
+    order = np.empty(3, dtype=np.int64)
+    counts = np.empty(3, dtype=np.int64)
+    assert N.load().ifdtd_stable_group(N.ptr_i64(bad), 3, 3, N.ptr_i64(order), N.ptr_i64(counts)) != 0
+    assert N.load().ifdtd_stable_group(N.ptr_i64(bad), 3, 0, N.ptr_i64(order), N.ptr_i64(counts)) != 0
+
+
+def test_vertex_face_tables_equal_the_incidence_scan():
+    """The incident faces of every vertex in face order with area weights, as a
+    sequential scan over the faces builds them (plasma.py:572-588)."""
+
+    for level in (0, 2, 4):
+        mesh = P.build_geodesic_mesh(level)
+        faces, weights = PL.vertex_face_average(mesh)
+        inc = [[] for _ in range(mesh.n_vertices)]
+        for f, tri in enumerate(mesh.faces.tolist()):
+            for v in tri:
+                inc[v].append(f)
+        width = max(len(x) for x in inc)
+        assert faces.shape == (mesh.n_vertices, width)
+        for v, fl in enumerate(inc):
+            np.testing.assert_array_equal(faces[v, : len(fl)], fl)
+            assert not faces[v, len(fl) :].any() and not weights[v, len(fl) :].any()
+            w = mesh.face_solid_angles[fl] / np.sum(mesh.face_solid_angles[fl])
+            np.testing.assert_allclose(weights[v, : len(fl)], w, rtol=1e-15, atol=0)
