@@ -238,12 +238,29 @@ ORACLE_SAMPLE_SUB = {"config2": 7, "config4": 7}
 
 
 def host_threads() -> int:
-    """Host threads this process may run on (its CPU affinity set)."""
+    """Host threads this process may run on: its CPU affinity set, capped by a cgroup CPU
+    quota when one is set (a container may see more cores than it may use)."""
 
     try:
-        return len(os.sched_getaffinity(0))
+        n = len(os.sched_getaffinity(0))
     except AttributeError:
-        return os.cpu_count() or 1
+        n = os.cpu_count() or 1
+    quota = None
+    try:  # cgroup v2: "<quota> <period>" or "max <period>"
+        q, period = Path("/sys/fs/cgroup/cpu.max").read_text().split()[:2]
+        if q != "max":
+            quota = int(q) / int(period)
+    except (OSError, ValueError):
+        try:  # cgroup v1
+            q = int(Path("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read_text())
+            period = int(Path("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read_text())
+            if q > 0 and period > 0:
+                quota = q / period
+        except (OSError, ValueError):
+            pass
+    if quota is not None:
+        n = min(n, max(1, int(quota)))
+    return max(1, n)
 
 
 def oracle_build(workload: str, sub: int | None = None):
