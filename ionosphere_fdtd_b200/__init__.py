@@ -31,6 +31,7 @@ from .plasma import (
     MeshPlasmaModel,
 )
 from .provenance import DatasetProvenance, VariableProvenance, array_sha256
+from .receivers import Receiver, ReceiverTraces, receiver_location, record_receiver_traces
 from .solver import GeodesicFDTD, SimulationConfig
 from .sources import (
     GaussianCurrent,
@@ -84,5 +85,9 @@ __all__ = [
     "geographic_face_index",
     "load_checkpoint",
     "radial_linear_distribution",
+    "Receiver",
+    "ReceiverTraces",
+    "receiver_location",
+    "record_receiver_traces",
     "save_checkpoint",
 ]

@@ -257,3 +257,17 @@ def initial_fields(shapes: dict[str, tuple[int, ...]], seed: int, amplitude: flo
 
     rng = np.random.default_rng(seed)
     return {name: amplitude * rng.standard_normal(shapes[name]) for name in ("er", "et", "hr", "ht")}
+
+
+# record_receiver_traces fixture (visualization.py:212-252): receivers as
+# (latitude, longitude, altitude, label), 11 steps sampled every 4 (rows at 0, 4, 8, 11)
+RECEIVER_TRACES = dict(
+    case="source_s1",
+    steps=11,
+    sample_every=4,
+    receivers=(
+        (35.1595, 126.8526, 0.0, "gwangju"),
+        (-12.5, 40.0, 30_000.0, None),
+        (89.0, -170.0, 95_000.0, "polar"),
+    ),
+)

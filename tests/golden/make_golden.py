@@ -196,10 +196,30 @@ def checkpoint_fixture(mods) -> None:
     )
 
 
+def receiver_traces_fixture(mods) -> None:
+    """The reference's ``record_receiver_traces`` (visualization.py:212-252) on the
+    receiver-trace case of ``cases.py``."""
+
+    from ionosphere_fdtd import visualization as rvis
+
+    spec = C.RECEIVER_TRACES
+    sim = build_reference(C.CASES[spec["case"]], mods)
+    receivers = [rvis.Receiver(lat, lon, alt, label) for lat, lon, alt, label in spec["receivers"]]
+    traces = rvis.record_receiver_traces(sim, receivers, spec["steps"], sample_every=spec["sample_every"])
+    np.savez_compressed(
+        HERE / "receiver_traces_source_s1.npz",
+        time_s=traces.time_s, er_v_m=traces.er_v_m, labels=np.asarray(traces.labels),
+        steps_after=np.asarray(sim.steps), time_after=np.asarray(sim.time_s),
+    )
+
+
 def main(src: str) -> None:
     mods = _import_reference(src)
     if "--checkpoint-only" in sys.argv:
         checkpoint_fixture(mods)
+        return
+    if "--receivers-only" in sys.argv:
+        receiver_traces_fixture(mods)
         return
     only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--cases=")]
     if only:
@@ -230,6 +250,7 @@ def main(src: str) -> None:
         sample_every=3,
     )
     np.savez_compressed(HERE / "obs_h_source_s1.npz", hr=hr, ht=ht)
+    receiver_traces_fixture(mods)
     print("done")
 
 

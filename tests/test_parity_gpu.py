@@ -92,6 +92,24 @@ def test_h_observations_with_decimation_match_reference():
     np.testing.assert_allclose(ht, ref["ht"], rtol=1e-8, atol=1e-10 * np.max(np.abs(ref["ht"])))
 
 
+def test_receiver_helper_matches_the_reference_helper():
+    """record_receiver_traces (visualization.py:212-252) through the engine's sampled
+    steps: the reference's receiver placement, sample rows, clock and labels."""
+
+    from ionosphere_fdtd_b200 import Receiver, record_receiver_traces
+
+    spec = C.RECEIVER_TRACES
+    ref = golden(f"receiver_traces_{spec['case']}")
+    sim = build_product(C.CASES[spec["case"]], "float64")
+    out = record_receiver_traces(sim, [Receiver(*r) for r in spec["receivers"]], spec["steps"],
+                                 sample_every=spec["sample_every"])
+    assert out.labels == tuple(str(x) for x in ref["labels"])
+    np.testing.assert_allclose(out.time_s, ref["time_s"], rtol=1e-14, atol=0)
+    scale = float(np.max(np.abs(ref["er_v_m"])))
+    np.testing.assert_allclose(out.er_v_m, ref["er_v_m"], rtol=1e-8, atol=1e-10 * scale)
+    assert sim.steps == int(ref["steps_after"])
+
+
 @pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "surface_map_s2"])
 def test_engine_is_bitwise_repeatable(name):
     first = run_product(C.CASES[name], "float32")
