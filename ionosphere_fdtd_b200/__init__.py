@@ -10,7 +10,7 @@ from .adaptive_mesh import (
     build_adaptive_geodesic_mesh,
     validate_adaptive_mesh,
 )
-from .backend import CudaBackend, create_backend
+from .backend import ArrayBackend, CudaBackend, TorchBackend, create_backend
 from .checkpoint import load_checkpoint, save_checkpoint
 from .constants import C_0, EARTH_RADIUS_M, EPSILON_0, MU_0
 from .ensemble import Ensemble
@@ -30,7 +30,7 @@ from .plasma import (
     MagnetizedPlasmaADE,
     MeshPlasmaModel,
 )
-from .provenance import DatasetProvenance, VariableProvenance, array_sha256
+from .provenance import DataArtifactError, DatasetProvenance, VariableProvenance, array_sha256
 from .receivers import Receiver, ReceiverTraces, receiver_location, record_receiver_traces
 from .solver import GeodesicFDTD, SimulationConfig
 from .sources import (
@@ -51,6 +51,9 @@ __all__ = [
     "build_adaptive_geodesic_mesh",
     "validate_adaptive_mesh",
     "Ensemble",
+    "ArrayBackend",
+    "TorchBackend",
+    "DataArtifactError",
     "BackendUnavailableError",
     "C_0",
     "CheckpointError",

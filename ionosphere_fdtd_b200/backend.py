@@ -10,6 +10,7 @@ it is one fused H launch and one fused E launch per step (see ``engine``).
 
 from __future__ import annotations
 
+from abc import ABC, abstractmethod
 from collections.abc import Callable
 from typing import Any
 
@@ -27,7 +28,65 @@ def _torch():
     return torch
 
 
-class CudaBackend:
+class ArrayBackend(ABC):
+    """The array operations the time integrator needs (the reference's backend
+    contract, backends/base.py:19-89): allocation and transfer, adjacent
+    differences, the four oriented topology sums, and host reads.  ``CudaBackend``
+    is the only implementation here; the contract is kept so that code written
+    against the reference's seam (type checks, duck-typed callers) keeps working."""
+
+    name: str
+    device: str
+    dtype_name: str
+    threads: int | None = None
+
+    def compile_step(self, step: Callable[[Any], None]) -> Callable[[Any], None]:
+        raise BackendUnavailableError(f"the {self.name} backend does not support compiled field steps")
+
+    def synchronize(self) -> None:
+        """Wait for queued device work (no-op for synchronous backends)."""
+
+    @abstractmethod
+    def asarray(self, values: Any) -> Any: ...
+
+    @abstractmethod
+    def index_array(self, values: Any) -> Any: ...
+
+    @abstractmethod
+    def zeros(self, shape: tuple[int, ...]) -> Any: ...
+
+    @abstractmethod
+    def empty_like(self, values: Any) -> Any: ...
+
+    @abstractmethod
+    def diff(self, values: Any, axis: int) -> Any: ...
+
+    @abstractmethod
+    def edge_difference(self, vertex_values: Any) -> Any: ...
+
+    @abstractmethod
+    def dual_edge_difference(self, face_values: Any) -> Any: ...
+
+    @abstractmethod
+    def face_circulation(self, edge_values: Any) -> Any: ...
+
+    @abstractmethod
+    def dual_cell_circulation(self, edge_values: Any) -> Any: ...
+
+    @abstractmethod
+    def to_numpy(self, values: Any) -> np.ndarray: ...
+
+    @abstractmethod
+    def scalar(self, value: Any) -> float: ...
+
+    @abstractmethod
+    def max_abs(self, values: Any) -> float: ...
+
+    @abstractmethod
+    def nbytes(self, values: Any) -> int: ...
+
+
+class CudaBackend(ArrayBackend):
     """Tensor plumbing on one CUDA device plus the CUDA topology primitives."""
 
     name = "torch"
@@ -172,3 +231,8 @@ def create_backend(name: str, mesh: Any, *, device: str = "auto", dtype: str = "
             "this engine runs the time step on CUDA only; use backend='torch' with a CUDA device"
         )
     raise ValueError("backend must be 'numpy' or 'torch'")
+
+
+# The reference's name for its PyTorch backend (backends/torch_backend.py:13); here
+# it is the CUDA-only engine backend.
+TorchBackend = CudaBackend

@@ -476,3 +476,18 @@ def test_vertex_face_tables_equal_the_incidence_scan():
             assert not faces[v, len(fl) :].any() and not weights[v, len(fl) :].any()
             w = mesh.face_solid_angles[fl] / np.sum(mesh.face_solid_angles[fl])
             np.testing.assert_allclose(weights[v, : len(fl)], w, rtol=1e-15, atol=0)
+
+
+def test_backend_contract_names_of_the_reference_are_available():
+    """The reference's seam (backends/base.py:19-89): CudaBackend implements every
+    abstract method of ArrayBackend and answers to the Torch backend's name."""
+
+    import inspect
+
+    assert issubclass(P.CudaBackend, P.ArrayBackend) and not inspect.isabstract(P.CudaBackend)
+    assert P.TorchBackend is P.CudaBackend and P.CudaBackend.name == "torch"
+    assert issubclass(P.DataArtifactError, ValueError)
+    with pytest.raises(P.BackendUnavailableError):
+        P.create_backend("numpy", P.build_geodesic_mesh(0))
+    with pytest.raises(ValueError, match="backend must be"):
+        P.create_backend("jax", P.build_geodesic_mesh(0))
