@@ -321,11 +321,14 @@ def test_threaded_row_chunks_give_the_same_mesh_bits(monkeypatch):
     import ionosphere_fdtd_b200.mesh as M
 
     serial = M.build_geodesic_mesh(3)
+    serial_midpoints = serial.edge_midpoints()
     monkeypatch.setattr(M, "_ROWS_PER_CHUNK", 97)  # many uneven chunks on several threads
     chunked = M.build_geodesic_mesh(3)
     for name in ("faces", "edges", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles",
                  "dual_cell_solid_angles", "vertex_degree"):
         np.testing.assert_array_equal(getattr(chunked, name), getattr(serial, name), err_msg=name)
+    np.testing.assert_array_equal(chunked.edge_midpoints(), serial_midpoints)
+    np.testing.assert_array_equal(serial_midpoints, M._unit(serial.vertices[serial.edges].sum(axis=1)))
 
 
 def test_first_use_numbering_matches_a_sequential_dict():
