@@ -58,7 +58,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--decoder", default="16x64:4:32,16,1",
                    help="config5: decoder shape t0 x c0 : stride : channels (t0 * stride ** len(channels) = 1024)")
     p.add_argument("--members", type=int, default=64, help="config3: ensemble members")
-    p.add_argument("--no-autotune", action="store_true", help="config3: keep the automatic launch geometry")
+    p.add_argument("--no-autotune", action="store_true", help="keep the automatic launch geometry (no tuning run)")
     p.add_argument("--time-steps", type=int, default=None, help="leapfrog steps per bench step")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -726,6 +726,24 @@ def main() -> None:
     wl = build(args.workload, device, subdivision=args.subdivision)
     setup_s = time.perf_counter() - t_setup
     sim = wl.simulation
+    tuning = None
+    if not args.no_autotune:
+        # launch geometries that fix no patch size, timed on this simulation's own state
+        # (restored afterwards); every candidate computes the same bits
+        from ionosphere_fdtd_b200.autotune import SHAPE_FREE_CANDIDATES, autotune
+
+        t_tune = time.perf_counter()
+        try:
+            res = autotune(sim, SHAPE_FREE_CANDIDATES, steps=32, repeats=3)
+            tuning = {
+                "seconds": time.perf_counter() - t_tune,
+                "candidates": len(SHAPE_FREE_CANDIDATES),
+                "best": {"producer_warps": res.best.producer_warps, "staging": res.best.staging, "ms_per_step": res.best_ms},
+                "timings": [{"producer_warps": t.producer_warps, "staging": t.staging, "ms_per_step": ms, "error": err}
+                            for t, ms, err in res.timings],
+            }
+        except (RuntimeError, ValueError) as err:  # the automatic geometry stays installed
+            tuning = {"seconds": time.perf_counter() - t_tune, "error": str(err)}
     T = args.time_steps or (1000 if args.workload == "config2" else 100)
     stream = torch.cuda.current_stream()
 
@@ -822,6 +840,7 @@ def main() -> None:
         "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
         "parallelism": f"replicas x{world}",
         "setup_s": setup_s,
+        "autotune": tuning,
     }
     drift = None
     if rank == 0 and world == 1 and not args.no_drift:
