@@ -697,6 +697,27 @@ def reference_arm(args, world: int, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def tune_launch_geometry(sim) -> dict:
+    """Time the launch geometries that fix no patch size on the simulation's own state
+    (restored afterwards) and keep the fastest; every candidate computes the same bits.
+    Returns the record for the JSON line; on a failure the automatic geometry stays."""
+
+    from ionosphere_fdtd_b200.autotune import SHAPE_FREE_CANDIDATES, autotune
+
+    t_tune = time.perf_counter()
+    try:
+        res = autotune(sim, SHAPE_FREE_CANDIDATES, steps=32, repeats=3)
+    except (RuntimeError, ValueError) as err:
+        return {"seconds": time.perf_counter() - t_tune, "error": str(err)}
+    return {
+        "seconds": time.perf_counter() - t_tune,
+        "candidates": len(SHAPE_FREE_CANDIDATES),
+        "best": {"producer_warps": res.best.producer_warps, "staging": res.best.staging, "ms_per_step": res.best_ms},
+        "timings": [{"producer_warps": t.producer_warps, "staging": t.staging, "ms_per_step": ms, "error": err}
+                    for t, ms, err in res.timings],
+    }
+
+
 def main() -> None:
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -726,24 +747,7 @@ def main() -> None:
     wl = build(args.workload, device, subdivision=args.subdivision)
     setup_s = time.perf_counter() - t_setup
     sim = wl.simulation
-    tuning = None
-    if not args.no_autotune:
-        # launch geometries that fix no patch size, timed on this simulation's own state
-        # (restored afterwards); every candidate computes the same bits
-        from ionosphere_fdtd_b200.autotune import SHAPE_FREE_CANDIDATES, autotune
-
-        t_tune = time.perf_counter()
-        try:
-            res = autotune(sim, SHAPE_FREE_CANDIDATES, steps=32, repeats=3)
-            tuning = {
-                "seconds": time.perf_counter() - t_tune,
-                "candidates": len(SHAPE_FREE_CANDIDATES),
-                "best": {"producer_warps": res.best.producer_warps, "staging": res.best.staging, "ms_per_step": res.best_ms},
-                "timings": [{"producer_warps": t.producer_warps, "staging": t.staging, "ms_per_step": ms, "error": err}
-                            for t, ms, err in res.timings],
-            }
-        except (RuntimeError, ValueError) as err:  # the automatic geometry stays installed
-            tuning = {"seconds": time.perf_counter() - t_tune, "error": str(err)}
+    tuning = None if args.no_autotune else tune_launch_geometry(sim)
     T = args.time_steps or (1000 if args.workload == "config2" else 100)
     stream = torch.cuda.current_stream()
 

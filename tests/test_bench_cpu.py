@@ -96,3 +96,30 @@ def test_ensemble_cells_follow_the_member_generator():
     assert all(24 <= d["radial_cells"] <= 60 for d in draws)
     assert all(1e-8 <= d["sigma0"] <= 1e-6 and 1e-3 <= d["ground"] <= 1e-1 for d in draws)
     assert all(55e3 <= d["h0"] <= 70e3 and 3e3 <= d["zeta"] <= 6e3 and 10.0 <= d["carrier"] <= 60.0 for d in draws)
+
+
+def test_launch_geometry_record_lists_every_candidate(monkeypatch):
+    """The bench's tuning record from an autotune result (the timing itself needs a GPU)."""
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import ionosphere_fdtd_b200.autotune as A
+
+    def fake(sim, candidates, *, steps, repeats):
+        assert candidates == A.SHAPE_FREE_CANDIDATES and steps == 32 and repeats == 3
+        timings = [(c, 1.0 + i, None) for i, c in enumerate(candidates)]
+        timings[-1] = (candidates[-1], None, "stage does not fit")
+        return A.AutotuneResult(best=candidates[0], best_ms=1.0, timings=timings)
+
+    monkeypatch.setattr(A, "autotune", fake)
+    rec = bench.tune_launch_geometry(object())
+    assert rec["candidates"] == len(A.SHAPE_FREE_CANDIDATES) == len(rec["timings"])
+    assert rec["best"] == {"producer_warps": A.SHAPE_FREE_CANDIDATES[0].producer_warps,
+                           "staging": A.SHAPE_FREE_CANDIDATES[0].staging, "ms_per_step": 1.0}
+    assert rec["timings"][-1]["error"] == "stage does not fit"
+
+    def failing(sim, candidates, *, steps, repeats):
+        raise RuntimeError("plan build failed")
+
+    monkeypatch.setattr(A, "autotune", failing)
+    assert bench.tune_launch_geometry(object())["error"] == "plan build failed"
