@@ -123,3 +123,33 @@ def test_launch_geometry_record_lists_every_candidate(monkeypatch):
 
     monkeypatch.setattr(A, "autotune", failing)
     assert bench.tune_launch_geometry(object())["error"] == "plan build failed"
+
+
+def test_profile_traffic_and_clock_records_parse():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    for workload in ("config2", "config4"):
+        traffic = bench.traffic_from_profile(workload)
+        assert set(traffic) == {"kh_tma", "ke_tma"} and all(v > 1e8 for v in traffic.values())
+    assert bench.traffic_from_profile("no-such-workload") == {}
+
+    sampler = bench.ClockSampler(None)  # no nvidia-smi process: parse a recorded file instead
+    sampler.path.write_text(
+        "1965, 1965, 700.1, Not Active, Not Active, Not Active, Not Active\n"
+        "1800, 1965, 990.0, Not Active, Not Active, Not Active, Active\n"
+        "[N/A], 1965, 10.0, Not Active, Not Active, Not Active, Not Active\n"
+        "1815, 1965, 995.5, Not Active, Not Active, Not Active, Active\n"
+    )
+
+    class Done:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout):
+            return 0
+
+    sampler.proc, sampler.handle = Done(), open(os.devnull, "w")
+    rec = sampler.stop()
+    assert rec == {"sm_mhz": 1815.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    assert not sampler.path.exists()
