@@ -57,3 +57,28 @@ def test_architecture_checks_the_sample_count():
 
     with pytest.raises(ValueError, match="samples"):
         architecture(samples=1000)
+
+
+def test_receiver_geometry_round_trips_through_the_features():
+    """A receiver placed at a bearing and great-circle distance from the source is
+    encoded back to that distance and bearing (host geometry of the training data)."""
+
+    from ionosphere_fdtd_b200.surrogate import _destination, encode_features
+
+    rng = np.random.default_rng(4)
+    rows = []
+    truth = []
+    for _ in range(200):
+        lat, lon = float(rng.uniform(-80, 80)), float(rng.uniform(-180, 180))
+        bearing, dist = float(rng.uniform(-180, 180)), float(rng.uniform(0.5, 12.0))
+        lat2, lon2 = _destination(lat, lon, bearing, dist)
+        assert -90.0 <= lat2 <= 90.0 and -180.0 <= lon2 < 180.0
+        rows.append((-7.0, 62.5, 4.5, -2.0, lat, lon, lat2, lon2))
+        truth.append((dist, bearing, lat))
+    feats = encode_features(np.asarray(rows))
+    truth = np.asarray(truth)
+    np.testing.assert_allclose(feats[:, 4], truth[:, 0] / 10.0, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(feats[:, 5], np.cos(np.radians(truth[:, 1])), rtol=0, atol=1e-7)
+    np.testing.assert_allclose(feats[:, 6], np.sin(np.radians(truth[:, 1])), rtol=0, atol=1e-7)
+    np.testing.assert_allclose(feats[:, 7], np.sin(np.radians(truth[:, 2])), rtol=0, atol=1e-15)
+    np.testing.assert_allclose(feats[:, :4], 0.0, atol=1e-15)  # centre of every parameter range
