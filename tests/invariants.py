@@ -1,0 +1,57 @@
+"""Surface-eigenmode helpers shared by the CPU and GPU invariant tests: the TM-r
+and TE-r surface operators of the mesh, one of their l = 1 eigenvectors, and
+the exact leapfrog dispersion of its amplitude (the reference's
+tests/test_maxwell_invariants.py:60-163)."""
+
+import numpy as np
+
+from ionosphere_fdtd_b200.constants import C_0
+
+# a shell thin against a huge radius, so the radial metric leaves the surface modes alone
+SURFACE_MODE = dict(subdivision=1, radial_cells=2, minimum_altitude_m=-1.0e9, maximum_altitude_m=1.0e9,
+                    earth_radius_m=1.0e10, courant_factor=0.8)
+
+
+class Vacuum:
+    """sigma = 0, relative permittivity 1 everywhere."""
+
+    def sample(self, directions, altitudes_m, earth_radius_m):
+        shape = (len(directions), len(altitudes_m))
+        return np.zeros(shape), np.ones(shape)
+
+
+def tm_operator(mesh, values):
+    """Circumcentric finite-volume Laplacian on the unit sphere: dual/primal weighted
+    edge differences summed around each dual cell, over its solid angle."""
+
+    flux = mesh.dual_edge_angles / mesh.primal_edge_angles * mesh.edge_difference(values)
+    return mesh.dual_cell_circulation(flux) / mesh.dual_cell_solid_angles
+
+
+def te_operator(mesh, values):
+    """The face counterpart: primal/dual weighted dual differences around each face."""
+
+    grad = mesh.primal_edge_angles / mesh.dual_edge_angles * mesh.dual_edge_difference(values)
+    return mesh.face_circulation(grad) / mesh.face_solid_angles
+
+
+def surface_mode(mesh, kind: str):
+    """A real eigenvector of the TM (vertex) or TE (face) operator with eigenvalue
+    near the l = 1 value (-2 for TM, +2 for TE), and minus that eigenvalue's sign."""
+
+    n = mesh.n_vertices if kind == "tm" else mesh.n_faces
+    apply = (lambda v: tm_operator(mesh, v)) if kind == "tm" else (lambda v: te_operator(mesh, v))
+    eye = np.eye(n)
+    matrix = np.column_stack([apply(eye[:, i]) for i in range(n)])
+    values, vectors = np.linalg.eig(matrix)
+    target = -2.0 if kind == "tm" else 2.0
+    pick = int(np.argmin(np.abs(values.real - target)))
+    eigen = -float(values[pick].real) if kind == "tm" else float(values[pick].real)
+    return eigen, vectors[:, pick].real
+
+
+def expected_amplitudes(eigen, dt, radius, steps, offset):
+    q = (C_0 * dt) ** 2 * eigen / radius**2
+    phase = np.arccos(1.0 - 0.5 * q)
+    n = np.arange(steps + 1)
+    return np.cos((n + offset) * phase) / np.cos(0.5 * phase)

@@ -1,0 +1,59 @@
+"""Discrete invariants of the reference's test strategy
+(tests/test_maxwell_invariants.py:76-163 in the reference), on the CPU: the
+adjoint pairs of the mesh's incidence operators, and the exact leapfrog
+dispersion of surface TM-r and TE-r eigenmodes run through the oracle's half
+steps.  ``tests/test_solver_gpu.py`` runs the same eigenmodes through the
+engine."""
+
+import numpy as np
+import pytest
+
+import ionosphere_fdtd_b200 as P
+import oracle.fdtd as O
+from invariants import SURFACE_MODE, Vacuum, expected_amplitudes, surface_mode
+
+
+def test_incidence_operators_are_adjoint_pairs():
+    mesh = P.build_geodesic_mesh(2)
+    rng = np.random.default_rng(20260805)
+    e = rng.standard_normal(mesh.n_edges)
+    f = rng.standard_normal(mesh.n_faces)
+    v = rng.standard_normal(mesh.n_vertices)
+    assert f @ mesh.face_circulation(e) == pytest.approx(mesh.dual_edge_difference(f) @ e, abs=2.0e-13)
+    assert v @ mesh.dual_cell_circulation(e) == pytest.approx(-mesh.edge_difference(v) @ e, abs=2.0e-13)
+
+
+def _oracle():
+    return O.OracleFDTD(material=Vacuum(), dtype=np.float64, **SURFACE_MODE)
+
+
+def test_oracle_tm_surface_mode_follows_the_leapfrog_dispersion():
+    sim = _oracle()
+    eigen, mode = surface_mode(P.build_geodesic_mesh(1), "tm")
+    sim.er[:, 1] = mode
+    amplitudes = [1.0]
+    for _ in range(100):
+        sim.update_magnetic()
+        sim.update_electric(0.0)
+        sim.et[:] = 0.0
+        sim.hr[:] = 0.0
+        amplitudes.append(float(sim.er[:, 1] @ mode / (mode @ mode)))
+    expected = expected_amplitudes(eigen, sim.dt, sim.radii_m[1], 100, 0.5)
+    np.testing.assert_allclose(amplitudes, expected, rtol=0.0, atol=8.0e-14)
+    assert not np.any(sim.hr)
+
+
+def test_oracle_te_surface_mode_follows_the_leapfrog_dispersion():
+    sim = _oracle()
+    eigen, mode = surface_mode(P.build_geodesic_mesh(1), "te")
+    sim.hr[:, 1] = mode
+    amplitudes = [1.0]
+    for _ in range(100):
+        sim.update_magnetic()
+        sim.ht[:] = 0.0
+        sim.update_electric(0.0)
+        sim.er[:] = 0.0
+        amplitudes.append(float(sim.hr[:, 1] @ mode / (mode @ mode)))
+    expected = expected_amplitudes(eigen, sim.dt, sim.midpoints_m[1], 100, -0.5)
+    np.testing.assert_allclose(amplitudes, expected, rtol=0.0, atol=8.0e-14)
+    assert not np.any(sim.er)

@@ -264,3 +264,34 @@ def test_uncompressed_checkpoint_has_the_same_arrays_and_resumes(tmp_path):
     resumed.step(5)
     for f in ("er", "et", "hr", "ht"):
         np.testing.assert_array_equal(resumed.to_numpy(getattr(resumed, f)), whole.to_numpy(getattr(whole, f)))
+
+
+@pytest.mark.parametrize("kind", ["tm", "te"])
+def test_surface_eigenmodes_follow_the_leapfrog_dispersion(kind):
+    """The reference's eigenmode invariants (tests/test_maxwell_invariants.py:91-163)
+    through the engine's half steps: an l = 1 surface mode keeps its shape and its
+    amplitude follows the exact leapfrog dispersion (the oracle meets it to 8e-14,
+    tests/test_invariants_cpu.py)."""
+
+    from invariants import SURFACE_MODE, Vacuum, expected_amplitudes, surface_mode
+
+    s = sim(SimulationConfig(**SURFACE_MODE), material=Vacuum())
+    eigen, mode = surface_mode(s.mesh, kind)
+    (s.er if kind == "tm" else s.hr)[:, 1] = s.backend.asarray(mode)
+    amplitudes = [1.0]
+    for _ in range(100):
+        s._update_magnetic_fields()
+        if kind == "te":
+            s.ht.zero_()
+        s._update_electric_fields()
+        if kind == "tm":
+            s.et.zero_()
+            s.hr.zero_()
+        else:
+            s.er.zero_()
+        values = s.to_numpy(s.er if kind == "tm" else s.hr)[:, 1]
+        amplitudes.append(float(values @ mode / (mode @ mode)))
+    radius = s.radii_m[1] if kind == "tm" else s.radial_midpoints_m[1]
+    expected = expected_amplitudes(eigen, s.time_step_s, radius, 100, 0.5 if kind == "tm" else -0.5)
+    np.testing.assert_allclose(amplitudes, expected, rtol=0.0, atol=1.0e-11)
+    assert not np.any(s.to_numpy(s.hr if kind == "tm" else s.er))
