@@ -55,3 +55,31 @@ def expected_amplitudes(eigen, dt, radius, steps, offset):
     phase = np.arccos(1.0 - 0.5 * q)
     n = np.arange(steps + 1)
     return np.cos((n + offset) * phase) / np.cos(0.5 * phase)
+
+
+class UniformConductive(Vacuum):
+    """One conductivity everywhere, vacuum permittivity."""
+
+    def __init__(self, conductivity_s_m: float) -> None:
+        self.conductivity_s_m = conductivity_s_m
+
+    def sample(self, directions, altitudes_m, earth_radius_m):
+        sigma, eps = super().sample(directions, altitudes_m, earth_radius_m)
+        sigma.fill(self.conductivity_s_m)
+        return sigma, eps
+
+
+class UniformPermittivity(Vacuum):
+    """One relative permittivity everywhere, no conductivity."""
+
+    def __init__(self, relative_permittivity: float) -> None:
+        self.relative_permittivity = relative_permittivity
+
+    def sample(self, directions, altitudes_m, earth_radius_m):
+        sigma, eps = super().sample(directions, altitudes_m, earth_radius_m)
+        eps.fill(self.relative_permittivity)
+        return sigma, eps
+
+
+# an abruptly graded radial grid (the reference's nonuniform-stencil cases)
+GRADED_ALTITUDES = (-10_000.0, -6_000.0, -2_000.0, -1_000.0, 0.0, 4_000.0)

@@ -295,3 +295,94 @@ def test_surface_eigenmodes_follow_the_leapfrog_dispersion(kind):
     expected = expected_amplitudes(eigen, s.time_step_s, radius, 100, 0.5 if kind == "tm" else -0.5)
     np.testing.assert_allclose(amplitudes, expected, rtol=0.0, atol=1.0e-11)
     assert not np.any(s.to_numpy(s.hr if kind == "tm" else s.er))
+
+
+def _peak(s) -> float:
+    return max(float(np.max(np.abs(s.to_numpy(s.er)))), float(np.max(np.abs(s.to_numpy(s.et)))))
+
+
+def test_conductive_update_is_passive_and_exact_in_the_stiff_limit():
+    """The reference's loss invariants (tests/test_maxwell_invariants.py:219-291): a
+    stiff conductor decays monotonically, to the exact exp(-sigma dt / eps0), with
+    no sign flip."""
+
+    from invariants import UniformConductive
+
+    from ionosphere_fdtd_b200.constants import EPSILON_0
+
+    s = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=0.2), material=UniformConductive(1.0))
+    s.er.fill_(1.0)
+    norms = [float(np.linalg.norm(s.to_numpy(s.er)))]
+    s.step()
+    np.testing.assert_allclose(s.to_numpy(s.er), np.exp(-1.0 * s.time_step_s / EPSILON_0), rtol=0.0, atol=1.0e-300)
+    assert np.all(s.to_numpy(s.er) >= 0.0)
+    norms.append(float(np.linalg.norm(s.to_numpy(s.er))))
+    for _ in range(19):
+        s.step()
+        norms.append(float(np.linalg.norm(s.to_numpy(s.er))))
+    assert np.all(np.diff(norms) <= 0.0)
+    ca = s.to_numpy(s._ca_er)
+    assert np.max(ca) < 1.0 and np.min(ca) >= 0.0
+
+
+def test_exponential_conductive_forcing_converges_at_second_order():
+    from invariants import UniformConductive, Vacuum
+
+    from ionosphere_fdtd_b200.constants import EPSILON_0
+
+    base = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=1.0), material=Vacuum())
+    coarse_dt = 0.4 * base.cfl_time_step_limit_s
+    coarse_steps = 20
+    duration = coarse_steps * coarse_dt
+    conductivity = 0.5 * EPSILON_0 / duration
+    errors = []
+    for refinement in (1, 2):
+        dt = coarse_dt / refinement
+        s = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=1.0, time_step_s=dt),
+                material=UniformConductive(conductivity))
+        a, b = float(s.to_numpy(s._ca_er)[0, 0]), float(s.to_numpy(s._cb_er)[0, 0])
+        field = 0.0
+        for step in range(coarse_steps * refinement):
+            field = a * field + b * (step + 0.5) * dt
+        exact = duration / conductivity - EPSILON_0 / conductivity**2 * (1.0 - np.exp(-conductivity * duration / EPSILON_0))
+        errors.append(abs(field - exact))
+    assert errors[0] / errors[1] == pytest.approx(4.0, rel=3.0e-3)
+
+
+def test_trapezoidal_loss_keeps_its_coefficients():
+    from invariants import UniformConductive
+
+    from ionosphere_fdtd_b200.constants import EPSILON_0
+
+    s = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=0.2, loss_integration="trapezoidal"),
+            material=UniformConductive(1.0))
+    loss = 1.0 * s.time_step_s / (2.0 * EPSILON_0)
+    ca = s.to_numpy(s._ca_er)
+    np.testing.assert_allclose(ca, (1.0 - loss) / (1.0 + loss), rtol=0.0, atol=0.0)
+    assert np.all(ca < 0.0)
+
+
+@pytest.mark.parametrize("case", ["subvacuum", "graded"])
+def test_runs_at_the_material_aware_cfl_limit_stay_bounded(case):
+    """tests/test_maxwell_invariants.py:317-342 and 463-497 of the reference: random
+    fields at the CFL limit stay below twice their initial peak."""
+
+    from invariants import GRADED_ALTITUDES, UniformPermittivity, Vacuum
+
+    if case == "subvacuum":
+        s = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=1.0), material=UniformPermittivity(0.01))
+        steps = 400
+    else:
+        a = GRADED_ALTITUDES
+        s = sim(SimulationConfig(subdivision=0, radial_cells=len(a) - 1, minimum_altitude_m=a[0], maximum_altitude_m=a[-1],
+                                 radial_altitudes_m=a, radial_grid_policy="allow-abrupt", courant_factor=1.0),
+                material=Vacuum())
+        steps = 1000
+    rng = np.random.default_rng(20260805)
+    s.er.copy_(s.backend.asarray(rng.standard_normal(tuple(s.er.shape))))
+    s.et.copy_(s.backend.asarray(rng.standard_normal(tuple(s.et.shape))))
+    initial = peak = _peak(s)
+    for _ in range(steps):
+        s.step()
+        peak = max(peak, _peak(s))
+    assert np.isfinite(peak) and peak < 2.0 * initial
