@@ -1,0 +1,59 @@
+"""The reference's configuration and source-waveform validation tests
+(tests/test_solver.py there) on the package's SimulationConfig,
+GaussianCurrent and TangentialGaussianCurrent: the same rejections with the
+same message keys, and the default source."""
+
+import numpy as np
+import pytest
+
+from ionosphere_fdtd_b200 import GaussianCurrent, SimulationConfig, TangentialGaussianCurrent
+
+
+def config(**changes):
+    values = dict(subdivision=1, radial_cells=6, courant_factor=0.25)
+    values.update(changes)
+    return SimulationConfig(**values)
+
+
+@pytest.mark.parametrize(
+    "changes, message",
+    [
+        (dict(mesh_relaxations=-1), "mesh_relaxations"),
+        (dict(mesh_optimization_steps=-1), "mesh_optimization_steps"),
+        (dict(time_step_s=np.nan), "finite"),
+        (dict(earth_radius_m=np.nan), "finite"),
+        (dict(radial_altitudes_m=(-100_000.0, 0.0, 100_000.0)), "radial_cells"),
+        (dict(mesh_orientation="sideways"), "mesh_orientation"),
+        (dict(tangential_material_support="unknown"), "tangential_material_support"),
+        (dict(radial_material_support="unknown"), "radial_material_support"),
+        (dict(radial_boundary_condition="absorbing"), "radial_boundary_condition"),
+        (dict(loss_integration="forward-euler"), "loss_integration"),
+        (dict(radial_grid_policy="unchecked"), "radial_grid_policy"),
+        (dict(geometry_mode="cylindrical"), "geometry_mode"),
+        (dict(radial_cells=4, radial_altitudes_m=(-100_000.0, -5_000.0, -1_250.0, 0.0, 100_000.0)), "smoothly graded"),
+    ],
+)
+def test_config_rejections_match_the_reference(changes, message):
+    with pytest.raises(ValueError, match=message):
+        config(**changes)
+
+
+def test_source_waveform_rejections_match_the_reference():
+    with pytest.raises(ValueError, match="finite"):
+        GaussianCurrent(one_over_e_half_width_s=np.nan)
+    with pytest.raises(ValueError, match="positive"):
+        GaussianCurrent(one_over_e_half_width_s=0.0)
+    with pytest.raises(ValueError, match="latitude"):
+        TangentialGaussianCurrent(latitude_deg=91.0)
+    with pytest.raises(ValueError, match="finite"):
+        TangentialGaussianCurrent(line_lengths_m=(np.inf,))
+    with pytest.raises(ValueError, match="finite"):
+        GaussianCurrent(vertical_element_length_m=np.inf)
+    with pytest.raises(ValueError, match="positive"):
+        GaussianCurrent(vertical_element_length_m=0.0)
+
+
+def test_default_source_and_modulated_envelope():
+    source = GaussianCurrent()
+    assert source.latitude_deg == pytest.approx(35.1595) and source.longitude_deg == pytest.approx(126.8526)
+    assert GaussianCurrent(carrier_frequency_hz=20.0, peak_current_a=1.0).current_a(0.1, 1.0e-6) == pytest.approx(1.0)
