@@ -386,3 +386,56 @@ def test_runs_at_the_material_aware_cfl_limit_stay_bounded(case):
         s.step()
         peak = max(peak, _peak(s))
     assert np.isfinite(peak) and peak < 2.0 * initial
+
+
+def test_source_supports_keep_the_direction_and_staggered_altitude():
+    """tests/test_solver.py of the reference: barycentric source weights reproduce the
+    source direction, and the two radial nodes reproduce its altitude."""
+
+    source = P.GaussianCurrent(altitude_m=2_500.0)
+    s = sim(small_config(), source=source)
+    vertices, _, weights = source.distribution(s)
+    represented = weights @ s.mesh.vertices[vertices]
+    represented /= np.linalg.norm(represented)
+    assert weights.sum() == pytest.approx(1.0) and np.all(weights >= 0.0)
+    assert represented @ source.direction() == pytest.approx(1.0)
+    vertices, layers, weights = source.staggered_distribution(s)
+    assert weights @ s.altitudes_m[layers] == pytest.approx(source.altitude_m)
+    assert weights.sum() == pytest.approx(1.0) and len(np.unique(layers)) == 2
+    s3 = sim(small_config(subdivision=3))
+    assert P.geographic_face_index(s3, 0.0, 43.0) != P.geographic_face_index(s3, 0.0, -137.0)
+    for lat, lon in ((0.0, 43.0), (0.0, -137.0), (89.9, 12.0), (-45.0, 180.0)):
+        v, _, w = P.geographic_distribution(s3, lat, lon, 0.0)
+        d = w @ s3.mesh.vertices[v]
+        np.testing.assert_allclose(d / np.linalg.norm(d), P.geographic_direction(lat, lon), atol=1.0e-12)
+
+
+def _represented_moments(s, source, current):
+    vertices, layers, weights = source.staggered_distribution(s)
+    s._update_electric_fields(current)
+    er = s.to_numpy(s.er)
+    cb = np.broadcast_to(s.to_numpy(s._cb_er), er.shape)
+    density = -er[vertices, layers] / cb[vertices, layers]
+    area = s.mesh.dual_cell_solid_angles[vertices] * s.radii_m[layers] ** 2
+    return density * area * s.radial_node_control_lengths_m[layers], weights
+
+
+@pytest.mark.parametrize("grid", ["uniform-24", "uniform-40", "uniform-80", "graded"])
+def test_vertical_source_deposits_its_current_moment(grid):
+    """The E update with current I deposits exactly I x element length, split by the
+    support weights, on any radial grid (tests/test_solver.py of the reference)."""
+
+    from invariants import GRADED_ALTITUDES
+
+    if grid == "graded":
+        a = GRADED_ALTITUDES
+        cfg = SimulationConfig(subdivision=0, radial_cells=len(a) - 1, minimum_altitude_m=a[0], maximum_altitude_m=a[-1],
+                               radial_altitudes_m=a, radial_grid_policy="allow-abrupt", courant_factor=0.2)
+        source = P.GaussianCurrent(altitude_m=-500.0, peak_current_a=3.0, vertical_element_length_m=7_500.0)
+    else:
+        cfg = SimulationConfig(subdivision=0, radial_cells=int(grid.split("-")[1]), courant_factor=0.2)
+        source = P.GaussianCurrent(altitude_m=2_500.0, peak_current_a=3.0, vertical_element_length_m=7_500.0)
+    s = sim(cfg, source=source)
+    moments, weights = _represented_moments(s, source, source.peak_current_a)
+    np.testing.assert_allclose(moments, source.peak_current_a * source.vertical_element_length_m * weights, rtol=1e-12)
+    assert moments.sum() == pytest.approx(source.peak_current_a * source.vertical_element_length_m)
