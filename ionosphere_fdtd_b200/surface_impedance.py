@@ -141,6 +141,47 @@ class SurfaceImpedanceADE:
         self._scale = backend.asarray(self.scale_host)
         self.memory = backend.zeros((edge_count, model.terms))
 
+    # -- array-level updates (surface_impedance.py:205-270) -------------------------
+    # The engine's H kernel applies the lower-boundary update inside the step; these
+    # are the same formulas on the backend's arrays for callers that drive the ADE
+    # directly (harmonic-response checks, custom boundary experiments).
+
+    def _history(self, rows):
+        memory = self.memory if rows is None else self.memory[rows]
+        scale = self._scale if rows is None else self._scale[rows]
+        history = scale * (memory * self._history_weights[None, :]).sum(axis=1)
+        return memory, history, scale * self._history_weights.sum()
+
+    def _store_memory(self, memory, h_old, h_new, rows) -> None:
+        """Trapezoidal pole memories: m <- m (1 - a) / (1 + a) + (h_old + h_new) a / (1 + a)."""
+
+        updated = memory * self._decay[None, :] + (h_new + h_old)[:, None] * self._drive[None, :]
+        if rows is None:
+            self.memory[:] = updated
+        else:
+            self.memory[rows] = updated
+
+    def advance_prescribed_magnetic(self, h_old, h_new, *, rows=None):
+        """Boundary E for a prescribed H history, advancing the memories
+        (surface_impedance.py:205-223): E = history - gain x (H_old + H_new) / 2."""
+
+        memory, history, gain = self._history(rows)
+        electric = history - gain * (0.5 * (h_new + h_old))
+        self._store_memory(memory, h_old, h_new, rows)
+        return electric
+
+    def advance_lower_boundary(self, h_old, electric_first_cell, surface_gradient_er, radial_step_m, time_step_s, *, rows=None):
+        """Implicit lower-boundary Ht coupled to the impedance memories
+        (surface_impedance.py:225-254); the engine's H kernel runs the same update."""
+
+        memory, history, gain = self._history(rows)
+        kappa = 2.0 * time_step_s / (MU_0 * radial_step_m)
+        coupling = kappa * gain
+        h_new = ((1.0 - 0.5 * coupling) * h_old + time_step_s / MU_0 * surface_gradient_er
+                 - kappa * electric_first_cell + kappa * history) / (1.0 + 0.5 * coupling)
+        self._store_memory(memory, h_old, h_new, rows)
+        return h_new
+
     @property
     def state_bytes(self) -> int:
         return self.backend.nbytes(self.memory)
