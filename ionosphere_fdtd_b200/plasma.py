@@ -398,6 +398,24 @@ def vertex_face_average(mesh) -> tuple[NDArray[np.int64], NDArray[np.float64]]:
     return faces, areas / total[:, None]
 
 
+def _face_layer_component_view(component_major):
+    """(F, 3, L) storage seen as the reference's (F, L, 3) array, without a copy."""
+
+    if hasattr(component_major, "permute"):
+        return component_major.permute(0, 2, 1)
+    return np.swapaxes(component_major, 1, 2)
+
+
+def _cross_with(v, b, backend):
+    """v x b over the last axis (plasma.py:591-596)."""
+
+    out = backend.empty_like(v)
+    out[..., 0] = v[..., 1] * b[..., 2] - v[..., 2] * b[..., 1]
+    out[..., 1] = v[..., 2] * b[..., 0] - v[..., 0] * b[..., 2]
+    out[..., 2] = v[..., 0] * b[..., 1] - v[..., 1] * b[..., 0]
+    return out
+
+
 class MagnetizedPlasmaADE:
     """Species coefficients and device current densities.
 
@@ -413,7 +431,32 @@ class MagnetizedPlasmaADE:
         n_faces, layers = model.magnetic_field_t.shape[:2]
         pitch = mid_pitch or (layers + 3) // 4 * 4
         self.buffers = [backend.zeros((n_faces, 3, pitch)) for _ in model.species]
-        self.current_density = [buf[:, :, :layers].permute(0, 2, 1) for buf in self.buffers]
+        self.current_density = [_face_layer_component_view(buf[:, :, :layers]) for buf in self.buffers]
+        self._arrays = None  # backend copies of coef / bdir for ``advance``, made on first use
+
+    def advance(self, electric_v_m: Any) -> Any:
+        """Advance every species' current by one step under the face-centred field
+        ``electric_v_m`` (F, L, 3) and return their sum (plasma.py:413-442).  The
+        engine's H kernel runs this update inside the step; this is the same
+        arithmetic on the backend's arrays, for callers that drive the ADE directly."""
+
+        if self._arrays is None:
+            asarray = self.backend.asarray
+            self._arrays = ([[asarray(c[k])[..., None] for k in range(6)] for c in self.coef], asarray(self.bdir))
+        coefs, b = self._arrays
+        e_par = (electric_v_m * b).sum(-1)[..., None] * b
+        e_perp = electric_v_m - e_par
+        e_cross = _cross_with(e_perp, b, self.backend)
+        total = None
+        for current, (decay, cosine, sine, d_par, d_re, d_im) in zip(self.current_density, coefs):
+            j_par = (current * b).sum(-1)[..., None] * b
+            j_perp = current - j_par
+            j_cross = _cross_with(j_perp, b, self.backend)
+            updated = (decay * j_par + d_par * e_par + decay * (cosine * j_perp + sine * j_cross)
+                       + d_re * e_perp + d_im * e_cross)
+            current[...] = updated
+            total = updated if total is None else total + updated
+        return total
 
     @property
     def state_bytes(self) -> int:
