@@ -439,3 +439,34 @@ def test_vertical_source_deposits_its_current_moment(grid):
     moments, weights = _represented_moments(s, source, source.peak_current_a)
     np.testing.assert_allclose(moments, source.peak_current_a * source.vertical_element_length_m * weights, rtol=1e-12)
     assert moments.sum() == pytest.approx(source.peak_current_a * source.vertical_element_length_m)
+
+
+@pytest.mark.parametrize("version", [1, 2])
+def test_legacy_checkpoints_load_to_the_same_state(tmp_path, version):
+    """Version-1 files (no face table) and version-2 files (no surface-impedance
+    entry) restore the state of the current format (tests/test_checkpoint.py:163-202
+    of the reference)."""
+
+    import json
+
+    s = sim(small_config(radial_cells=4), source=P.GaussianCurrent(peak_current_a=1.0e6))
+    s.step(7)
+    path = s.save_checkpoint(tmp_path / "current.npz")
+    drop = {"mesh_faces", "mesh_face_levels"} if version == 1 else {"surface_impedance_memory"}
+    with np.load(path, allow_pickle=False) as archive:
+        arrays = {n: np.array(archive[n], copy=True) for n in archive.files if n not in drop}
+    meta = json.loads(str(arrays["metadata"].item()))
+    meta["version"] = version
+    meta.pop("mesh" if version == 1 else "surface_impedance")
+    arrays["metadata"] = np.asarray(json.dumps(meta))
+    legacy = tmp_path / f"legacy-v{version}.npz"
+    np.savez_compressed(legacy, **arrays)
+    restored = GeodesicFDTD.load_checkpoint(legacy, device="cuda")
+    assert restored.steps == s.steps and restored.time_s == s.time_s
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(restored.to_numpy(getattr(restored, f)), s.to_numpy(getattr(s, f)))
+    np.testing.assert_array_equal(restored.mesh.faces, s.mesh.faces)
+    s.step(3)
+    restored.step(3)
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(restored.to_numpy(getattr(restored, f)), s.to_numpy(getattr(s, f)))
