@@ -57,3 +57,22 @@ def test_default_source_and_modulated_envelope():
     source = GaussianCurrent()
     assert source.latitude_deg == pytest.approx(35.1595) and source.longitude_deg == pytest.approx(126.8526)
     assert GaussianCurrent(carrier_frequency_hz=20.0, peak_current_a=1.0).current_a(0.1, 1.0e-6) == pytest.approx(1.0)
+
+
+@pytest.mark.parametrize("chunk_size", (0, True, 1.5))
+def test_compile_chunk_size_must_be_a_positive_integer(chunk_size):
+    from ionosphere_fdtd_b200 import GeodesicFDTD
+
+    with pytest.raises(ValueError, match="compile_chunk_size"):
+        GeodesicFDTD(config=config(), compile_chunk_size=chunk_size)
+
+
+def test_gpu_alias_reports_a_missing_cuda_device():
+    import torch
+
+    from ionosphere_fdtd_b200 import BackendUnavailableError, GeodesicFDTD
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present; the GPU tests cover the alias")
+    with pytest.raises(BackendUnavailableError, match="CUDA"):
+        GeodesicFDTD(config=config(), backend="torch", device="gpu")

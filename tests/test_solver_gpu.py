@@ -470,3 +470,20 @@ def test_legacy_checkpoints_load_to_the_same_state(tmp_path, version):
     restored.step(3)
     for f in ("er", "et", "hr", "ht"):
         np.testing.assert_array_equal(restored.to_numpy(getattr(restored, f)), s.to_numpy(getattr(s, f)))
+
+
+def test_compiled_steps_match_eager_and_the_gpu_alias_resolves_to_cuda():
+    """tests/test_backends.py of the reference: compiled chunks of 8 plus a remainder
+    give the eager result; ``device="gpu"`` is the CUDA device."""
+
+    source = P.GaussianCurrent(peak_current_a=1.0e6)
+    eager = sim(small_config(), source=source)
+    compiled = sim(small_config(), source=source, compile_step=True, compile_chunk_size=8)
+    eager.step(19)
+    compiled.step(19)
+    assert compiled.diagnostics()["compile_chunk_size"] == 8 and compiled.steps == 19
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_allclose(compiled.to_numpy(getattr(compiled, f)), eager.to_numpy(getattr(eager, f)),
+                                   rtol=5.0e-13, atol=5.0e-29)
+    alias = sim(small_config(), device="gpu")
+    assert alias.er.device.type == "cuda" and alias.backend.device.startswith("cuda")
