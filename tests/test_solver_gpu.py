@@ -487,3 +487,54 @@ def test_compiled_steps_match_eager_and_the_gpu_alias_resolves_to_cuda():
                                    rtol=5.0e-13, atol=5.0e-29)
     alias = sim(small_config(), device="gpu")
     assert alias.er.device.type == "cuda" and alias.backend.device.startswith("cuda")
+
+
+def _same_state(a, b):
+    assert a.steps == b.steps and a.time_s == b.time_s
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(a.to_numpy(getattr(a, f)), b.to_numpy(getattr(b, f)))
+
+
+def test_checkpoint_keeps_tangential_source_optimised_mesh_and_precision(tmp_path):
+    """tests/test_checkpoint.py:103-128 of the reference: a float32 run with a
+    tangential source on an optimised mesh restores bitwise, and loads as float64."""
+
+    source = P.TangentialGaussianCurrent(azimuths_deg=(15.0, 90.0), line_lengths_m=(10_000.0, 20_000.0),
+                                         edge_assignment="nearest")
+    s = sim(small_config(radial_cells=4, mesh_optimization_steps=1), source=source, dtype="float32")
+    s.step(3)
+    path = s.save_checkpoint(tmp_path / "tangential.npz")
+    restored = GeodesicFDTD.load_checkpoint(path, device="cuda")
+    assert restored.backend.dtype_name == "float32"
+    _same_state(s, restored)
+    np.testing.assert_array_equal(restored.mesh.vertices, s.mesh.vertices)
+    converted = GeodesicFDTD.load_checkpoint(path, device="cuda", dtype="float64")
+    assert converted.backend.dtype_name == "float64"
+    for f in ("er", "et", "hr", "ht"):
+        np.testing.assert_array_equal(converted.to_numpy(getattr(converted, f)),
+                                      s.to_numpy(getattr(s, f)).astype(np.float64))
+
+
+def test_checkpoint_keeps_custom_topology_and_refinement_metadata(tmp_path):
+    """tests/test_checkpoint.py:131-162 of the reference."""
+
+    import json
+
+    uniform = P.build_geodesic_mesh(1)
+    faces = np.roll(uniform.faces, 7, axis=0)
+    levels = np.where(np.arange(len(faces)) % 2, 2, 1)
+    mesh = P.build_geodesic_mesh_from_topology(uniform.vertices, faces, subdivision=1, face_levels=levels,
+                                               refinement_spec={"balance": "2:1", "regions": [{"level": 2}]})
+    s = sim(small_config(radial_cells=4), mesh=mesh, source=P.GaussianCurrent(peak_current_a=1.0e6))
+    s.step(3)
+    path = s.save_checkpoint(tmp_path / "adaptive.npz")
+    with np.load(path, allow_pickle=False) as archive:
+        assert json.loads(str(archive["metadata"].item()))["version"] == 4
+        np.testing.assert_array_equal(archive["mesh_faces"], faces)
+        np.testing.assert_array_equal(archive["mesh_face_levels"], levels)
+    restored = GeodesicFDTD.load_checkpoint(path, device="cuda")
+    assert restored.mesh.topology_kind == mesh.topology_kind and restored.mesh.refinement_spec == mesh.refinement_spec
+    _same_state(s, restored)
+    s.step(2)
+    restored.step(2)
+    _same_state(s, restored)
