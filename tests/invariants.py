@@ -83,3 +83,18 @@ class UniformPermittivity(Vacuum):
 
 # an abruptly graded radial grid (the reference's nonuniform-stencil cases)
 GRADED_ALTITUDES = (-10_000.0, -6_000.0, -2_000.0, -1_000.0, 0.0, 4_000.0)
+
+
+def extreme_surface_eigenvalues(mesh) -> tuple[float, float]:
+    """The largest |eigenvalue| of the TM (vertex) and TE (face) surface operators."""
+
+    tm = np.column_stack([tm_operator(mesh, e) for e in np.eye(mesh.n_vertices)])
+    te = np.column_stack([te_operator(mesh, e) for e in np.eye(mesh.n_faces)])
+    return -float(np.linalg.eigvals(tm).real.min()), float(np.linalg.eigvals(te).real.max())
+
+
+def courant_numbers(mesh, dt, node_radius_min, mid_radius_min) -> tuple[float, float]:
+    """(c dt / r)^2 x the extreme surface eigenvalues: leapfrog is stable below 4."""
+
+    tm, te = extreme_surface_eigenvalues(mesh)
+    return (C_0 * dt / node_radius_min) ** 2 * tm, (C_0 * dt / mid_radius_min) ** 2 * te

@@ -57,3 +57,26 @@ def test_oracle_te_surface_mode_follows_the_leapfrog_dispersion():
     expected = expected_amplitudes(eigen, sim.dt, sim.midpoints_m[1], 100, -0.5)
     np.testing.assert_allclose(amplitudes, expected, rtol=0.0, atol=8.0e-14)
     assert not np.any(sim.er)
+
+
+def test_surface_laplacian_spectrum_is_rotation_invariant():
+    from invariants import tm_operator
+
+    spectra = []
+    for orientation in ("native", "polar"):
+        mesh = P.build_geodesic_mesh(1, orientation=orientation)
+        matrix = np.column_stack([tm_operator(mesh, e) for e in np.eye(mesh.n_vertices)])
+        spectra.append(np.sort(np.linalg.eigvals(matrix).real))
+    np.testing.assert_allclose(spectra[0], spectra[1], rtol=0.0, atol=2.0e-13)
+
+
+@pytest.mark.parametrize("orientation", ("native", "polar"))
+def test_oracle_time_step_keeps_surface_spectra_inside_the_cfl_limit(orientation):
+    from invariants import courant_numbers
+
+    ora = O.OracleFDTD(material=Vacuum(), dtype=np.float64, orientation=orientation,
+                       **dict(SURFACE_MODE, courant_factor=1.0))
+    mesh = P.build_geodesic_mesh(1, orientation=orientation)  # the oracle's mesh, bit for bit
+    np.testing.assert_array_equal(mesh.vertices, ora.mesh.vertices)
+    tm_q, te_q = courant_numbers(mesh, ora.dt, ora.radii_m.min(), ora.midpoints_m.min())
+    assert 0.0 < tm_q < 4.0 and 0.0 < te_q < 4.0

@@ -538,3 +538,14 @@ def test_checkpoint_keeps_custom_topology_and_refinement_metadata(tmp_path):
     s.step(2)
     restored.step(2)
     _same_state(s, restored)
+
+
+@pytest.mark.parametrize("orientation", ("native", "polar"))
+def test_time_step_keeps_surface_spectra_inside_the_cfl_limit(orientation):
+    """tests/test_maxwell_invariants.py:499-536 of the reference, on the engine's CFL step."""
+
+    from invariants import SURFACE_MODE, Vacuum, courant_numbers
+
+    s = sim(SimulationConfig(**dict(SURFACE_MODE, courant_factor=1.0, mesh_orientation=orientation)), material=Vacuum())
+    tm_q, te_q = courant_numbers(s.mesh, s.time_step_s, float(s.radii_m.min()), float(s.radial_midpoints_m.min()))
+    assert 0.0 < tm_q < 4.0 and 0.0 < te_q < 4.0
