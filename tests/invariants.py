@@ -98,3 +98,30 @@ def courant_numbers(mesh, dt, node_radius_min, mid_radius_min) -> tuple[float, f
 
     tm, te = extreme_surface_eigenvalues(mesh)
     return (C_0 * dt / node_radius_min) ** 2 * tm, (C_0 * dt / mid_radius_min) ** 2 * te
+
+
+def tangential_moment_error(simulation, source, line_length):
+    """Reconstruct the (east, north) line moments from the covariant edge samples
+    of a tangential source and return their error (tests/test_maxwell_invariants.py:165-217)."""
+
+    from ionosphere_fdtd_b200.sources import geographic_tangent_basis
+
+    edges, _, weights = source.edge_distribution(simulation)
+    unique = np.unique(edges)
+    ends = simulation.mesh.vertices[simulation.mesh.edges[unique]]
+    dirs = ends[:, 1] - ends[:, 0]
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    lengths = simulation.mesh.primal_edge_angles[unique] * simulation.config.earth_radius_m
+    samples = np.asarray([weights[edges == e].sum() * ln for e, ln in zip(unique, lengths, strict=True)])
+    east, north = geographic_tangent_basis(source.latitude_deg, source.longitude_deg)
+    moments = np.linalg.pinv(np.column_stack((dirs @ east, dirs @ north))) @ samples
+    return np.abs(moments - line_length).max()
+
+
+def tangential_case():
+    line = 22_500.0
+    from ionosphere_fdtd_b200 import TangentialGaussianCurrent
+
+    source = TangentialGaussianCurrent(latitude_deg=46.5, longitude_deg=-90.9, altitude_m=0.0, azimuths_deg=(0.0, 90.0),
+                                         line_lengths_m=(line, line))
+    return source, line

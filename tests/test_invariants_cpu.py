@@ -10,7 +10,7 @@ import pytest
 
 import ionosphere_fdtd_b200 as P
 import oracle.fdtd as O
-from invariants import SURFACE_MODE, Vacuum, expected_amplitudes, surface_mode
+from invariants import SURFACE_MODE, Vacuum, expected_amplitudes, surface_mode, tangential_case, tangential_moment_error
 
 
 def test_incidence_operators_are_adjoint_pairs():
@@ -80,3 +80,20 @@ def test_oracle_time_step_keeps_surface_spectra_inside_the_cfl_limit(orientation
     np.testing.assert_array_equal(mesh.vertices, ora.mesh.vertices)
     tm_q, te_q = courant_numbers(mesh, ora.dt, ora.radii_m.min(), ora.midpoints_m.min())
     assert 0.0 < tm_q < 4.0 and 0.0 < te_q < 4.0
+
+
+@pytest.mark.parametrize("orientation", ("polar", "native"))
+@pytest.mark.parametrize("subdivision", (1, 3))
+def test_tangential_source_samples_reconstruct_the_requested_moment(subdivision, orientation):
+    """On the package's mesh and source code, with the radial midpoints of a
+    -5 km .. 5 km two-cell grid (the GPU tests repeat it on a simulation)."""
+
+    from types import SimpleNamespace
+
+    source, line = tangential_case()
+    config = P.SimulationConfig(subdivision=subdivision, radial_cells=2, minimum_altitude_m=-5_000.0,
+                                maximum_altitude_m=5_000.0, mesh_orientation=orientation)
+    radii = config.earth_radius_m + np.linspace(-5_000.0, 5_000.0, 3)
+    host = SimpleNamespace(mesh=P.build_geodesic_mesh(subdivision, orientation=orientation), config=config,
+                           radial_midpoint_altitudes_m=0.5 * (radii[:-1] + radii[1:]) - config.earth_radius_m)
+    assert tangential_moment_error(host, source, line) < 2.0e-11

@@ -549,3 +549,16 @@ def test_time_step_keeps_surface_spectra_inside_the_cfl_limit(orientation):
     s = sim(SimulationConfig(**dict(SURFACE_MODE, courant_factor=1.0, mesh_orientation=orientation)), material=Vacuum())
     tm_q, te_q = courant_numbers(s.mesh, s.time_step_s, float(s.radii_m.min()), float(s.radial_midpoints_m.min()))
     assert 0.0 < tm_q < 4.0 and 0.0 < te_q < 4.0
+
+
+@pytest.mark.parametrize("orientation", ("polar", "native"))
+@pytest.mark.parametrize("subdivision", (1, 3))
+def test_tangential_source_samples_reconstruct_the_requested_moment(subdivision, orientation):
+    """tests/test_maxwell_invariants.py:165-217 of the reference, on a simulation."""
+
+    from invariants import tangential_case, tangential_moment_error
+
+    source, line = tangential_case()
+    s = sim(SimulationConfig(subdivision=subdivision, radial_cells=2, minimum_altitude_m=-5_000.0, maximum_altitude_m=5_000.0,
+                             mesh_orientation=orientation), source=source)
+    assert tangential_moment_error(s, source, line) < 2.0e-11
