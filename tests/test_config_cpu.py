@@ -76,3 +76,42 @@ def test_gpu_alias_reports_a_missing_cuda_device():
         pytest.skip("a CUDA device is present; the GPU tests cover the alias")
     with pytest.raises(BackendUnavailableError, match="CUDA"):
         GeodesicFDTD(config=config(), backend="torch", device="gpu")
+
+
+def _host(config):
+    """Mesh and radial midpoints of a configuration: what the source supports read."""
+
+    from types import SimpleNamespace
+
+    from ionosphere_fdtd_b200 import build_geodesic_mesh
+
+    alt = (np.asarray(config.radial_altitudes_m) if config.radial_altitudes_m is not None
+           else np.linspace(config.minimum_altitude_m, config.maximum_altitude_m, config.radial_cells + 1))
+    radii = config.earth_radius_m + alt
+    mids = 0.5 * (radii[:-1] + radii[1:])
+    return SimpleNamespace(mesh=build_geodesic_mesh(config.subdivision), config=config, altitudes_m=alt,
+                           radial_midpoint_altitudes_m=mids - config.earth_radius_m)
+
+
+def test_tangential_source_lines_and_edge_assignment():
+    """tests/test_solver.py of the reference: ground lines must match the azimuths,
+    nearest-edge assignment uses at most one edge per line."""
+
+    with pytest.raises(ValueError, match="line_lengths_m must match"):
+        TangentialGaussianCurrent(azimuths_deg=(0.0, 90.0), line_lengths_m=(22_500.0,))
+    source = TangentialGaussianCurrent(azimuths_deg=(0.0, 90.0), line_lengths_m=(22_500.0, 22_500.0), edge_assignment="nearest")
+    edges, _, weights = source.edge_distribution(_host(config()))
+    assert len(np.unique(edges[weights != 0.0])) <= 2
+
+
+def test_tangential_surface_source_keeps_its_staggered_altitude():
+    source = TangentialGaussianCurrent(altitude_m=0.0, azimuths_deg=(0.0,), line_lengths_m=(22_500.0,))
+    host = _host(config(radial_altitudes_m=(-5_000.0, -3_750.0, -2_500.0, -1_250.0, 0.0, 5_000.0, 10_000.0), radial_cells=6,
+                        minimum_altitude_m=-5_000.0, maximum_altitude_m=10_000.0, radial_grid_policy="allow-abrupt"))
+    edges, layers, weights = source.edge_distribution(host)
+    assert set(host.radial_midpoint_altitudes_m[layers]) == {-625.0, 2_500.0}
+    for edge in np.unique(edges):
+        w = weights[edges == edge]
+        if np.any(w):
+            assert w.sum() != pytest.approx(0.0)
+            assert w @ host.radial_midpoint_altitudes_m[layers[edges == edge]] / w.sum() == pytest.approx(source.altitude_m)
