@@ -31,6 +31,7 @@ from .plasma import (
     MeshPlasmaModel,
 )
 from .provenance import DataArtifactError, DatasetProvenance, VariableProvenance, array_sha256
+from .radial_grid import RadialGridValidation, RadialRefinementRegion, build_refined_radial_grid, validate_radial_grid
 from .receivers import Receiver, ReceiverTraces, receiver_location, record_receiver_traces
 from .solver import GeodesicFDTD, SimulationConfig
 from .sources import (
@@ -88,6 +89,10 @@ __all__ = [
     "geographic_face_index",
     "load_checkpoint",
     "radial_linear_distribution",
+    "RadialGridValidation",
+    "RadialRefinementRegion",
+    "build_refined_radial_grid",
+    "validate_radial_grid",
     "Receiver",
     "ReceiverTraces",
     "receiver_location",

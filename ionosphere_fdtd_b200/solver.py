@@ -28,17 +28,9 @@ from .materials import EarthIonosphereMaterial
 from .mesh import GeodesicMesh, build_geodesic_mesh
 from .plasma import GeodesicPlasmaCoupler, MeshPlasmaModel
 from .provenance import distinct_elements
+from .radial_grid import validate_radial_grid
 from .sources import GaussianCurrent, TangentialGaussianCurrent
 from .surface_impedance import ConductiveHalfSpaceSurface, SurfaceImpedanceADE
-
-
-def _validate_radial_grid(altitudes: NDArray[np.float64], maximum_adjacent_step_ratio: float) -> None:
-    """Adjacent radial steps may differ by at most the given ratio (radial_grid.py:135-165)."""
-
-    steps = np.diff(altitudes)
-    ratio = np.maximum(steps[1:] / steps[:-1], steps[:-1] / steps[1:])
-    if np.any(ratio > maximum_adjacent_step_ratio * (1.0 + 1.0e-12)):
-        raise ValueError("radial grid violates the 2:1 balance between adjacent cells")
 
 
 @dataclass(frozen=True, slots=True)
@@ -121,7 +113,7 @@ class SimulationConfig:
                     "mapping or explicitly select radial_grid_policy='allow-abrupt'"
                 )
             if self.radial_grid_policy == "balanced-2to1":
-                _validate_radial_grid(alt, maximum_adjacent_step_ratio=2.0)
+                validate_radial_grid(alt, maximum_adjacent_step_ratio=2.0)
 
 
 def _validated_material_sample(values, expected_shape, label):

@@ -271,3 +271,14 @@ RECEIVER_TRACES = dict(
         (89.0, -170.0, 95_000.0, "polar"),
     ),
 )
+
+
+# build_refined_radial_grid fixtures (radial_grid.py:44-132): (minimum, maximum,
+# background step, ((region minimum, region maximum, region step), ...))
+RADIAL_GRIDS = (
+    (0.0, 100_000.0, 10_000.0, ((60_000.0, 90_000.0, 1_000.0),)),
+    (0.0, 100_000.0, 10_000.0, ((40_000.0, 80_000.0, 2_000.0), (60_000.0, 70_000.0, 500.0))),
+    (-100_000.0, 100_000.0, 7_000.0, ((-3_000.0, 4_000.0, 150.0), (55_000.0, 99_000.0, 900.0))),
+    (0.0, 90_000.0, 3_333.0, ((0.0, 1_000.0, 37.0),)),
+    (-5_000.0, 5_000.0, 2_500.0, ()),
+)

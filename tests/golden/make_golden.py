@@ -213,8 +213,25 @@ def receiver_traces_fixture(mods) -> None:
     )
 
 
+def radial_grid_fixture() -> None:
+    """The reference's refined radial grids and their validation records."""
+
+    from ionosphere_fdtd.radial_grid import RadialRefinementRegion, build_refined_radial_grid, validate_radial_grid
+
+    out = {}
+    for i, (lo, hi, step, regions) in enumerate(C.RADIAL_GRIDS):
+        nodes = build_refined_radial_grid(lo, hi, step, tuple(RadialRefinementRegion(*r) for r in regions))
+        v = validate_radial_grid(nodes)
+        out[f"nodes_{i}"] = np.asarray(nodes)
+        out[f"validation_{i}"] = np.asarray((v.cells, v.minimum_step_m, v.maximum_step_m, v.maximum_adjacent_step_ratio))
+    np.savez_compressed(HERE / "radial_grids.npz", **out)
+
+
 def main(src: str) -> None:
     mods = _import_reference(src)
+    if "--radial-grids-only" in sys.argv:
+        radial_grid_fixture()
+        return
     if "--checkpoint-only" in sys.argv:
         checkpoint_fixture(mods)
         return
@@ -251,6 +268,7 @@ def main(src: str) -> None:
     )
     np.savez_compressed(HERE / "obs_h_source_s1.npz", hr=hr, ht=ht)
     receiver_traces_fixture(mods)
+    radial_grid_fixture()
     print("done")
 
 

@@ -362,16 +362,22 @@ def test_trapezoidal_loss_keeps_its_coefficients():
     assert np.all(ca < 0.0)
 
 
-@pytest.mark.parametrize("case", ["subvacuum", "graded"])
+@pytest.mark.parametrize("case", ["subvacuum", "graded", "balanced"])
 def test_runs_at_the_material_aware_cfl_limit_stay_bounded(case):
-    """tests/test_maxwell_invariants.py:317-342 and 463-497 of the reference: random
-    fields at the CFL limit stay below twice their initial peak."""
+    """tests/test_maxwell_invariants.py:317-342 and 463-497 and tests/test_radial_grid.py
+    of the reference: random fields at the CFL limit stay below twice their initial
+    peak (sub-vacuum permittivity, an abruptly graded grid, a refined 2:1 grid)."""
 
     from invariants import GRADED_ALTITUDES, UniformPermittivity, Vacuum
 
     if case == "subvacuum":
         s = sim(SimulationConfig(subdivision=0, radial_cells=2, courant_factor=1.0), material=UniformPermittivity(0.01))
         steps = 400
+    elif case == "balanced":
+        a = P.build_refined_radial_grid(0.0, 100_000.0, 10_000.0, (P.RadialRefinementRegion(60_000.0, 90_000.0, 2_000.0),))
+        s = sim(SimulationConfig(subdivision=0, radial_cells=len(a) - 1, minimum_altitude_m=a[0], maximum_altitude_m=a[-1],
+                                 radial_altitudes_m=a, radial_grid_policy="balanced-2to1", courant_factor=1.0))
+        steps = 1000
     else:
         a = GRADED_ALTITUDES
         s = sim(SimulationConfig(subdivision=0, radial_cells=len(a) - 1, minimum_altitude_m=a[0], maximum_altitude_m=a[-1],
