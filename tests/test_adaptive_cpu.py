@@ -72,3 +72,31 @@ def test_refinement_inputs_are_checked_with_the_reference_messages():
         build_adaptive_geodesic_mesh(1, (), relaxations_per_level=0)
     with pytest.raises(ValueError, match="optimization_steps_per_level"):
         build_adaptive_geodesic_mesh(1, (), optimization_steps_per_level=-1)
+
+
+def test_two_labelled_regions_reach_their_levels_with_positive_supports():
+    """tests/test_adaptive_mesh.py:67-96 of the reference."""
+
+
+    regions = (SphericalRefinementRegion(46.5, -90.9, 6.0, 2, 6.0, "source"), SphericalRefinementRegion(69.0, -156.0, 6.0, 2, 6.0, "oil"))
+    mesh = build_adaptive_geodesic_mesh(1, regions)
+    for region in regions:
+        assert mesh.face_levels[int(np.argmax(mesh.face_centers @ region.direction()))] == region.target_subdivision
+    assert [r["label"] for r in mesh.refinement_spec["regions"]] == ["source", "oil"]
+    deep = build_adaptive_geodesic_mesh(1, (SphericalRefinementRegion(46.5, -90.9, 8.0, 3, 8.0, "source"),
+                                            SphericalRefinementRegion(69.0, -156.0, 8.0, 3, 8.0, "oil")))
+    assert validate_adaptive_mesh(deep).minimum_dual_edge_angle > 0.0
+    assert np.all(deep.dual_cell_solid_angles > 0.0) and np.all(deep.edge_diamond_solid_angles() > 0.0)
+    assert np.sum(deep.edge_diamond_solid_angles()) == pytest.approx(4.0 * np.pi)
+
+
+def test_default_relaxation_keeps_transition_dual_edges_open():
+    """tests/test_adaptive_mesh.py:98-113 of the reference."""
+
+
+    mesh = build_adaptive_geodesic_mesh(3, (SphericalRefinementRegion(46.5, -90.9, 3.0, 5, 3.0, "source"),
+                                            SphericalRefinementRegion(69.0, -156.0, 3.0, 5, 3.0, "oil")))
+    assert validate_adaptive_mesh(mesh).minimum_dual_to_primal_ratio > 0.05
+    spec = mesh.refinement_spec
+    assert spec["algorithm"] == "conforming-red-transition-v3"
+    assert spec["relaxations_per_level"] == 4 and spec["optimization_steps_per_level"] == 0
