@@ -115,3 +115,16 @@ def test_tangential_surface_source_keeps_its_staggered_altitude():
         if np.any(w):
             assert w.sum() != pytest.approx(0.0)
             assert w @ host.radial_midpoint_altitudes_m[layers[edges == edge]] / w.sum() == pytest.approx(source.altitude_m)
+
+
+def test_provided_meshes_must_match_the_configuration():
+    """tests/test_solver.py of the reference; the checks run before any device work."""
+
+    from ionosphere_fdtd_b200 import GeodesicFDTD, build_geodesic_mesh
+
+    with pytest.raises(ValueError, match="orientation"):
+        GeodesicFDTD(config=config(), mesh=build_geodesic_mesh(1, orientation="native"))
+    with pytest.raises(ValueError, match="cannot accompany"):
+        GeodesicFDTD(config=config(mesh_optimization_steps=1), mesh=build_geodesic_mesh(1, orientation="polar"))
+    with pytest.raises(ValueError, match="subdivision"):
+        GeodesicFDTD(config=config(subdivision=2), mesh=build_geodesic_mesh(1))
