@@ -97,3 +97,46 @@ def test_tangential_source_samples_reconstruct_the_requested_moment(subdivision,
     host = SimpleNamespace(mesh=P.build_geodesic_mesh(subdivision, orientation=orientation), config=config,
                            radial_midpoint_altitudes_m=0.5 * (radii[:-1] + radii[1:]) - config.earth_radius_m)
     assert tangential_moment_error(host, source, line) < 2.0e-11
+
+
+def _graded_oracle(geometry_mode):
+    from invariants import GRADED_ALTITUDES
+
+    a = GRADED_ALTITUDES
+    return O.OracleFDTD(subdivision=0, radial_cells=len(a) - 1, minimum_altitude_m=a[0], maximum_altitude_m=a[-1],
+                        radial_altitudes_m=a, geometry_mode=geometry_mode, material=Vacuum(), dtype=np.float64)
+
+
+def test_oracle_radial_stencils_are_weighted_adjoints():
+    """tests/test_maxwell_invariants.py:344-430 of the reference on the oracle's radial
+    stencils (the engine's fused rows are pinned to them by the parity tests)."""
+
+    rng = np.random.default_rng(20260805)
+    thin = _graded_oracle("thin-shell")
+    thin.et[:] = rng.standard_normal(thin.et.shape)
+    thin.ht[:] = rng.standard_normal(thin.ht.shape)
+    left = np.sum(thin.ht * thin._d_et() * thin.control_m[None, :])
+    right = np.sum(thin.et * thin._d_ht() * thin.steps_m[None, :])
+    assert left + right == pytest.approx(0.0, abs=2.0e-11)
+    thin.ht[:] = 1.0
+    np.testing.assert_array_equal(thin._d_ht(), 0.0)
+
+    full = _graded_oracle("full-spherical")
+    full.et[:] = rng.standard_normal(full.et.shape)
+    full.ht[:] = rng.standard_normal(full.ht.shape)
+    left = np.sum(full.ht * full._d_et() * (full.control_m * full.radii_m**2)[None, :])
+    right = np.sum(full.et * full._d_ht() * (full.steps_m * full.midpoints_m**2)[None, :])
+    assert abs(left + right) <= 2.0e-15 * max(abs(left), abs(right))
+
+
+def test_oracle_full_spherical_metric_annihilates_inverse_radius_profiles():
+    base = dict(subdivision=0, radial_cells=8, minimum_altitude_m=-100_000.0, maximum_altitude_m=100_000.0,
+                material=Vacuum(), dtype=np.float64)
+    full = O.OracleFDTD(geometry_mode="full-spherical", **base)
+    full.et[:] = 1.0 / full.midpoints_m[None, :]
+    full.ht[:] = 1.0 / full.radii_m[None, :]
+    np.testing.assert_allclose(full._d_et()[:, 1:-1], 0.0, atol=1.0e-27)
+    np.testing.assert_allclose(full._d_ht(), 0.0, atol=1.0e-27)
+    thin = O.OracleFDTD(geometry_mode="thin-shell", **base)
+    thin.et[:] = 1.0 / thin.midpoints_m[None, :]
+    assert np.max(np.abs(thin._d_et()[:, 1:-1])) > 2.0e-14
