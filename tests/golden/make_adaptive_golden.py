@@ -1,8 +1,9 @@
 """Golden adaptive meshes from the reference's own builder.
 
-Run in the build container, where the reference source tree is available:
+Run it where the reference source tree is available, giving the reference's
+``src`` directory as the only argument (required):
 
-    python tests/golden/make_adaptive_golden.py /root/reference/src
+    python tests/golden/make_adaptive_golden.py <reference>/src
 
 It imports the reference package from the given source directory, builds the
 adaptive meshes of ``ADAPTIVE_CASES`` (and one Lawson-flip repair) with the
@@ -63,4 +64,6 @@ def main(src: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "../reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_adaptive_golden.py <reference src directory>")
+    main(sys.argv[1])

@@ -1,8 +1,9 @@
 """Generate golden fixtures by running the reference solver itself.
 
-Run in the build container, where the reference source tree is available:
+Run it where the reference source tree is available, giving the reference's
+``src`` directory as the first argument (required):
 
-    python tests/golden/make_golden.py /root/reference/src
+    python tests/golden/make_golden.py <reference>/src [--mesh-levels=7,8,9]
 
 It imports the reference package from the given source directory, runs every
 case of ``cases.py`` on the reference NumPy float64 backend (plus the float32
@@ -149,13 +150,17 @@ def run_case(name: str, case: dict, mods, dtype: str = "float64") -> dict:
     return out
 
 
-def mesh_fixtures(mods) -> None:
+def mesh_fixtures(mods, levels=range(0, 7)) -> None:
+    """SHA-256 digests of the reference's mesh tables per subdivision level
+    (merged into ``mesh_digests.json``), and full tables up to level 3."""
+
     rmesh = mods[0]
     rnb = mods[7]
-    digests = {}
+    path = HERE / "mesh_digests.json"
+    digests = json.loads(path.read_text()) if path.exists() else {}
     tables = ("edges", "faces", "face_edges", "face_edge_signs", "edge_left_faces", "edge_right_faces", "vertex_degree")
     floats = ("vertices", "face_centers", "primal_edge_angles", "dual_edge_angles", "face_solid_angles", "dual_cell_solid_angles")
-    for level in range(0, 7):
+    for level in levels:
         mesh = rmesh.build_geodesic_mesh(level)
         backend = rnb.NumPyBackend(mesh)
         entry = {t: _sha(np.asarray(getattr(mesh, t), dtype=np.int64)) for t in tables}
@@ -163,12 +168,13 @@ def mesh_fixtures(mods) -> None:
         entry["vertex_edge_signs"] = _sha(np.asarray(backend.vertex_edge_signs, dtype=np.float64))
         entry.update({f: _sha(np.asarray(getattr(mesh, f), dtype=np.float64)) for f in floats})
         digests[str(level)] = entry
+        print("mesh digests", level, flush=True)
         if level <= 3:
             arrays = {t: np.asarray(getattr(mesh, t)) for t in tables + floats}
             arrays["vertex_edges"] = backend.vertex_edges
             arrays["vertex_edge_signs"] = backend.vertex_edge_signs
             np.savez_compressed(HERE / f"mesh_s{level}.npz", **arrays)
-    (HERE / "mesh_digests.json").write_text(json.dumps(digests, indent=1, sort_keys=True) + "\n")
+        path.write_text(json.dumps(digests, indent=1, sort_keys=True) + "\n")
 
 
 def checkpoint_fixture(mods) -> None:
@@ -238,6 +244,11 @@ def main(src: str) -> None:
     if "--receivers-only" in sys.argv:
         receiver_traces_fixture(mods)
         return
+    levels = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--mesh-levels=")]
+    if levels:
+        # the large levels only (s9 takes the reference's builder minutes): --mesh-levels=7,8,9
+        mesh_fixtures(mods, [int(v) for v in levels[0].split(",")])
+        return
     only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--cases=")]
     if only:
         # regenerate the named cases only: --cases=name1,name2
@@ -274,4 +285,6 @@ def main(src: str) -> None:
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    main(args[0] if args else "/root/reference/src")
+    if not args:
+        sys.exit("usage: make_golden.py <reference src directory> [--cases=a,b | --mesh-levels=7,8,9 | ...]")
+    main(args[0])

@@ -29,7 +29,9 @@ def test_mesh_tables_are_bit_exact_with_reference(level):
         np.testing.assert_array_equal(getattr(mesh, name), ref[name], err_msg=name)
 
 
-@pytest.mark.parametrize("level", [4, 5, 6])
+# levels 7-9 are the benchmark meshes (s7: 163,842 vertices; s9: 2,621,442),
+# whose digests the reference's own builder produced
+@pytest.mark.parametrize("level", [4, 5, 6, 7, 8, 9])
 def test_mesh_digests_match_reference(level):
     digests = json.loads((GOLDEN / "mesh_digests.json").read_text())[str(level)]
     mesh = P.build_geodesic_mesh(level)
