@@ -1,16 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the B200 geodesic FDTD time step (prints one JSON line).
 
-Workload (default ``config2``): icosahedral subdivision 7 (163,842 dual
-cells) x 40 radial cells, FP32 fields, exponential conductive integrator,
-Drude electron plasma ADE, one 50 Hz Gaussian source and 64 barycentric
-receivers; seeded synthetic inputs, random 1e-6 initial fields.  One bench
-"step" is ``--time-steps`` leapfrog steps (default 1000) of that simulation,
-launched as CUDA-graph chunks on one GPU.  ``value`` is whole-job
-Gcell-updates/s (cells = vertices x radial cells) with the state resident in
-HBM; ``e2e`` is the same metric through the public API
-(``GeodesicFDTD.record_er_observations``) with host-computed source currents
-copied in and receiver traces copied out every bench step.
+Workload (default ``config4``): icosahedral subdivision 9 (2,621,442 dual
+cells) x 80 radial cells over 0-100 km (209.7 M cells), FP32 fields,
+exponential conductive integrator, surface-impedance lower boundary over a
+seeded smooth log-normal ground-conductivity map, Drude electron plasma ADE,
+one 20 Hz Gaussian source and 256 barycentric receivers; seeded synthetic
+inputs, random 1e-6 initial fields.  One bench "step" is ``--time-steps``
+leapfrog steps (default 100) of that simulation, launched as CUDA-graph chunks
+on one GPU, each leapfrog step sampling the 256 receivers into a
+device-resident float64 trace buffer (``ifdtd_step_sampled``).  ``value`` is
+whole-job Gcell-updates/s (cells = vertices x radial cells) with the state and
+the step currents resident in HBM; ``e2e`` is the same metric through the
+public API (``GeodesicFDTD.record_er_observations``) with host-computed source
+currents copied in and receiver traces copied out every bench step.
+``--workload config2`` runs the s7 / 40-cell plasma workload (64 receivers,
+1000 leapfrog steps per bench step) the same way.
 
 ``--workload config3`` measures ensemble runs/s instead: 64 seeded members
 of uneven size (s5-s7, 24-60 radial cells, exponential ionospheres, 16
@@ -19,14 +24,17 @@ receivers each), each run being 5000 leapfrog steps; ``value`` is the batched
 stepped one after another, both with the receivers sampled on the device.
 
 ``--impl reference`` times the CPU oracle (a NumPy restatement of the
-reference's own NumPy path, the reference being pure Python) on a bounded
-sample of the same workload.  Under torchrun every rank runs an independent
-replica (the plain solver does not shard), timing is the max over ranks.
+reference's own solver, the reference being pure Python, run on PyTorch CPU
+tensors over every host thread) on a bounded sample of the same workload,
+built with the oracle's own mesh builder and inputs (nothing of the CUDA
+product is loaded).  Under torchrun every rank runs an independent replica
+(the plain solver does not shard), timing is the max over ranks.
 """
 
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -51,7 +59,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("engine", "reference"), default="engine")
-    p.add_argument("--workload", choices=("config2", "config3", "config4", "config5"), default="config2")
+    p.add_argument("--workload", choices=("config2", "config3", "config4", "config5"), default="config4")
     p.add_argument("--runs", type=int, default=256, help="config5: training runs generated by the engine")
     p.add_argument("--eval-runs", type=int, default=32, help="config5: held-out runs (16 receivers each)")
     p.add_argument("--iterations", type=int, default=3000, help="config5: training iterations per network")
@@ -263,39 +271,52 @@ def host_threads() -> int:
     return max(1, n)
 
 
+# The plain-solver workloads: mesh level, radial cells, receivers, leapfrog steps per bench step.
+PLAIN = {
+    "config2": {"subdivision": 7, "radial_cells": 40, "receivers": 64, "time_steps": 1000, "surface_impedance": False},
+    "config4": {"subdivision": 9, "radial_cells": 80, "receivers": 256, "time_steps": 100, "surface_impedance": True},
+}
+
+
+def workload_config(workload: str, subdivision: int | None, world: int) -> dict:
+    """The ``config`` object of the JSON line, the same in both arms: the workload's
+    static description (no timings or tuning results)."""
+
+    spec = PLAIN[workload]
+    sub = spec["subdivision"] if subdivision is None else subdivision
+    L = spec["radial_cells"]
+    V, E, F = 10 * 4**sub + 2, 30 * 4**sub, 20 * 4**sub
+    state = 4 * (V * (L + 1) + E * (L + 1) + E * L + F * L + 3 * F * L + (16 * E if spec["surface_impedance"] else 0))
+    return {
+        "workload": workload,
+        "subdivision": sub,
+        "radial_cells": L,
+        "cells": V * L,
+        "plasma": "drude (1 species)",
+        "surface_impedance": spec["surface_impedance"],
+        "receivers": spec["receivers"],
+        "precision": "float32 fields, float64 receiver accumulation",
+        "l2": f"state {state / 1e6:.0f} MB > 126 MB L2, no flush needed",
+        "parallelism": f"replicas x{world}",
+    }
+
+
 def oracle_build(workload: str, sub: int | None = None):
-    """The CPU oracle on the workload's radial column, plasma and surface (float32), fields
-    seeded as the engine's; ``sub`` overrides the mesh level (the sample level by default)."""
+    """The CPU oracle on the workload's radial column, plasma and surface (float32), built
+    from the oracle's own mesh builder and inputs, fields seeded; ``sub`` overrides the mesh
+    level (the sample level by default)."""
 
-    import oracle.fdtd as O
-    from ionosphere_fdtd_b200 import workloads as W
-    from ionosphere_fdtd_b200.mesh import build_geodesic_mesh
+    import oracle.workloads as OW
 
-    L = 80 if workload == "config4" else 40
+    spec = PLAIN[workload]
+    L = spec["radial_cells"]
     sub = ORACLE_SAMPLE_SUB[workload] if sub is None else sub
-    lo = 0.0 if workload == "config4" else -100_000.0
-    mesh = build_geodesic_mesh(sub)
-    alt = np.linspace(lo, 100_000.0, L + 1)
-    mids = 0.5 * (alt[:-1] + alt[1:])
-    shape = (mesh.n_faces, L)
-    plasma = O.OraclePlasma(
-        np.zeros((*shape, 3)),
-        [O.OracleSpecies(-1.602_176_634e-19, 9.109_383_713_9e-31,
-                         np.broadcast_to(1.0e6 * np.exp((mids - 85_000.0) / 3_000.0), shape),
-                         np.broadcast_to(1.0e7 * np.exp(-(mids - 70_000.0) / 6_000.0), shape))],
-    )
-    surface = O.OracleSurface(W.smooth_log_normal(mesh.edge_midpoints(), 20260814)) if workload == "config4" else None
-    sim = O.OracleFDTD(
-        subdivision=sub, radial_cells=L, minimum_altitude_m=lo, material=W.ProfileMaterial(), plasma=plasma,
-        surface=surface, mesh=mesh, dtype=np.float32,
-        source=O.OracleSource(peak_current_a=1.0, carrier_frequency_hz=50.0 if workload == "config2" else 20.0),
-    )
-    rng = np.random.default_rng(20260814)
-    for f in ("er", "et", "hr", "ht"):
-        getattr(sim, f)[:] = (1.0e-6 * rng.standard_normal(getattr(sim, f).shape)).astype(np.float32)
-    full = 9 if workload == "config4" else 7
+    builder = OW.config4 if workload == "config4" else OW.config2
+    sim = builder(subdivision=sub, radial_cells=L, dtype=np.float32)
+    OW.seed_fields(sim)
+    full = spec["subdivision"]
     note = "" if sub == full else f" (the s{full} workload's column, plasma and surface on an s{sub} mesh)"
-    return sim, {"cells": mesh.n_vertices * L, "sub": sub, "L": L, "note": note}
+    return sim, {"cells": sim.mesh.n_vertices * L, "sub": sub, "L": L, "note": note}
 
 
 def oracle_stepper(sim):
@@ -342,8 +363,6 @@ def oracle_ensemble_rate(steps: int = 1) -> dict:
 
 
 def ensemble_reference_arm(args) -> None:
-    from ionosphere_fdtd_b200 import workloads as W
-
     cells = ensemble_cells(args.members)
     mean_cells = statistics.mean(cells)
     rates, secs = [], 0.0
@@ -369,11 +388,12 @@ def ensemble_reference_arm(args) -> None:
 
 
 def ensemble_cells(members: int) -> list[int]:
-    """Cells (vertices x radial cells) of the config3 members."""
+    """Cells (vertices x radial cells) of the config3 members (the oracle's restatement
+    of the seeded draws, so the reference arm loads nothing of the product)."""
 
-    from ionosphere_fdtd_b200 import workloads as W
+    import oracle.workloads as OW
 
-    return [(10 * 4 ** d["subdivision"] + 2) * d["radial_cells"] for d in W.config3_draws(members=members)]
+    return [(10 * 4 ** d["subdivision"] + 2) * d["radial_cells"] for d in OW.config3_draws(members=members)]
 
 
 def ensemble_main(args, world: int, rank: int, local: int) -> None:
@@ -664,7 +684,7 @@ def reference_arm(args, world: int, rank: int) -> None:
         ensemble_reference_arm(args)
         return
     per_step = 1
-    sim, info = oracle_build(args.workload)
+    sim, info = oracle_build(args.workload, None if args.subdivision is None else min(args.subdivision, ORACLE_SAMPLE_SUB[args.workload]))
     stepper = oracle_stepper(sim)
     for _ in range(args.warmup):
         oracle_time(stepper, info, per_step)
@@ -675,7 +695,8 @@ def reference_arm(args, world: int, rank: int) -> None:
         secs += r["seconds"]
     value = statistics.median(rates)
     sample = (f"{per_step} leapfrog step(s) of s{r['sub']}/L{r['L']} float32 per bench step{r['note']}, the oracle's "
-              f"step on PyTorch CPU tensors over {r['cores']} threads (the reference's Torch-on-CPU path)")
+              f"step on PyTorch CPU tensors over {r['cores']} threads (the reference's Torch-on-CPU path); "
+              f"Gcell/s = sample cells / step time")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -690,7 +711,9 @@ def reference_arm(args, world: int, rank: int) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": args.workload, "cells": r["cells"], "time_steps_per_step": per_step, "device": "cpu"},
+        "config": workload_config(args.workload, args.subdivision, world),
+        "time_steps_per_step": per_step,
+        "device": "cpu",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -734,6 +757,8 @@ def main() -> None:
         return
     import torch
 
+    from ionosphere_fdtd_b200 import _native as N
+
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -748,53 +773,78 @@ def main() -> None:
     setup_s = time.perf_counter() - t_setup
     sim = wl.simulation
     tuning = None if args.no_autotune else tune_launch_geometry(sim)
-    T = args.time_steps or (1000 if args.workload == "config2" else 100)
+    T = args.time_steps or PLAIN[args.workload]["time_steps"]
+    K = args.steps
     stream = torch.cuda.current_stream()
+    eng = sim._engine
+    lib = N.load()
 
-    for _ in range(max(args.warmup, 3)):
-        sim.step(T)
+    # receivers sampled every leapfrog step into device-resident float64 traces
+    v, k, w = wl.receivers
+    probe = eng.probe("er", v, np.broadcast_to(k[:, None], v.shape), w)
+    traces = torch.zeros((T, v.shape[0]), dtype=torch.float64, device=device)
+
+    def device_currents(first_step: int):
+        """The source currents I((n + 1/2) dt) of T steps from ``first_step``, on the device."""
+        dt = sim.time_step_s
+        times = (first_step + np.arange(T, dtype=np.float64) + 0.5) * dt
+        series = getattr(sim.source, "current_series", None)
+        host = (np.asarray(series(times, dt), dtype=np.float64) if series is not None
+                else np.fromiter((sim.source.current_a(float(t), dt) for t in times), dtype=np.float64, count=T))
+        return torch.tensor(host, dtype=torch.float64, device=device)
+
+    def bench_step(cur) -> None:
+        N.check(lib.ifdtd_step_sampled(eng.plan, ctypes.byref(sim._state()), cur.data_ptr(), T, probe.handle,
+                                       traces.data_ptr(), eng.backend.stream_handle()), "ifdtd_step_sampled")
+        sim.steps += T
+        sim.time_s = sim.steps * sim.time_step_s
+
+    W_ = max(args.warmup, 3)
+    warm = [device_currents(sim.steps + i * T) for i in range(W_)]
+    for cur in warm:
+        bench_step(cur)
+    # every timed bench step's currents are uploaded before the timed region
+    timed_cur = [device_currents(sim.steps + i * T) for i in range(K)]
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     uuid = getattr(torch.cuda.get_device_properties(local), "uuid", None)
     sampler = ClockSampler(f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else (str(uuid) if uuid else None))
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
-    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
     torch.cuda.synchronize()
-    start.record(stream)
     marks[0].record(stream)
-    for i in range(args.steps):
-        sim.step(T)
+    for i in range(K):
+        bench_step(timed_cur[i])
         marks[i + 1].record(stream)
-    stop.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    elapsed_ms = start.elapsed_time(stop)
-    per_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps)]
+    elapsed_ms = marks[0].elapsed_time(marks[K])
+    per_step_ms = [marks[i].elapsed_time(marks[i + 1]) for i in range(K)]
     if dist:
         elapsed_ms = max_over_ranks(elapsed_ms, dist, device)
         dist.barrier()
-    total_cells = wl.cells * T * args.steps * world
+    total_cells = wl.cells * T * K * world
     value = total_cells / (elapsed_ms / 1e3) / 1e9
+    trace_finite = bool(torch.isfinite(traces).all())
+    probe.close()
 
     # end to end through the public API: host currents in, receiver traces out
     e2e = None
     if not args.no_e2e:
-        v, k, w = wl.receivers
         torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            traces = sim.record_er_observations(v, k, w, T)
-        t1 = time.perf_counter()
-        wall = t1 - t0
+        for _ in range(K):
+            out = sim.record_er_observations(v, k, w, T)
+        wall = time.perf_counter() - t0
         if dist:
             wall = max_over_ranks(wall, dist, device)
         e2e = {
-            "value": wl.cells * T * args.steps * world / wall / 1e9,
+            "value": wl.cells * T * K * world / wall / 1e9,
             "unit": UNIT,
             "h2d_bytes_per_step": 8 * T,
-            "d2h_bytes_per_step": int(traces.nbytes),
+            "d2h_bytes_per_step": int(out.nbytes),
             "api": "GeodesicFDTD.record_er_observations",
         }
 
@@ -804,7 +854,7 @@ def main() -> None:
     # per-kernel roofline: each phase kernel timed alone after the timed region
     phase_ms = phase_times_ms(sim, 50, stream)
     nbytes = kernel_bytes(sim)
-    modes = sim._engine.kernel_modes
+    modes = eng.kernel_modes
     names = {"h_phase": "kh_tma" if modes[0] == "pipeline" else "kh_kernel", "e_phase": "ke_tma" if modes[1] == "pipeline" else "ke_kernel"}
     traffic = traffic_from_profile(args.workload) if args.subdivision is None else {}
     kernels = {
@@ -818,7 +868,7 @@ def main() -> None:
         }
         for phase in ("h_phase", "e_phase")
     }
-    top = max(kernels, key=lambda k: kernels[k]["launch_ms"])
+    top = max(kernels, key=lambda q: kernels[q]["launch_ms"])
     roofline = {
         "bound": "hbm",
         "kernel": f"{kernels[top]['kernel']} ({top.replace('_', ' ')}, dominant)",
@@ -830,25 +880,13 @@ def main() -> None:
         "traffic": kernels[top]["traffic"],
         "algorithmic_bytes_per_launch": kernels[top]["algorithmic_bytes_per_launch"],
         "kernels": kernels,
-        "step": {"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": wl.bytes_per_step, "ms": step_ms},
+        "step": {"achieved": achieved, "frac": achieved / peak, "algorithmic_bytes_per_step": wl.bytes_per_step, "ms": step_ms,
+                 "note": "timed region: both phase kernels and the receiver sampling of every leapfrog step"},
     }
-    config = {
-        "workload": args.workload,
-        "subdivision": sim.config.subdivision,
-        "radial_cells": sim.config.radial_cells,
-        "cells": wl.cells,
-        "time_steps_per_step": T,
-        "plasma": "drude (1 species)",
-        "surface_impedance": sim._surface_impedance_ade is not None,
-        "receivers": int(wl.receivers[0].shape[0]),
-        "l2": f"state {wl.bytes_per_step // 2 / 1e6:.0f} MB > 126 MB L2, no flush needed",
-        "parallelism": f"replicas x{world}",
-        "setup_s": setup_s,
-        "autotune": tuning,
-    }
+    config = workload_config(args.workload, args.subdivision, world)
     drift = None
     if rank == 0 and world == 1 and not args.no_drift:
-        del wl, sim
+        del wl, sim, eng
         torch.cuda.empty_cache()
         drift = fp32_drift(args.workload, device, T, args.subdivision)
     cpu = None
@@ -868,22 +906,26 @@ def main() -> None:
             "value": value,
             "unit": UNIT,
             "n_gpus": world,
-            "steps": args.steps,
+            "steps": K,
             "warmup": args.warmup,
-            "ms_per_step": elapsed_ms / args.steps,
+            "ms_per_step": elapsed_ms / K,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
             "config": config,
+            "time_steps_per_step": T,
+            "setup_s": setup_s,
+            "autotune": tuning,
             "hbm_gbs": achieved,
             "kernel_modes": list(modes),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp32_drift": drift,
-            "gpu_launches": 2 * T * args.steps,
+            "traces_finite": trace_finite,
+            "gpu_launches": 3 * T * K,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

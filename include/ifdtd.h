@@ -164,16 +164,24 @@ int32_t ifdtd_step(ifdtd_plan* plan, const ifdtd_state* state, const double* cur
 
 /* Same as ifdtd_step, but allocates no device memory in any call.  It has no
  * counterpart in the reference.  It is for callers that may not call
- * cudaMalloc while they run: code between the reservations of a custom memory
- * pool, host callbacks, or processes whose device memory budget is fixed after
- * start-up.  The scratch that a step with more than one plasma species needs
- * (the summed current, F x 3 x mid_pitch reals) lives in a 16 MiB static device
- * array that every GPU loading this library holds until exit; larger meshes
- * are rejected with IFDTD_ERR_UNSUPPORTED.  currents may be NULL (zero
+ * cudaMalloc while they run: a process that hands all free device memory to
+ * its own pool at start-up (cudaMalloc would fail there), or a latency-bound
+ * loop that cannot afford the device-wide synchronisation cudaMalloc and
+ * cudaFree may perform.  Do not call it from a CUDA stream callback (host
+ * functions enqueued on a stream may make no CUDA calls).  The scratch that
+ * a step with more than one plasma species needs (the summed current,
+ * F x 3 x mid_pitch reals) lives in a 16 MiB static device array that every
+ * GPU loading this library holds until exit; larger meshes are rejected with
+ * IFDTD_ERR_UNSUPPORTED before any device work.  currents may be NULL (zero
  * source).  The first call on a device looks up the static arrays' device
- * addresses, so make it before any stream capture.  All calls share the
- * static arrays: calls that overlap on the GPU (other streams, other plans)
- * race and must be serialised by the caller. */
+ * addresses, so make it before any stream capture.  A call whose launch
+ * record differs from the one last uploaded on that device (another plan,
+ * other state or currents pointers) copies the record from host memory.  All
+ * calls share the static arrays, which keep the last call's contents: calls
+ * that overlap on the GPU (other streams, other plans) race and must be
+ * serialised by the caller.  The first lookup and the record comparison are
+ * guarded per device, so calls from several host threads leave that host
+ * state intact; the race on the GPU above still applies to them. */
 int32_t ifdtd_step_static_scratch(ifdtd_plan* plan, const ifdtd_state* state, const double* currents,
                                   int32_t n_steps, void* stream);
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -2058,9 +2059,10 @@ int32_t ifdtd_dual_cell_circulation(ifdtd_plan* plan, const void* in, int32_t co
 // ---------------------------------------------------------------------------
 // Allocation-free stepping (no counterpart in the reference).
 //
-// Callers that must not allocate device memory while they run (code that runs
-// between a custom allocator's pool reservations, inside host callbacks, or
-// in processes whose memory budget is fixed after start-up) use
+// Some callers may not allocate device memory while they run: a process that
+// hands all free device memory to its own pool at start-up (cudaMalloc would
+// then fail), or a latency-bound loop that cannot afford the device-wide
+// synchronisation that cudaMalloc and cudaFree may perform.  They use
 // ifdtd_step_static_scratch.  A multi-species plasma step needs one scratch
 // buffer, the summed species current (F x 3 x mid_pitch reals) that the H
 // kernel writes and the E kernel reads; the plan allocates it with cudaMalloc.
@@ -2081,33 +2083,36 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 static __device__ __align__(256) unsigned char g_static_record[sizeof(Rec<double>)];
 static __device__ __align__(256) double g_static_zero_current[1];
 
-struct StaticAddresses {
+// Per device: the arrays' device addresses and a host copy of the record last
+// uploaded to g_static_record (uploaded = false until the first upload).  The
+// mutex makes the first lookup and the record comparison safe when several
+// host threads call on the same device.
+struct StaticDevice {
+  std::mutex lock;
   bool ready = false;
   void* scratch = nullptr;
   void* record = nullptr;
   void* zero_current = nullptr;
+  bool uploaded = false;
+  unsigned char last_record[sizeof(Rec<double>)];
 };
-StaticAddresses g_static_addresses[kStaticMaxDevices];
+StaticDevice g_static_devices[kStaticMaxDevices];
 
 // Device addresses of the static arrays on `device` (which must be current);
-// looked up on the first call for that device.
-int static_addresses(int device, StaticAddresses** out) {
-  if (device < 0 || device >= kStaticMaxDevices) return fail(IFDTD_ERR_UNSUPPORTED, "device ordinal too large");
-  StaticAddresses& a = g_static_addresses[device];
-  if (!a.ready) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString(e));
-    a.scratch = p;
-    e = cudaGetSymbolAddress(&p, g_static_record);
-    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static record address: ") + cudaGetErrorString(e));
-    a.record = p;
-    e = cudaGetSymbolAddress(&p, g_static_zero_current);
-    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static current address: ") + cudaGetErrorString(e));
-    a.zero_current = p;
-    a.ready = true;
-  }
-  *out = &a;
+// looked up on the first call for that device.  The caller holds a.lock.
+int static_addresses(StaticDevice& a) {
+  if (a.ready) return IFDTD_OK;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString(e));
+  a.scratch = p;
+  e = cudaGetSymbolAddress(&p, g_static_record);
+  if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static record address: ") + cudaGetErrorString(e));
+  a.record = p;
+  e = cudaGetSymbolAddress(&p, g_static_zero_current);
+  if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static current address: ") + cudaGetErrorString(e));
+  a.zero_current = p;
+  a.ready = true;
   return IFDTD_OK;
 }
 
@@ -2118,23 +2123,33 @@ int step_static(ifdtd_plan* P, const ifdtd_state* st, const double* currents, in
     return fail(IFDTD_ERR_UNSUPPORTED, "ifdtd_step_static_scratch: the summed plasma current needs " +
                                            std::to_string(need) + " bytes, above the " +
                                            std::to_string(kStaticScratchBytes) + "-byte static scratch");
+  if (P->device < 0 || P->device >= kStaticMaxDevices) return fail(IFDTD_ERR_UNSUPPORTED, "device ordinal too large");
   int rc = bind_state<real>(P, st, stream);
   if (rc) return rc;
   if (n <= 0) return IFDTD_OK;
-  StaticAddresses* A = nullptr;
-  rc = static_addresses(P->device, &A);
+  StaticDevice& A = g_static_devices[P->device];
+  std::lock_guard<std::mutex> hold(A.lock);
+  rc = static_addresses(A);
   if (rc) return rc;
+  // the plan's record with the summed current and the source row pointed at
+  // the static arrays; the bytes not covered by Rec<real> stay zero
+  unsigned char bytes[sizeof(Rec<double>)] = {};
   Rec<real> rec;
   std::memcpy(&rec, P->h_rec.data(), sizeof(rec));
-  rec.Jtot = P->S > 1 ? static_cast<real*>(A->scratch) : nullptr;
-  rec.cur = currents ? currents : static_cast<const double*>(A->zero_current);
+  rec.Jtot = P->S > 1 ? static_cast<real*>(A.scratch) : nullptr;
+  rec.cur = currents ? currents : static_cast<const double*>(A.zero_current);
+  std::memcpy(bytes, &rec, sizeof(rec));
   // the summed current is fully rewritten each step; clearing it keeps a call
   // independent of what the previous call left behind
-  if (need) CUDA_TRY(cudaMemsetAsync(A->scratch, 0, need, stream));
-  if (!currents) CUDA_TRY(cudaMemsetAsync(A->zero_current, 0, sizeof(double), stream));
-  // pageable source: copied to staging before the call returns
-  CUDA_TRY(cudaMemcpyAsync(A->record, &rec, sizeof(rec), cudaMemcpyHostToDevice, stream));
-  const Rec<real>* drec = static_cast<const Rec<real>*>(A->record);
+  if (need) CUDA_TRY(cudaMemsetAsync(A.scratch, 0, need, stream));
+  if (!currents) CUDA_TRY(cudaMemsetAsync(A.zero_current, 0, sizeof(double), stream));
+  if (!A.uploaded || std::memcmp(A.last_record, bytes, sizeof(bytes)) != 0) {
+    // pageable source: copied to staging before the call returns
+    CUDA_TRY(cudaMemcpyAsync(A.record, bytes, sizeof(bytes), cudaMemcpyHostToDevice, stream));
+    std::memcpy(A.last_record, bytes, sizeof(bytes));
+    A.uploaded = true;
+  }
+  const Rec<real>* drec = static_cast<const Rec<real>*>(A.record);
   for (int i = 0; i < n; ++i) {
     cudaError_t e = P->plasma ? launch_kh_t<real, true>(P, drec, stream) : launch_kh_t<real, false>(P, drec, stream);
     if (e == cudaSuccess) {

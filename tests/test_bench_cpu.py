@@ -153,3 +153,33 @@ def test_profile_traffic_and_clock_records_parse():
     rec = sampler.stop()
     assert rec == {"sm_mhz": 1815.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
     assert not sampler.path.exists()
+
+
+def test_reference_arm_loads_nothing_of_the_product():
+    """The reference arm times the oracle on its own mesh and inputs: the product
+    package is never imported and its CUDA library never mapped, and its config
+    object is the engine arm's."""
+
+    import json
+    import subprocess
+
+    code = r"""
+import json, sys
+sys.path.insert(0, sys.argv[1])
+import bench
+
+class Args:
+    workload, steps, warmup, gpus, subdivision = "config4", 1, 0, 1, 2
+
+bench.reference_arm(Args, world=1, rank=0)
+maps = open("/proc/self/maps").read()
+print(json.dumps({"imported": any(m.startswith("ionosphere_fdtd_b200") for m in sys.modules),
+                  "mapped": "libifdtd" in maps,
+                  "config": bench.workload_config("config4", 2, 1)}))
+"""
+    out = subprocess.run([sys.executable, "-c", code, str(ROOT)], capture_output=True, text=True, timeout=600, check=True)
+    lines = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    line, probe = lines[0], lines[1]
+    assert line["impl"] == "reference" and line["value"] > 0.0
+    assert line["config"] == probe["config"]
+    assert not probe["imported"] and not probe["mapped"]
