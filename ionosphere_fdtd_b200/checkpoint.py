@@ -1,20 +1,30 @@
-"""Portable, versioned NPZ checkpoints in the reference's layout.
+"""Portable, versioned NPZ checkpoints in the reference's file layout.
 
-Same keys, dtypes, JSON metadata and validation as the reference
-(checkpoint.py:23-477): format ``ionosphere-fdtd-checkpoint`` version 4,
-readable back to version 1.  Files written here load in the reference and
-vice versa.  Field arrays are copied device-to-host once per field.
+The file is the reference's (``checkpoint.py:23-477``): format
+``ionosphere-fdtd-checkpoint`` version 4, readable back to version 1, the same
+archive keys, dtypes, JSON metadata schema and error messages, so files
+written here load in the reference and vice versa.
+
+The code is organised around one declarative table, ``ARCHIVE``: every array
+of the archive is an ``Entry`` naming its key, the first format version that
+carries it, where its value comes from when writing, and, for the state
+arrays, how it is checked and restored when reading.  ``save_checkpoint``
+walks the table once to gather arrays (device arrays reach the host through
+pinned buffers with a single synchronisation); ``load_checkpoint`` walks it
+to find the keys a file of its version must hold, to read them, and, after
+the model is rebuilt from the metadata, to validate and restore the state.
 """
 
 from __future__ import annotations
 
+import contextlib
 import json
 import os
 import tempfile
 import zipfile
-from dataclasses import asdict, replace
+from dataclasses import asdict, dataclass, replace
 from pathlib import Path
-from typing import Any
+from typing import Any, Iterator
 
 import numpy as np
 
@@ -29,71 +39,308 @@ CHECKPOINT_FORMAT = "ionosphere-fdtd-checkpoint"
 CHECKPOINT_VERSION = 4
 SUPPORTED_CHECKPOINT_VERSIONS = (1, 2, 3, CHECKPOINT_VERSION)
 
+# Metadata sections and the first format version that requires each.
+METADATA_SECTIONS = {
+    "simulation_config": 1, "material": 1, "source": 1, "state": 1, "runtime": 1,
+    "mesh": 2, "surface_impedance": 3, "plasma": 4,
+}
 
-def _device_arrays_to_host(tensors: dict[str, Any]) -> dict[str, np.ndarray]:
-    """Copy device tensors into pinned host buffers with asynchronous copies on
-    the current stream and one synchronisation (instead of a blocking copy per
-    array)."""
+SOURCE_TYPES = {"GaussianCurrent": GaussianCurrent, "TangentialGaussianCurrent": TangentialGaussianCurrent}
+
+
+# ---------------------------------------------------------------------------
+# The archive table
+# ---------------------------------------------------------------------------
+
+
+@dataclass(frozen=True)
+class Entry:
+    """One array of the archive.
+
+    ``key``: archive key; entries of one per plasma species or model array
+    carry ``{}`` and are expanded by ``keys_for``.  ``since``: first format
+    version that carries it.  ``group``: how it is produced and consumed
+    (``mesh``, ``field``, ``surface``, ``plasma_model``, ``plasma_current``).
+    ``what``: its name in validation messages."""
+
+    key: str
+    since: int
+    group: str
+    what: str = ""
+
+
+ARCHIVE: tuple[Entry, ...] = (
+    Entry("metadata", 1, "metadata"),
+    Entry("mesh_vertices", 1, "mesh"),
+    Entry("mesh_faces", 2, "mesh"),
+    Entry("mesh_face_levels", 2, "mesh"),
+    Entry("er", 1, "field", "er"),
+    Entry("et", 1, "field", "et"),
+    Entry("hr", 1, "field", "hr"),
+    Entry("ht", 1, "field", "ht"),
+    Entry("surface_impedance_memory", 3, "surface", "surface impedance state"),
+    Entry("plasma_model_{}", 4, "plasma_model"),
+    Entry("plasma_current_{}", 4, "plasma_current", "plasma current {}"),
+)
+
+
+def keys_for(entry: Entry, plasma_meta: dict | None) -> list[str]:
+    """The archive keys of one table entry for a file with this plasma metadata."""
+
+    if entry.group == "plasma_model":
+        return [entry.key.format(n) for n in plasma_meta["arrays"]] if plasma_meta else []
+    if entry.group == "plasma_current":
+        return [entry.key.format(i) for i in range(len(plasma_meta["species"]))] if plasma_meta else []
+    return [entry.key]
+
+
+def required_keys(version: int, plasma_meta: dict | None) -> set[str]:
+    """Every archive key a file of ``version`` must hold."""
+
+    return {k for e in ARCHIVE if version >= e.since for k in keys_for(e, plasma_meta)}
+
+
+# ---------------------------------------------------------------------------
+# Writing
+# ---------------------------------------------------------------------------
+
+
+def _to_host(tensors: dict[str, Any]) -> dict[str, np.ndarray]:
+    """Device tensors to pinned host arrays: asynchronous copies on the current
+    stream, then one synchronisation."""
 
     import torch
 
-    hosts = {}
-    for name, t in tensors.items():
-        host = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
-        host.copy_(t, non_blocking=True)
-        hosts[name] = host
+    pinned = {}
+    for key, t in tensors.items():
+        pinned[key] = torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+        pinned[key].copy_(t, non_blocking=True)
     torch.cuda.current_stream().synchronize()
-    return {name: h.numpy() for name, h in hosts.items()}
+    return {key: p.numpy() for key, p in pinned.items()}
+
+
+def _entry_values(entry: Entry, sim: Any, payload: tuple | None) -> tuple[dict[str, Any], dict[str, Any]]:
+    """(host arrays, device tensors) that ``entry`` stores for ``sim``; ``payload``
+    is the plasma model's (metadata, arrays) archive payload or None."""
+
+    mesh = sim.mesh
+    if entry.group == "metadata":
+        meta = _metadata(sim, payload[0] if payload else None)
+        return {entry.key: np.asarray(json.dumps(meta, default=_json_default, sort_keys=True))}, {}
+    if entry.group == "mesh":
+        value = {
+            "mesh_vertices": lambda: np.asarray(mesh.vertices, dtype=np.float64),
+            "mesh_faces": lambda: np.asarray(mesh.faces, dtype=np.int64),
+            "mesh_face_levels": lambda: np.asarray(mesh.face_levels if mesh.face_levels is not None else (), dtype=np.int64),
+        }[entry.key]()
+        return {entry.key: value}, {}
+    if entry.group == "field":
+        return {}, {entry.key: getattr(sim, entry.key)}
+    if entry.group == "surface":
+        ade = sim._surface_impedance_ade
+        return ({}, {entry.key: ade.memory}) if ade is not None else ({entry.key: np.empty((0, 0), dtype=np.float64)}, {})
+    if payload is None:
+        return {}, {}
+    if entry.group == "plasma_model":
+        return {entry.key.format(n): v for n, v in payload[1].items()}, {}
+    currents = sim._plasma_coupler.ade.current_density
+    return {}, {entry.key.format(i): c for i, c in enumerate(currents)}
+
+
+@contextlib.contextmanager
+def _replacing(destination: Path) -> Iterator[Any]:
+    """A temporary file beside ``destination`` that replaces it atomically once
+    written and flushed to disk; removed if writing fails."""
+
+    fd, name = tempfile.mkstemp(dir=destination.parent, prefix=f".{destination.name}.")
+    try:
+        with os.fdopen(fd, "wb") as handle:
+            yield handle
+            handle.flush()
+            os.fsync(handle.fileno())
+        os.replace(name, destination)
+    finally:
+        if os.path.exists(name):
+            os.unlink(name)
 
 
 def save_checkpoint(simulation: Any, path: str | Path, *, compress: bool = True) -> Path:
-    """Atomically write the NPZ (checkpoint.py:32-93).
+    """Atomically write the simulation's checkpoint (the reference's
+    ``save_checkpoint``, checkpoint.py:32-93).
 
     ``compress=False`` writes the same keys, shapes and dtypes without zlib
     compression (a stored zip that ``np.load`` reads like the compressed one),
-    for large meshes where compression dominates the save time.  Device arrays
-    come to the host through pinned buffers with one synchronisation."""
+    for large meshes where compression dominates the save time."""
 
     destination = Path(path)
-    metadata = _metadata(simulation)
+    payload = simulation.plasma.archive_payload() if simulation.plasma is not None else None
+    host: dict[str, Any] = {}
+    device: dict[str, Any] = {}
+    for entry in ARCHIVE:
+        h, d = _entry_values(entry, simulation, payload)
+        host.update(h)
+        device.update(d)
+    host.update(_to_host(device))
+    arrays = {k: host[k] for e in ARCHIVE for k in keys_for(e, payload[0] if payload else None)}
     destination.parent.mkdir(parents=True, exist_ok=True)
-    ade = simulation._surface_impedance_ade
-    device = {f: getattr(simulation, f) for f in ("er", "et", "hr", "ht")}
-    if ade is not None:
-        device["surface_impedance_memory"] = ade.memory
-    if simulation.plasma is not None:
-        for i, v in enumerate(simulation._plasma_coupler.ade.current_density):
-            device[f"plasma_current_{i}"] = v
-    host = _device_arrays_to_host(device)
-    arrays = {
-        "metadata": np.asarray(json.dumps(metadata, default=_json_default, sort_keys=True)),
-        "mesh_vertices": np.asarray(simulation.mesh.vertices, dtype=np.float64),
-        "mesh_faces": np.asarray(simulation.mesh.faces, dtype=np.int64),
-        "mesh_face_levels": (
-            np.asarray(simulation.mesh.face_levels, dtype=np.int64) if simulation.mesh.face_levels is not None else np.empty(0, dtype=np.int64)
-        ),
-        "er": host["er"],
-        "et": host["et"],
-        "hr": host["hr"],
-        "ht": host["ht"],
-        "surface_impedance_memory": host["surface_impedance_memory"] if ade is not None else np.empty((0, 0), dtype=np.float64),
-    }
-    if simulation.plasma is not None:
-        _, plasma_arrays = simulation.plasma.archive_payload()
-        arrays.update({f"plasma_model_{n}": v for n, v in plasma_arrays.items()})
-        arrays.update({k: v for k, v in host.items() if k.startswith("plasma_current_")})
-    temporary = None
-    try:
-        with tempfile.NamedTemporaryFile(mode="wb", dir=destination.parent, prefix=f".{destination.name}.", delete=False) as handle:
-            temporary = handle.name
-            (np.savez_compressed if compress else np.savez)(handle, **arrays)
-            handle.flush()
-            os.fsync(handle.fileno())
-        os.replace(temporary, destination)
-    finally:
-        if temporary is not None and os.path.exists(temporary):
-            os.unlink(temporary)
+    with _replacing(destination) as handle:
+        (np.savez_compressed if compress else np.savez)(handle, **arrays)
     return destination
+
+
+# ---------------------------------------------------------------------------
+# Reading
+# ---------------------------------------------------------------------------
+
+
+def _read_archive(path: Path) -> tuple[dict[str, Any], dict[str, np.ndarray]]:
+    """The metadata and every array the file's version requires (copied out)."""
+
+    try:
+        with np.load(path, allow_pickle=False) as archive:
+            if "metadata" not in archive.files:
+                raise CheckpointError("checkpoint is missing arrays: metadata")
+            metadata = _read_metadata(archive["metadata"])
+            plasma_meta = metadata.get("plasma") if metadata["version"] >= 4 else None
+            wanted = required_keys(metadata["version"], plasma_meta) - {"metadata"}
+            missing = wanted.difference(archive.files)
+            if missing:
+                raise CheckpointError(f"checkpoint is missing arrays: {', '.join(sorted(missing))}")
+            return metadata, {k: np.array(archive[k], copy=True) for k in wanted}
+    except CheckpointError:
+        raise
+    except (OSError, ValueError, KeyError, EOFError, zipfile.BadZipFile, json.JSONDecodeError) as error:
+        raise CheckpointError(f"cannot read checkpoint {path}: {error}") from error
+
+
+def _read_metadata(value: np.ndarray) -> dict[str, Any]:
+    if value.shape != () or value.dtype.kind not in {"U", "S"}:
+        raise CheckpointError("checkpoint metadata must be a scalar string")
+    metadata = json.loads(str(value.item()))
+    if not isinstance(metadata, dict):
+        raise CheckpointError("checkpoint metadata must be a JSON object")
+    if metadata.get("format") != CHECKPOINT_FORMAT:
+        raise CheckpointError("file is not an ionosphere-fdtd checkpoint")
+    version = metadata.get("version")
+    if version not in SUPPORTED_CHECKPOINT_VERSIONS:
+        raise CheckpointError(f"unsupported checkpoint version {version!r}; supported versions are {SUPPORTED_CHECKPOINT_VERSIONS}")
+    missing = {name for name, since in METADATA_SECTIONS.items() if version >= since}.difference(metadata)
+    if missing:
+        raise CheckpointError(f"checkpoint metadata is missing: {', '.join(sorted(missing))}")
+    return metadata
+
+
+def _mesh_from(metadata: dict, arrays: dict, config: Any):
+    """The mesh: rebuilt from the vertices alone (version 1) or from the stored
+    topology and refinement metadata (version 2 on)."""
+
+    vertices = np.asarray(arrays["mesh_vertices"], dtype=np.float64)
+    if metadata["version"] == 1:
+        return build_geodesic_mesh_from_vertices(config.subdivision, vertices, orientation=config.mesh_orientation, normalize_vertices=False)
+    about = metadata["mesh"]
+    if not isinstance(about, dict):
+        raise CheckpointError("checkpoint mesh metadata must be an object")
+    if not isinstance(about["has_face_levels"], bool):
+        raise CheckpointError("checkpoint has_face_levels must be boolean")
+    levels = arrays["mesh_face_levels"]
+    if not about["has_face_levels"]:
+        if levels.shape != (0,):
+            raise CheckpointError("checkpoint has unexpected face-level values")
+        levels = None
+    return build_geodesic_mesh_from_topology(
+        vertices, arrays["mesh_faces"], subdivision=about["subdivision"], face_levels=levels,
+        refinement_spec=about["refinement_spec"], topology_kind=about["topology_kind"],
+        normalize_vertices=False, require_well_centered=False,
+    )
+
+
+def _config_from(metadata: dict):
+    from .solver import SimulationConfig
+
+    values = dict(metadata["simulation_config"])
+    if values["radial_altitudes_m"] is not None:
+        values["radial_altitudes_m"] = tuple(values["radial_altitudes_m"])
+    return SimulationConfig(**values)
+
+
+def _model_from(metadata: dict, arrays: dict) -> dict[str, Any]:
+    """Configuration, mesh and physics models described by the metadata."""
+
+    version = metadata["version"]
+    try:
+        config = _config_from(metadata)
+        plasma_meta = metadata["plasma"] if version >= 4 else None
+        plasma_arrays = {n: arrays[f"plasma_model_{n}"] for n in plasma_meta["arrays"]} if plasma_meta else {}
+        return {
+            "config": config,
+            "mesh": _mesh_from(metadata, arrays, config),
+            "material": _material_from(metadata["material"]),
+            "source": _source_from(metadata["source"]),
+            "surface_impedance": _surface_from(metadata["surface_impedance"]) if version >= 3 else None,
+            "plasma": MeshPlasmaModel.from_archive_payload(plasma_meta, plasma_arrays) if plasma_meta is not None else None,
+        }
+    except CheckpointError:
+        raise
+    except (KeyError, TypeError, ValueError, RuntimeError) as error:
+        raise CheckpointError(f"invalid checkpoint model metadata: {error}") from error
+
+
+def _checked_state(what: str, saved: np.ndarray, expected: tuple, *, check_dtype_first: bool) -> None:
+    """The shape, dtype and finiteness checks of one restored state array."""
+
+    if saved.shape != expected:
+        raise CheckpointError(f"checkpoint {what} has shape {saved.shape}, expected {expected}")
+    if check_dtype_first:
+        if not np.issubdtype(saved.dtype, np.floating):
+            raise CheckpointError(f"checkpoint {what} must be floating point")
+        if not np.all(np.isfinite(saved)):
+            raise CheckpointError(f"checkpoint {what} contains non-finite values")
+    elif not np.issubdtype(saved.dtype, np.floating) or not np.all(np.isfinite(saved)):
+        raise CheckpointError(f"checkpoint {what} is invalid")
+
+
+def _restore(entry: Entry, sim: Any, arrays: dict[str, np.ndarray], version: int) -> None:
+    """Validate and restore the state arrays of one table entry."""
+
+    b = sim.backend
+    if entry.group == "field":
+        saved = arrays[entry.key]
+        _checked_state(f"field {entry.what}", saved, tuple(getattr(sim, entry.key).shape), check_dtype_first=True)
+        setattr(sim, entry.key, b.asarray(saved))
+    elif entry.group == "surface":
+        saved = arrays[entry.key] if version >= entry.since else np.empty((0, 0), dtype=np.float64)
+        ade = sim._surface_impedance_ade
+        if ade is None:
+            if saved.shape != (0, 0):
+                raise CheckpointError("checkpoint has ADE state without a surface impedance model")
+            return
+        _checked_state(entry.what, saved, tuple(ade.memory.shape), check_dtype_first=False)
+        ade.memory = b.asarray(saved)
+    elif entry.group == "plasma_current" and sim._plasma_coupler is not None:
+        targets = sim._plasma_coupler.ade.current_density
+        saved = [arrays[k] for k in sorted((k for k in arrays if k.startswith("plasma_current_")), key=lambda k: int(k.rsplit("_", 1)[1]))]
+        if len(saved) != len(targets):
+            raise CheckpointError("checkpoint plasma species state count is invalid")
+        for i, (values, target) in enumerate(zip(saved, targets, strict=True)):
+            _checked_state(entry.what.format(i), values, tuple(target.shape), check_dtype_first=False)
+            target.copy_(b.asarray(values))
+
+
+def _restore_clock(sim: Any, state: dict) -> None:
+    """Step count, time step and time of the saved state (checked against the
+    rebuilt model's time step)."""
+
+    steps = state["steps"]
+    if isinstance(steps, bool) or not isinstance(steps, int) or steps < 0:
+        raise CheckpointError("checkpoint step count must be a non-negative integer")
+    dt = float(state["time_step_s"])
+    if not np.isclose(dt, sim.time_step_s, rtol=0.0, atol=1.0e-15):
+        raise CheckpointError("checkpoint time step is inconsistent with the reconstructed model")
+    t = float(state["time_s"])
+    if not np.isfinite(t) or not np.isclose(t, steps * dt, rtol=1.0e-12, atol=1.0e-15):
+        raise CheckpointError("checkpoint time is inconsistent with its step count")
+    sim.steps = steps
+    sim.time_s = steps * dt
 
 
 def load_checkpoint(
@@ -106,204 +353,70 @@ def load_checkpoint(
     compile_chunk_size: int = 8,
     torch_threads: int | None = None,
 ) -> Any:
-    """Restore a checkpoint onto the CUDA engine (checkpoint.py:96-332)."""
+    """Restore a checkpoint onto the CUDA engine (the reference's
+    ``load_checkpoint``, checkpoint.py:96-332)."""
 
-    from .solver import GeodesicFDTD, SimulationConfig
+    from .solver import GeodesicFDTD
 
-    source_path = Path(path)
-    try:
-        with np.load(source_path, allow_pickle=False) as archive:
-            if "metadata" not in archive.files:
-                raise CheckpointError("checkpoint is missing arrays: metadata")
-            metadata = _read_metadata(archive["metadata"])
-            version = metadata["version"]
-            required = {"metadata", "mesh_vertices", "er", "et", "hr", "ht"}
-            if version >= 2:
-                required.update(("mesh_faces", "mesh_face_levels"))
-            if version >= 3:
-                required.add("surface_impedance_memory")
-            plasma_meta = metadata.get("plasma") if version >= 4 else None
-            if plasma_meta is not None:
-                required.update(f"plasma_model_{n}" for n in plasma_meta["arrays"])
-                required.update(f"plasma_current_{i}" for i in range(len(plasma_meta["species"])))
-            missing = required.difference(archive.files)
-            if missing:
-                raise CheckpointError(f"checkpoint is missing arrays: {', '.join(sorted(missing))}")
-            vertices = np.array(archive["mesh_vertices"], dtype=np.float64, copy=True)
-            faces = np.array(archive["mesh_faces"], copy=True) if version >= 2 else None
-            face_levels = np.array(archive["mesh_face_levels"], copy=True) if version >= 2 else None
-            fields = {n: np.array(archive[n], copy=True) for n in ("er", "et", "hr", "ht")}
-            si_memory = np.array(archive["surface_impedance_memory"], copy=True) if version >= 3 else np.empty((0, 0), dtype=np.float64)
-            plasma_arrays = {n: np.array(archive[f"plasma_model_{n}"], copy=True) for n in plasma_meta["arrays"]} if plasma_meta else {}
-            plasma_currents = (
-                tuple(np.array(archive[f"plasma_current_{i}"], copy=True) for i in range(len(plasma_meta["species"]))) if plasma_meta else ()
-            )
-    except CheckpointError:
-        raise
-    except (OSError, ValueError, KeyError, EOFError, zipfile.BadZipFile, json.JSONDecodeError) as error:
-        raise CheckpointError(f"cannot read checkpoint {source_path}: {error}") from error
-
-    try:
-        config_values = dict(metadata["simulation_config"])
-        if config_values["radial_altitudes_m"] is not None:
-            config_values["radial_altitudes_m"] = tuple(config_values["radial_altitudes_m"])
-        config = SimulationConfig(**config_values)
-        if version == 1:
-            mesh = build_geodesic_mesh_from_vertices(config.subdivision, vertices, orientation=config.mesh_orientation, normalize_vertices=False)
-        else:
-            mesh_meta = metadata["mesh"]
-            if not isinstance(mesh_meta, dict):
-                raise CheckpointError("checkpoint mesh metadata must be an object")
-            has_levels = mesh_meta["has_face_levels"]
-            if not isinstance(has_levels, bool):
-                raise CheckpointError("checkpoint has_face_levels must be boolean")
-            if has_levels:
-                restored_levels = face_levels
-            else:
-                if face_levels.shape != (0,):
-                    raise CheckpointError("checkpoint has unexpected face-level values")
-                restored_levels = None
-            mesh = build_geodesic_mesh_from_topology(
-                vertices,
-                faces,
-                subdivision=mesh_meta["subdivision"],
-                face_levels=restored_levels,
-                refinement_spec=mesh_meta["refinement_spec"],
-                topology_kind=mesh_meta["topology_kind"],
-                normalize_vertices=False,
-                require_well_centered=False,
-            )
-        material = _deserialize_material(metadata["material"])
-        source = _deserialize_source(metadata["source"])
-        surface = _deserialize_surface_impedance(metadata["surface_impedance"]) if version >= 3 else None
-        plasma = MeshPlasmaModel.from_archive_payload(plasma_meta, plasma_arrays) if plasma_meta is not None else None
-    except CheckpointError:
-        raise
-    except (KeyError, TypeError, ValueError, RuntimeError) as error:
-        raise CheckpointError(f"invalid checkpoint model metadata: {error}") from error
-
-    selected_dtype = dtype or str(metadata["runtime"]["dtype"])
-    simulation = GeodesicFDTD(
+    metadata, arrays = _read_archive(Path(path))
+    model = _model_from(metadata, arrays)
+    config = model.pop("config")
+    sim = GeodesicFDTD(
         replace(config, mesh_relaxations=0, mesh_optimization_steps=0),
-        material=material,
-        source=source,
-        surface_impedance=surface,
-        plasma=plasma,
-        mesh=mesh,
+        **model,
         backend=backend,
         device=device,
-        dtype=selected_dtype,
+        dtype=dtype or str(metadata["runtime"]["dtype"]),
         compile_step=compile_step,
         compile_chunk_size=compile_chunk_size,
         torch_threads=torch_threads,
     )
-    simulation.config = config
-    for name, values in fields.items():
-        expected = tuple(getattr(simulation, name).shape)
-        if values.shape != expected:
-            raise CheckpointError(f"checkpoint field {name} has shape {values.shape}, expected {expected}")
-        if not np.issubdtype(values.dtype, np.floating):
-            raise CheckpointError(f"checkpoint field {name} must be floating point")
-        if not np.all(np.isfinite(values)):
-            raise CheckpointError(f"checkpoint field {name} contains non-finite values")
-        setattr(simulation, name, simulation.backend.asarray(values))
-    ade = simulation._surface_impedance_ade
-    if ade is None:
-        if si_memory.shape != (0, 0):
-            raise CheckpointError("checkpoint has ADE state without a surface impedance model")
-    else:
-        if si_memory.shape != tuple(ade.memory.shape):
-            raise CheckpointError(f"checkpoint surface impedance state has shape {si_memory.shape}, expected {tuple(ade.memory.shape)}")
-        if not np.issubdtype(si_memory.dtype, np.floating) or not np.all(np.isfinite(si_memory)):
-            raise CheckpointError("checkpoint surface impedance state is invalid")
-        ade.memory = simulation.backend.asarray(si_memory)
-    if simulation._plasma_coupler is not None:
-        expected_currents = simulation._plasma_coupler.ade.current_density
-        if len(plasma_currents) != len(expected_currents):
-            raise CheckpointError("checkpoint plasma species state count is invalid")
-        for i, (saved, current) in enumerate(zip(plasma_currents, expected_currents, strict=True)):
-            if saved.shape != tuple(current.shape):
-                raise CheckpointError(f"checkpoint plasma current {i} has shape {saved.shape}, expected {tuple(current.shape)}")
-            if not np.issubdtype(saved.dtype, np.floating) or not np.all(np.isfinite(saved)):
-                raise CheckpointError(f"checkpoint plasma current {i} is invalid")
-            current.copy_(simulation.backend.asarray(saved))
-    steps = metadata["state"]["steps"]
-    if isinstance(steps, bool) or not isinstance(steps, int) or steps < 0:
-        raise CheckpointError("checkpoint step count must be a non-negative integer")
-    saved_dt = float(metadata["state"]["time_step_s"])
-    if not np.isclose(saved_dt, simulation.time_step_s, rtol=0.0, atol=1.0e-15):
-        raise CheckpointError("checkpoint time step is inconsistent with the reconstructed model")
-    saved_time = float(metadata["state"]["time_s"])
-    expected_time = steps * saved_dt
-    if not np.isfinite(saved_time) or not np.isclose(saved_time, expected_time, rtol=1.0e-12, atol=1.0e-15):
-        raise CheckpointError("checkpoint time is inconsistent with its step count")
-    simulation.steps = steps
-    simulation.time_s = expected_time
-    return simulation
+    sim.config = config
+    for entry in ARCHIVE:
+        _restore(entry, sim, arrays, metadata["version"])
+    _restore_clock(sim, metadata["state"])
+    return sim
 
 
-def _metadata(simulation: Any) -> dict[str, Any]:
-    if not isinstance(simulation.material, EarthIonosphereMaterial):
+# ---------------------------------------------------------------------------
+# Metadata (the reference's JSON schema)
+# ---------------------------------------------------------------------------
+
+
+def _metadata(sim: Any, plasma_meta: dict | None) -> dict[str, Any]:
+    if not isinstance(sim.material, EarthIonosphereMaterial):
         raise CheckpointError("checkpoints currently support EarthIonosphereMaterial only")
-    if simulation.source is not None and not isinstance(simulation.source, (GaussianCurrent, TangentialGaussianCurrent)):
+    if sim.source is not None and not isinstance(sim.source, tuple(SOURCE_TYPES.values())):
         raise CheckpointError("checkpoints currently support GaussianCurrent and TangentialGaussianCurrent sources only")
+    mesh = sim.mesh
+    material = asdict(sim.material)
+    material["anomalies"] = [asdict(a) for a in sim.material.anomalies]
     return {
         "format": CHECKPOINT_FORMAT,
         "version": CHECKPOINT_VERSION,
-        "simulation_config": asdict(simulation.config),
+        "simulation_config": asdict(sim.config),
         "mesh": {
-            "topology_kind": simulation.mesh.topology_kind,
-            "subdivision": simulation.mesh.subdivision,
-            "has_face_levels": simulation.mesh.face_levels is not None,
-            "refinement_spec": simulation.mesh.refinement_spec,
+            "topology_kind": mesh.topology_kind,
+            "subdivision": mesh.subdivision,
+            "has_face_levels": mesh.face_levels is not None,
+            "refinement_spec": mesh.refinement_spec,
         },
-        "material": _serialize_material(simulation.material),
-        "source": None if simulation.source is None else {"type": type(simulation.source).__name__, "parameters": asdict(simulation.source)},
-        "surface_impedance": simulation.surface_impedance.to_metadata() if simulation.surface_impedance is not None else None,
-        "plasma": simulation.plasma.archive_payload()[0] if simulation.plasma is not None else None,
-        "state": {"steps": simulation.steps, "time_s": simulation.time_s, "time_step_s": simulation.time_step_s},
+        "material": {"type": "EarthIonosphereMaterial", "parameters": material},
+        "source": None if sim.source is None else {"type": type(sim.source).__name__, "parameters": asdict(sim.source)},
+        "surface_impedance": sim.surface_impedance.to_metadata() if sim.surface_impedance is not None else None,
+        "plasma": plasma_meta,
+        "state": {"steps": sim.steps, "time_s": sim.time_s, "time_step_s": sim.time_step_s},
         "runtime": {
-            "backend": simulation.backend.name,
-            "device": simulation.backend.device,
-            "dtype": simulation.backend.dtype_name,
-            "compiled": simulation.compiled,
-            "compile_chunk_size": simulation.compile_chunk_size,
+            "backend": sim.backend.name,
+            "device": sim.backend.device,
+            "dtype": sim.backend.dtype_name,
+            "compiled": sim.compiled,
+            "compile_chunk_size": sim.compile_chunk_size,
         },
     }
 
 
-def _read_metadata(value: np.ndarray) -> dict[str, Any]:
-    if value.shape != () or value.dtype.kind not in {"U", "S"}:
-        raise CheckpointError("checkpoint metadata must be a scalar string")
-    metadata = json.loads(str(value.item()))
-    if not isinstance(metadata, dict):
-        raise CheckpointError("checkpoint metadata must be a JSON object")
-    if metadata.get("format") != CHECKPOINT_FORMAT:
-        raise CheckpointError("file is not an ionosphere-fdtd checkpoint")
-    if metadata.get("version") not in SUPPORTED_CHECKPOINT_VERSIONS:
-        raise CheckpointError(
-            f"unsupported checkpoint version {metadata.get('version')!r}; supported versions are {SUPPORTED_CHECKPOINT_VERSIONS}"
-        )
-    required = {"simulation_config", "material", "source", "state", "runtime"}
-    if metadata["version"] >= 2:
-        required.add("mesh")
-    if metadata["version"] >= 3:
-        required.add("surface_impedance")
-    if metadata["version"] >= 4:
-        required.add("plasma")
-    missing = required.difference(metadata)
-    if missing:
-        raise CheckpointError(f"checkpoint metadata is missing: {', '.join(sorted(missing))}")
-    return metadata
-
-
-def _serialize_material(material: EarthIonosphereMaterial) -> dict[str, Any]:
-    values = asdict(material)
-    values["anomalies"] = [asdict(a) for a in material.anomalies]
-    return {"type": "EarthIonosphereMaterial", "parameters": values}
-
-
-def _deserialize_material(data: Any) -> EarthIonosphereMaterial:
+def _material_from(data: Any) -> EarthIonosphereMaterial:
     if not isinstance(data, dict) or data.get("type") != "EarthIonosphereMaterial":
         raise CheckpointError("checkpoint material type is unsupported")
     values = dict(data.get("parameters", {}))
@@ -314,24 +427,21 @@ def _deserialize_material(data: Any) -> EarthIonosphereMaterial:
         raise CheckpointError(f"invalid checkpoint material: {error}") from error
 
 
-def _deserialize_source(data: Any):
+def _source_from(data: Any):
     if data is None:
         return None
     if not isinstance(data, dict):
         raise CheckpointError("checkpoint source metadata must be an object")
-    kinds = {"GaussianCurrent": GaussianCurrent, "TangentialGaussianCurrent": TangentialGaussianCurrent}
     try:
-        kind = kinds[data["type"]]
-        values = dict(data.get("parameters", {}))
-        for name in ("azimuths_deg", "line_lengths_m"):
-            if name in values and values[name] is not None:
-                values[name] = tuple(values[name])
+        kind = SOURCE_TYPES[data["type"]]
+        values = {k: tuple(v) if k in ("azimuths_deg", "line_lengths_m") and v is not None else v
+                  for k, v in dict(data.get("parameters", {})).items()}
         return kind(**values)
     except (KeyError, TypeError, ValueError) as error:
         raise CheckpointError(f"invalid checkpoint source: {error}") from error
 
 
-def _deserialize_surface_impedance(data: Any):
+def _surface_from(data: Any):
     if data is None:
         return None
     if not isinstance(data, dict):
@@ -346,3 +456,7 @@ def _json_default(value: Any) -> Any:
     if isinstance(value, np.generic):
         return value.item()
     raise TypeError(f"cannot encode {type(value).__name__} in checkpoint metadata")
+
+
+__all__ = ["ARCHIVE", "CHECKPOINT_FORMAT", "CHECKPOINT_VERSION", "Entry", "SUPPORTED_CHECKPOINT_VERSIONS",
+           "load_checkpoint", "required_keys", "save_checkpoint"]

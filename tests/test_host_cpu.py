@@ -162,6 +162,37 @@ def test_checkpoint_metadata_rejects_foreign_files(tmp_path):
         P.load_checkpoint(tmp_path / "trunc.npz")
 
 
+def test_checkpoint_table_gives_the_keys_of_every_version():
+    """The archive keys each format version must hold (checkpoint.py:23-477 of the
+    reference: v2 adds the mesh topology, v3 the surface memory, v4 the plasma)."""
+
+    from ionosphere_fdtd_b200 import checkpoint as CK
+
+    base = {"metadata", "mesh_vertices", "er", "et", "hr", "ht"}
+    assert CK.required_keys(1, None) == base
+    assert CK.required_keys(2, None) == base | {"mesh_faces", "mesh_face_levels"}
+    assert CK.required_keys(3, None) == base | {"mesh_faces", "mesh_face_levels", "surface_impedance_memory"}
+    plasma = {"arrays": ["number_density", "magnetic_field"], "species": [{}, {}]}
+    assert CK.required_keys(4, plasma) == CK.required_keys(3, None) | {
+        "plasma_model_number_density", "plasma_model_magnetic_field", "plasma_current_0", "plasma_current_1"}
+    assert [e.key for e in CK.ARCHIVE][:8] == ["metadata", "mesh_vertices", "mesh_faces", "mesh_face_levels", "er", "et", "hr", "ht"]
+
+
+def test_checkpoint_reports_missing_arrays_and_metadata_sections(tmp_path):
+    meta = {"format": "ionosphere-fdtd-checkpoint", "version": 1, "simulation_config": {}, "material": {}, "source": None,
+            "state": {}, "runtime": {}}
+    path = tmp_path / "v1.npz"
+    np.savez(path, metadata=np.asarray(json.dumps(meta)), mesh_vertices=np.zeros((12, 3)), er=np.zeros(1))
+    with pytest.raises(P.CheckpointError, match="checkpoint is missing arrays: et, hr, ht"):
+        P.load_checkpoint(path)
+    np.savez(path, metadata=np.asarray(json.dumps(dict(meta, version=3))))
+    with pytest.raises(P.CheckpointError, match="checkpoint metadata is missing: mesh, surface_impedance"):
+        P.load_checkpoint(path)
+    np.savez(path, er=np.zeros(1))
+    with pytest.raises(P.CheckpointError, match="checkpoint is missing arrays: metadata"):
+        P.load_checkpoint(path)
+
+
 def test_plasma_artifact_round_trip_and_corruption(tmp_path):
     from casebuild import product_provenance
 
