@@ -427,7 +427,7 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
         tuning = {
             "seconds": time.perf_counter() - t_tune,
             "candidates": len(SHAPE_FREE_CANDIDATES),
-            "classes": {f"s{k[0]}": {"producer_warps": r.best.producer_warps, "staging": r.best.staging, "ms_per_step": r.best_ms}
+            "classes": {f"s{k[0]}": {**tuning_fields(r.best), "ms_per_step": r.best_ms}
                         for k, r in tuned.items()},
         }
     T = args.time_steps or 100
@@ -720,6 +720,18 @@ def reference_arm(args, world: int, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def tuning_fields(t) -> dict:
+    """The launch-geometry fields of a tuning that differ from the automatic plan's
+    (patch sizes, staging, producer warps, lane layout, E-phase threads and stages)."""
+
+    from dataclasses import asdict
+
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    default = asdict(Tuning())
+    return {k: v for k, v in asdict(t).items() if k != "graph_chunk" and v != default[k]}
+
+
 def tune_launch_geometry(sim) -> dict:
     """Time the launch geometries that fix no patch size on the simulation's own state
     (restored afterwards) and keep the fastest; every candidate computes the same bits.
@@ -735,9 +747,8 @@ def tune_launch_geometry(sim) -> dict:
     return {
         "seconds": time.perf_counter() - t_tune,
         "candidates": len(SHAPE_FREE_CANDIDATES),
-        "best": {"producer_warps": res.best.producer_warps, "staging": res.best.staging, "ms_per_step": res.best_ms},
-        "timings": [{"producer_warps": t.producer_warps, "staging": t.staging, "ms_per_step": ms, "error": err}
-                    for t, ms, err in res.timings],
+        "best": {**tuning_fields(res.best), "ms_per_step": res.best_ms},
+        "timings": [{**tuning_fields(t), "ms_per_step": ms, "error": err} for t, ms, err in res.timings],
     }
 
 

@@ -117,6 +117,13 @@ typedef struct ifdtd_tuning {
   int32_t e_faces_per_patch; /* faces whose vertices/edges one E-phase patch owns (0: fit the stage to shared memory) */
   int32_t staging;           /* 0 auto, 1 direct global gathers, 2 pipeline (TMA bulk copies), 3 pipeline (cp.async) */
   int32_t producer_warps;    /* copy-issuing warps per pipelined CTA (default 2, at most 4) */
+  int32_t lane_layout;       /* pipelined consumers: 0 auto (packed), 1 rows packed back to back across lanes,
+                                2 every row starting on an 8-lane boundary (no shared-memory bank conflicts
+                                between rows; rows stay packed when a rounded-up row exceeds the threads) */
+  int32_t e_threads;         /* compute threads of a pipelined E-phase CTA (0: as threads); with the producer
+                                warps above 384 the E phase runs wide CTAs at 96 registers (at most 640
+                                threads, TMA bulk copies only) */
+  int32_t e_stages;          /* E-phase ring stages the balanced patches are sized for (0: 2, else 2 to 4) */
 } ifdtd_tuning;
 
 /* Mutable state of one simulation: device pointers owned by the caller. */

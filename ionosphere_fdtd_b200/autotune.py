@@ -7,7 +7,8 @@ bulk copies, cp.async, or direct global gathers).  ``autotune`` builds a plan
 for every candidate from the simulation's own mesh and physics, times
 graph-captured steps of each on the simulation's own state with CUDA events,
 restores that state, and installs the fastest plan.  Every candidate computes
-the same bits (patch size and kernel family do not change any result), so
+the same bits (patch size, lane layout and kernel family do not change any
+result), so
 tuning changes speed only.  ``autotune_ensemble`` tunes the largest member
 of each class (by default: mesh level, radial cells, precision and physics)
 and gives the winner to the whole class.
@@ -32,6 +33,8 @@ DEFAULT_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(e_faces_per_patch=16),
     Tuning(staging=3),
     Tuning(staging=1),
+    Tuning(lane_layout=2),
+    Tuning(producer_warps=3, lane_layout=2),
 )
 
 
@@ -153,7 +156,8 @@ SHAPE_FREE_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(),
     Tuning(producer_warps=1),
     Tuning(producer_warps=3),
-    Tuning(staging=3),
+    Tuning(lane_layout=2),
+    Tuning(producer_warps=3, lane_layout=2),
 )
 
 

@@ -98,6 +98,8 @@ struct ifdtd_plan {
   int h_mode = 1, e_mode = 1;  // 1 direct gathers, 2 pipeline
   int pipe_copy = 0;           // pipeline copy engine: 0 TMA bulk copies, 1 cp.async
   int producers = 2;           // copy-issuing warps per pipelined CTA
+  int lanes = 0;               // lane layout of the pipelined consumers: 0 packed rows, 1 rows on 8-lane boundaries
+  int e_threads = 0;           // compute threads of a pipelined E-phase CTA (above 384 - 32 x producers: wide CTAs)
   bool pipe_h_ok = false, pipe_e_ok = false;
   int kh_stage = 0, ke_stage = 0, kh_stages = 0, ke_stages = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
@@ -490,6 +492,17 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     return fail(IFDTD_ERR_ARGUMENT,
                 "staging must be 0 (auto), 1 (direct gathers), 2 (pipeline, TMA bulk copies) or 3 (pipeline, cp.async)");
   P->pipe_copy = staging == 3 ? 1 : 0;
+  const int lane_layout = tune ? tune->lane_layout : 0;
+  if (lane_layout < 0 || lane_layout > 2)
+    return fail(IFDTD_ERR_ARGUMENT, "lane_layout must be 0 (auto), 1 (packed rows) or 2 (rows on 8-lane boundaries)");
+  const int e_threads_req = tune ? tune->e_threads : 0;
+  if (e_threads_req != 0 && (e_threads_req % 32 || e_threads_req < 32 || e_threads_req + 32 * producers > pipe::kWideMaxThreads))
+    return fail(IFDTD_ERR_ARGUMENT, "e_threads must be 0 or a multiple of 32 with e_threads + 32 * producer_warps <= 640");
+  if (e_threads_req + 32 * producers > pipe::kMaxThreads && staging == 3)
+    return fail(IFDTD_ERR_ARGUMENT, "wide E-phase CTAs (e_threads + 32 * producer_warps > 384) use TMA bulk copies only");
+  const int e_stages_req = tune ? tune->e_stages : 0;
+  if (e_stages_req != 0 && (e_stages_req < 2 || e_stages_req > 4))
+    return fail(IFDTD_ERR_ARGUMENT, "e_stages must be 0 (auto) or 2 to 4");
   if ((int64_t)std::max(fpp, fpp_e) * 3 * Pn >= (1 << 24)) return fail(IFDTD_ERR_ARGUMENT, "patch too large");
   P->threads = threads;
   // graph_chunk: > 0 steps per captured graph, 0 direct launches, < 0 default
@@ -944,7 +957,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     // so no row may have more quads than the CTA has compute threads (at least
     // 256 when the count is automatic)
     const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
-    const bool quads_fit = row_quads <= (auto_threads ? 256 : threads);
+    const bool quads_fit = row_quads <= (auto_threads ? 256 : threads) && (e_threads_req == 0 || row_quads <= e_threads_req);
     std::vector<int> h_cand = auto_h ? std::vector<int>{256, 128, 64, 32, 16, 8} : std::vector<int>{fpp};
     if (!quads_fit) h_cand.clear();
     for (const int c : h_cand) {
@@ -963,7 +976,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     }
     // E phase: balanced patches for two, then three stages; then fixed face counts
     std::vector<int> e_try;  // > 0: faces per patch; < 0: balanced for -n stages
-    if (auto_e) e_try = {-2, -3, 32, 16, 8};
+    if (auto_e && e_stages_req > 0) e_try = {-e_stages_req, 32, 16, 8};
+    else if (auto_e) e_try = {-2, -3, 32, 16, 8};
     else e_try = {fpp_e};
     if (!quads_fit) e_try.clear();
     std::vector<char> v_src(nV, 0), e_src(nE, 0);
@@ -1071,6 +1085,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       return fail(IFDTD_ERR_ARGUMENT, "direct kernels take at most 256 threads per CTA");
     if (auto_threads && P->h_mode == 2 && P->e_mode == 2) threads = pipe::kMaxThreads - 32 * producers;
     P->threads = threads;
+    P->e_threads = e_threads_req > 0 ? e_threads_req : threads;
+    // rows on 8-lane boundaries only while a rounded-up row still fits the
+    // compute threads of both phases (otherwise the rows stay packed)
+    const int wide = std::max((Pn / (int)(16 / sizeof(real)) + 7) & ~7, (Pm / (int)(16 / sizeof(real)) + 7) & ~7);
+    P->lanes = lane_layout == 2 && wide <= std::min(threads, P->e_threads) ? 1 : 0;
   }
   {
     void* st = nullptr;
@@ -1154,7 +1173,7 @@ cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
     cudaError_t e = allow_smem(k, P->kh_smem);
     if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->kh_smem, P->n_patches, &P->kh_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->kh_grid, threads, P->kh_smem, st>>>(rec, P->kh_stage, P->kh_stages, P->producers);
+    k<<<P->kh_grid, threads, P->kh_smem, st>>>(rec, P->kh_stage, P->kh_stages, P->producers, P->lanes);
   } else {
     auto k = kh_kernel<real, PL>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
@@ -1167,12 +1186,14 @@ cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
 template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, int istep, cudaStream_t st) {
   if (P->e_mode == 2) {
-    auto k = P->pipe_copy == 0 ? pipe::ke_tma<real, PL, MD, 0> : pipe::ke_tma<real, PL, MD, 1>;
-    const int threads = P->threads + 32 * P->producers;
+    const int threads = P->e_threads + 32 * P->producers;
+    auto k = threads > pipe::kMaxThreads ? pipe::ke_tma<real, PL, MD, 0, pipe::kWideRegs>
+             : P->pipe_copy == 0         ? pipe::ke_tma<real, PL, MD, 0, pipe::kMaxRegs>
+                                         : pipe::ke_tma<real, PL, MD, 1, pipe::kMaxRegs>;
     cudaError_t e = allow_smem(k, P->ke_smem);
     if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->ke_smem, P->n_patches_e, &P->ke_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, P->producers, istep);
+    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, P->producers, istep, P->lanes);
   } else {
     auto k = ke_kernel<real, PL, MD>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
@@ -1289,7 +1310,7 @@ int grid_for(size_t n) {
 // are sampled by one launch per step.
 // ---------------------------------------------------------------------------
 struct BatchGroup {
-  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2;
+  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2, lanes = 0, e_threads = 0;
   std::vector<int> members;
   size_t kh_smem = 0, ke_smem = 0;
   int kh_grid = 0, ke_grid = 0;
@@ -1388,12 +1409,19 @@ auto batch_kh_kernel(const BatchGroup& g) {
 template <typename real>
 auto batch_ke_kernel(const BatchGroup& g) {
   using namespace pipe;
+  const bool wide = g.e_threads + 32 * g.producers > kMaxThreads;
   if (g.plasma) {
-    if (g.maxdeg == 6) return g.copy ? ke_tma_batch<real, true, 6, 1> : ke_tma_batch<real, true, 6, 0>;
-    return g.copy ? ke_tma_batch<real, true, 12, 1> : ke_tma_batch<real, true, 12, 0>;
+    if (g.maxdeg == 6)
+      return wide ? ke_tma_batch<real, true, 6, 0, kWideRegs>
+                  : g.copy ? ke_tma_batch<real, true, 6, 1, kMaxRegs> : ke_tma_batch<real, true, 6, 0, kMaxRegs>;
+    return wide ? ke_tma_batch<real, true, 12, 0, kWideRegs>
+                : g.copy ? ke_tma_batch<real, true, 12, 1, kMaxRegs> : ke_tma_batch<real, true, 12, 0, kMaxRegs>;
   }
-  if (g.maxdeg == 6) return g.copy ? ke_tma_batch<real, false, 6, 1> : ke_tma_batch<real, false, 6, 0>;
-  return g.copy ? ke_tma_batch<real, false, 12, 1> : ke_tma_batch<real, false, 12, 0>;
+  if (g.maxdeg == 6)
+    return wide ? ke_tma_batch<real, false, 6, 0, kWideRegs>
+                : g.copy ? ke_tma_batch<real, false, 6, 1, kMaxRegs> : ke_tma_batch<real, false, 6, 0, kMaxRegs>;
+  return wide ? ke_tma_batch<real, false, 12, 0, kWideRegs>
+              : g.copy ? ke_tma_batch<real, false, 12, 1, kMaxRegs> : ke_tma_batch<real, false, 12, 0, kMaxRegs>;
 }
 
 template <typename K>
@@ -1423,10 +1451,12 @@ int batch_build(ifdtd_batch* B) {
     key.copy = P->pipe_copy;
     key.threads = P->threads;
     key.producers = P->producers;
+    key.lanes = P->lanes;
+    key.e_threads = P->e_threads;
     BatchGroup* g = nullptr;
     for (auto& x : B->groups)
       if (x.plasma == key.plasma && x.maxdeg == key.maxdeg && x.copy == key.copy && x.threads == key.threads &&
-          x.producers == key.producers)
+          x.producers == key.producers && x.lanes == key.lanes && x.e_threads == key.e_threads)
         g = &x;
     if (!g) {
       B->groups.push_back(key);
@@ -1456,9 +1486,9 @@ int batch_build(ifdtd_batch* B) {
       ch.push_back(&P->kh_cost);
       ce.push_back(&P->ke_cost);
     }
-    const int threads = g.threads + 32 * g.producers;
+    const int threads = g.threads + 32 * g.producers, e_threads = g.e_threads + 32 * g.producers;
     cudaError_t e = batch_grid(batch_kh_kernel<real>(g), threads, g.kh_smem, sm_count, nh, &g.kh_grid);
-    if (e == cudaSuccess) e = batch_grid(batch_ke_kernel<real>(g), threads, g.ke_smem, sm_count, ne, &g.ke_grid);
+    if (e == cudaSuccess) e = batch_grid(batch_ke_kernel<real>(g), e_threads, g.ke_smem, sm_count, ne, &g.ke_grid);
     if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batched launch shape: ") + cudaGetErrorString(e));
     std::vector<int4> segs;
     std::vector<int> sptr;
@@ -1494,7 +1524,8 @@ cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row,
   for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
     const BatchGroup& g = B->groups[q];
     auto k = batch_kh_kernel<real>(g);
-    k<<<g.kh_grid, g.threads + 32 * g.producers, g.kh_smem, st>>>(recs, g.segs_h, g.sptr_h, B->d_ring_h, g.producers);
+    k<<<g.kh_grid, g.threads + 32 * g.producers, g.kh_smem, st>>>(recs, g.segs_h, g.sptr_h, B->d_ring_h, g.producers,
+                                                                   g.lanes);
     e = cudaGetLastError();
     if (e != cudaSuccess) B->failed = "kh_tma_batch of group " + std::to_string(q);
   }
@@ -1505,8 +1536,8 @@ cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row,
   for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
     const BatchGroup& g = B->groups[q];
     auto k = batch_ke_kernel<real>(g);
-    k<<<g.ke_grid, g.threads + 32 * g.producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.producers,
-                                                                   istep);
+    k<<<g.ke_grid, g.e_threads + 32 * g.producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.producers,
+                                                                   istep, g.lanes);
     e = cudaGetLastError();
     if (e != cudaSuccess) B->failed = "ke_tma_batch of group " + std::to_string(q);
   }

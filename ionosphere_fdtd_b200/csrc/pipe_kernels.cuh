@@ -32,6 +32,10 @@ constexpr int kMaxDesc = 32 * kDescPerLane;  // copy descriptors per patch
 constexpr int kMaxThreads = 384;             // producer warps + compute warps
 // Registers are granted to warps in groups of four: 12 warps x 32 x 168 <= 65536.
 constexpr int kMaxRegs = 168;
+// Wide E-phase CTAs: up to 20 warps at 96 registers (20 x 32 x 96 <= 65536);
+// the E consumer fits 96 registers without spilling, the H consumer does not.
+constexpr int kWideRegs = 96;
+constexpr int kWideMaxThreads = 640;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;  // bound of one wait (0.5 s)
 
 // Descriptor sources (int4 {src, first row, stage byte offset, bytes}).
@@ -260,9 +264,30 @@ __host__ __device__ inline bool si_lane_groups(int T) {
   return T > 0 && (T & 3) == 0 && q <= 32 && (q & (q - 1)) == 0;
 }
 
+// Lane layout of the per-run loops.  Thread ct of the nct compute threads
+// takes radial quad q = ct % G of the entity rows ct / G, ct / G + per, ...
+// (per = nct / G rows per sweep) when q < c, the row's quad count.  G = c
+// packs the rows back to back (layout 0); G = c rounded up to a multiple of 8
+// (layout 1) starts every row on an 8-lane boundary, so each 8-lane phase of a
+// 16-byte shared load reads a single row and gathered rows never meet in one
+// phase (no bank conflicts between rows), at the cost of G - c idle lanes per
+// row.  Both layouts compute the same values.
+struct LaneMap {
+  int G, per, q;
+  bool on;
+};
+__device__ __forceinline__ LaneMap lane_map(int ct, int nct, int c, int layout) {
+  LaneMap m;
+  m.G = layout ? (c + 7) & ~7 : c;
+  m.per = nct / m.G;
+  m.q = ct % m.G;
+  m.on = ct < m.per * m.G && m.q < c;
+  return m;
+}
+
 template <typename real, bool PLASMA>
 __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
-                                           int nct, uint64_t* group, uint32_t ph, const Ring& G) {
+                                           int nct, uint64_t* group, uint32_t ph, const Ring& G, int layout) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
   const int ea = hd[kh_ea], ne = hd[kh_ne], fa = hd[kh_fa], nf = hd[kh_nf];
@@ -313,11 +338,11 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
   // edge runs (nodes) and face runs (midpoints), each thread on a fixed
   // radial quad (layer factors loaded once per patch; see ke_consume)
   {
-    const int per = nct / cn;
-    if (ct < per * cn) {
-      const int k0 = (ct % cn) * N;
+    const LaneMap lm = lane_map(ct, nct, cn, layout);
+    if (lm.on) {
+      const int k0 = lm.q * N;
       const HEdgeLayer<real> y = h_edge_layer(R, Ls, k0);
-      for (int el = ct / cn; el < ne; el += per) {
+      for (int el = ct / lm.G; el < ne; el += lm.per) {
         const int e = ea + el;
         const int4 loc = eloc[el];
         h_edge_run(R, Ls, y, e, k0, s_er + loc.y * Pn, s_er + loc.x * Pn, s_et + loc.z * Pm, s_ht + el * Pn,
@@ -327,11 +352,11 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
     }
   }
   {
-    const int per = nct / cm;
-    if (ct < per * cm) {
-      const int j0 = (ct % cm) * N;
+    const LaneMap lm = lane_map(ct, nct, cm, layout);
+    if (lm.on) {
+      const int j0 = lm.q * N;
       const Run<real> fc = ld16(Ls.hC + j0);
-      for (int fl = ct / cm; fl < nf; fl += per) {
+      for (int fl = ct / lm.G; fl < nf; fl += lm.per) {
         const int f = fa + fl;
         const int4 l0 = floc[2 * fl];
         const int4 l1 = floc[2 * fl + 1];
@@ -351,7 +376,7 @@ __device__ __forceinline__ void kh_consume(const Rec<real>& R, const Layers<real
 // factors of its quad load once per patch instead of once per run.
 template <typename real, bool PLASMA, int MAXDEG>
 __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real>& Ls, unsigned char* st, int ct,
-                                           int nct, real current) {
+                                           int nct, real current, int layout, unsigned pattern) {
   constexpr int N = Lanes<real>::N;
   const int* hd = reinterpret_cast<const int*>(st);
   const int nv = hd[ke_nv], ea = hd[ke_ea], ne = hd[ke_ne], src = hd[ke_src];
@@ -395,18 +420,19 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     // (midpoints k0 .. k0+N-1) and takes the one below, k0-1, from lane - 1,
     // which holds quad q-1 of the same vertex; a lane whose quad q-1 sits in
     // the previous warp (lane 0) computes that value directly
-    const int per = nct / cn;
-    if (ct < per * cn) {
-      const int q = ct % cn, k0 = q * N;
+    const LaneMap lm = lane_map(ct, nct, cn, layout);
+    if (lm.on) {
+      const int q = lm.q, k0 = q * N, per = lm.per;
       const int lane = threadIdx.x & 31, wbase = ct - lane;
       // the vertex layer factors are re-read per run here: hoisting them too
       // would push this kernel past its register budget into local memory
       for (int k = 0;; ++k) {
-        const int vl = ct / cn + k * per;
+        const int vl = ct / lm.G + k * per;
         if (vl >= nv) break;
-        // lanes in this iteration: those whose thread index is below limit
-        const int cnt = min(per, nv - k * per) * cn - wbase;
-        const unsigned mask = cnt >= 32 ? 0xFFFFFFFFu : ((1u << cnt) - 1u);
+        // lanes in this iteration: those of the pattern (a valid quad of a
+        // row slot) whose thread index is below the sweep's limit
+        const int cnt = min(per, nv - k * per) * lm.G - wbase;
+        const unsigned mask = pattern & (cnt >= 32 ? 0xFFFFFFFFu : ((1u << cnt) - 1u));
         const int v = vid[vl];
         const real* hrows[MAXDEG];
         const real* jrows[MAXDEG];
@@ -428,11 +454,11 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     }
   }
   {
-    const int per = nct / cm;
-    if (ct < per * cm) {
-      const int j0 = (ct % cm) * N;
+    const LaneMap lm = lane_map(ct, nct, cm, layout);
+    if (lm.on) {
+      const int j0 = lm.q * N;
       const EdgeLayer<real> fixed = edge_layer(R, Ls, ea, j0);
-      for (int el = ct / cm; el < ne; el += per) {
+      for (int el = ct / lm.G; el < ne; el += lm.per) {
         const int e = ea + el;
         const int4 loc = eloc[el];
         e_edge_run<real, PLASMA>(R, full ? edge_layer(R, Ls, e, j0) : fixed, (src & 2) != 0, e, j0,
@@ -443,6 +469,17 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
       }
     }
   }
+}
+
+// Bit l set when lane l of this thread's warp holds a valid quad (q < c) in
+// the vertex-run lane map: the shuffle mask of the lanes that take part in a
+// sweep, before the sweep's row limit is applied.
+__device__ __forceinline__ unsigned lane_pattern(int ct, int nct, int c, int layout) {
+  const int wbase = ct - (threadIdx.x & 31);
+  unsigned bits = 0;
+  for (int l = 0; l < 32; ++l)
+    if (lane_map(wbase + l, nct, c, layout).on) bits |= 1u << l;
+  return bits;
 }
 
 // Shared prologue: barriers, record, per-layer rows, this CTA's patch range.
@@ -471,7 +508,7 @@ __device__ __forceinline__ void ring_setup(Rec<real>& R, const Rec<real>* recs, 
 
 template <typename real, bool PLASMA, int COPY>
 __global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
-                                             int producers) {
+                                             int producers, int layout) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
@@ -489,14 +526,14 @@ __global__ void __maxnreg__(kMaxRegs) kh_tma(const Rec<real>* __restrict__ recs,
   } else {
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
-      kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G);
+      kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G, layout);
     });
   }
 }
 
-template <typename real, bool PLASMA, int MAXDEG, int COPY>
-__global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
-                                             int producers, int istep) {
+template <typename real, bool PLASMA, int MAXDEG, int COPY, int REGS>
+__global__ void __maxnreg__(REGS) ke_tma(const Rec<real>* __restrict__ recs, int stage_bytes, int n_stages,
+                                         int producers, int istep, int layout) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages];
@@ -512,8 +549,9 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma(const Rec<real>* __restrict__ recs,
   } else {
     const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
     const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+    const unsigned pattern = lane_pattern(ct, nct, R.Pn / Lanes<real>::N, layout);
     consume_ring(G, p0, p1, [&](unsigned char* st, int s, uint32_t ph) {
-      ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current);
+      ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, layout, pattern);
     });
   }
 }
@@ -544,7 +582,7 @@ __device__ __forceinline__ void batch_segment_start(uint64_t* full, uint64_t* em
 template <typename real, bool PLASMA, int COPY>
 __global__ void __maxnreg__(kMaxRegs) kh_tma_batch(const Rec<real>* __restrict__ recs, const int4* __restrict__ segs,
                                                    const int* __restrict__ sptr, const int2* __restrict__ rings,
-                                                   int producers) {
+                                                   int producers, int layout) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
@@ -567,16 +605,16 @@ __global__ void __maxnreg__(kMaxRegs) kh_tma_batch(const Rec<real>* __restrict__
     } else {
       const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
       consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
-        kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G);
+        kh_consume<real, PLASMA>(R, Ls, st, ct, nct, group + s, ph, G, layout);
       });
     }
   }
 }
 
-template <typename real, bool PLASMA, int MAXDEG, int COPY>
-__global__ void __maxnreg__(kMaxRegs) ke_tma_batch(const Rec<real>* __restrict__ recs, const int4* __restrict__ segs,
-                                                   const int* __restrict__ sptr, const int2* __restrict__ rings,
-                                                   int producers, int istep) {
+template <typename real, bool PLASMA, int MAXDEG, int COPY, int REGS>
+__global__ void __maxnreg__(REGS) ke_tma_batch(const Rec<real>* __restrict__ recs, const int4* __restrict__ segs,
+                                               const int* __restrict__ sptr, const int2* __restrict__ rings,
+                                               int producers, int istep, int layout) {
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   __shared__ Rec<real> R;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
@@ -599,8 +637,9 @@ __global__ void __maxnreg__(kMaxRegs) ke_tma_batch(const Rec<real>* __restrict__
     } else {
       const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
       const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+      const unsigned pattern = lane_pattern(ct, nct, R.Pn / Lanes<real>::N, layout);
       consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
-        ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current);
+        ke_consume<real, PLASMA, MAXDEG>(R, Ls, st, ct, nct, current, layout, pattern);
       });
     }
   }

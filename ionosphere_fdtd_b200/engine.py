@@ -43,7 +43,13 @@ class Tuning:
     CUDA graph, and the kernel family (0 auto: the pipeline wherever two patch
     stages fit in shared memory, 1 direct global gathers, 2 the warp-specialised
     pipeline fed by TMA bulk copies, 3 the same pipeline fed by 16-byte cp.async
-    copies), and the copy-issuing warps per pipelined CTA (1 to 4)."""
+    copies), the copy-issuing warps per pipelined CTA (1 to 4), and the lane
+    layout of the pipelined consumers (0 auto = 1, rows packed back to back
+    across lanes; 2, every row starting on an 8-lane boundary), the compute
+    threads of an E-phase CTA (0: as ``threads``; above 384 minus the producer
+    warps the E phase runs wide CTAs of at most 640 threads at 96 registers)
+    and the ring stages the balanced E patches are sized for (0: 2).  Every
+    choice computes the same bits."""
 
     faces_per_patch: int = 0
     threads: int = 0
@@ -51,6 +57,9 @@ class Tuning:
     e_faces_per_patch: int = 0
     staging: int = 0
     producer_warps: int = 2
+    lane_layout: int = 0
+    e_threads: int = 0
+    e_stages: int = 0
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -160,7 +169,8 @@ class Engine:
             pd.vertex_faces = i64(p["vertex_faces"])
             pd.vertex_face_weights = f64(p["vertex_face_weights"])
         t = self.tuning
-        td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps)
+        td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps, t.lane_layout,
+                      t.e_threads, t.e_stages)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(

@@ -114,8 +114,8 @@ def test_launch_geometry_record_lists_every_candidate(monkeypatch):
     monkeypatch.setattr(A, "autotune", fake)
     rec = bench.tune_launch_geometry(object())
     assert rec["candidates"] == len(A.SHAPE_FREE_CANDIDATES) == len(rec["timings"])
-    assert rec["best"] == {"producer_warps": A.SHAPE_FREE_CANDIDATES[0].producer_warps,
-                           "staging": A.SHAPE_FREE_CANDIDATES[0].staging, "ms_per_step": 1.0}
+    assert rec["best"] == {**bench.tuning_fields(A.SHAPE_FREE_CANDIDATES[0]), "ms_per_step": 1.0}
+    assert rec["timings"][1] == {"producer_warps": A.SHAPE_FREE_CANDIDATES[1].producer_warps, "ms_per_step": 2.0, "error": None}
     assert rec["timings"][-1]["error"] == "stage does not fit"
 
     def failing(sim, candidates, *, steps, repeats):

@@ -119,17 +119,19 @@ def test_members_with_different_launch_tunings_form_groups_and_match_their_own_r
 
     # producer warps 1 / 2 / 3 and the cp.async copy engine: four groups, two of
     # which share a kernel instantiation with different shared-memory sizes
+    # (and rows on 8-lane boundaries: a fifth group)
     spec = [
         ("config1_s2", Tuning(producer_warps=1)),
         ("plasma_drude_s2", Tuning()),
         ("source_s1", Tuning(producer_warps=3)),
         ("config4_mini_s2", Tuning(staging=3)),
         ("surface_s1", Tuning(producer_warps=1)),
+        ("plasma_magnetized_s1", Tuning(lane_layout=2)),
     ]
     together = [build_product(CS.CASES[n], "float32", tuning=t) for n, t in spec]
     alone = [build_product(CS.CASES[n], "float32", tuning=t) for n, t in spec]
     with Ensemble(together) as ens:
-        assert ens.launch_layout()["groups"] == 4
+        assert ens.launch_layout()["groups"] == 5
         ens.step(34)
     for sim in alone:
         sim.step(34)

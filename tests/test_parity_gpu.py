@@ -163,12 +163,50 @@ def test_pipeline_and_direct_kernels_agree_bitwise(name, fpp, staging):
     assert staged["_sim"]._engine.status_word() == 0
 
 
-@pytest.mark.parametrize("threads,producers", [(32, 1), (128, 4), (352, 1), (256, 2), (64, 3)])
-def test_pipeline_warp_counts_do_not_change_results(threads, producers):
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+@pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "config1_s2", "adaptive_plasma_si_s1", "tangential_s1"])
+def test_lane_layouts_agree_bitwise(name, dtype):
+    """Rows packed across lanes and rows started on 8-lane boundaries run the
+    same per-run arithmetic on the same quads: bit-for-bit equal results, with
+    and without plasma, float32 (4 reals per quad) and float64 (2)."""
+
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    packed = run_product(C.CASES[name], dtype, tuning=Tuning(staging=2, lane_layout=1))
+    aligned = run_product(C.CASES[name], dtype, tuning=Tuning(staging=2, lane_layout=2))
+    assert aligned["_sim"]._engine.kernel_modes == ("pipeline", "pipeline")
+    for key in ("er", "et", "hr", "ht", "si_memory", "plasma_current_0", "plasma_current_1", "traces"):
+        if key in packed:
+            np.testing.assert_array_equal(packed[key], aligned[key], err_msg=key)
+    assert aligned["_sim"]._engine.status_word() == 0
+
+
+@pytest.mark.parametrize("tuning", [dict(e_threads=576), dict(e_threads=608, producer_warps=1, lane_layout=2),
+                                    dict(e_stages=3), dict(e_stages=3, e_threads=544, producer_warps=3)])
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+@pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "adaptive_plasma_si_s1", "tangential_s1"])
+def test_wide_e_ctas_and_deeper_e_rings_agree_bitwise(name, dtype, tuning):
+    """E-phase CTAs of up to 20 warps at 96 registers, and E patches sized for
+    three ring stages, compute the same bits as the default plan."""
+
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    ref = run_product(C.CASES[name], dtype, tuning=Tuning(staging=2))
+    other = run_product(C.CASES[name], dtype, tuning=Tuning(staging=2, **tuning))
+    assert other["_sim"]._engine.kernel_modes == ("pipeline", "pipeline")
+    for key in ("er", "et", "hr", "ht", "si_memory", "plasma_current_0", "plasma_current_1", "traces"):
+        if key in ref:
+            np.testing.assert_array_equal(ref[key], other[key], err_msg=key)
+    assert other["_sim"]._engine.status_word() == 0
+
+
+@pytest.mark.parametrize("threads,producers,lanes", [(32, 1, 0), (128, 4, 0), (352, 1, 0), (256, 2, 0), (64, 3, 0),
+                                                     (32, 1, 2), (96, 2, 2), (352, 1, 2)])
+def test_pipeline_warp_counts_do_not_change_results(threads, producers, lanes):
     from ionosphere_fdtd_b200.engine import Tuning
 
     case = C.CASES["plasma_magnetized_s1"]
     ref = run_product(case, "float64", tuning=Tuning(staging=2))
-    other = run_product(case, "float64", tuning=Tuning(staging=2, threads=threads, producer_warps=producers))
+    other = run_product(case, "float64", tuning=Tuning(staging=2, threads=threads, producer_warps=producers, lane_layout=lanes))
     for f in STATE:
         np.testing.assert_array_equal(ref[f], other[f])
