@@ -25,6 +25,14 @@ extern "C" {
  * op(b) is k x n: b is bf16 row-major k x n (trans_b = 0) or n x k (trans_b = 1). */
 int32_t ifdtd_nn_gemm(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
                       int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream);
+/* The same product on the 5th-generation tensor cores: tcgen05.mma (bf16 inputs, fp32 accumulation
+ * in tensor memory), one 128 x 128 tile of c per 128-thread CTA, K in chunks of 64 staged in shared
+ * memory.  Same arguments and result as ifdtd_nn_gemm up to fp32 rounding of the accumulation. */
+int32_t ifdtd_nn_gemm_tc(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
+                         int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream);
+/* Status word of ifdtd_nn_gemm_tc: bit 0 set when an mbarrier wait ran out its 0.2 s bound (that
+ * call's result is then invalid).  Reading it synchronises the device; reset != 0 clears it. */
+int32_t ifdtd_nn_gemm_tc_status(int32_t reset, int32_t* out);
 /* z (rows x cols, fp32) += bias (cols); y_bf16 = act(z) (act 0 identity, 1 SiLU; y may be NULL). */
 int32_t ifdtd_nn_bias_act(int32_t rows, int32_t cols, float* z, const float* bias, int32_t act, void* y_bf16,
                           void* stream);

@@ -91,7 +91,8 @@ class PhysicsDesc(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("faces_per_patch", _i32), ("threads", _i32), ("graph_chunk", _i32), ("e_faces_per_patch", _i32), ("staging", _i32),
-                ("producer_warps", _i32), ("lane_layout", _i32), ("e_threads", _i32), ("e_stages", _i32)]
+                ("producer_warps", _i32), ("lane_layout", _i32), ("e_threads", _i32), ("e_stages", _i32),
+                ("e_producer_warps", _i32)]
 
 
 class State(C.Structure):
@@ -135,6 +136,8 @@ _SIGNATURES = {
     "ifdtd_batch_info": ([_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)], _i32),
     "ifdtd_max_abs": ([_vp, C.POINTER(State), _vp, _vp], _i32),
     "ifdtd_nn_gemm": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp], _i32),
+    "ifdtd_nn_gemm_tc": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp], _i32),
+    "ifdtd_nn_gemm_tc_status": ([_i32, C.POINTER(_i32)], _i32),
     "ifdtd_nn_bias_act": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp], _i32),
     "ifdtd_nn_act_grad": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp, _vp], _i32),
     "ifdtd_nn_col_sum": ([_i32, _i32, _vp, _vp, _vp], _i32),

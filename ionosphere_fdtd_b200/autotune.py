@@ -34,7 +34,9 @@ DEFAULT_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(staging=3),
     Tuning(staging=1),
     Tuning(lane_layout=2),
-    Tuning(producer_warps=3, lane_layout=2),
+    Tuning(e_producer_warps=3),
+    Tuning(e_threads=576),
+    Tuning(e_stages=3),
 )
 
 
@@ -156,8 +158,8 @@ SHAPE_FREE_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(),
     Tuning(producer_warps=1),
     Tuning(producer_warps=3),
-    Tuning(lane_layout=2),
-    Tuning(producer_warps=3, lane_layout=2),
+    Tuning(e_producer_warps=3),
+    Tuning(e_producer_warps=4),
 )
 
 

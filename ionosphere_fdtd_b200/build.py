@@ -15,7 +15,7 @@ from pathlib import Path
 
 PACKAGE = Path(__file__).resolve().parent
 ROOT = PACKAGE.parent
-SOURCES = [PACKAGE / "csrc" / "ifdtd.cu", PACKAGE / "csrc" / "surrogate.cu"]
+SOURCES = [PACKAGE / "csrc" / "ifdtd.cu", PACKAGE / "csrc" / "surrogate.cu", PACKAGE / "csrc" / "gemm_tcgen05.cu"]
 HEADERS = [
     PACKAGE / "csrc" / "step_kernels.cuh",
     PACKAGE / "csrc" / "pipe_kernels.cuh",

@@ -1,0 +1,277 @@
+// BF16 GEMM of the trace surrogate on the 5th-generation tensor cores
+// (tcgen05.mma, sm_100a): C (M x N, fp32) = alpha * op(A) op(B) + beta * C.
+//
+// One CTA of 128 threads (one warpgroup) computes a 128 x 128 tile of C.  The
+// accumulator lives in tensor memory: warp 0 allocates 128 TMEM columns (fp32,
+// one column per output column, lane = output row).  K runs in chunks of 64:
+// all threads stage the chunk's A tile (128 rows x 64) and B tile (128 output
+// columns x 64) in shared memory, K-major, in the no-swizzle core-matrix
+// layout the MMA reads (8 rows x 16 bytes per core matrix, 128 bytes apart
+// along K, 1024 bytes apart along M / N), zero outside the matrices, so ragged
+// shapes and both transposes need no special case in the MMA.  One elected
+// thread issues four tcgen05.mma (M 128, N 128, K 16 each, bf16 inputs, fp32
+// accumulate) per chunk and commits them to the chunk's mbarrier; two stages
+// let the next chunk load while the MMAs of the previous one run.  The
+// epilogue reads the accumulator with tcgen05.ld (each warp its 32 TMEM lanes)
+// and writes alpha * acc + beta * C.
+//
+// Every mbarrier wait is bounded by the global timer (0.2 s).  A wait that runs
+// out sets bit 0 of the module status word (ifdtd_nn_gemm_tc_status), the CTA
+// skips its remaining chunks and its epilogue, waits (again bounded) for the
+// MMAs it issued, frees its tensor memory and returns.  No operand is another
+// GPU's memory and no copy uses cluster multicast.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ifdtd_surrogate.h"
+#include "errors.cuh"
+
+namespace ifdtd {
+namespace tc {
+
+constexpr int TM = 128, TN = 128, TK = 64, THREADS = 128, STAGES = 2;
+constexpr int A_BYTES = TM * TK * 2, B_BYTES = TN * TK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + room to align the stages to 1024 bytes
+constexpr uint32_t TMEM_COLS = 128;
+constexpr uint64_t kWaitNs = 200ull * 1000 * 1000;
+
+__device__ int g_status;
+
+// Instruction descriptor of tcgen05.mma.kind::f16: fp32 accumulator (bits 4-5
+// = 1), A and B bf16 (bits 7-9 and 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28; dense, no negation.
+constexpr uint32_t kInstrDesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor: start address >> 4 (bits 0-13), leading
+// byte offset >> 4 (bits 16-29: the next core matrix along K, 128 B), stride
+// byte offset >> 4 (bits 32-45: the next 8-row group, 1024 B), the sm_100
+// descriptor version 1 (bits 46-48), base offset 0, no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+// Byte offset of the 16-byte row piece (row, k-group) in a 128 x 64 tile: core
+// matrix (row / 8, kg) at ((row / 8) * 8 + kg) * 128, row % 8 at 16 * (row % 8).
+__device__ __forceinline__ uint32_t core_offset(int row, int kg) {
+  return (uint32_t)((((row >> 3) << 3) + kg) * 128 + ((row & 7) << 4));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase of `bar` with this parity; false (and the status
+// bit set) when it did not complete within kWaitNs.
+__device__ __forceinline__ bool wait_bounded(uint32_t bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 1; i < (1u << 30); ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 15u) == 0 && global_ns() - t0 > kWaitNs) break;
+  }
+  atomicOr(&g_status, 1);
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// The 8 bf16 of op(X)[row][k0 .. k0 + 7] (zero outside rows x cols) as one
+// 16-byte piece.  op(X) is rows x cols: X row-major rows x cols (trans = 0,
+// contiguous along k) or cols x rows (trans = 1, strided); `vec` allows one
+// 16-byte load when the piece lies inside a contiguous row.
+__device__ __forceinline__ uint4 load_piece(const __nv_bfloat16* __restrict__ X, int ld, int trans, int rows, int cols,
+                                            int row, int k0, bool vec) {
+  uint4 v = make_uint4(0u, 0u, 0u, 0u);
+  if (row >= rows || k0 >= cols) return v;
+  if (!trans && vec && k0 + 8 <= cols) return __ldg(reinterpret_cast<const uint4*>(X + (size_t)row * ld + k0));
+  uint16_t h[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int k = k0 + q;
+    h[q] = k < cols ? __bfloat16_as_ushort(trans ? X[(size_t)k * ld + row] : X[(size_t)row * ld + k]) : (uint16_t)0;
+  }
+  v.x = (uint32_t)h[0] | ((uint32_t)h[1] << 16);
+  v.y = (uint32_t)h[2] | ((uint32_t)h[3] << 16);
+  v.z = (uint32_t)h[4] | ((uint32_t)h[5] << 16);
+  v.w = (uint32_t)h[6] | ((uint32_t)h[7] << 16);
+  return v;
+}
+
+__global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
+                                                        int lda, int ta, const __nv_bfloat16* __restrict__ B, int ldb,
+                                                        int tb, float alpha, float beta, float* __restrict__ C,
+                                                        int ldc) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mma_done[STAGES];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mma_done[s])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const bool vec_a = !ta && lda % 8 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0;
+  const bool vec_b = tb && ldb % 8 == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+  const int nk = (K + TK - 1) / TK;
+  int issued = 0;  // chunks whose MMAs were issued (thread 0)
+  for (int c = 0; c < nk; ++c) {
+    const int s = c % STAGES;
+    // the stage is free once the MMAs of chunk c - STAGES, which read it, are done
+    if (c >= STAGES && !wait_bounded(smem_u32(&mma_done[s]), (uint32_t)((c - STAGES) / STAGES) & 1u)) abort_flag = 1;
+    __syncthreads();
+    if (abort_flag) break;
+    unsigned char* as = smem + s * STAGE_BYTES;
+    unsigned char* bs = as + A_BYTES;
+    const int k0 = c * TK;
+    // piece p: row (p >> 6) * 8 + (p & 7), k-group (p >> 3) & 7, so consecutive
+    // threads fill consecutive 16-byte slots of one core matrix
+    for (int p = threadIdx.x; p < TM * (TK / 8); p += THREADS) {
+      const int row = ((p >> 6) << 3) + (p & 7), kg = (p >> 3) & 7;
+      *reinterpret_cast<uint4*>(as + core_offset(row, kg)) = load_piece(A, lda, ta, M, K, m0 + row, k0 + 8 * kg, vec_a);
+      // op(B) is K x N: the tile's row n holds op(B)[k][n0 + n] along k
+      *reinterpret_cast<uint4*>(bs + core_offset(row, kg)) =
+          load_piece(B, ldb, !tb, N, K, n0 + row, k0 + 8 * kg, vec_b);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(as), b0 = smem_u32(bs);
+#pragma unroll
+      for (int kk = 0; kk < TK / 16; ++kk) {
+        const uint64_t ad = smem_desc(a0 + kk * 256), bd = smem_desc(b0 + kk * 256);
+        const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kInstrDesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mma_done[s]))
+                   : "memory");
+      issued = c + 1;
+    }
+  }
+  // every thread waits for the last issued chunk's commit (it covers all earlier MMAs)
+  __syncthreads();
+  const int done_chunks = abort_flag ? -1 : nk;
+  bool ok = true;
+  if (done_chunks > 0) {
+    const int last = nk - 1;
+    ok = wait_bounded(smem_u32(&mma_done[last % STAGES]), (uint32_t)(last / STAGES) & 1u);
+  } else if (threadIdx.x == 0 && issued > 0) {
+    // aborted: wait (bounded) for the MMAs already issued before freeing TMEM
+    wait_bounded(smem_u32(&mma_done[(issued - 1) % STAGES]), (uint32_t)((issued - 1) / STAGES) & 1u);
+  }
+  if (!ok) abort_flag = 1;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (!abort_flag) {
+    const int row = m0 + 32 * warp + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll 1
+    for (int cb = 0; cb < TN; cb += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(lane_base + (uint32_t)cb));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+        float* crow = C + (size_t)row * ldc;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int col = n0 + cb + q;
+          if (col < N) {
+            const float v = alpha * __uint_as_float(r[q]);
+            crow[col] = beta == 0.f ? v : v + beta * crow[col];
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace ifdtd
+
+extern "C" {
+
+int32_t ifdtd_nn_gemm_tc(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
+                         int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream) {
+  using namespace ifdtd::tc;
+  if (m <= 0 || n <= 0 || k <= 0 || !a || !b || !c) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad gemm shape");
+  if (lda < (trans_a ? m : k) || ldb < (trans_b ? k : n) || ldc < n)
+    return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm leading dimension too small");
+  if ((n + TN - 1) / TN > 65535) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm has too many columns");
+  // the opt-in above 48 KiB of dynamic shared memory holds per device; setting it is cheap
+  cudaError_t e = cudaFuncSetAttribute(gemm_tcgen05, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05 attribute: ") + cudaGetErrorString(e));
+  const dim3 grid((m + TM - 1) / TM, (n + TN - 1) / TN);
+  gemm_tcgen05<<<grid, THREADS, SMEM_BYTES, (cudaStream_t)stream>>>(m, n, k, (const __nv_bfloat16*)a, lda, trans_a != 0,
+                                                                      (const __nv_bfloat16*)b, ldb, trans_b != 0, alpha,
+                                                                      beta, c, ldc);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05: ") + cudaGetErrorString(e));
+  return IFDTD_OK;
+}
+
+int32_t ifdtd_nn_gemm_tc_status(int32_t reset, int32_t* out) {
+  using namespace ifdtd::tc;
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_status, sizeof(int));
+  if (e == cudaSuccess && reset) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_status, &zero, sizeof(int));
+  }
+  if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm status: ") + cudaGetErrorString(e));
+  if (out) *out = v;
+  return IFDTD_OK;
+}
+
+}  // extern "C"

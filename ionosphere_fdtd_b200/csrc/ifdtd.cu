@@ -99,7 +99,8 @@ struct ifdtd_plan {
   int pipe_copy = 0;           // pipeline copy engine: 0 TMA bulk copies, 1 cp.async
   int producers = 2;           // copy-issuing warps per pipelined CTA
   int lanes = 0;               // lane layout of the pipelined consumers: 0 packed rows, 1 rows on 8-lane boundaries
-  int e_threads = 0;           // compute threads of a pipelined E-phase CTA (above 384 - 32 x producers: wide CTAs)
+  int e_threads = 0;           // compute threads of a pipelined E-phase CTA (above 384 - 32 x e_producers: wide CTAs)
+  int e_producers = 2;         // copy-issuing warps of a pipelined E-phase CTA
   bool pipe_h_ok = false, pipe_e_ok = false;
   int kh_stage = 0, ke_stage = 0, kh_stages = 0, ke_stages = 0, kh_grid = 0, ke_grid = 0, sm_count = 148;
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
@@ -495,11 +496,15 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int lane_layout = tune ? tune->lane_layout : 0;
   if (lane_layout < 0 || lane_layout > 2)
     return fail(IFDTD_ERR_ARGUMENT, "lane_layout must be 0 (auto), 1 (packed rows) or 2 (rows on 8-lane boundaries)");
+  const int e_producers = (tune && tune->e_producer_warps > 0) ? tune->e_producer_warps : producers;
+  if (e_producers > 4) return fail(IFDTD_ERR_ARGUMENT, "e_producer_warps must be 0 (as producer_warps) or 1 to 4");
+  P->e_producers = e_producers;
   const int e_threads_req = tune ? tune->e_threads : 0;
-  if (e_threads_req != 0 && (e_threads_req % 32 || e_threads_req < 32 || e_threads_req + 32 * producers > pipe::kWideMaxThreads))
-    return fail(IFDTD_ERR_ARGUMENT, "e_threads must be 0 or a multiple of 32 with e_threads + 32 * producer_warps <= 640");
-  if (e_threads_req + 32 * producers > pipe::kMaxThreads && staging == 3)
-    return fail(IFDTD_ERR_ARGUMENT, "wide E-phase CTAs (e_threads + 32 * producer_warps > 384) use TMA bulk copies only");
+  if (e_threads_req != 0 &&
+      (e_threads_req % 32 || e_threads_req < 32 || e_threads_req + 32 * e_producers > pipe::kWideMaxThreads))
+    return fail(IFDTD_ERR_ARGUMENT, "e_threads must be 0 or a multiple of 32 with e_threads + 32 * E producer warps <= 640");
+  if (e_threads_req + 32 * e_producers > pipe::kMaxThreads && staging == 3)
+    return fail(IFDTD_ERR_ARGUMENT, "wide E-phase CTAs (e_threads + 32 * E producer warps > 384) use TMA bulk copies only");
   const int e_stages_req = tune ? tune->e_stages : 0;
   if (e_stages_req != 0 && (e_stages_req < 2 || e_stages_req > 4))
     return fail(IFDTD_ERR_ARGUMENT, "e_stages must be 0 (auto) or 2 to 4");
@@ -1085,7 +1090,14 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       return fail(IFDTD_ERR_ARGUMENT, "direct kernels take at most 256 threads per CTA");
     if (auto_threads && P->h_mode == 2 && P->e_mode == 2) threads = pipe::kMaxThreads - 32 * producers;
     P->threads = threads;
-    P->e_threads = e_threads_req > 0 ? e_threads_req : threads;
+    // E-phase compute threads: as given; automatic with automatic threads: the
+    // pipelined CTA's 384 less the E producer warps; otherwise as threads
+    P->e_threads = e_threads_req > 0 ? e_threads_req
+                   : (auto_threads && P->h_mode == 2 && P->e_mode == 2) ? pipe::kMaxThreads - 32 * e_producers
+                                                                        : threads;
+    if (P->e_mode == 2 && P->e_threads + 32 * e_producers > pipe::kMaxThreads &&
+        (e_threads_req == 0 || P->pipe_copy != 0))
+      return fail(IFDTD_ERR_ARGUMENT, "threads + 32 * E producer warps must not exceed 384");
     // rows on 8-lane boundaries only while a rounded-up row still fits the
     // compute threads of both phases (otherwise the rows stay packed)
     const int wide = std::max((Pn / (int)(16 / sizeof(real)) + 7) & ~7, (Pm / (int)(16 / sizeof(real)) + 7) & ~7);
@@ -1186,14 +1198,14 @@ cudaError_t launch_kh_t(ifdtd_plan* P, const Rec<real>* rec, cudaStream_t st) {
 template <typename real, bool PL, int MD>
 cudaError_t launch_ke_t(ifdtd_plan* P, const Rec<real>* rec, int istep, cudaStream_t st) {
   if (P->e_mode == 2) {
-    const int threads = P->e_threads + 32 * P->producers;
+    const int threads = P->e_threads + 32 * P->e_producers;
     auto k = threads > pipe::kMaxThreads ? pipe::ke_tma<real, PL, MD, 0, pipe::kWideRegs>
              : P->pipe_copy == 0         ? pipe::ke_tma<real, PL, MD, 0, pipe::kMaxRegs>
                                          : pipe::ke_tma<real, PL, MD, 1, pipe::kMaxRegs>;
     cudaError_t e = allow_smem(k, P->ke_smem);
     if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->ke_smem, P->n_patches_e, &P->ke_grid);
     if (e != cudaSuccess) return e;
-    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, P->producers, istep, P->lanes);
+    k<<<P->ke_grid, threads, P->ke_smem, st>>>(rec, P->ke_stage, P->ke_stages, P->e_producers, istep, P->lanes);
   } else {
     auto k = ke_kernel<real, PL, MD>;
     cudaError_t e = allow_smem(k, P->smem_bytes);
@@ -1310,7 +1322,7 @@ int grid_for(size_t n) {
 // are sampled by one launch per step.
 // ---------------------------------------------------------------------------
 struct BatchGroup {
-  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2, lanes = 0, e_threads = 0;
+  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2, lanes = 0, e_threads = 0, e_producers = 2;
   std::vector<int> members;
   size_t kh_smem = 0, ke_smem = 0;
   int kh_grid = 0, ke_grid = 0;
@@ -1409,7 +1421,7 @@ auto batch_kh_kernel(const BatchGroup& g) {
 template <typename real>
 auto batch_ke_kernel(const BatchGroup& g) {
   using namespace pipe;
-  const bool wide = g.e_threads + 32 * g.producers > kMaxThreads;
+  const bool wide = g.e_threads + 32 * g.e_producers > kMaxThreads;
   if (g.plasma) {
     if (g.maxdeg == 6)
       return wide ? ke_tma_batch<real, true, 6, 0, kWideRegs>
@@ -1453,10 +1465,12 @@ int batch_build(ifdtd_batch* B) {
     key.producers = P->producers;
     key.lanes = P->lanes;
     key.e_threads = P->e_threads;
+    key.e_producers = P->e_producers;
     BatchGroup* g = nullptr;
     for (auto& x : B->groups)
       if (x.plasma == key.plasma && x.maxdeg == key.maxdeg && x.copy == key.copy && x.threads == key.threads &&
-          x.producers == key.producers && x.lanes == key.lanes && x.e_threads == key.e_threads)
+          x.producers == key.producers && x.lanes == key.lanes && x.e_threads == key.e_threads &&
+          x.e_producers == key.e_producers)
         g = &x;
     if (!g) {
       B->groups.push_back(key);
@@ -1486,7 +1500,7 @@ int batch_build(ifdtd_batch* B) {
       ch.push_back(&P->kh_cost);
       ce.push_back(&P->ke_cost);
     }
-    const int threads = g.threads + 32 * g.producers, e_threads = g.e_threads + 32 * g.producers;
+    const int threads = g.threads + 32 * g.producers, e_threads = g.e_threads + 32 * g.e_producers;
     cudaError_t e = batch_grid(batch_kh_kernel<real>(g), threads, g.kh_smem, sm_count, nh, &g.kh_grid);
     if (e == cudaSuccess) e = batch_grid(batch_ke_kernel<real>(g), e_threads, g.ke_smem, sm_count, ne, &g.ke_grid);
     if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batched launch shape: ") + cudaGetErrorString(e));
@@ -1536,7 +1550,7 @@ cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row,
   for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
     const BatchGroup& g = B->groups[q];
     auto k = batch_ke_kernel<real>(g);
-    k<<<g.ke_grid, g.e_threads + 32 * g.producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.producers,
+    k<<<g.ke_grid, g.e_threads + 32 * g.e_producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.e_producers,
                                                                    istep, g.lanes);
     e = cudaGetLastError();
     if (e != cudaSuccess) B->failed = "ke_tma_batch of group " + std::to_string(q);

@@ -9,8 +9,11 @@ Network: an MLP (``depth`` SiLU layers of ``width``) and a projection to a
 ``t0`` x ``c0`` sequence, then non-overlapping 1-D transposed convolutions
 (stride = kernel = ``stride``, SiLU between them, per-tap biases) up to
 ``samples`` outputs.  Activations stay channels-last, so every layer is a
-dense product over rows and one kernel, ``ifdtd_nn_gemm`` (BF16 tensor-core
-inputs, FP32 accumulation), runs all forward and backward products.  Weights
+dense product over rows and one GEMM runs all forward and backward products:
+``ifdtd_nn_gemm_tc`` (tcgen05.mma on the 5th-generation tensor cores, BF16
+inputs, FP32 accumulation in tensor memory) by default, or ``ifdtd_nn_gemm``
+(warp-level mma.sync, the same inputs and accumulation) as the checked
+alternative (``gemm="mma"``).  Weights
 are FP32 masters with BF16 copies; activations between layers are BF16.
 Training uses the library's own kernels for every step (GEMMs, bias + SiLU,
 its derivative, bias sums, mean-squared error, Adam); PyTorch only holds the
@@ -61,12 +64,19 @@ def architecture(inputs: int = 8, width: int = 512, depth: int = 4, samples: int
     return layers
 
 
-class TraceSurrogate:
-    """One network with its parameters, Adam state and activation buffers."""
+GEMM_ENTRIES = {"tcgen05": "ifdtd_nn_gemm_tc", "mma": "ifdtd_nn_gemm"}
 
-    def __init__(self, layers: list[Layer], *, seed: int = 0, device: str = "cuda"):
+
+class TraceSurrogate:
+    """One network with its parameters, Adam state and activation buffers;
+    ``gemm`` picks the product kernel ("tcgen05" or "mma")."""
+
+    def __init__(self, layers: list[Layer], *, seed: int = 0, device: str = "cuda", gemm: str = "tcgen05"):
         import torch
 
+        if gemm not in GEMM_ENTRIES:
+            raise ValueError(f"gemm must be one of {sorted(GEMM_ENTRIES)}")
+        self.gemm_entry = GEMM_ENTRIES[gemm]
         self.torch = torch
         self.device = torch.device(device)
         if self.device.type != "cuda":
@@ -99,8 +109,8 @@ class TraceSurrogate:
         z = None
         for i, L in enumerate(self.layers):
             z = torch.empty((rows, L.fan_out), dtype=torch.float32, device=self.device)
-            _check(lib.ifdtd_nn_gemm(rows, L.fan_out, L.fan_in, inp.data_ptr(), L.fan_in, 0, self.w16[i].data_ptr(), L.fan_in, 1,
-                                     1.0, 0.0, z.data_ptr(), L.fan_out, s), "ifdtd_nn_gemm")
+            _check(getattr(lib, self.gemm_entry)(rows, L.fan_out, L.fan_in, inp.data_ptr(), L.fan_in, 0, self.w16[i].data_ptr(),
+                                                 L.fan_in, 1, 1.0, 0.0, z.data_ptr(), L.fan_out, s), self.gemm_entry)
             last = i == len(self.layers) - 1
             y = None if last else torch.empty((rows, L.fan_out), dtype=torch.bfloat16, device=self.device)
             _check(lib.ifdtd_nn_bias_act(rows, L.fan_out, z.data_ptr(), self.b[i].data_ptr(), L.act, None if last else y.data_ptr(), s),
@@ -127,15 +137,15 @@ class TraceSurrogate:
             _check(lib.ifdtd_nn_act_grad(rows, L.fan_out, z.data_ptr(), dy.data_ptr(), L.act, dz.data_ptr(), dz16.data_ptr(), s),
                    "ifdtd_nn_act_grad")
             gw = torch.empty((L.fan_out, L.fan_in), dtype=torch.float32, device=self.device)
-            _check(lib.ifdtd_nn_gemm(L.fan_out, L.fan_in, rows, dz16.data_ptr(), L.fan_out, 1, x.data_ptr(), L.fan_in, 0,
-                                     1.0, 0.0, gw.data_ptr(), L.fan_in, s), "ifdtd_nn_gemm")
+            _check(getattr(lib, self.gemm_entry)(L.fan_out, L.fan_in, rows, dz16.data_ptr(), L.fan_out, 1, x.data_ptr(), L.fan_in, 0,
+                                                 1.0, 0.0, gw.data_ptr(), L.fan_in, s), self.gemm_entry)
             gb = torch.empty(L.fan_out, dtype=torch.float32, device=self.device)
             _check(lib.ifdtd_nn_col_sum(rows, L.fan_out, dz.data_ptr(), gb.data_ptr(), s), "ifdtd_nn_col_sum")
             self.gw[i], self.gb[i] = gw, gb
             if i > 0:
                 dx = torch.empty((rows, L.fan_in), dtype=torch.float32, device=self.device)
-                _check(lib.ifdtd_nn_gemm(rows, L.fan_in, L.fan_out, dz16.data_ptr(), L.fan_out, 0, self.w16[i].data_ptr(), L.fan_in, 0,
-                                         1.0, 0.0, dx.data_ptr(), L.fan_in, s), "ifdtd_nn_gemm")
+                _check(getattr(lib, self.gemm_entry)(rows, L.fan_in, L.fan_out, dz16.data_ptr(), L.fan_out, 0, self.w16[i].data_ptr(),
+                                                     L.fan_in, 0, 1.0, 0.0, dx.data_ptr(), L.fan_in, s), self.gemm_entry)
                 prev = self.layers[i - 1]
                 dy = dx.view(rows // prev.expand, prev.fan_out)
 
@@ -211,11 +221,12 @@ class SurrogateEnsemble:
 
     @classmethod
     def train(cls, layers: list[Layer], x, y, *, k: int = 4, iterations: int = 1000, batch: int = 256, lr: float = 1e-3,
-              lr_final: float | None = 1e-4, device: str = "cuda", seed: int = 0, relative: bool = False):
+              lr_final: float | None = 1e-4, device: str = "cuda", seed: int = 0, relative: bool = False,
+              gemm: str = "tcgen05"):
         ens = cls()
         histories = []
         for m in range(k):
-            net = TraceSurrogate(layers, seed=seed + 1000 * m, device=device)
+            net = TraceSurrogate(layers, seed=seed + 1000 * m, device=device, gemm=gemm)
             histories.append(net.fit(x, y, iterations=iterations, batch=batch, lr=lr, lr_final=lr_final, seed=seed + m,
                                      relative=relative))
             ens.members.append(net)
@@ -339,3 +350,49 @@ def generate_traces(n_runs: int, *, subdivision: int = 6, radial_cells: int = 40
         params.extend(rows)
         del sims
     return np.asarray(params, dtype=np.float64), np.concatenate(traces, axis=0)
+
+
+def gemm_throughput(m: int, n: int, k: int, *, gemm: str = "tcgen05", reps: int = 20, device: str = "cuda") -> dict:
+    """Time one surrogate GEMM shape (bf16 inputs, fp32 output, C = A B^T as the
+    forward pass calls it) with CUDA events on the current stream: median
+    milliseconds per call over ``reps`` calls after three warm-up calls, the
+    TFLOP/s of 2 m n k, and the relative error against a float32 product."""
+
+    import statistics
+
+    import torch
+
+    if gemm not in GEMM_ENTRIES:
+        raise ValueError(f"gemm must be one of {sorted(GEMM_ENTRIES)}")
+    entry = getattr(_lib(), GEMM_ENTRIES[gemm])
+    g = torch.Generator(device=device).manual_seed(m + 3 * n + 7 * k)
+    a = torch.randn((m, k), device=device, generator=g).to(torch.bfloat16)
+    b = torch.randn((n, k), device=device, generator=g).to(torch.bfloat16)
+    c = torch.empty((m, n), device=device, dtype=torch.float32)
+    s = int(torch.cuda.current_stream(device).cuda_stream)
+
+    def call():
+        _check(entry(m, n, k, a.data_ptr(), k, 0, b.data_ptr(), k, 1, 1.0, 0.0, c.data_ptr(), n, s), GEMM_ENTRIES[gemm])
+
+    for _ in range(3):
+        call()
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+    marks[0].record()
+    for i in range(reps):
+        call()
+        marks[i + 1].record()
+    torch.cuda.synchronize()
+    ms = statistics.median(marks[i].elapsed_time(marks[i + 1]) for i in range(reps))
+    ref = a.float() @ b.float().T
+    err = float((c - ref).norm() / ref.norm())
+    return {"m": m, "n": n, "k": k, "gemm": gemm, "ms": ms, "tflops": 2.0 * m * n * k / (ms / 1e3) / 1e12, "rel_err": err}
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    # python -m ionosphere_fdtd_b200.surrogate M N K [tcgen05|mma]: one GEMM timing line
+    shape = [int(v) for v in sys.argv[1:4]] if len(sys.argv) >= 4 else [4096, 4096, 4096]
+    kind = sys.argv[4] if len(sys.argv) >= 5 else "tcgen05"
+    print(json.dumps(gemm_throughput(*shape, gemm=kind)))

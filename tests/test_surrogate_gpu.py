@@ -17,9 +17,15 @@ def _bf16(t):
     return t.to(torch.bfloat16)
 
 
-@pytest.mark.parametrize("m,n,k", [(70, 45, 37), (1, 130, 8), (300, 4, 520), (64, 64, 64)])
+@pytest.mark.parametrize("entry", ["ifdtd_nn_gemm_tc", "ifdtd_nn_gemm"])
+@pytest.mark.parametrize("m,n,k", [(70, 45, 37), (1, 130, 8), (300, 4, 520), (64, 64, 64), (257, 300, 200), (128, 128, 128)])
 @pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
-def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb):
+def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb, entry):
+    """Both GEMMs (tcgen05.mma with the accumulator in tensor memory, and the
+    warp-level mma.sync) against a float64 product of the same bf16 inputs:
+    ragged shapes, several 128 x 128 tiles, K over many 64-wide chunks (the
+    two-stage ring reused), all transposes, alpha and beta."""
+
     import torch
 
     from ionosphere_fdtd_b200 import _native as N
@@ -30,22 +36,27 @@ def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb):
     c0 = torch.randn((m, n), device="cuda", generator=g)
     c = c0.clone()
     stream = torch.cuda.current_stream().cuda_stream
-    N.check(N.load().ifdtd_nn_gemm(m, n, k, a.data_ptr(), a.shape[1], ta, b.data_ptr(), b.shape[1], tb, 0.5, 2.0,
-                                   c.data_ptr(), n, stream), "ifdtd_nn_gemm")
+    N.check(getattr(N.load(), entry)(m, n, k, a.data_ptr(), a.shape[1], ta, b.data_ptr(), b.shape[1], tb, 0.5, 2.0,
+                                     c.data_ptr(), n, stream), entry)
     A = (a.float().T if ta else a.float()).double()
     B = (b.float().T if tb else b.float()).double()
     expected = 0.5 * (A @ B) + 2.0 * c0.double()
     err = (c.double() - expected).norm() / expected.norm()
     assert float(err) < 1e-6
+    if entry == "ifdtd_nn_gemm_tc":
+        status = N.C.c_int32(-1)
+        N.check(N.load().ifdtd_nn_gemm_tc_status(1, N.C.byref(status)), "ifdtd_nn_gemm_tc_status")
+        assert status.value == 0
 
 
-def test_forward_and_backward_match_the_cpu_oracle():
+@pytest.mark.parametrize("gemm", ["tcgen05", "mma"])
+def test_forward_and_backward_match_the_cpu_oracle(gemm):
     import torch
 
     from ionosphere_fdtd_b200.surrogate import TraceSurrogate, architecture
 
     layers = architecture(inputs=8, width=48, depth=3, samples=64, t0=4, c0=8, channels=(4, 1), stride=4)
-    net = TraceSurrogate(layers, seed=5)
+    net = TraceSurrogate(layers, seed=5, gemm=gemm)
     rng = np.random.default_rng(1)
     x = rng.standard_normal((6, 8))
     t = rng.standard_normal((6, 64)) * 0.1
