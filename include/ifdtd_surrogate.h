@@ -30,6 +30,14 @@ int32_t ifdtd_nn_gemm(int32_t m, int32_t n, int32_t k, const void* a, int32_t ld
  * memory.  Same arguments and result as ifdtd_nn_gemm up to fp32 rounding of the accumulation. */
 int32_t ifdtd_nn_gemm_tc(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
                          int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream);
+/* ifdtd_nn_gemm_tc with a caller-owned device workspace (workspace_bytes may be 0): when the
+ * output tiles would leave most SMs idle and K is long (the weight gradients of the decoder, whose K
+ * is the number of rows), K is split over CTAs that write fp32 partial tiles into the workspace
+ * (at most workspace_bytes / (4 m n) splits), and a second kernel adds them in split order, so the
+ * result is the same on every run.  Calls that share a workspace must not overlap on the GPU. */
+int32_t ifdtd_nn_gemm_tc_ws(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
+                            int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* workspace,
+                            int64_t workspace_bytes, void* stream);
 /* Status word of ifdtd_nn_gemm_tc: bit 0 set when an mbarrier wait ran out its 0.2 s bound (that
  * call's result is then invalid).  Reading it synchronises the device; reset != 0 clears it. */
 int32_t ifdtd_nn_gemm_tc_status(int32_t reset, int32_t* out);

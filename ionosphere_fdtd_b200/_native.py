@@ -137,6 +137,8 @@ _SIGNATURES = {
     "ifdtd_max_abs": ([_vp, C.POINTER(State), _vp, _vp], _i32),
     "ifdtd_nn_gemm": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp], _i32),
     "ifdtd_nn_gemm_tc": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp], _i32),
+    "ifdtd_nn_gemm_tc_ws": ([_i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _i32, C.c_float, C.c_float, _vp, _i32, _vp, C.c_int64, _vp],
+                            _i32),
     "ifdtd_nn_gemm_tc_status": ([_i32, C.POINTER(_i32)], _i32),
     "ifdtd_nn_bias_act": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp], _i32),
     "ifdtd_nn_act_grad": ([_i32, _i32, _vp, _vp, _i32, _vp, _vp, _vp], _i32),

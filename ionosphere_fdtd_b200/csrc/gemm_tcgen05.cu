@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 
 #include "../../include/ifdtd_surrogate.h"
@@ -117,10 +118,14 @@ __device__ __forceinline__ uint4 load_piece(const __nv_bfloat16* __restrict__ X,
   return v;
 }
 
+// Split K (blockIdx.z = split, kps chunks each): with `partial` set, CTA z
+// writes its raw tile sums to partial[z] (M x N, leading dimension N) and a
+// second kernel adds the splits in order; otherwise kps covers all chunks and
+// the CTA writes alpha * acc + beta * C.
 __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
                                                         int lda, int ta, const __nv_bfloat16* __restrict__ B, int ldb,
                                                         int tb, float alpha, float beta, float* __restrict__ C,
-                                                        int ldc) {
+                                                        int ldc, int kps, float* __restrict__ partial) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t mma_done[STAGES];
   __shared__ uint32_t tmem_slot;
@@ -146,7 +151,8 @@ __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, con
   const uint32_t tmem = tmem_slot;
   const bool vec_a = !ta && lda % 8 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0;
   const bool vec_b = tb && ldb % 8 == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
-  const int nk = (K + TK - 1) / TK;
+  const int c_first = blockIdx.z * kps;
+  const int nk = max(0, min((K + TK - 1) / TK - c_first, kps));  // this split's chunks
   int issued = 0;  // chunks whose MMAs were issued (thread 0)
   for (int c = 0; c < nk; ++c) {
     const int s = c % STAGES;
@@ -156,7 +162,7 @@ __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, con
     if (abort_flag) break;
     unsigned char* as = smem + s * STAGE_BYTES;
     unsigned char* bs = as + A_BYTES;
-    const int k0 = c * TK;
+    const int k0 = (c_first + c) * TK;
     // piece p: row (p >> 6) * 8 + (p & 7), k-group (p >> 3) & 7, so consecutive
     // threads fill consecutive 16-byte slots of one core matrix
     for (int p = threadIdx.x; p < TM * (TK / 8); p += THREADS) {
@@ -191,6 +197,7 @@ __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, con
   // every thread waits for the last issued chunk's commit (it covers all earlier MMAs)
   __syncthreads();
   const int done_chunks = abort_flag ? -1 : nk;
+  if (nk == 0 && threadIdx.x == 0) abort_flag = 1;  // an empty split (not launched by the host) writes nothing
   bool ok = true;
   if (done_chunks > 0) {
     const int last = nk - 1;
@@ -216,7 +223,12 @@ __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, con
             "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(lane_base + (uint32_t)cb));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
+      if (row < M && partial) {
+        float* prow = partial + ((size_t)blockIdx.z * M + row) * N;
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (n0 + cb + q < N) prow[n0 + cb + q] = __uint_as_float(r[q]);
+      } else if (row < M) {
         float* crow = C + (size_t)row * ldc;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
@@ -237,28 +249,71 @@ __global__ void __launch_bounds__(THREADS) gemm_tcgen05(int M, int N, int K, con
   }
 }
 
+// C = alpha * (sum of the splits' partial tiles, in split order) + beta * C.
+__global__ void splitk_reduce(int M, int N, int splits, const float* __restrict__ partial, float alpha, float beta,
+                              float* __restrict__ C, int ldc) {
+  const size_t n = (size_t)M * N;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    float acc = partial[i];
+    for (int z = 1; z < splits; ++z) acc += partial[(size_t)z * n + i];
+    const size_t row = i / N, col = i - row * N;
+    float* p = C + row * ldc + col;
+    const float v = alpha * acc;
+    *p = beta == 0.f ? v : v + beta * *p;
+  }
+}
+
+// Splits of K for a product of `tiles` output tiles and nk chunks of 64: only
+// when the tiles leave most SMs idle and K is long, at least 4 chunks per
+// split, at most 2 CTAs per SM in total, within the workspace.
+int choose_splits(int tiles, int nk, size_t mn, size_t workspace_bytes) {
+  if (workspace_bytes == 0 || tiles >= 74 || nk < 8) return 1;
+  int s = std::min(nk / 4, std::max(1, 296 / tiles));
+  s = (int)std::min<size_t>((size_t)s, workspace_bytes / (mn * sizeof(float)));
+  return std::max(1, s);
+}
+
 }  // namespace tc
 }  // namespace ifdtd
 
 extern "C" {
 
-int32_t ifdtd_nn_gemm_tc(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
-                         int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream) {
+int32_t ifdtd_nn_gemm_tc_ws(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
+                            int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* workspace,
+                            int64_t workspace_bytes, void* stream) {
   using namespace ifdtd::tc;
   if (m <= 0 || n <= 0 || k <= 0 || !a || !b || !c) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad gemm shape");
   if (lda < (trans_a ? m : k) || ldb < (trans_b ? k : n) || ldc < n)
     return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm leading dimension too small");
   if ((n + TN - 1) / TN > 65535) return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "gemm has too many columns");
+  if (workspace_bytes < 0 || (workspace_bytes > 0 && !workspace))
+    return ifdtd::record_error(IFDTD_ERR_ARGUMENT, "bad gemm workspace");
   // the opt-in above 48 KiB of dynamic shared memory holds per device; setting it is cheap
   cudaError_t e = cudaFuncSetAttribute(gemm_tcgen05, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05 attribute: ") + cudaGetErrorString(e));
-  const dim3 grid((m + TM - 1) / TM, (n + TN - 1) / TN);
-  gemm_tcgen05<<<grid, THREADS, SMEM_BYTES, (cudaStream_t)stream>>>(m, n, k, (const __nv_bfloat16*)a, lda, trans_a != 0,
-                                                                      (const __nv_bfloat16*)b, ldb, trans_b != 0, alpha,
-                                                                      beta, c, ldc);
+  const int tm = (m + TM - 1) / TM, tn = (n + TN - 1) / TN, nk = (k + TK - 1) / TK;
+  const int want = choose_splits(tm * tn, nk, (size_t)m * n, (size_t)workspace_bytes);
+  const int kps = (nk + want - 1) / want, splits = (nk + kps - 1) / kps;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* partial = splits > 1 ? static_cast<float*>(workspace) : nullptr;
+  gemm_tcgen05<<<dim3(tm, tn, splits), THREADS, SMEM_BYTES, st>>>(m, n, k, (const __nv_bfloat16*)a, lda, trans_a != 0,
+                                                                  (const __nv_bfloat16*)b, ldb, trans_b != 0, alpha,
+                                                                  beta, c, ldc, kps, partial);
   e = cudaGetLastError();
   if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05: ") + cudaGetErrorString(e));
+  if (partial) {
+    const size_t mn = (size_t)m * n;
+    const int blocks = (int)std::min<size_t>((mn + 255) / 256, 148 * 8);
+    splitk_reduce<<<blocks, 256, 0, st>>>(m, n, splits, partial, alpha, beta, c, ldc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("splitk_reduce: ") + cudaGetErrorString(e));
+  }
   return IFDTD_OK;
+}
+
+int32_t ifdtd_nn_gemm_tc(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
+                         int32_t ldb, int32_t trans_b, float alpha, float beta, float* c, int32_t ldc, void* stream) {
+  return ifdtd_nn_gemm_tc_ws(m, n, k, a, lda, trans_a, b, ldb, trans_b, alpha, beta, c, ldc, nullptr, 0, stream);
 }
 
 int32_t ifdtd_nn_gemm_tc_status(int32_t reset, int32_t* out) {

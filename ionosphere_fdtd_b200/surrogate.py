@@ -64,7 +64,8 @@ def architecture(inputs: int = 8, width: int = 512, depth: int = 4, samples: int
     return layers
 
 
-GEMM_ENTRIES = {"tcgen05": "ifdtd_nn_gemm_tc", "mma": "ifdtd_nn_gemm"}
+GEMM_ENTRIES = {"tcgen05": "ifdtd_nn_gemm_tc_ws", "mma": "ifdtd_nn_gemm"}
+WORKSPACE_BYTES = 16 << 20  # split-K partial tiles of the tcgen05 GEMM
 
 
 class TraceSurrogate:
@@ -78,6 +79,7 @@ class TraceSurrogate:
             raise ValueError(f"gemm must be one of {sorted(GEMM_ENTRIES)}")
         self.gemm_entry = GEMM_ENTRIES[gemm]
         self.torch = torch
+        self._workspace = None
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("the surrogate kernels run on a CUDA device")
@@ -98,6 +100,18 @@ class TraceSurrogate:
     def _stream(self) -> int:
         return int(self.torch.cuda.current_stream(self.device).cuda_stream)
 
+    def _gemm(self, m, n, k, a, lda, ta, b, ldb, tb, c, ldc) -> None:
+        """c = op(a) op(b) with the network's product kernel (bf16 in, fp32 out)."""
+
+        lib, s = _lib(), self._stream()
+        if self.gemm_entry == "ifdtd_nn_gemm":
+            _check(lib.ifdtd_nn_gemm(m, n, k, a, lda, ta, b, ldb, tb, 1.0, 0.0, c, ldc, s), "ifdtd_nn_gemm")
+            return
+        if self._workspace is None:
+            self._workspace = self.torch.empty(WORKSPACE_BYTES // 4, dtype=self.torch.float32, device=self.device)
+        _check(lib.ifdtd_nn_gemm_tc_ws(m, n, k, a, lda, ta, b, ldb, tb, 1.0, 0.0, c, ldc, self._workspace.data_ptr(), WORKSPACE_BYTES, s),
+               "ifdtd_nn_gemm_tc_ws")
+
     def forward(self, x16):
         """x16: (B, inputs) bf16 device tensor -> (B, samples) fp32 predictions."""
 
@@ -109,8 +123,7 @@ class TraceSurrogate:
         z = None
         for i, L in enumerate(self.layers):
             z = torch.empty((rows, L.fan_out), dtype=torch.float32, device=self.device)
-            _check(getattr(lib, self.gemm_entry)(rows, L.fan_out, L.fan_in, inp.data_ptr(), L.fan_in, 0, self.w16[i].data_ptr(),
-                                                 L.fan_in, 1, 1.0, 0.0, z.data_ptr(), L.fan_out, s), self.gemm_entry)
+            self._gemm(rows, L.fan_out, L.fan_in, inp.data_ptr(), L.fan_in, 0, self.w16[i].data_ptr(), L.fan_in, 1, z.data_ptr(), L.fan_out)
             last = i == len(self.layers) - 1
             y = None if last else torch.empty((rows, L.fan_out), dtype=torch.bfloat16, device=self.device)
             _check(lib.ifdtd_nn_bias_act(rows, L.fan_out, z.data_ptr(), self.b[i].data_ptr(), L.act, None if last else y.data_ptr(), s),
@@ -137,15 +150,14 @@ class TraceSurrogate:
             _check(lib.ifdtd_nn_act_grad(rows, L.fan_out, z.data_ptr(), dy.data_ptr(), L.act, dz.data_ptr(), dz16.data_ptr(), s),
                    "ifdtd_nn_act_grad")
             gw = torch.empty((L.fan_out, L.fan_in), dtype=torch.float32, device=self.device)
-            _check(getattr(lib, self.gemm_entry)(L.fan_out, L.fan_in, rows, dz16.data_ptr(), L.fan_out, 1, x.data_ptr(), L.fan_in, 0,
-                                                 1.0, 0.0, gw.data_ptr(), L.fan_in, s), self.gemm_entry)
+            self._gemm(L.fan_out, L.fan_in, rows, dz16.data_ptr(), L.fan_out, 1, x.data_ptr(), L.fan_in, 0, gw.data_ptr(), L.fan_in)
             gb = torch.empty(L.fan_out, dtype=torch.float32, device=self.device)
             _check(lib.ifdtd_nn_col_sum(rows, L.fan_out, dz.data_ptr(), gb.data_ptr(), s), "ifdtd_nn_col_sum")
             self.gw[i], self.gb[i] = gw, gb
             if i > 0:
                 dx = torch.empty((rows, L.fan_in), dtype=torch.float32, device=self.device)
-                _check(getattr(lib, self.gemm_entry)(rows, L.fan_in, L.fan_out, dz16.data_ptr(), L.fan_out, 0, self.w16[i].data_ptr(),
-                                                     L.fan_in, 0, 1.0, 0.0, dx.data_ptr(), L.fan_in, s), self.gemm_entry)
+                self._gemm(rows, L.fan_in, L.fan_out, dz16.data_ptr(), L.fan_out, 0, self.w16[i].data_ptr(), L.fan_in, 0, dx.data_ptr(),
+                           L.fan_in)
                 prev = self.layers[i - 1]
                 dy = dx.view(rows // prev.expand, prev.fan_out)
 
@@ -364,15 +376,21 @@ def gemm_throughput(m: int, n: int, k: int, *, gemm: str = "tcgen05", reps: int 
 
     if gemm not in GEMM_ENTRIES:
         raise ValueError(f"gemm must be one of {sorted(GEMM_ENTRIES)}")
-    entry = getattr(_lib(), GEMM_ENTRIES[gemm])
+    lib = _lib()
     g = torch.Generator(device=device).manual_seed(m + 3 * n + 7 * k)
     a = torch.randn((m, k), device=device, generator=g).to(torch.bfloat16)
     b = torch.randn((n, k), device=device, generator=g).to(torch.bfloat16)
     c = torch.empty((m, n), device=device, dtype=torch.float32)
     s = int(torch.cuda.current_stream(device).cuda_stream)
 
+    ws = torch.empty(WORKSPACE_BYTES // 4, dtype=torch.float32, device=device)
+
     def call():
-        _check(entry(m, n, k, a.data_ptr(), k, 0, b.data_ptr(), k, 1, 1.0, 0.0, c.data_ptr(), n, s), GEMM_ENTRIES[gemm])
+        if gemm == "mma":
+            _check(lib.ifdtd_nn_gemm(m, n, k, a.data_ptr(), k, 0, b.data_ptr(), k, 1, 1.0, 0.0, c.data_ptr(), n, s), "ifdtd_nn_gemm")
+        else:
+            _check(lib.ifdtd_nn_gemm_tc_ws(m, n, k, a.data_ptr(), k, 0, b.data_ptr(), k, 1, 1.0, 0.0, c.data_ptr(), n, ws.data_ptr(),
+                                           WORKSPACE_BYTES, s), "ifdtd_nn_gemm_tc_ws")
 
     for _ in range(3):
         call()

@@ -49,6 +49,34 @@ def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb, entry)
         assert status.value == 0
 
 
+@pytest.mark.parametrize("m,n,k,ta,tb", [(4, 16, 65536, 1, 0), (64, 200, 3000, 1, 0), (32, 4, 20000, 0, 1), (130, 70, 1024, 0, 0)])
+def test_split_k_gemm_matches_float32_product_and_repeats_bitwise(m, n, k, ta, tb):
+    """The tcgen05 GEMM with a workspace splits a long K over CTAs (the decoder's
+    weight gradients have K = rows) and adds the partial tiles in split order:
+    the product of the float64 reference to 1e-6, and the same bits on every run."""
+
+    import torch
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    a = _bf16(torch.randn((k, m) if ta else (m, k), device="cuda", generator=g))
+    b = _bf16(torch.randn((n, k) if tb else (k, n), device="cuda", generator=g))
+    ws = torch.empty(4 << 20, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    outs = []
+    for _ in range(2):
+        c = torch.full((m, n), 3.0, device="cuda")
+        N.check(N.load().ifdtd_nn_gemm_tc_ws(m, n, k, a.data_ptr(), a.shape[1], ta, b.data_ptr(), b.shape[1], tb, 0.5, -1.0,
+                                             c.data_ptr(), n, ws.data_ptr(), ws.numel() * 4, stream), "ifdtd_nn_gemm_tc_ws")
+        outs.append(c)
+    A = (a.float().T if ta else a.float()).double()
+    B = (b.float().T if tb else b.float()).double()
+    expected = 0.5 * (A @ B) - 3.0
+    assert float((outs[0].double() - expected).norm() / expected.norm()) < 1e-6
+    assert torch.equal(outs[0], outs[1])
+
+
 @pytest.mark.parametrize("gemm", ["tcgen05", "mma"])
 def test_forward_and_backward_match_the_cpu_oracle(gemm):
     import torch
