@@ -356,7 +356,7 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
                   const std::vector<int>& ps_face, const std::vector<real>& ps_coef, const std::vector<real>& ps_wc,
                   const std::vector<real>& inv_phi, const std::vector<real>& tn, bool plasma, int Pn, int Pm,
                   const std::vector<char>& v_src, const std::vector<char>& e_src, std::vector<int>& locA,
-                  std::vector<int>& locB, int max_stage) {
+                  std::vector<int>& locB, int max_stage, int min_gap) {
   using namespace pipe;
   const int rb = (int)sizeof(real);
   std::vector<int> h_ids, f_ids, v_ids, vloc;
@@ -389,7 +389,9 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
     sort_unique(h_ids);
     sort_unique(f_ids);
     make_runs(v_ids, 0, v_runs, vloc);
-    int gap = 0, n_h = 0, n_f = 0, nd = 0;
+    // gaps of up to min_gap rows are always bridged (fewer, longer copies for
+    // a few unread rows); wider ones only while the patch has too many copies
+    int gap = min_gap, n_h = 0, n_f = 0, nd = 0;
     for (;;) {
       n_h = make_runs(h_ids, gap, h_runs, locA);
       n_f = make_runs(f_ids, gap, f_runs, locB);
@@ -505,6 +507,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     return fail(IFDTD_ERR_ARGUMENT, "e_threads must be 0 or a multiple of 32 with e_threads + 32 * E producer warps <= 640");
   if (e_threads_req + 32 * e_producers > pipe::kMaxThreads && staging == 3)
     return fail(IFDTD_ERR_ARGUMENT, "wide E-phase CTAs (e_threads + 32 * E producer warps > 384) use TMA bulk copies only");
+  const int e_copy_gap = tune ? tune->e_copy_gap : 0;
+  if (e_copy_gap < 0 || e_copy_gap > 8) return fail(IFDTD_ERR_ARGUMENT, "e_copy_gap must be 0 to 8");
   const int e_stages_req = tune ? tune->e_stages : 0;
   if (e_stages_req != 0 && (e_stages_req < 2 || e_stages_req > 4))
     return fail(IFDTD_ERR_ARGUMENT, "e_stages must be 0 (auto) or 2 to 4");
@@ -990,14 +994,16 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     for (int s = 0; s < X->n_src_et; ++s) e_src[X->src_et_edge[s]] = 1;
     for (const int c : e_try) {
       const int stages_wanted = c < 0 ? -c : 2;
-      Own o = c < 0 ? ownership_bounds(balanced_e_bounds(stage_budget / stages_wanted * 97 / 100, plasma, (int)sizeof(real)))
+      // bridged gaps add rows the balance does not count: leave them room
+      const int margin = 97 - 3 * e_copy_gap;
+      Own o = c < 0 ? ownership_bounds(balanced_e_bounds(stage_budget / stages_wanted * margin / 100, plasma, (int)sizeof(real)))
                     : ownership(c);
       Slots sl;
       if (!build_slots(o.vlist, sl)) break;
       PipeTables t;
       const bool ok = build_pipe_e<real>(t, o.n, o.vptr, o.vlist, o.eptr, lr, SW, sl.edge, sl.face, sl.coef, sl.wc,
                                          inv_phi, tn, plasma, Pn, Pm, v_src, e_src, locA, locB,
-                                         stage_budget / stages_wanted);
+                                         stage_budget / stages_wanted, e_copy_gap);
       if (ok && stages_wanted * t.stage_bytes <= stage_budget) {
         P->pipe_e_ok = true;
         fpp_e = c > 0 ? c : 0;

@@ -48,9 +48,10 @@ class Tuning:
     across lanes; 2, every row starting on an 8-lane boundary), the compute
     threads of an E-phase CTA (0: as ``threads``; above 384 minus the producer
     warps the E phase runs wide CTAs of at most 640 threads at 96 registers)
-    the ring stages the balanced E patches are sized for (0: 2), and the
-    copy-issuing warps of an E-phase CTA (0: as ``producer_warps``).  Every
-    choice computes the same bits."""
+    the ring stages the balanced E patches are sized for (0: 2), the
+    copy-issuing warps of an E-phase CTA (0: as ``producer_warps``), and the
+    row gaps every E-phase copy bridges (0-8: fewer, longer bulk copies).
+    Every choice computes the same bits."""
 
     faces_per_patch: int = 0
     threads: int = 0
@@ -62,6 +63,7 @@ class Tuning:
     e_threads: int = 0
     e_stages: int = 0
     e_producer_warps: int = 0
+    e_copy_gap: int = 0
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -172,7 +174,7 @@ class Engine:
             pd.vertex_face_weights = f64(p["vertex_face_weights"])
         t = self.tuning
         td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps, t.lane_layout,
-                      t.e_threads, t.e_stages, t.e_producer_warps)
+                      t.e_threads, t.e_stages, t.e_producer_warps, t.e_copy_gap)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(

@@ -305,7 +305,7 @@ def _destination(lat_deg: float, lon_deg: float, bearing_deg: float, distance_de
 
 def generate_traces(n_runs: int, *, subdivision: int = 6, radial_cells: int = 40, steps: int = 1024, receivers: int = 16,
                     distance_deg: tuple[float, float] = (2.0, 12.0), seed: int = 20260805, batch_members: int = 32,
-                    device: str = "cuda", dtype: str = "float32"):
+                    device: str = "cuda", dtype: str = "float32", workers: int | None = None):
     """Run ``n_runs`` seeded members at one mesh level and radial grid through
     ``Ensemble`` and return raw parameters (n_runs * receivers, 8) and surface
     Er traces (n_runs * receivers, steps).  Each member draws sigma0, h0, zeta
@@ -313,7 +313,12 @@ def generate_traces(n_runs: int, *, subdivision: int = 6, radial_cells: int = 40
     vertex at random; its Gaussian source pulse sits inside the window, and its
     receivers lie at random bearings and at great-circle distances within
     ``distance_deg`` of the source, close enough for the pulse to reach them
-    within ``steps`` steps."""
+    within ``steps`` steps.  The draws are made in member order from one seeded
+    generator; the members of a batch are then built on ``workers`` host
+    threads (default: up to 8), which changes no value."""
+
+    import os
+    from concurrent.futures import ThreadPoolExecutor
 
     from .constants import EPSILON_0
     from .ensemble import Ensemble
@@ -329,38 +334,47 @@ def generate_traces(n_runs: int, *, subdivision: int = 6, radial_cells: int = 40
     # the time step depends on the mesh and radial grid only, so one material-free
     # run gives the window that places every source pulse
     window = steps * GeodesicFDTD(cfg, mesh=mesh, device=device, dtype=dtype).time_step_s
+    workers = workers or max(1, min(8, os.cpu_count() or 1))
+
+    def build(draw):
+        sigma0, h0, zeta, ground, lat, lon, bearings, distances = draw
+        material = EarthIonosphereMaterial(lithosphere_conductivity_s_m=ground, ionosphere_reference_height_m=h0,
+                                           ionosphere_scale_height_m=zeta, ionosphere_prefactor_hz=sigma0 / EPSILON_0)
+        source = GaussianCurrent(latitude_deg=lat, longitude_deg=lon, peak_current_a=1.0e6, carrier_frequency_hz=0.0,
+                                 center_time_s=0.35 * window, one_over_e_half_width_s=0.12 * window)
+        sim = GeodesicFDTD(cfg, material=material, source=source, mesh=mesh, device=device, dtype=dtype)
+        rows, supports = [], []
+        for b, d in zip(bearings, distances):
+            rlat, rlon = _destination(lat, lon, b, d)
+            supports.append(geographic_distribution(sim, rlat, rlon, 0.0))
+            rows.append((np.log10(sigma0), h0 / 1e3, zeta / 1e3, np.log10(ground), lat, lon, rlat, rlon))
+        v = np.stack([r[0] for r in supports]).astype(np.int64)
+        k = np.asarray([r[1] for r in supports], dtype=np.int64)
+        w = np.stack([r[2] for r in supports])
+        return sim, (v, k, w), rows
+
     params, traces = [], []
-    for start in range(0, n_runs, batch_members):
-        sims, obs, rows = [], [], []
-        for _ in range(min(batch_members, n_runs - start)):
-            sigma0 = 10.0 ** rng.uniform(-8.0, -6.0)
-            h0 = rng.uniform(55_000.0, 70_000.0)
-            zeta = rng.uniform(3_000.0, 6_000.0)
-            ground = 10.0 ** rng.uniform(-3.0, -1.0)
-            lat, lon = vertex_lat_lon(mesh.vertices, int(rng.integers(mesh.n_vertices)))
-            bearings = rng.uniform(0.0, 360.0, receivers)
-            distances = rng.uniform(distance_deg[0], distance_deg[1], receivers)
-            material = EarthIonosphereMaterial(lithosphere_conductivity_s_m=ground, ionosphere_reference_height_m=h0,
-                                               ionosphere_scale_height_m=zeta, ionosphere_prefactor_hz=sigma0 / EPSILON_0)
-            source = GaussianCurrent(latitude_deg=lat, longitude_deg=lon, peak_current_a=1.0e6, carrier_frequency_hz=0.0,
-                                     center_time_s=0.35 * window, one_over_e_half_width_s=0.12 * window)
-            sim = GeodesicFDTD(cfg, material=material, source=source, mesh=mesh, device=device, dtype=dtype)
-            supports = []
-            for b, d in zip(bearings, distances):
-                rlat, rlon = _destination(lat, lon, b, d)
-                supports.append(geographic_distribution(sim, rlat, rlon, 0.0))
-                rows.append((np.log10(sigma0), h0 / 1e3, zeta / 1e3, np.log10(ground), lat, lon, rlat, rlon))
-            v = np.stack([r[0] for r in supports]).astype(np.int64)
-            k = np.asarray([r[1] for r in supports], dtype=np.int64)
-            w = np.stack([r[2] for r in supports])
-            sims.append(sim)
-            obs.append((v, k, w))
-        with Ensemble(sims) as ens:
-            out = ens.record_er_observations(obs, steps)
-        for t in out:
-            traces.append(np.asarray(t[1:], dtype=np.float64).T)  # (receivers, steps)
-        params.extend(rows)
-        del sims
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        for start in range(0, n_runs, batch_members):
+            draws = []
+            for _ in range(min(batch_members, n_runs - start)):
+                sigma0 = 10.0 ** rng.uniform(-8.0, -6.0)
+                h0 = rng.uniform(55_000.0, 70_000.0)
+                zeta = rng.uniform(3_000.0, 6_000.0)
+                ground = 10.0 ** rng.uniform(-3.0, -1.0)
+                lat, lon = vertex_lat_lon(mesh.vertices, int(rng.integers(mesh.n_vertices)))
+                bearings = rng.uniform(0.0, 360.0, receivers)
+                distances = rng.uniform(distance_deg[0], distance_deg[1], receivers)
+                draws.append((sigma0, h0, zeta, ground, lat, lon, bearings, distances))
+            built = list(pool.map(build, draws))
+            sims = [b[0] for b in built]
+            with Ensemble(sims) as ens:
+                out = ens.record_er_observations([b[1] for b in built], steps)
+            for t in out:
+                traces.append(np.asarray(t[1:], dtype=np.float64).T)  # (receivers, steps)
+            for b in built:
+                params.extend(b[2])
+            del sims, built
     return np.asarray(params, dtype=np.float64), np.concatenate(traces, axis=0)
 
 

@@ -184,7 +184,8 @@ def test_lane_layouts_agree_bitwise(name, dtype):
 @pytest.mark.parametrize("tuning", [dict(e_threads=576), dict(e_threads=608, producer_warps=1, lane_layout=2),
                                     dict(e_stages=3), dict(e_stages=3, e_threads=544, producer_warps=3),
                                     dict(e_producer_warps=3), dict(e_producer_warps=4, producer_warps=1),
-                                    dict(e_producer_warps=1, e_threads=576)])
+                                    dict(e_producer_warps=1, e_threads=576), dict(e_copy_gap=2, e_producer_warps=4),
+                                    dict(e_copy_gap=8)])
 @pytest.mark.parametrize("dtype", ["float32", "float64"])
 @pytest.mark.parametrize("name", ["config4_mini_s2", "plasma_magnetized_s1", "adaptive_plasma_si_s1", "tangential_s1"])
 def test_wide_e_ctas_and_deeper_e_rings_agree_bitwise(name, dtype, tuning):
