@@ -602,8 +602,8 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
     y = torch.tensor(traces / scale, dtype=torch.float32, device=device)
     n_train = args.runs * receivers
     shape, stride, chans = args.decoder.split(":")
-    t0, c0 = (int(v) for v in shape.split("x"))
-    layers = architecture(samples=steps, t0=t0, c0=c0, channels=tuple(int(c) for c in chans.split(",")), stride=int(stride))
+    seq0, c0 = (int(v) for v in shape.split("x"))
+    layers = architecture(samples=steps, t0=seq0, c0=c0, channels=tuple(int(c) for c in chans.split(",")), stride=int(stride))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     # each trace weighted by the inverse of its mean square: the loss is the
@@ -677,7 +677,7 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
         "data": "synthetic (engine-generated traces)",
         "config": {
             "workload": "config5", "subdivision": 6, "radial_cells": 40, "samples": steps, "receivers_per_run": receivers,
-            "train_runs": args.runs, "eval_runs": args.eval_runs, "network": f"MLP 8-512x4 + transposed-conv decoder ({t0}x{c0}, stride {stride}, channels {chans} -> 1024)",
+            "train_runs": args.runs, "eval_runs": args.eval_runs, "network": f"MLP 8-512x4 + transposed-conv decoder ({seq0}x{c0}, stride {stride}, channels {chans} -> 1024)",
             "ensemble": 4, "iterations": args.iterations, "batch": args.batch, "loss": "per-trace relative squared error",
             "gemm": args.gemm, "parallelism": f"replicas x{world}",
         },

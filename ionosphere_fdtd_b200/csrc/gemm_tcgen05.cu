@@ -20,6 +20,8 @@
 // skips its remaining chunks and its epilogue, waits (again bounded) for the
 // MMAs it issued, frees its tensor memory and returns.  No operand is another
 // GPU's memory and no copy uses cluster multicast.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -276,6 +278,200 @@ int choose_splits(int tiles, int nk, size_t mn, size_t workspace_bytes) {
 }  // namespace tc
 }  // namespace ifdtd
 
+
+// ---------------------------------------------------------------------------
+// TMA-fed kernel for the K-major / K-major case (op(A) = A row-major M x K,
+// op(B) = B^T with B row-major N x K: the forward products of the surrogate
+// and square benchmark products).  One CTA of 6 warps computes a 128 x 256
+// tile; the accumulator takes 256 TMEM columns.  Warp 0 (one lane) streams
+// 64-wide K chunks of A (128 x 64) and B (256 x 64) with 2-D TMA tile loads
+// (128-byte swizzle, zero fill outside the matrices) into a 4-stage ring,
+// completing on the stage's "full" mbarrier by transaction count; warp 1 (one
+// lane) waits on "full", issues four tcgen05.mma (M 128, N 256, K 16) per
+// chunk and commits them to the stage's "empty" mbarrier, which frees the
+// stage for the producer; after the last chunk it commits to "done".  Warps
+// 2-5 wait on "done" and read the accumulator with tcgen05.ld, each from the
+// 32 TMEM lanes of its warp index modulo 4.  Every wait is bounded as in the
+// generic kernel; a wait that runs out sets the status bit, the roles stop
+// issuing, and the CTA waits (bounded) for the MMAs it issued before it frees
+// the tensor memory.  Loads read this GPU's memory only, without multicast.
+// ---------------------------------------------------------------------------
+namespace ifdtd {
+namespace tc {
+
+constexpr int XM = 128, XN = 256, XK = 64, XSTAGES = 4, XTHREADS = 192;
+constexpr int XA_BYTES = XM * XK * 2, XB_BYTES = XN * XK * 2, XSTAGE = XA_BYTES + XB_BYTES;
+constexpr int XSMEM = XSTAGES * XSTAGE + 1024;
+constexpr uint32_t XTMEM_COLS = 256;
+// fp32 accumulator, bf16 A and B, both K-major, N 256, M 128
+constexpr uint32_t kInstrDescX =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XN >> 3) << 17) | ((uint32_t)(XM >> 4) << 24);
+
+// K-major operand with the 128-byte swizzle: rows of 128 bytes (64 bf16),
+// 8-row groups 1024 bytes apart (stride byte offset), the leading byte offset
+// unused (1), descriptor version 1, layout 2 (128-byte swizzle).  The K step of
+// 16 elements inside the 128-byte atom advances the start address by 32 bytes.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024u >> 4) << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mbar_init_x(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(XTHREADS) gemm_tcgen05_tma(const __grid_constant__ CUtensorMap map_a,
+                                                             const __grid_constant__ CUtensorMap map_b, int M, int N,
+                                                             int K, float alpha, float beta, float* __restrict__ C,
+                                                             int ldc) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full[XSTAGES], empty[XSTAGES], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * XM, n0 = blockIdx.y * XN;
+  const int nk = (K + XK - 1) / XK;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(XTMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < XSTAGES; ++s) {
+      mbar_init_x(smem_u32(&full[s]), 1);
+      mbar_init_x(smem_u32(&empty[s]), 1);
+    }
+    mbar_init_x(smem_u32(&done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  int issued = 0;  // chunks whose MMAs the MMA lane issued
+  if (warp == 0 && lane == 0) {
+    // producer
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+    for (int c = 0; c < nk; ++c) {
+      const int s = c % XSTAGES;
+      if (c >= XSTAGES && !wait_bounded(smem_u32(&empty[s]), (uint32_t)((c - XSTAGES) / XSTAGES) & 1u)) {
+        abort_flag = 1;
+        break;
+      }
+      if (*(volatile int*)&abort_flag) break;
+      const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(XSTAGE)
+                   : "memory");
+      tma_load_2d(as, &map_a, c * XK, m0, smem_u32(&full[s]));
+      tma_load_2d(bs, &map_b, c * XK, n0, smem_u32(&full[s]));
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    for (int c = 0; c < nk; ++c) {
+      const int s = c % XSTAGES;
+      if (!wait_bounded(smem_u32(&full[s]), (uint32_t)(c / XSTAGES) & 1u)) {
+        abort_flag = 1;
+        break;
+      }
+      if (*(volatile int*)&abort_flag) break;
+      tc_fence_after();
+      const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
+#pragma unroll
+      for (int kk = 0; kk < XK / 16; ++kk) {
+        const uint64_t ad = smem_desc_sw128(as + kk * 32), bd = smem_desc_sw128(bs + kk * 32);
+        const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kInstrDescX), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&empty[s]))
+                   : "memory");
+      issued = c + 1;
+    }
+    // "done" fires once every issued MMA has completed (also after an abort)
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&done))
+                 : "memory");
+  }
+  // everyone waits for "done": the accumulator is complete (or the issued MMAs drained)
+  __syncwarp();
+  const bool ok = wait_bounded(smem_u32(&done), 0u);
+  if (!ok) abort_flag = 1;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp >= 2 && !abort_flag && issued >= 0) {
+    const int quarter = warp & 3;
+    const int row = m0 + 32 * quarter + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+#pragma unroll 1
+    for (int cb = 0; cb < XN; cb += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(lane_base + (uint32_t)cb));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+        float* crow = C + (size_t)row * ldc;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int col = n0 + cb + q;
+          if (col < N) {
+            const float v = alpha * __uint_as_float(r[q]);
+            crow[col] = beta == 0.f ? v : v + beta * crow[col];
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(XTMEM_COLS) : "memory");
+  }
+}
+
+// 2-D tensor map of a row-major rows x K bf16 matrix with leading dimension
+// ld, boxes of box_rows x 64 with the 128-byte swizzle (zero fill outside).
+bool encode_kmajor(CUtensorMap* map, const void* base, int rows, int K, int ld, int box_rows) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)XK, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1, 1};
+  return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace tc
+}  // namespace ifdtd
+
 extern "C" {
 
 int32_t ifdtd_nn_gemm_tc_ws(int32_t m, int32_t n, int32_t k, const void* a, int32_t lda, int32_t trans_a, const void* b,
@@ -291,6 +487,23 @@ int32_t ifdtd_nn_gemm_tc_ws(int32_t m, int32_t n, int32_t k, const void* a, int3
   // the opt-in above 48 KiB of dynamic shared memory holds per device; setting it is cheap
   cudaError_t e = cudaFuncSetAttribute(gemm_tcgen05, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05 attribute: ") + cudaGetErrorString(e));
+  // the TMA-fed kernel: both operands K-major (trans_a = 0, trans_b = 1), 16-byte aligned rows, and
+  // enough output tiles to spread over the SMs
+  const bool kmajor = !trans_a && trans_b && lda % 8 == 0 && ldb % 8 == 0 && k % 8 == 0 &&
+                      (reinterpret_cast<uintptr_t>(a) & 15) == 0 && (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+  if (kmajor && (size_t)((m + XM - 1) / XM) * ((n + XN - 1) / XN) >= 32) {
+    CUtensorMap ma, mb;
+    if (encode_kmajor(&ma, a, m, k, lda, XM) && encode_kmajor(&mb, b, n, k, ldb, XN)) {
+      e = cudaFuncSetAttribute(gemm_tcgen05_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, XSMEM);
+      if (e != cudaSuccess)
+        return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05_tma attribute: ") + cudaGetErrorString(e));
+      gemm_tcgen05_tma<<<dim3((m + XM - 1) / XM, (n + XN - 1) / XN), XTHREADS, XSMEM, (cudaStream_t)stream>>>(
+          ma, mb, m, n, k, alpha, beta, c, ldc);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05_tma: ") + cudaGetErrorString(e));
+      return IFDTD_OK;
+    }
+  }
   const int tm = (m + TM - 1) / TM, tn = (n + TN - 1) / TN, nk = (k + TK - 1) / TK;
   const int want = choose_splits(tm * tn, nk, (size_t)m * n, (size_t)workspace_bytes);
   const int kps = (nk + want - 1) / want, splits = (nk + kps - 1) / kps;

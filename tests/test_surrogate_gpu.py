@@ -49,6 +49,37 @@ def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb, entry)
         assert status.value == 0
 
 
+@pytest.mark.parametrize("m,n,k", [(1024, 2048, 520), (4096, 512, 8), (1000, 1500, 96), (8192, 512, 512)])
+def test_tma_fed_gemm_matches_float32_product(m, n, k):
+    """K-major operands with enough output tiles take the TMA-fed kernel
+    (128 x 256 tiles, 2-D TMA loads with the 128-byte swizzle into a 4-stage
+    ring, zero fill outside the matrices): ragged M and N, K below one chunk
+    and K with a partial last chunk, against a float64 product, twice (the
+    same bits)."""
+
+    import torch
+
+    from ionosphere_fdtd_b200 import _native as N
+
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    a = _bf16(torch.randn((m, k), device="cuda", generator=g))
+    b = _bf16(torch.randn((n, k), device="cuda", generator=g))
+    c0 = torch.randn((m, n), device="cuda", generator=g)
+    stream = torch.cuda.current_stream().cuda_stream
+    outs = []
+    for _ in range(2):
+        c = c0.clone()
+        N.check(N.load().ifdtd_nn_gemm_tc(m, n, k, a.data_ptr(), k, 0, b.data_ptr(), k, 1, 0.75, 0.5, c.data_ptr(), n, stream),
+                "ifdtd_nn_gemm_tc")
+        outs.append(c)
+    expected = 0.75 * (a.double() @ b.double().T) + 0.5 * c0.double()
+    assert float((outs[0].double() - expected).norm() / expected.norm()) < 1e-6
+    assert torch.equal(outs[0], outs[1])
+    status = N.C.c_int32(-1)
+    N.check(N.load().ifdtd_nn_gemm_tc_status(1, N.C.byref(status)), "ifdtd_nn_gemm_tc_status")
+    assert status.value == 0
+
+
 @pytest.mark.parametrize("m,n,k,ta,tb", [(4, 16, 65536, 1, 0), (64, 200, 3000, 1, 0), (32, 4, 20000, 0, 1), (130, 70, 1024, 0, 0)])
 def test_split_k_gemm_matches_float32_product_and_repeats_bitwise(m, n, k, ta, tb):
     """The tcgen05 GEMM with a workspace splits a long K over CTAs (the decoder's
