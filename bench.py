@@ -62,7 +62,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--workload", choices=("config2", "config3", "config4", "config5"), default="config4")
     p.add_argument("--runs", type=int, default=4096, help="config5: training runs generated by the engine")
     p.add_argument("--eval-runs", type=int, default=512, help="config5: held-out runs (16 receivers each)")
-    p.add_argument("--iterations", type=int, default=6000, help="config5: training iterations per network")
+    p.add_argument("--iterations", type=int, default=30000, help="config5: training iterations per network")
+    p.add_argument("--lr", type=float, default=2e-3, help="config5: initial Adam learning rate")
+    p.add_argument("--lr-final", type=float, default=2e-5, help="config5: final learning rate (geometric schedule)")
     p.add_argument("--batch", type=int, default=512, help="config5: traces per training iteration")
     p.add_argument("--gemm", choices=("tcgen05", "mma"), default="tcgen05", help="config5: the surrogate's GEMM kernel")
     p.add_argument("--decoder", default="16x64:4:32,16,1",
@@ -609,7 +611,7 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
     # each trace weighted by the inverse of its mean square: the loss is the
     # mean squared relative error, the metric the held-out traces are scored by
     ens, hist = SurrogateEnsemble.train(layers, x[:n_train], y[:n_train], k=4, iterations=args.iterations, batch=args.batch,
-                                        lr=1e-3, lr_final=5e-5, device=device, seed=11, relative=True, gemm=args.gemm)
+                                        lr=args.lr, lr_final=args.lr_final, device=device, seed=11, relative=True, gemm=args.gemm)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     xe, ye = x[n_train:], y[n_train:]
@@ -678,7 +680,8 @@ def surrogate_main(args, world: int, rank: int, local: int) -> None:
         "config": {
             "workload": "config5", "subdivision": 6, "radial_cells": 40, "samples": steps, "receivers_per_run": receivers,
             "train_runs": args.runs, "eval_runs": args.eval_runs, "network": f"MLP 8-512x4 + transposed-conv decoder ({seq0}x{c0}, stride {stride}, channels {chans} -> 1024)",
-            "ensemble": 4, "iterations": args.iterations, "batch": args.batch, "loss": "per-trace relative squared error",
+            "ensemble": 4, "iterations": args.iterations, "batch": args.batch, "lr": [args.lr, args.lr_final],
+            "loss": "per-trace relative squared error",
             "gemm": args.gemm, "parallelism": f"replicas x{world}",
         },
         "engine": {"traces_per_s": engine_traces_s, "generation_s": gen_s, "api": "Ensemble.record_er_observations (setup included)"},
