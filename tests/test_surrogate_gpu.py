@@ -174,3 +174,19 @@ def test_weighted_squared_error_matches_a_float64_reference():
     expected = float((w.double()[:, None] * d * d).sum() / d.numel())
     assert float(loss) == pytest.approx(expected, rel=1e-5)
     torch.testing.assert_close(grad.double(), 2.0 * w.double()[:, None] * d / d.numel(), rtol=1e-6, atol=1e-9)
+
+
+def test_training_data_does_not_depend_on_the_builder_threads():
+    """generate_traces draws every member's parameters in order from one seeded
+    generator and only then builds the members on host threads: one thread and
+    four give the same parameters and the same traces, bit for bit."""
+
+    from ionosphere_fdtd_b200.surrogate import generate_traces
+
+    kw = dict(subdivision=3, radial_cells=12, steps=64, receivers=4, distance_deg=(2.0, 10.0), batch_members=6, seed=21)
+    p1, t1 = generate_traces(9, workers=1, **kw)
+    p4, t4 = generate_traces(9, workers=4, **kw)
+    np.testing.assert_array_equal(p1, p4)
+    np.testing.assert_array_equal(t1, t4)
+    assert t1.shape == (36, 64) and np.abs(t1).max() > 0.0
+
