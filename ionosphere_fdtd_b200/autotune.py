@@ -24,7 +24,7 @@ from .engine import Engine, Tuning
 from .errors import BackendUnavailableError
 
 DEFAULT_CANDIDATES: tuple[Tuning, ...] = (
-    Tuning(),  # largest H patch whose stage fits twice; balanced E patches; 2 producer warps
+    Tuning(),  # largest H patch whose stage fits twice; balanced E patches; 2 H-phase and 4 E-phase producer warps
     Tuning(producer_warps=1),
     Tuning(producer_warps=3),
     Tuning(faces_per_patch=32),
@@ -34,6 +34,7 @@ DEFAULT_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(staging=3),
     Tuning(staging=1),
     Tuning(lane_layout=2),
+    Tuning(e_producer_warps=2),
     Tuning(e_producer_warps=3),
     Tuning(e_threads=576),
     Tuning(e_stages=3),
@@ -158,8 +159,8 @@ SHAPE_FREE_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(),
     Tuning(producer_warps=1),
     Tuning(producer_warps=3),
+    Tuning(e_producer_warps=2),
     Tuning(e_producer_warps=3),
-    Tuning(e_producer_warps=4),
 )
 
 
