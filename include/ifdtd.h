@@ -124,8 +124,8 @@ typedef struct ifdtd_tuning {
                                 warps above 384 the E phase runs wide CTAs at 96 registers (at most 640
                                 threads, TMA bulk copies only) */
   int32_t e_stages;          /* E-phase ring stages the balanced patches are sized for (0: 2, else 2 to 4) */
-  int32_t e_producer_warps;  /* copy-issuing warps of a pipelined E-phase CTA (0: 4 when threads is automatic,
-                                else as producer_warps; or 1 to 4) */
+  int32_t e_producer_warps;  /* copy-issuing warps of a pipelined E-phase CTA (0: 4 when threads and e_threads
+                                are automatic, else as producer_warps; or 1 to 4) */
   int32_t e_copy_gap;        /* E-phase copies: gaps of up to this many rows (0 to 8) between staged rows of one
                                 array are always copied over, giving fewer and longer bulk copies */
 } ifdtd_tuning;

@@ -498,12 +498,15 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int lane_layout = tune ? tune->lane_layout : 0;
   if (lane_layout < 0 || lane_layout > 2)
     return fail(IFDTD_ERR_ARGUMENT, "lane_layout must be 0 (auto), 1 (packed rows) or 2 (rows on 8-lane boundaries)");
-  // E-phase copy warps: as given; automatic: 4 with automatic threads (the E stages
-  // take about twice the H stages' copies per patch), else the H phase's count
-  const int e_producers = (tune && tune->e_producer_warps > 0) ? tune->e_producer_warps : (auto_threads ? 4 : producers);
+  const int e_threads_req = tune ? tune->e_threads : 0;
+  // E-phase copy warps: as given; automatic: 4 when both thread counts are
+  // automatic (the E stages take about twice the H stages' copies per patch),
+  // else the H phase's count
+  const int e_producers = (tune && tune->e_producer_warps > 0) ? tune->e_producer_warps
+                          : (auto_threads && e_threads_req == 0) ? 4
+                                                                  : producers;
   if (e_producers > 4) return fail(IFDTD_ERR_ARGUMENT, "e_producer_warps must be 0 (automatic) or 1 to 4");
   P->e_producers = e_producers;
-  const int e_threads_req = tune ? tune->e_threads : 0;
   if (e_threads_req != 0 &&
       (e_threads_req % 32 || e_threads_req < 32 || e_threads_req + 32 * e_producers > pipe::kWideMaxThreads))
     return fail(IFDTD_ERR_ARGUMENT, "e_threads must be 0 or a multiple of 32 with e_threads + 32 * E producer warps <= 640");

@@ -551,10 +551,10 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
     auto crow = [&](int c) -> Run<real> {
       return full_rows ? ldg16(R.pcoef + ((size_t)(s * 6 + c) * R.nF + f) * Pm + j0) : ld16(Ls.pc + (s * 6 + c) * Pm + j0);
     };
-    const Run<real> decay = crow(0), cs = crow(1), dre = crow(4);
+    const Run<real> decay = crow(0), dre = crow(4);
     Run<real> jn[3];
     if (mag) {
-      const Run<real> sn = crow(2), dpar = crow(3), dim = crow(5);
+      const Run<real> cs = crow(1), sn = crow(2), dpar = crow(3), dim = crow(5);
       Run<real> bd[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) bd[c] = full_rows ? ldg16(R.bdir + ((size_t)f * 3 + c) * Pm + j0) : ld16(Ls.bd + c * Pm + j0);
@@ -589,10 +589,12 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
                        dre.x[r] * Eq[c] + dim.x[r] * Ex[c];
       }
     } else {
+      // B = 0 everywhere: the rotation angle is 0 and its cosine exactly 1, so
+      // decay * (cos * J) is decay * J bit for bit (plasma.py:430-439)
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) jn[c].x[r] = decay.x[r] * (cs.x[r] * jc[c].x[r]) + dre.x[r] * E[r][c];
+        for (int c = 0; c < 3; ++c) jn[c].x[r] = decay.x[r] * jc[c].x[r] + dre.x[r] * E[r][c];
     }
     if (tail) {
 #pragma unroll

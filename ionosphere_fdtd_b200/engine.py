@@ -49,8 +49,8 @@ class Tuning:
     threads of an E-phase CTA (0: as ``threads``; above 384 minus the producer
     warps the E phase runs wide CTAs of at most 640 threads at 96 registers)
     the ring stages the balanced E patches are sized for (0: 2), the
-    copy-issuing warps of an E-phase CTA (0: 4 with automatic threads, else as
-    ``producer_warps``), and the
+    copy-issuing warps of an E-phase CTA (0: 4 when both thread counts are
+    automatic, else as ``producer_warps``), and the
     row gaps every E-phase copy bridges (0-8: fewer, longer bulk copies).
     Every choice computes the same bits."""
 
