@@ -282,19 +282,23 @@ int choose_splits(int tiles, int nk, size_t mn, size_t workspace_bytes) {
 // ---------------------------------------------------------------------------
 // TMA-fed kernel for the K-major / K-major case (op(A) = A row-major M x K,
 // op(B) = B^T with B row-major N x K: the forward products of the surrogate
-// and square benchmark products).  One CTA of 6 warps computes a 128 x 256
-// tile; the accumulator takes 256 TMEM columns.  Warp 0 (one lane) streams
+// and square benchmark products).  Persistent: one CTA of 6 warps per SM
+// walks 128 x 256 output tiles in grouped order.  Warp 0 (one lane) streams
 // 64-wide K chunks of A (128 x 64) and B (256 x 64) with 2-D TMA tile loads
 // (128-byte swizzle, zero fill outside the matrices) into a 4-stage ring,
 // completing on the stage's "full" mbarrier by transaction count; warp 1 (one
 // lane) waits on "full", issues four tcgen05.mma (M 128, N 256, K 16) per
 // chunk and commits them to the stage's "empty" mbarrier, which frees the
-// stage for the producer; after the last chunk it commits to "done".  Warps
-// 2-5 wait on "done" and read the accumulator with tcgen05.ld, each from the
-// 32 TMEM lanes of its warp index modulo 4.  Every wait is bounded as in the
-// generic kernel; a wait that runs out sets the status bit, the roles stop
-// issuing, and the CTA waits (bounded) for the MMAs it issued before it frees
-// the tensor memory.  Loads read this GPU's memory only, without multicast.
+// stage for the producer.  The accumulator alternates between two 256-column
+// halves of the CTA's 512 TMEM columns: after a tile's last chunk the MMA lane
+// commits to that half's "acc_full" barrier and goes on with the next tile in
+// the other half, while warps 2-5 read the finished half with tcgen05.ld
+// (each from the 32 TMEM lanes of its warp index modulo 4), write C and arrive
+// on the half's "acc_empty" barrier.  Every wait is bounded as in the generic
+// kernel; a wait that runs out sets the status bit and a stop flag, every role
+// leaves its loop, and the CTA waits (bounded) for the MMAs it issued before it
+// frees the tensor memory.  Loads read this GPU's memory only, without
+// multicast.
 // ---------------------------------------------------------------------------
 namespace ifdtd {
 namespace tc {
@@ -302,7 +306,8 @@ namespace tc {
 constexpr int XM = 128, XN = 256, XK = 64, XSTAGES = 4, XTHREADS = 192;
 constexpr int XA_BYTES = XM * XK * 2, XB_BYTES = XN * XK * 2, XSTAGE = XA_BYTES + XB_BYTES;
 constexpr int XSMEM = XSTAGES * XSTAGE + 1024;
-constexpr uint32_t XTMEM_COLS = 256;
+constexpr uint32_t XTMEM_COLS = 512;  // two 256-column accumulators: a tile's epilogue overlaps the next tile's MMAs
+constexpr int XGROUP = 8;              // tile rasterisation: M-tiles per group
 // fp32 accumulator, bf16 A and B, both K-major, N 256, M 128
 constexpr uint32_t kInstrDescX =
     (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(XN >> 3) << 17) | ((uint32_t)(XM >> 4) << 24);
@@ -327,18 +332,37 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// Output tile t of a tiles_m x tiles_n grid in grouped order: XGROUP M-tiles
+// sweep each N column together, so the CTAs running at once share B panels
+// (and A panels within a group) in L2.
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int& tm, int& tn) {
+  const int per_group = XGROUP * tiles_n;
+  const int g = t / per_group, first = g * XGROUP;
+  const int rows = min(tiles_m - first, XGROUP);
+  const int r = t - g * per_group;
+  tm = first + r % rows;
+  tn = r / rows;
+}
+
+__device__ __forceinline__ void mbar_arrive_x(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
 __global__ void __launch_bounds__(XTHREADS) gemm_tcgen05_tma(const __grid_constant__ CUtensorMap map_a,
                                                              const __grid_constant__ CUtensorMap map_b, int M, int N,
                                                              int K, float alpha, float beta, float* __restrict__ C,
-                                                             int ldc) {
+                                                             int ldc, int tiles_m, int tiles_n) {
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full[XSTAGES], empty[XSTAGES], done;
+  __shared__ __align__(8) uint64_t full[XSTAGES], empty[XSTAGES], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * XM, n0 = blockIdx.y * XN;
-  const int nk = (K + XK - 1) / XK;
+  const int nk = (K + XK - 1) / XK, n_tiles = tiles_m * tiles_n;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
                  "r"(XTMEM_COLS)
@@ -350,7 +374,11 @@ __global__ void __launch_bounds__(XTHREADS) gemm_tcgen05_tma(const __grid_consta
       mbar_init_x(smem_u32(&full[s]), 1);
       mbar_init_x(smem_u32(&empty[s]), 1);
     }
-    mbar_init_x(smem_u32(&done), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init_x(smem_u32(&acc_full[b]), 1);
+      mbar_init_x(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+    }
+    mbar_init_x(smem_u32(&drain), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
   }
@@ -358,88 +386,104 @@ __global__ void __launch_bounds__(XTHREADS) gemm_tcgen05_tma(const __grid_consta
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  int issued = 0;  // chunks whose MMAs the MMA lane issued
+  volatile int* stop = &abort_flag;
   if (warp == 0 && lane == 0) {
-    // producer
+    // producer: every chunk of every tile of this CTA, through the ring
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
-    for (int c = 0; c < nk; ++c) {
-      const int s = c % XSTAGES;
-      if (c >= XSTAGES && !wait_bounded(smem_u32(&empty[s]), (uint32_t)((c - XSTAGES) / XSTAGES) & 1u)) {
-        abort_flag = 1;
-        break;
+    int g = 0;
+    for (int t = blockIdx.x; t < n_tiles && !*stop; t += gridDim.x) {
+      int tm, tn;
+      tile_coords(t, tiles_m, tiles_n, tm, tn);
+      for (int c = 0; c < nk; ++c, ++g) {
+        const int s = g % XSTAGES;
+        if (g >= XSTAGES && !wait_bounded(smem_u32(&empty[s]), (uint32_t)((g - XSTAGES) / XSTAGES) & 1u)) *stop = 1;
+        if (*stop) break;
+        const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(XSTAGE)
+                     : "memory");
+        tma_load_2d(as, &map_a, c * XK, tm * XM, smem_u32(&full[s]));
+        tma_load_2d(bs, &map_b, c * XK, tn * XN, smem_u32(&full[s]));
       }
-      if (*(volatile int*)&abort_flag) break;
-      const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(XSTAGE)
-                   : "memory");
-      tma_load_2d(as, &map_a, c * XK, m0, smem_u32(&full[s]));
-      tma_load_2d(bs, &map_b, c * XK, n0, smem_u32(&full[s]));
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer
-    for (int c = 0; c < nk; ++c) {
-      const int s = c % XSTAGES;
-      if (!wait_bounded(smem_u32(&full[s]), (uint32_t)(c / XSTAGES) & 1u)) {
-        abort_flag = 1;
+    // MMA issuer: tile i accumulates in TMEM columns (i % 2) * 256
+    int g = 0, i = 0;
+    for (int t = blockIdx.x; t < n_tiles && !*stop; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      if (i >= 2 && !wait_bounded(smem_u32(&acc_empty[b]), (uint32_t)((i - 2) / 2) & 1u)) *stop = 1;
+      if (*stop) break;
+      tc_fence_after();
+      const uint32_t d = tmem + (uint32_t)(b * XN);
+      for (int c = 0; c < nk; ++c, ++g) {
+        const int s = g % XSTAGES;
+        if (!wait_bounded(smem_u32(&full[s]), (uint32_t)(g / XSTAGES) & 1u)) *stop = 1;
+        if (*stop) break;
+        tc_fence_after();
+        const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < XK / 16; ++kk) {
+          const uint64_t ad = smem_desc_sw128(as + kk * 32), bd = smem_desc_sw128(bs + kk * 32);
+          const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+              "l"(ad), "l"(bd), "r"(kInstrDescX), "r"(acc)
+              : "memory");
+        }
+        tc_commit(smem_u32(&empty[s]));  // frees the stage once these MMAs are done
+      }
+      if (*stop) break;
+      tc_commit(smem_u32(&acc_full[b]));  // the tile's accumulator is complete
+    }
+    // "drain" fires once every MMA this thread issued has completed (also after a stop)
+    tc_commit(smem_u32(&drain));
+  } else if (warp >= 2) {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31
+    const int quarter = warp & 3;
+    int i = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      if (!__all_sync(0xFFFFFFFFu, wait_bounded(smem_u32(&acc_full[b]), (uint32_t)(i / 2) & 1u))) {
+        *stop = 1;
         break;
       }
-      if (*(volatile int*)&abort_flag) break;
       tc_fence_after();
-      const uint32_t as = smem_u32(smem + s * XSTAGE), bs = as + XA_BYTES;
-#pragma unroll
-      for (int kk = 0; kk < XK / 16; ++kk) {
-        const uint64_t ad = smem_desc_sw128(as + kk * 32), bd = smem_desc_sw128(bs + kk * 32);
-        const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(kInstrDescX), "r"(acc)
-            : "memory");
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&empty[s]))
-                   : "memory");
-      issued = c + 1;
-    }
-    // "done" fires once every issued MMA has completed (also after an abort)
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&done))
-                 : "memory");
-  }
-  // everyone waits for "done": the accumulator is complete (or the issued MMAs drained)
-  __syncwarp();
-  const bool ok = wait_bounded(smem_u32(&done), 0u);
-  if (!ok) abort_flag = 1;
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (warp >= 2 && !abort_flag && issued >= 0) {
-    const int quarter = warp & 3;
-    const int row = m0 + 32 * quarter + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16);
+      int tm, tn;
+      tile_coords(t, tiles_m, tiles_n, tm, tn);
+      const int row = tm * XM + 32 * quarter + lane, n0 = tn * XN;
+      const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(b * XN);
 #pragma unroll 1
-    for (int cb = 0; cb < XN; cb += 16) {
-      uint32_t r[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(lane_base + (uint32_t)cb));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
-        float* crow = C + (size_t)row * ldc;
+      for (int cb = 0; cb < XN; cb += 16) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+            "%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(lane_base + (uint32_t)cb));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < M) {
+          float* crow = C + (size_t)row * ldc;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int col = n0 + cb + q;
-          if (col < N) {
-            const float v = alpha * __uint_as_float(r[q]);
-            crow[col] = beta == 0.f ? v : v + beta * crow[col];
+          for (int q = 0; q < 16; ++q) {
+            const int col = n0 + cb + q;
+            if (col < N) {
+              const float v = alpha * __uint_as_float(r[q]);
+              crow[col] = beta == 0.f ? v : v + beta * crow[col];
+            }
           }
         }
       }
+      // the accumulator may be overwritten once all four warps have read it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_x(smem_u32(&acc_empty[b]));
     }
   }
+  __syncwarp();
+  // no MMA may still write TMEM when it is freed
+  if (!wait_bounded(smem_u32(&drain), 0u)) *stop = 1;
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -497,8 +541,13 @@ int32_t ifdtd_nn_gemm_tc_ws(int32_t m, int32_t n, int32_t k, const void* a, int3
       e = cudaFuncSetAttribute(gemm_tcgen05_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, XSMEM);
       if (e != cudaSuccess)
         return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05_tma attribute: ") + cudaGetErrorString(e));
-      gemm_tcgen05_tma<<<dim3((m + XM - 1) / XM, (n + XN - 1) / XN), XTHREADS, XSMEM, (cudaStream_t)stream>>>(
-          ma, mb, m, n, k, alpha, beta, c, ldc);
+      int dev = 0, sms = 148;
+      if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const int tiles_m = (m + XM - 1) / XM, tiles_n = (n + XN - 1) / XN;
+      // persistent: one CTA per SM (the ring takes 198 KB of shared memory), each walking its tiles
+      const int grid = std::min(tiles_m * tiles_n, std::max(sms, 1));
+      gemm_tcgen05_tma<<<grid, XTHREADS, XSMEM, (cudaStream_t)stream>>>(ma, mb, m, n, k, alpha, beta, c, ldc, tiles_m,
+                                                                        tiles_n);
       e = cudaGetLastError();
       if (e != cudaSuccess) return ifdtd::record_error(IFDTD_ERR_CUDA, std::string("gemm_tcgen05_tma: ") + cudaGetErrorString(e));
       return IFDTD_OK;

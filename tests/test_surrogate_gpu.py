@@ -49,13 +49,16 @@ def test_gemm_matches_float32_product_of_the_bf16_inputs(m, n, k, ta, tb, entry)
         assert status.value == 0
 
 
-@pytest.mark.parametrize("m,n,k", [(1024, 2048, 520), (4096, 512, 8), (1000, 1500, 96), (8192, 512, 512)])
+@pytest.mark.parametrize("m,n,k", [(1024, 2048, 520), (4096, 512, 8), (1000, 1500, 96), (8192, 512, 512),
+                                   (4096, 4096, 192), (5000, 2600, 136)])
 def test_tma_fed_gemm_matches_float32_product(m, n, k):
     """K-major operands with enough output tiles take the TMA-fed kernel
-    (128 x 256 tiles, 2-D TMA loads with the 128-byte swizzle into a 4-stage
-    ring, zero fill outside the matrices): ragged M and N, K below one chunk
-    and K with a partial last chunk, against a float64 product, twice (the
-    same bits)."""
+    (persistent CTAs over 128 x 256 tiles, 2-D TMA loads with the 128-byte
+    swizzle into a 4-stage ring, two TMEM accumulators so a tile's epilogue
+    overlaps the next tile's MMAs, zero fill outside the matrices): ragged M
+    and N, K below one chunk and K with a partial last chunk, one tile per CTA
+    and several (512 and 440 tiles on 148 SMs), against a float64 product,
+    twice (the same bits)."""
 
     import torch
 
