@@ -128,6 +128,15 @@ typedef struct ifdtd_tuning {
                                 are automatic, else as producer_warps; or 1 to 4) */
   int32_t e_copy_gap;        /* E-phase copies: gaps of up to this many rows (0 to 8) between staged rows of one
                                 array are always copied over, giving fewer and longer bulk copies */
+  int32_t fused_step;        /* 1: one launch per leapfrog step, each E-phase patch recomputing the new H it
+                                reads on its halo (plans without plasma or surface impedance; the plan holds a
+                                second copy of the four field arrays and alternates between the copies, copying
+                                back after an odd number of steps; graph_chunk must be even; the plan cannot
+                                join a batch).  staging 0 / 2 / 3: patches staged through the pipelined ring
+                                (TMA bulk copies / cp.async), the new H overwriting the old in the stage;
+                                staging 1: direct gathers with the halo's new H in shared memory.
+                                e_faces_per_patch sets the patch (0: the largest of 64 ... 8 faces whose stage
+                                fits twice, direct: of 128 ... 16 faces whose rows fit 110 KiB); 0: two launches */
 } ifdtd_tuning;
 
 /* Mutable state of one simulation: device pointers owned by the caller. */
@@ -160,7 +169,8 @@ int32_t ifdtd_status_word(ifdtd_plan* plan, int32_t reset, int32_t* out);
  * Synchronises the stream. */
 int32_t ifdtd_wait_selftest(ifdtd_plan* plan, double* waited_seconds, void* stream);
 /* Which step kernels the plan launches: 1 direct gathers, 2 shared-memory
- * pipeline (H phase, E phase). */
+ * pipeline (H phase, E phase); h_mode 3: the fused one-launch step, whose
+ * kernel family e_mode gives. */
 int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode);
 /* Bytes of device memory held by the plan (tables, staging, scratch). */
 int32_t ifdtd_plan_bytes(const ifdtd_plan* plan, int64_t* bytes);

@@ -92,7 +92,8 @@ class PhysicsDesc(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("faces_per_patch", _i32), ("threads", _i32), ("graph_chunk", _i32), ("e_faces_per_patch", _i32), ("staging", _i32),
                 ("producer_warps", _i32), ("lane_layout", _i32), ("e_threads", _i32), ("e_stages", _i32),
-                ("e_producer_warps", _i32), ("e_copy_gap", _i32)]
+                ("e_producer_warps", _i32), ("e_copy_gap", _i32),
+                ("fused_step", _i32)]
 
 
 class State(C.Structure):

@@ -7,8 +7,8 @@ bulk copies, cp.async, or direct global gathers).  ``autotune`` builds a plan
 for every candidate from the simulation's own mesh and physics, times
 graph-captured steps of each on the simulation's own state with CUDA events,
 restores that state, and installs the fastest plan.  Every candidate computes
-the same bits (patch size, lane layout and kernel family do not change any
-result), so
+the same bits (patch size, lane layout, kernel family and the fused
+one-launch step do not change any result), so
 tuning changes speed only.  ``autotune_ensemble`` tunes the largest member
 of each class (by default: mesh level, radial cells, precision and physics)
 and gives the winner to the whole class.
@@ -38,6 +38,11 @@ DEFAULT_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(e_producer_warps=3),
     Tuning(e_threads=576),
     Tuning(e_stages=3),
+    # one launch per step with halo recomputation (plans without plasma or
+    # surface impedance; the others reject it)
+    Tuning(fused_step=1),
+    Tuning(fused_step=1, e_faces_per_patch=32),
+    Tuning(fused_step=1, e_faces_per_patch=16),
 )
 
 
@@ -173,6 +178,8 @@ def autotune_ensemble(members: Sequence, candidates: Sequence[Tuning] = DEFAULT_
     ``SHAPE_FREE_CANDIDATES``).  Call it before building the ``Ensemble``: the
     batch reads the members' plans when it is created."""
 
+    # a fused-step plan cannot join a batch
+    candidates = [c for c in candidates if not c.fused_step]
     classes: dict[tuple, list] = {}
     for m in members:
         classes.setdefault((key or _tuning_class)(m), []).append(m)
@@ -190,3 +197,48 @@ def autotune_ensemble(members: Sequence, candidates: Sequence[Tuning] = DEFAULT_
                 m.backend._engine = engine
                 old.close()
     return out
+
+
+def main(argv: Sequence[str] | None = None) -> None:
+    """Time the candidates on one benchmark workload and print one JSON line
+    per candidate (median milliseconds per leapfrog step, or the plan
+    builder's refusal): ``python -m ionosphere_fdtd_b200.autotune config1
+    --subdivision 9 --radial-cells 80``."""
+
+    import argparse
+    import json
+    from dataclasses import asdict
+
+    from . import workloads as W
+
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("workload", choices=("config1", "config2", "config4"))
+    p.add_argument("--subdivision", type=int, default=None)
+    p.add_argument("--radial-cells", type=int, default=None)
+    p.add_argument("--dtype", choices=("float32", "float64"), default="float32")
+    p.add_argument("--steps", type=int, default=32)
+    p.add_argument("--repeats", type=int, default=5)
+    p.add_argument("--fused-only", action="store_true", help="the default plan, the direct kernels and the fused step only")
+    a = p.parse_args(argv)
+    kw = {k: v for k, v in (("subdivision", a.subdivision), ("radial_cells", a.radial_cells)) if v is not None}
+    wl = getattr(W, a.workload)(device="cuda", dtype=a.dtype, **kw)
+    W.seed_fields(wl.simulation)
+    cands = DEFAULT_CANDIDATES
+    if a.fused_only:
+        cands = [Tuning(), Tuning(staging=1)] + [c for c in DEFAULT_CANDIDATES if c.fused_step] + [
+            Tuning(fused_step=1, e_faces_per_patch=48), Tuning(fused_step=1, e_faces_per_patch=24),
+            Tuning(fused_step=1, e_producer_warps=2), Tuning(fused_step=1, e_producer_warps=3),
+            Tuning(fused_step=1, lane_layout=2), Tuning(fused_step=1, staging=1, e_faces_per_patch=32)]
+    res = autotune(wl.simulation, cands, steps=a.steps, repeats=a.repeats)
+    for t, ms, err in res.timings:
+        line = {"workload": a.workload, "cells": wl.cells, "dtype": a.dtype, "tuning": asdict(t), "ms_per_step": ms}
+        if ms is not None:
+            line["gcell_per_s"] = wl.cells / (ms / 1e3) / 1e9
+            line["algorithmic_gbs"] = wl.bytes_per_step / (ms / 1e3) / 1e9
+        if err:
+            line["error"] = err
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

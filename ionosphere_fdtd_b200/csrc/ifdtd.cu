@@ -15,6 +15,7 @@
 
 #include "../../include/ifdtd.h"
 #include "errors.cuh"
+#include "fused_kernels.cuh"
 #include "pipe_kernels.cuh"
 #include "step_kernels.cuh"
 
@@ -125,6 +126,16 @@ struct ifdtd_plan {
   std::vector<GraphEntry> graphs;
   std::vector<ifdtd_probe*> probes;
   std::vector<float> kh_cost, ke_cost;  // staged bytes per pipelined patch (balances batched launches)
+  // fused step: halo tables, the record of the second field copy and its arrays
+  bool fused = false;
+  bool fused_pipe = false;  // the fused step through the ring (pipe::kf_tma) rather than direct gathers
+  int kf_stage = 0, kf_stages = 0, kf_grid = 0, kf_threads = 0, kf_producers = 0, kf_lanes = 0;
+  size_t kf_smem = 0;
+  FusedTables fused_tab{};
+  size_t fused_smem = 0;
+  void* d_rec_b = nullptr;
+  void* fb[4] = {nullptr, nullptr, nullptr, nullptr};  // second er, et, hr, ht
+  size_t fb_bytes[4] = {0, 0, 0, 0};
   ~ifdtd_plan() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
     if (capture_stream) cudaStreamDestroy(capture_stream);
@@ -462,6 +473,151 @@ bool build_pipe_e(PipeTables& T, int n, const std::vector<int>& vptr, const std:
   return true;
 }
 
+// Fused step through the ring (patch = vertices vlist[vptr[q]..vptr[q+1]) and
+// edges eptr[q]..eptr[q+1]; no plasma, no surface impedance).  H edges: the
+// owned edges and the slot edges of the owned vertices; H faces: the faces
+// beside the owned edges; a face is written by the patch that owns its first
+// edge (owner_of_edge).  Stage: blob, er rows (ends of the H edges, which
+// include the owned vertices), et rows (H edges and the edges of the H faces),
+// ht rows (H edges), hr rows (H faces).
+template <typename real>
+bool build_pipe_f(PipeTables& T, int n, const std::vector<int>& vptr, const std::vector<int>& vlist,
+                  const std::vector<int>& eptr, const std::vector<int>& owner_of_edge, const std::vector<int2>& th,
+                  const std::vector<int2>& lr, const std::vector<int4>& fe, int SW, const std::vector<int>& ps_edge,
+                  const std::vector<real>& ps_coef, const std::vector<real>& inv_theta, const std::vector<real>& inv_phi,
+                  const std::vector<real>& fw, int Pn, int Pm, const std::vector<char>& v_src,
+                  const std::vector<char>& e_src, std::vector<int>& locV, std::vector<int>& locE, std::vector<int>& locH,
+                  std::vector<int>& locF, int max_stage) {
+  using namespace pipe;
+  const int rb = (int)sizeof(real);
+  std::vector<int> h_ids, f_ids, v_ids, t_ids;
+  std::vector<std::pair<int, int>> h_runs, f_runs, v_runs, t_runs;
+  std::vector<std::pair<int, int>> own;  // (vertex, slot)
+  std::vector<int4> hel, fel, eloc;
+  std::vector<int> hid, fid, vid, vh, vel;
+  std::vector<real> hinv, fwl, vcoef;
+  for (int q = 0; q < n; ++q) {
+    const int va = vptr[q], vb = vptr[q + 1], ea = eptr[q], eb = eptr[q + 1], nv = vb - va, ne = eb - ea;
+    own.clear();
+    for (int sl = va; sl < vb; ++sl) own.push_back({vlist[sl], sl});
+    std::sort(own.begin(), own.end());
+    h_ids.clear();
+    f_ids.clear();
+    for (const auto& o : own)
+      for (int k = 0; k < SW; ++k) h_ids.push_back(ps_edge[(size_t)o.second * SW + k]);
+    for (int e = ea; e < eb; ++e) {
+      h_ids.push_back(e);
+      f_ids.push_back(lr[e].x);
+      f_ids.push_back(lr[e].y);
+    }
+    sort_unique(h_ids);
+    sort_unique(f_ids);
+    v_ids.clear();
+    t_ids.clear();
+    for (const int e : h_ids) {
+      v_ids.push_back(th[e].x);
+      v_ids.push_back(th[e].y);
+      t_ids.push_back(e);
+    }
+    for (const int f : f_ids) {
+      t_ids.push_back(fe[f].x);
+      t_ids.push_back(fe[f].y);
+      t_ids.push_back(fe[f].z);
+    }
+    sort_unique(v_ids);
+    sort_unique(t_ids);
+    int gap = 0, n_v = 0, n_t = 0, n_h = 0, n_f = 0, nd = 0;
+    for (;;) {
+      n_v = make_runs(v_ids, gap, v_runs, locV);
+      n_t = make_runs(t_ids, gap, t_runs, locE);
+      n_h = make_runs(h_ids, gap, h_runs, locH);
+      n_f = make_runs(f_ids, gap, f_runs, locF);
+      nd = 1 + (int)(v_runs.size() + t_runs.size() + h_runs.size() + f_runs.size());
+      if (nd <= kMaxDesc || gap >= 64) break;
+      gap = 2 * gap + 1;
+    }
+    if (nd > kMaxDesc) return false;
+    const int nhe = (int)h_ids.size(), nhf = (int)f_ids.size();
+    hel.resize(nhe);
+    hid.resize(nhe);
+    hinv.resize(nhe);
+    for (int i = 0; i < nhe; ++i) {
+      const int e = h_ids[i];
+      hel[i] = make_int4(locV[th[e].y], locV[th[e].x], locE[e], locH[e]);
+      hid[i] = e | (e >= ea && e < eb ? 0 : kNotOwned);
+      hinv[i] = inv_theta[e];
+    }
+    fel.resize(nhf);
+    fid.resize(nhf);
+    fwl.resize(4 * (size_t)nhf);
+    for (int i = 0; i < nhf; ++i) {
+      const int f = f_ids[i];
+      fel[i] = make_int4(locE[fe[f].x], locE[fe[f].y], locE[fe[f].z], locF[f]);
+      fid[i] = f | (owner_of_edge[fe[f].x] == q ? 0 : kNotOwned);
+      for (int c = 0; c < 4; ++c) fwl[4 * (size_t)i + c] = fw[4 * (size_t)f + c];
+    }
+    vid.assign(nv, 0);
+    vel.assign(nv, 0);
+    vh.assign((size_t)nv * SW, 0);
+    vcoef.assign((size_t)nv * SW, real(0));
+    for (int vl = 0; vl < nv; ++vl) {
+      const int sl = own[vl].second;
+      vid[vl] = own[vl].first;
+      vel[vl] = locV[own[vl].first];
+      for (int k = 0; k < SW; ++k) {
+        const size_t i = (size_t)sl * SW + k, o = (size_t)vl * SW + k;
+        vh[o] = locH[ps_edge[i]];
+        vcoef[o] = ps_coef[i];
+      }
+    }
+    eloc.resize(ne);
+    for (int el = 0; el < ne; ++el) {
+      const int e = ea + el;
+      eloc[el] = make_int4(locH[e], locF[lr[e].x], locF[lr[e].y], locE[e]);
+    }
+    const size_t base = T.tab.size();
+    int head[kf_head_ints] = {0};
+    T.tab.resize(base + sizeof(head), 0);
+    head[kf_o_hel] = blob_put(T.tab, base, hel.data(), nhe * sizeof(int4));
+    head[kf_o_hinv] = blob_put(T.tab, base, hinv.data(), nhe * (size_t)rb);
+    head[kf_o_hid] = blob_put(T.tab, base, hid.data(), nhe * sizeof(int));
+    head[kf_o_fel] = blob_put(T.tab, base, fel.data(), nhf * sizeof(int4));
+    head[kf_o_fw] = blob_put(T.tab, base, fwl.data(), fwl.size() * (size_t)rb);
+    head[kf_o_fid] = blob_put(T.tab, base, fid.data(), nhf * sizeof(int));
+    head[kf_o_vid] = blob_put(T.tab, base, vid.data(), nv * sizeof(int));
+    head[kf_o_vh] = blob_put(T.tab, base, vh.data(), vh.size() * sizeof(int));
+    head[kf_o_vcoef] = blob_put(T.tab, base, vcoef.data(), vcoef.size() * (size_t)rb);
+    head[kf_o_vel] = blob_put(T.tab, base, vel.data(), nv * sizeof(int));
+    head[kf_o_eloc] = blob_put(T.tab, base, eloc.data(), ne * sizeof(int4));
+    head[kf_o_einv] = blob_put(T.tab, base, inv_phi.data() + ea, ne * (size_t)rb);
+    const int B = (int)(T.tab.size() - base);
+    head[kf_nhe] = nhe;
+    head[kf_nhf] = nhf;
+    head[kf_nv] = nv;
+    head[kf_ea] = ea;
+    head[kf_ne] = ne;
+    for (const auto& o : own) head[kf_src] |= v_src[o.first] ? 1 : 0;
+    for (int e = ea; e < eb; ++e) head[kf_src] |= e_src[e] ? 2 : 0;
+    head[kf_o_er] = B;
+    head[kf_o_et] = head[kf_o_er] + n_v * Pn * rb;
+    head[kf_o_ht] = head[kf_o_et] + n_t * Pm * rb;
+    head[kf_o_hr] = head[kf_o_ht] + n_h * Pn * rb;
+    head[kf_o_end] = head[kf_o_hr] + n_f * Pm * rb;
+    const int end = head[kf_o_end];
+    if (round128(end) > max_stage) return false;  // the stage would not fit: stop early
+    std::memcpy(T.tab.data() + base, head, sizeof(head));
+    T.desc.push_back(make_int4(kSrcTab, (int)(base / 16), 0, B));
+    add_runs(T.desc, kSrcEr, v_runs, head[kf_o_er], Pn * rb);
+    add_runs(T.desc, kSrcEt, t_runs, head[kf_o_et], Pm * rb);
+    add_runs(T.desc, kSrcHt, h_runs, head[kf_o_ht], Pn * rb);
+    add_runs(T.desc, kSrcHr, f_runs, head[kf_o_hr], Pm * rb);
+    T.dptr.push_back((int)T.desc.size());
+    T.stage_bytes = std::max(T.stage_bytes, round128(end));
+    if (T.tab.size() / 16 >= (size_t)1 << 31) return false;
+  }
+  return true;
+}
+
 template <typename real>
 int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G, const ifdtd_physics_desc* X,
                const ifdtd_tuning* tune) {
@@ -482,7 +638,13 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const bool auto_h = !(tune && tune->faces_per_patch > 0), auto_e = !(tune && tune->e_faces_per_patch > 0);
   int fpp = auto_h ? 32 : tune->faces_per_patch;
   int fpp_e = auto_e ? 16 : tune->e_faces_per_patch;
-  const int staging = tune ? tune->staging : 0;
+  const bool fused = tune && tune->fused_step != 0;
+  if (tune && (tune->fused_step < 0 || tune->fused_step > 1)) return fail(IFDTD_ERR_ARGUMENT, "fused_step must be 0 or 1");
+  // the fused step replaces both phases; its plan keeps the direct kernels for
+  // the single-phase entry points
+  const int staging = fused ? 1 : (tune ? tune->staging : 0);
+  // fused step: 1 direct gathers; 0 or 2 the ring fed by TMA bulk copies; 3 the ring fed by cp.async
+  const int fused_staging = fused && tune ? tune->staging : 0;
   // threads: > 0 as given; 0 picks 320 compute threads for pipelined CTAs and 256 for direct CTAs
   const bool auto_threads = !(tune && tune->threads > 0);
   int threads = auto_threads ? 256 : tune->threads;
@@ -772,6 +934,173 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   const int S = std::max(0, X->plasma_species);
   const bool plasma = S > 0;
 
+  // ---- fused step: E patches with their halo edge and face lists ----
+  PipeTables tf_tab;  // the ring's descriptors and blobs (uploaded with the E-phase tables)
+  if (fused) {
+    if (S > 0 || X->si_terms > 0)
+      return fail(IFDTD_ERR_UNSUPPORTED, "fused_step supports plans without plasma and without surface impedance");
+    if (P->chunk % 2) return fail(IFDTD_ERR_ARGUMENT, "fused_step needs an even graph_chunk");
+    std::vector<int> patch_of_edge(nE), stamp_e(nE), stamp_f(nF), loc_e(nE), loc_f(nF);
+    std::vector<int> halo_e, own_f, halo_f;
+    // the halo tables of ownership o (slots sl in o.vlist order); false if a
+    // table would be inconsistent
+    auto build_fused = [&](const Own& o, const Slots& sl, std::vector<int4>& fpatch, std::vector<int>& hedge,
+                           std::vector<int>& hface, std::vector<int>& vslot, std::vector<int2>& eface,
+                           size_t& max_rows) {
+      for (int q = 0; q < o.n; ++q)
+        for (int e = o.eptr[q]; e < o.eptr[q + 1]; ++e) patch_of_edge[e] = q;
+      std::fill(stamp_e.begin(), stamp_e.end(), -1);
+      std::fill(stamp_f.begin(), stamp_f.end(), -1);
+      fpatch.assign(o.n + 1, make_int4(0, 0, 0, 0));
+      hedge.clear();
+      hface.clear();
+      vslot.assign((size_t)nV * SW, 0);
+      eface.assign(nE, make_int2(0, 0));
+      max_rows = 0;
+      size_t owned_faces = 0;
+      for (int q = 0; q < o.n; ++q) {
+        const int e0 = o.eptr[q], e1 = o.eptr[q + 1];
+        const int he0 = (int)hedge.size(), hf0 = (int)hface.size();
+        // owned edges first, in order, then the other edges of the owned vertices
+        for (int e = e0; e < e1; ++e) {
+          stamp_e[e] = q;
+          loc_e[e] = (int)hedge.size() - he0;
+          hedge.push_back(e);
+        }
+        halo_e.clear();
+        for (int k = o.vptr[q]; k < o.vptr[q + 1]; ++k) {
+          const int v = o.vlist[k];
+          for (int i = v_off[v]; i < v_off[v + 1]; ++i) {
+            const int e = v_edge[i];
+            if (stamp_e[e] != q) {
+              stamp_e[e] = q;
+              halo_e.push_back(e);
+            }
+          }
+        }
+        std::sort(halo_e.begin(), halo_e.end());
+        for (const int e : halo_e) {
+          loc_e[e] = (int)hedge.size() - he0;
+          hedge.push_back(e);
+        }
+        // faces beside the owned edges: first those whose first edge the patch owns (it writes them)
+        own_f.clear();
+        halo_f.clear();
+        for (int e = e0; e < e1; ++e)
+          for (const int f : {lr[e].x, lr[e].y})
+            if (stamp_f[f] != q) {
+              stamp_f[f] = q;
+              (patch_of_edge[fe[f].x] == q ? own_f : halo_f).push_back(f);
+            }
+        std::sort(own_f.begin(), own_f.end());
+        std::sort(halo_f.begin(), halo_f.end());
+        for (const auto* list : {&own_f, &halo_f})
+          for (const int f : *list) {
+            loc_f[f] = (int)hface.size() - hf0;
+            hface.push_back(f);
+          }
+        owned_faces += own_f.size();
+        fpatch[q] = make_int4(he0, e1 - e0, hf0, (int)own_f.size());
+        for (int k = o.vptr[q]; k < o.vptr[q + 1]; ++k)
+          for (int j = 0; j < SW; ++j) {
+            const int e = sl.edge[(size_t)k * SW + j];
+            if (stamp_e[e] != q) return false;
+            vslot[(size_t)k * SW + j] = loc_e[e];
+          }
+        for (int e = e0; e < e1; ++e) eface[e] = make_int2(loc_f[lr[e].x], loc_f[lr[e].y]);
+        const size_t rows = ((size_t)(hedge.size() - he0) * Pn + (size_t)(hface.size() - hf0) * Pm) * sizeof(real);
+        max_rows = std::max(max_rows, rows);
+      }
+      fpatch[o.n] = make_int4((int)hedge.size(), 0, (int)hface.size(), 0);
+      return owned_faces == (size_t)nF;  // every face written by exactly one patch
+    };
+    const int lreals = layer_reals(Pn, Pm, X->coef_rows_er != 1, 0, 0, 0, 0);
+    const size_t layer_bytes = (size_t)(lreals + 3) / 4 * 4 * sizeof(real);
+    bool done = false;
+    if (fused_staging != 1) {
+      // the ring: the largest patch whose stage fits twice beside the per-layer rows
+      const int f_budget = kSmemPerBlock - (int)sizeof(Rec<real>) - 1024 - pipe::layer_block_bytes(lreals, (int)sizeof(real));
+      const int W = P->e_producers;
+      const int f_threads = e_threads_req > 0 ? e_threads_req : pipe::kMaxThreads - 32 * W;
+      const int row_quads = std::max(Pn, Pm) / (16 / (int)sizeof(real));
+      if (f_threads + 32 * W > pipe::kMaxThreads)
+        return fail(IFDTD_ERR_ARGUMENT, "fused step: e_threads + 32 * E producer warps must not exceed 384");
+      std::vector<char> v_src(nV, 0), e_src(nE, 0);
+      for (int q = 0; q < X->n_src_er; ++q) v_src[X->src_er_vertex[q]] = 1;
+      for (int q = 0; q < X->n_src_et; ++q) e_src[X->src_et_edge[q]] = 1;
+      std::vector<int> locV(nV), locE(nE), locH(nE), locF(nF);
+      std::vector<int> cand_f = auto_e ? std::vector<int>{64, 48, 32, 24, 16, 8} : std::vector<int>{fpp_e};
+      if (row_quads > f_threads) cand_f.clear();
+      for (const int c : cand_f) {
+        Own o = ownership(c);
+        Slots sl;
+        if (!build_slots(o.vlist, sl)) break;
+        for (int q = 0; q < o.n; ++q)
+          for (int e = o.eptr[q]; e < o.eptr[q + 1]; ++e) patch_of_edge[e] = q;
+        PipeTables t;
+        const bool ok = build_pipe_f<real>(t, o.n, o.vptr, o.vlist, o.eptr, patch_of_edge, th, lr, fe, SW, sl.edge,
+                                           sl.coef, inv_theta, inv_phi, fw, Pn, Pm, v_src, e_src, locV, locE, locH,
+                                           locF, f_budget / 2);
+        if (!ok || 2 * t.stage_bytes > f_budget || !descriptors_valid(t, (int)sizeof(real), Pn, Pm, 0, nV, nE, nF, 0))
+          continue;
+        fpp_e = c;
+        oe = std::move(o);
+        slots = std::move(sl);
+        P->kf_stage = t.stage_bytes;
+        P->kf_stages = std::min(pipe::kMaxStages, f_budget / t.stage_bytes);
+        P->kf_smem = (size_t)pipe::layer_block_bytes(lreals, (int)sizeof(real)) + (size_t)P->kf_stages * P->kf_stage;
+        P->kf_threads = f_threads;
+        P->kf_producers = W;
+        const int wide = std::max((Pn / (int)(16 / sizeof(real)) + 7) & ~7, (Pm / (int)(16 / sizeof(real)) + 7) & ~7);
+        P->kf_lanes = lane_layout == 2 && wide <= f_threads ? 1 : 0;
+        P->pipe_copy = fused_staging == 3 ? 1 : 0;
+        tf_tab = std::move(t);
+        P->fused_pipe = true;
+        done = true;
+        break;
+      }
+      if (!done && fused_staging >= 2)
+        return fail(IFDTD_ERR_UNSUPPORTED, "fused step: no patch's stage fits twice in shared memory");
+    }
+    const size_t budget = 110 * 1024;  // direct gathers: two CTAs per SM
+    std::vector<int> cand = done ? std::vector<int>{} : auto_e ? std::vector<int>{128, 64, 32, 16} : std::vector<int>{fpp_e};
+    std::vector<int4> fpatch;
+    std::vector<int> hedge, hface, vslot;
+    std::vector<int2> eface;
+    for (const int c : cand) {
+      Own o = ownership(c);
+      Slots sl;
+      size_t max_rows = 0;
+      if (!build_slots(o.vlist, sl) || !build_fused(o, sl, fpatch, hedge, hface, vslot, eface, max_rows))
+        return fail(IFDTD_ERR_ARGUMENT, "fused step tables are inconsistent with the mesh");
+      if (layer_bytes + max_rows > (auto_e ? budget : (size_t)kSmemPerBlock - sizeof(Rec<real>) - 1024)) continue;
+      fpp_e = c;
+      oe = std::move(o);
+      slots = std::move(sl);
+      P->fused_smem = layer_bytes + max_rows;
+      done = true;
+      break;
+    }
+    if (!done) return fail(IFDTD_ERR_UNSUPPORTED, "fused step: no patch's halo rows fit in shared memory");
+    cudaError_t e = cudaSuccess;
+    if (!P->fused_pipe) {
+      FusedTables& F = P->fused_tab;
+      e = A.upload(fpatch, &F.patch);
+      if (e == cudaSuccess) e = A.upload(hedge, &F.hedge);
+      if (e == cudaSuccess) e = A.upload(hface, &F.hface);
+      if (e == cudaSuccess) e = A.upload(vslot, &F.vslot);
+      if (e == cudaSuccess) e = A.upload(eface, &F.eface);
+    }
+    const size_t rows[4] = {(size_t)nV * Pn, (size_t)nE * Pm, (size_t)nF * Pm, (size_t)nE * Pn};
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+      P->fb_bytes[i] = rows[i] * sizeof(real);
+      e = A.alloc(P->fb_bytes[i], &P->fb[i]);
+      if (e == cudaSuccess) e = cudaMemset(P->fb[i], 0, P->fb_bytes[i]);
+    }
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("fused step tables: ") + cudaGetErrorString(e));
+    P->fused = true;
+  }
+
   // ---- radial metric rows, zero padded to Pn / Pm ----
   const double* r = G->radii_m;
   std::vector<real> invr(Pn, 0), rr(Pn, 0), invcd(Pn, 0), mid(Pm, 0), invm(Pm, 0), invdr(Pm, 0);
@@ -1043,6 +1372,11 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
       UP(te_tab.tab, tab_e);
     }
   }
+  if (P->fused_pipe) {
+    UP(tf_tab.dptr, dptr_e);
+    UP(tf_tab.desc, desc_e);
+    UP(tf_tab.tab, tab_e);
+  }
   P->n_patches = oh.n;
   P->n_patches_e = oe.n;
   UP(oh.eptr, eptr_h);
@@ -1136,6 +1470,17 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     cudaError_t e = A.alloc(sizeof(Rec<real>), &P->d_rec);
     if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of launch record failed");
     CUDA_TRY(cudaMemcpy(P->d_rec, &R, sizeof(R), cudaMemcpyHostToDevice));
+  }
+  if (P->fused) {
+    // the record of the second field copy: the plan's record with the four field pointers moved
+    Rec<real> rb = R;
+    rb.er = (real*)P->fb[0];
+    rb.et = (real*)P->fb[1];
+    rb.hr = (real*)P->fb[2];
+    rb.ht = (real*)P->fb[3];
+    cudaError_t e = A.alloc(sizeof(Rec<real>), &P->d_rec_b);
+    if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "allocation of the second launch record failed");
+    CUDA_TRY(cudaMemcpy(P->d_rec_b, &rb, sizeof(rb), cudaMemcpyHostToDevice));
   }
   CUDA_TRY(cudaStreamCreateWithFlags(&P->capture_stream, cudaStreamNonBlocking));
   return IFDTD_OK;
@@ -1240,12 +1585,42 @@ cudaError_t launch_ke(ifdtd_plan* P, int istep, cudaStream_t st) {
   return P->plasma ? launch_ke_t<real, true, 12>(P, rec, istep, st) : launch_ke_t<real, false, 12>(P, rec, istep, st);
 }
 
+// One fused step: parity 0 reads the caller's arrays and writes the plan's
+// second copy, parity 1 the reverse.
 template <typename real>
-cudaError_t launch_step(ifdtd_plan* P, int istep, const ifdtd_probe* probe, int row, cudaStream_t st) {
-  const Rec<real>* rec = (const Rec<real>*)P->d_rec;
-  cudaError_t e = launch_kh<real>(P, st);
+cudaError_t launch_fused(ifdtd_plan* P, int istep, int parity, cudaStream_t st) {
+  const Rec<real>* a = (const Rec<real>*)P->d_rec;
+  const Rec<real>* b = (const Rec<real>*)P->d_rec_b;
+  if (P->fused_pipe) {
+    const int threads = P->kf_threads + 32 * P->kf_producers;
+    auto k = P->maxdeg == 6 ? (P->pipe_copy == 0 ? pipe::kf_tma<real, 6, 0> : pipe::kf_tma<real, 6, 1>)
+                            : (P->pipe_copy == 0 ? pipe::kf_tma<real, 12, 0> : pipe::kf_tma<real, 12, 1>);
+    cudaError_t e = allow_smem(k, P->kf_smem);
+    if (e == cudaSuccess) e = persistent_grid(P, k, threads, P->kf_smem, P->n_patches_e, &P->kf_grid);
+    if (e != cudaSuccess) return e;
+    k<<<P->kf_grid, threads, P->kf_smem, st>>>(parity ? b : a, parity ? a : b, P->kf_stage, P->kf_stages,
+                                               P->kf_producers, istep, P->kf_lanes);
+    return cudaGetLastError();
+  }
+  auto k = P->maxdeg == 6 ? fused_step_kernel<real, 6> : fused_step_kernel<real, 12>;
+  cudaError_t e = allow_smem(k, P->fused_smem);
   if (e != cudaSuccess) return e;
-  e = launch_ke<real>(P, istep, st);
+  k<<<P->n_patches_e, P->threads, P->fused_smem, st>>>(parity ? b : a, parity ? a : b, P->fused_tab, istep);
+  return cudaGetLastError();
+}
+
+template <typename real>
+cudaError_t launch_step(ifdtd_plan* P, int istep, const ifdtd_probe* probe, int row, cudaStream_t st, int parity = 0) {
+  const Rec<real>* rec = (const Rec<real>*)P->d_rec;
+  cudaError_t e;
+  if (P->fused) {
+    e = launch_fused<real>(P, istep, parity, st);
+    // the step's result is in the copy it wrote
+    if (!parity) rec = (const Rec<real>*)P->d_rec_b;
+  } else {
+    e = launch_kh<real>(P, st);
+    if (e == cudaSuccess) e = launch_ke<real>(P, istep, st);
+  }
   if (e != cudaSuccess) return e;
   if (probe) {
     const int blocks = (probe->rows * 32 + 255) / 256;
@@ -1268,6 +1643,7 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
     ~Range() { nvtxRangePop(); }
   } range(probe ? "ifdtd_step_sampled" : "ifdtd_step");
   const int cap = std::max(P->chunk, 1);
+  int parity = 0;  // fused step: 1 while the state is in the plan's second copy
   for (int s0 = 0; s0 < n; s0 += cap) {
     const int c = std::min(cap, n - s0);
     if (currents)
@@ -1282,7 +1658,9 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
         cudaGraph_t graph;
         CUDA_TRY(cudaStreamBeginCapture(P->capture_stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
-        for (int i = 0; i < c && le == cudaSuccess; ++i) le = launch_step<real>(P, i, probe, i, P->capture_stream);
+        // an even chunk (fused plans) starts and ends in the caller's arrays
+        for (int i = 0; i < c && le == cudaSuccess; ++i)
+          le = launch_step<real>(P, i, probe, i, P->capture_stream, P->fused ? (i & 1) : 0);
         cudaError_t ce = cudaStreamEndCapture(P->capture_stream, &graph);
         if (le != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le));
         if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
@@ -1294,13 +1672,20 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
       CUDA_TRY(cudaGraphLaunch(exec, stream));
     } else {
       for (int i = 0; i < c; ++i) {
-        cudaError_t e = launch_step<real>(P, i, probe, i, stream);
+        cudaError_t e = launch_step<real>(P, i, probe, i, stream, parity);
         if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+        if (P->fused) parity ^= 1;
       }
     }
     if (probe && out_rows)
       CUDA_TRY(cudaMemcpyAsync(out_rows + (size_t)s0 * probe->rows, probe->staging,
                                (size_t)c * probe->rows * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  }
+  if (parity) {
+    // an odd number of fused steps ended in the second copy: move it to the caller's arrays
+    void* const dst[4] = {st->er, st->et, st->hr, st->ht};
+    for (int i = 0; i < 4; ++i)
+      CUDA_TRY(cudaMemcpyAsync(dst[i], P->fb[i], P->fb_bytes[i], cudaMemcpyDeviceToDevice, stream));
   }
   return IFDTD_OK;
 }
@@ -1793,8 +2178,8 @@ int32_t ifdtd_wait_selftest(ifdtd_plan* plan, double* waited_seconds, void* stre
 
 int32_t ifdtd_plan_kernels(const ifdtd_plan* plan, int32_t* h_mode, int32_t* e_mode) {
   if (!plan || !h_mode || !e_mode) return fail(IFDTD_ERR_ARGUMENT, "null argument");
-  *h_mode = plan->h_mode;
-  *e_mode = plan->e_mode;
+  *h_mode = plan->fused ? 3 : plan->h_mode;
+  *e_mode = plan->fused ? (plan->fused_pipe ? 2 : 1) : plan->e_mode;
   return IFDTD_OK;
 }
 
@@ -1988,6 +2373,7 @@ int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t 
       return fail(IFDTD_ERR_ARGUMENT, "batch members must share one device and one precision");
     for (int j = 0; j < i; ++j)
       if (plans[j] == plans[i]) return fail(IFDTD_ERR_ARGUMENT, "a plan appears twice in the batch");
+    if (plans[i]->fused) return fail(IFDTD_ERR_UNSUPPORTED, "a fused-step plan cannot join a batch");
   }
   DeviceGuard guard(plans[0]->device);
   ifdtd_batch* B = new ifdtd_batch();

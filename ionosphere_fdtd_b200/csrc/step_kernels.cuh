@@ -448,11 +448,12 @@ __device__ __forceinline__ HEdgeLayer<real> h_edge_layer(const Rec<real>& R, con
   return y;
 }
 
+// The run's new values (h_edge_run stores them to htout).
 template <typename real>
-__device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, const HEdgeLayer<real>& y, int e,
-                                           int k0, const real* erh, const real* ert, const real* etr, const real* hto,
-                                           real* htout, real inv_t, const real* si_in, real* si_out, const real* si_sp,
-                                           const real* hnew = nullptr) {
+__device__ __forceinline__ Run<real> h_edge_value(const Rec<real>& R, const Layers<real>& Ls, const HEdgeLayer<real>& y,
+                                                  int e, int k0, const real* erh, const real* ert, const real* etr,
+                                                  const real* hto, real inv_t, const real* si_in, real* si_out,
+                                                  const real* si_sp, const real* hnew) {
   constexpr int N = Lanes<real>::N;
   const Run<real> vh = ld16(erh + k0), vt = ld16(ert + k0), vo = ld16(hto + k0);
   const Run<real> vu = y.up ? ld16(etr + k0) : zero_run<real>();
@@ -483,7 +484,26 @@ __device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real
       out.x[0] = h_new;
     }
   }
-  st16(htout + k0, out);
+  return out;
+}
+
+template <typename real>
+__device__ __forceinline__ void h_edge_run(const Rec<real>& R, const Layers<real>& Ls, const HEdgeLayer<real>& y, int e,
+                                           int k0, const real* erh, const real* ert, const real* etr, const real* hto,
+                                           real* htout, real inv_t, const real* si_in, real* si_out, const real* si_sp,
+                                           const real* hnew = nullptr) {
+  st16(htout + k0, h_edge_value(R, Ls, y, e, k0, erh, ert, etr, hto, inv_t, si_in, si_out, si_sp, hnew));
+}
+
+// New Hr at one face run from the old run hv, the three edges' Et runs and the
+// face's circulation weights w0..w2 (fc = hC at the run's midpoints).
+template <typename real>
+__device__ __forceinline__ Run<real> hr_value(const Run<real>& hv, const Run<real>& a0, const Run<real>& a1,
+                                              const Run<real>& a2, real w0, real w1, real w2, const Run<real>& fc) {
+  Run<real> hn;
+#pragma unroll
+  for (int r = 0; r < Lanes<real>::N; ++r) hn.x[r] = hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * fc.x[r];
+  return hn;
 }
 
 // Hr and the plasma current on midpoints j0..j0+N-1 of face f
@@ -506,10 +526,7 @@ __device__ __forceinline__ void h_face_run(const Rec<real>& R, const Layers<real
   real wv[4];
   ld4(fw, wv);
   const real w0 = wv[0], w1 = wv[1], w2 = wv[2];
-  Run<real> hn;
-#pragma unroll
-  for (int r = 0; r < N; ++r) hn.x[r] = hv.x[r] - (w0 * a0.x[r] + w1 * a1.x[r] + w2 * a2.x[r]) * fc.x[r];
-  st16(hrout + j0, hn);
+  st16(hrout + j0, hr_value(hv, a0, a1, a2, w0, w1, w2, fc));
   if (!PLASMA) return;
   // radial E at midpoints: mean of the three vertices' nodes j and j+1
   const Run<real> na = ld16(pa + j0), nb = ld16(pb + j0), nc = ld16(pc + j0);

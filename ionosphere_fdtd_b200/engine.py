@@ -50,8 +50,12 @@ class Tuning:
     warps the E phase runs wide CTAs of at most 640 threads at 96 registers)
     the ring stages the balanced E patches are sized for (0: 2), the
     copy-issuing warps of an E-phase CTA (0: 4 when both thread counts are
-    automatic, else as ``producer_warps``), and the
-    row gaps every E-phase copy bridges (0-8: fewer, longer bulk copies).
+    automatic, else as ``producer_warps``), the
+    row gaps every E-phase copy bridges (0-8: fewer, longer bulk copies), and
+    ``fused_step`` (1: one launch per leapfrog step in which every E patch
+    recomputes the new H on its halo, for plans without plasma or surface
+    impedance; the plan then holds a second copy of the field arrays and
+    cannot join an ``Ensemble``).
     Every choice computes the same bits."""
 
     faces_per_patch: int = 0
@@ -65,6 +69,7 @@ class Tuning:
     e_stages: int = 0
     e_producer_warps: int = 0
     e_copy_gap: int = 0
+    fused_step: int = 0
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -175,7 +180,8 @@ class Engine:
             pd.vertex_face_weights = f64(p["vertex_face_weights"])
         t = self.tuning
         td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps, t.lane_layout,
-                      t.e_threads, t.e_stages, t.e_producer_warps, t.e_copy_gap)
+                      t.e_threads, t.e_stages, t.e_producer_warps, t.e_copy_gap,
+                      t.fused_step)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(
@@ -208,11 +214,12 @@ class Engine:
     @property
     def kernel_modes(self) -> tuple[str, str]:
         """Kernel family of the H and E phases: "direct" (global gathers) or
-        "pipeline" (warp-specialised shared-memory pipeline)."""
+        "pipeline" (warp-specialised shared-memory pipeline); a fused plan
+        reports ("fused", family of its one-launch kernel)."""
 
         h, e = C.c_int32(), C.c_int32()
         N.check(N.load().ifdtd_plan_kernels(self.plan, C.byref(h), C.byref(e)), "ifdtd_plan_kernels")
-        name = {1: "direct", 2: "pipeline"}
+        name = {1: "direct", 2: "pipeline", 3: "fused"}
         return name[h.value], name[e.value]
 
     def status_word(self, reset: bool = False) -> int:

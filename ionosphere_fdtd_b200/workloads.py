@@ -5,7 +5,9 @@ setup (material profile, plasma profile, source, receivers) built from a seed.
 
 * ``config1``: s2 / 24 cells, ground sigma 1e-2 S/m, air sigma 0 below 50 km
   and 1e-7 exp((h - 60 km)/4 km) S/m capped at 1e-3 above, one vertical 20 Hz
-  Gaussian current at a seed-chosen vertex, 8 seed-chosen surface receivers.
+  Gaussian current at a seed-chosen vertex, 8 seed-uniform surface receivers
+  (mesh level and radial cells can be raised: the fused-step comparison runs
+  it at s9 / 80).
 * ``config2``: s7 / 40 cells, FP32, the config-1 conductivity plus a Drude
   electron plasma n_e(h) = 1e6 exp((h - 85 km)/3 km) m^-3,
   nu(h) = 1e7 exp(-(h - 70 km)/6 km) s^-1, a 50 Hz source and 64 receivers at
@@ -139,6 +141,19 @@ def algorithmic_bytes_per_step(sim) -> int:
     if sim._surface_impedance_ade is not None:
         n += int(sim._surface_impedance_ade.memory.numel())
     return 2 * item * n
+
+
+def config1(device: str = "cuda", dtype: str = "float32", seed: int = 20260801, subdivision: int = 2, radial_cells: int = 24, receivers: int = 8, **kwargs) -> Workload:
+    from .mesh import build_geodesic_mesh
+    from .solver import GeodesicFDTD, SimulationConfig
+
+    cfg = SimulationConfig(subdivision=subdivision, radial_cells=radial_cells)
+    mesh = build_geodesic_mesh(subdivision)
+    lat, lon = vertex_lat_lon(mesh.vertices, int(np.random.default_rng(seed).integers(mesh.n_vertices)))
+    source = GaussianCurrent(latitude_deg=lat, longitude_deg=lon, peak_current_a=1.0, carrier_frequency_hz=20.0)
+    sim = GeodesicFDTD(cfg, material=ProfileMaterial(), source=source, mesh=mesh, device=device, dtype=dtype, **kwargs)
+    rec = uniform_receivers(sim, receivers, seed)
+    return Workload("config1", sim, rec, mesh.n_vertices * radial_cells, algorithmic_bytes_per_step(sim))
 
 
 def config2(device: str = "cuda", dtype: str = "float32", seed: int = 20260805, subdivision: int = 7, radial_cells: int = 40, receivers: int = 64, **kwargs) -> Workload:

@@ -26,7 +26,7 @@ def _same(a: dict, b: dict) -> bool:
     return a.keys() == b.keys() and all(np.array_equal(a[k], b[k]) for k in a)
 
 
-@pytest.mark.parametrize("name", ["plasma_drude_s2", "config4_mini_s2"])
+@pytest.mark.parametrize("name", ["plasma_drude_s2", "config4_mini_s2", "source_s1"])
 def test_autotune_installs_the_fastest_plan_and_keeps_the_state(name):
     from ionosphere_fdtd_b200.autotune import DEFAULT_CANDIDATES, autotune
 
@@ -42,6 +42,9 @@ def test_autotune_installs_the_fastest_plan_and_keeps_the_state(name):
     assert timed
     assert res.best == min(timed, key=lambda x: x[1])[0] and res.best_ms == min(ms for _, ms in timed)
     assert sim._engine.tuning == res.best
+    # the fused candidates are timed on plans without plasma or surface impedance only
+    fused_timed = [t for t, ms, err in res.timings if t.fused_step and ms is not None]
+    assert bool(fused_timed) == (name == "source_s1")
     sim.step(40)
     twin.step(40)
     assert _same(_arrays(sim), _arrays(twin))
