@@ -352,34 +352,56 @@ ENSEMBLE_METRIC = "ensemble runs/s"
 RUN_STEPS = 5000  # leapfrog steps per ensemble run
 
 
-def oracle_ensemble_rate(steps: int = 1) -> dict:
-    """CPU oracle rate (Gcell/s) on a mid-size ensemble member: s6 / 40 cells,
-    exponential ionosphere, float32, one Gaussian source."""
+ENSEMBLE_SAMPLE = 4  # the first four members of the draws: s7/51, s6/41, s6/39 and s7/26 (15.9 M cells)
 
-    import oracle.fdtd as O
 
-    sim = O.OracleFDTD(subdivision=6, radial_cells=40, material=O.EarthIonosphereParams(lithosphere_conductivity_s_m=1.0e-2),
-                       dtype=np.float32, source=O.OracleSource(peak_current_a=1.0, carrier_frequency_hz=30.0))
-    info = {"cells": sim.mesh.n_vertices * 40, "sub": 6, "L": 40}
-    stepper = oracle_stepper(sim)
-    stepper.step(1)
-    return oracle_time(stepper, info, steps)
+def oracle_ensemble_sampler(members: int = ENSEMBLE_SAMPLE) -> tuple[list, int]:
+    """The oracle on the first ``members`` members of the ensemble workload
+    (float32, each member with its own threaded stepper) and their cells."""
+
+    import oracle.workloads as OW
+    from oracle.fdtd import build_mesh
+
+    meshes, steppers, cells = {}, [], 0
+    for d in OW.config3_draws(members=members):
+        sub = d["subdivision"]
+        if sub not in meshes:
+            meshes[sub] = build_mesh(sub)
+        steppers.append(oracle_stepper(OW.config3_member(d, mesh=meshes[sub])))
+        cells += meshes[sub].n_vertices * d["radial_cells"]
+    return steppers, cells
+
+
+def oracle_ensemble_time(steppers: list, cells: int, steps: int = 1) -> dict:
+    """Time ``steps`` leapfrog steps of every sampled member, one member after another."""
+
+    t0 = time.perf_counter()
+    for stepper in steppers:
+        stepper.step(steps)
+    dt = time.perf_counter() - t0
+    return {"gcells": cells * steps / dt / 1e9, "seconds": dt, "steps": steps, "cores": steppers[0].threads, "cells": cells}
+
+
+def ensemble_sample_text(r: dict, mean_cells: float, per: str) -> str:
+    return (f"{per} of the ensemble's first {ENSEMBLE_SAMPLE} members (s7/51, s6/41, s6/39, s7/26; {r['cells']} cells; "
+            f"{r['seconds']:.1f} s), oracle on PyTorch CPU tensors over {r['cores']} threads; runs/s = rate / "
+            f"({RUN_STEPS} steps x mean member cells {mean_cells:.0f})")
 
 
 def ensemble_reference_arm(args) -> None:
     cells = ensemble_cells(args.members)
     mean_cells = statistics.mean(cells)
+    steppers, sample_cells = oracle_ensemble_sampler()
     rates, secs = [], 0.0
     for _ in range(args.warmup):
-        oracle_ensemble_rate()
+        oracle_ensemble_time(steppers, sample_cells)
     for _ in range(args.steps):
-        r = oracle_ensemble_rate()
+        r = oracle_ensemble_time(steppers, sample_cells)
         rates.append(r["gcells"])
         secs += r["seconds"]
     gcells = statistics.median(rates)
     value = gcells * 1e9 / (RUN_STEPS * mean_cells)
-    sample = (f"1 leapfrog step of an s6/L40 float32 member per bench step ({r['cells']} cells), oracle on PyTorch CPU "
-              f"tensors over {r['cores']} threads; runs/s = rate / ({RUN_STEPS} steps x mean member cells {mean_cells:.0f})")
+    sample = ensemble_sample_text(r, mean_cells, "1 leapfrog step per bench step")
     line = {
         "impl": "reference", "metric": ENSEMBLE_METRIC, "value": value, "unit": "runs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
@@ -517,15 +539,17 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
     cells = [w.cells for w in wls]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = oracle_ensemble_rate()
+        steppers, sample_cells = oracle_ensemble_sampler()
+        oracle_ensemble_time(steppers, sample_cells)
+        r = oracle_ensemble_time(steppers, sample_cells, steps=60)
         cpu = {
             "value": r["gcells"] * 1e9 / (RUN_STEPS * statistics.mean(cells)),
             "unit": "runs/s",
             "cores": r["cores"],
             "kind": "port",
-            "sample": (f"1 leapfrog step of an s6/L40 float32 member ({r['seconds']:.1f} s), oracle on PyTorch CPU tensors over "
-                       f"{r['cores']} threads; runs/s = rate / ({RUN_STEPS} x mean member cells)"),
+            "sample": ensemble_sample_text(r, statistics.mean(cells), "60 leapfrog steps, after 1 warm-up step,"),
         }
+        del steppers
     for p in probes:
         p.close()
     if rank == 0:

@@ -28,7 +28,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .fdtd import OracleFDTD, OraclePlasma, OracleSource, OracleSpecies, OracleSurface, build_mesh
+from .fdtd import (EPSILON_0, EarthIonosphereParams, OracleFDTD, OraclePlasma, OracleSource, OracleSpecies, OracleSurface,
+                   build_mesh)
 
 ELEMENTARY_CHARGE_C = 1.602_176_634e-19
 ELECTRON_MASS_KG = 9.109_383_713_9e-31
@@ -158,3 +159,22 @@ def config3_draws(seed: int = 20260803, members: int = 64) -> list[dict]:
         d["receiver_seed"] = int(rng.integers(1 << 31))
         out.append(d)
     return out
+
+
+def config3_member(draw: dict, mesh=None, dtype=np.float32) -> OracleFDTD:
+    """One member of the ensemble workload on the oracle (fields zero): the
+    exponential ionosphere (``sigma0`` at ``h0``, scale height ``zeta``) over
+    a homogeneous ground of conductivity ``ground``, the default -100..100 km
+    column, and a Gaussian current of the drawn carrier at vertex
+    ``source_draw mod n_vertices``."""
+
+    mesh = build_mesh(draw["subdivision"]) if mesh is None else mesh
+    lat, lon = vertex_lat_lon(mesh.vertices, draw["source_draw"] % mesh.n_vertices)
+    material = EarthIonosphereParams(
+        lithosphere_conductivity_s_m=draw["ground"], ionosphere_reference_height_m=draw["h0"],
+        ionosphere_scale_height_m=draw["zeta"], ionosphere_prefactor_hz=draw["sigma0"] / EPSILON_0,
+    )
+    return OracleFDTD(
+        subdivision=draw["subdivision"], radial_cells=draw["radial_cells"], material=material, mesh=mesh, dtype=dtype,
+        source=OracleSource(latitude_deg=lat, longitude_deg=lon, peak_current_a=1.0, carrier_frequency_hz=draw["carrier"]),
+    )

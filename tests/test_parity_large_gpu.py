@@ -7,6 +7,9 @@ kernels run many patches per CTA, balanced E patches and bridged copy
 descriptors:
 
 * config 2: s7 x 40 radial cells, Drude plasma, 64 receivers;
+* config 3: the first five members of the 64-member ensemble (s5-s7, 26-57
+  radial cells, exponential ionospheres of their own draws, 16 receivers each)
+  advanced together through ``Ensemble`` (the batched kernels);
 * config 4 physics (surface impedance over the smooth ground map, Drude
   plasma, 256 receivers) on s8 x 80 radial cells: the full s9 workload's oracle
   needs about 4x the ~60 GB of host memory the s8 oracle takes (its plasma
@@ -98,7 +101,8 @@ def _oracle_run(sim, receivers, steps: int) -> dict:
     out["traces"] = traces
     if sim.surface is not None:
         out["si_memory"] = sim.si_memory
-    out["plasma_current_0"] = sim.p_current[0]
+    if getattr(sim, "p_current", None):
+        out["plasma_current_0"] = sim.p_current[0]
     return out
 
 
@@ -172,3 +176,57 @@ def test_float32_engine_tracks_float64_engine_on_the_s9_workload():
     for key in ("traces", "plasma_current_0", "si_memory"):
         assert rel_l2(runs["float32"][key], runs["float64"][key]) <= 1e-5, key
 
+
+def test_ensemble_members_match_oracle_at_benchmark_size():
+    """The first five members of the ensemble workload (s7/51, s6/41, s6/39,
+    s7/26 and s5/57: three mesh levels, five radial grids and five ionosphere
+    draws), seeded as the bench seeds them and advanced 5 steps together by
+    ``Ensemble`` in float64 and in float32, against each member's oracle run
+    with the same receivers: the same tolerances as above."""
+
+    import torch
+
+    import oracle.workloads as OW
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200 import workloads as W
+
+    members, steps = 5, 5
+    draws = OW.config3_draws(members=members)
+    meshes, oracles = {}, []
+    for i, d in enumerate(draws):
+        sub = d["subdivision"]
+        if sub not in meshes:
+            from oracle.fdtd import build_mesh
+
+            meshes[sub] = build_mesh(sub)
+        o = OW.config3_member(d, mesh=meshes[sub], dtype=np.float64)
+        OW.seed_fields(o, seed=20260814 + i)
+        oracles.append(o)
+    runs = {}
+    for dtype in ("float64", "float32"):
+        wls = W.config3_members(device="cuda", dtype=dtype, members=members)
+        for wl, o in zip(wls, oracles):
+            sim = wl.simulation
+            assert sim.time_step_s == pytest.approx(o.dt, rel=1e-14)
+            for f in ("er", "et", "hr", "ht"):
+                getattr(sim, f).copy_(torch.from_numpy(getattr(o, f)).to(getattr(sim, f).dtype))
+        receivers = [wl.receivers for wl in wls]
+        with Ensemble([wl.simulation for wl in wls]) as ens:
+            traces = ens.record_er_observations(receivers, steps)
+        runs[dtype] = []
+        for wl, tr in zip(wls, traces):
+            sim = wl.simulation
+            out = {f: sim.to_numpy(getattr(sim, f)) for f in ("er", "et", "hr", "ht")}
+            out["traces"] = tr
+            assert sim._engine.status_word() == 0
+            runs[dtype].append(out)
+        del wls, ens
+        torch.cuda.empty_cache()
+    for i, o in enumerate(oracles):
+        expected = _oracle_run(o, receivers[i], steps)
+        e64 = grouped_rel_l2(runs["float64"][i], expected)
+        assert max(e64.values()) < 1e-11, (i, e64)
+        e32 = grouped_rel_l2(runs["float32"][i], expected)
+        assert max(e32.values()) <= 1e-5, (i, e32)
+        assert rel_l2(runs["float64"][i]["traces"], expected["traces"]) < 1e-11, i
+        assert rel_l2(runs["float32"][i]["traces"], expected["traces"]) <= 1e-5, i
