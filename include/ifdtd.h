@@ -131,8 +131,9 @@ typedef struct ifdtd_tuning {
   int32_t fused_step;        /* 1: one launch per leapfrog step, each E-phase patch recomputing the new H it
                                 reads on its halo (plans without plasma or surface impedance; the plan holds a
                                 second copy of the four field arrays and alternates between the copies, copying
-                                back after an odd number of steps; graph_chunk must be even; the plan cannot
-                                join a batch).  staging 0 / 2 / 3: patches staged through the pipelined ring
+                                back after an odd number of steps; graph_chunk must be even; in a batch (even
+                                chunk) it runs the batched ring kernel).  staging 0 / 2 / 3: patches staged
+                                through the pipelined ring
                                 (TMA bulk copies / cp.async), the new H overwriting the old in the stage;
                                 staging 1: direct gathers with the halo's new H in shared memory.
                                 e_faces_per_patch sets the patch (0: the largest of 64 ... 8 faces whose stage

@@ -166,6 +166,8 @@ SHAPE_FREE_CANDIDATES: tuple[Tuning, ...] = (
     Tuning(producer_warps=3),
     Tuning(e_producer_warps=2),
     Tuning(e_producer_warps=3),
+    Tuning(fused_step=1),
+    Tuning(fused_step=1, lane_layout=2),
 )
 
 
@@ -178,8 +180,6 @@ def autotune_ensemble(members: Sequence, candidates: Sequence[Tuning] = DEFAULT_
     ``SHAPE_FREE_CANDIDATES``).  Call it before building the ``Ensemble``: the
     batch reads the members' plans when it is created."""
 
-    # a fused-step plan cannot join a batch
-    candidates = [c for c in candidates if not c.fused_step]
     classes: dict[tuple, list] = {}
     for m in members:
         classes.setdefault((key or _tuning_class)(m), []).append(m)

@@ -290,5 +290,49 @@ __global__ void __maxnreg__(kMaxRegs) kf_tma(const Rec<real>* __restrict__ rin, 
   }
 }
 
+// Batched fused step over ensemble members that share the template
+// arguments (the walk of kh_tma_batch): CTA b walks segments
+// segs[sptr[b]] .. segs[sptr[b + 1] - 1] = {member, first patch, end patch, 0};
+// rin[member] / rout[member] are that member's records of the copy it reads
+// and the copy it writes; rings[member] = {stage bytes, stages}.
+template <typename real, int MAXDEG, int COPY>
+__global__ void __maxnreg__(kMaxRegs) kf_tma_batch(const Rec<real>* __restrict__ rin, const Rec<real>* __restrict__ rout,
+                                                   const int4* __restrict__ segs, const int* __restrict__ sptr,
+                                                   const int2* __restrict__ rings, int producers, int istep,
+                                                   int layout) {
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  __shared__ Rec<real> R;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], group[kMaxStages];
+  __shared__ int abort_flag;
+  const int W = producers;
+  if (threadIdx.x == 0) abort_flag = 0;
+  int prev = 0;
+  for (int k = sptr[blockIdx.x]; k < sptr[blockIdx.x + 1]; ++k) {
+    __syncthreads();
+    if (abort_flag) break;
+    const int4 sg = segs[k];
+    const int2 rg = rings[sg.x];
+    batch_segment_start<real>(full, empty, group, prev, rg.y, (blockDim.x - 32 * W) / 32);
+    prev = rg.y;
+    Layers<real> Ls;
+    Ring G;
+    ring_setup(R, rin + sg.x, dyn_smem, full, empty, &abort_flag, rg.x, rg.y, COPY == 0 ? W : 32 * W, W, Ls, G);
+    if (threadIdx.x < 32 * W) {
+      produce<COPY>(R, G, sg.y, sg.z, R.n_patches_e, R.dptr_e, R.desc_e, R.tab_e, threadIdx.x / 32, W);
+    } else {
+      const Rec<real>* ro = rout + sg.x;
+      real* const er_out = ro->er;
+      real* const et_out = ro->et;
+      real* const hr_out = ro->hr;
+      real* const ht_out = ro->ht;
+      const int ct = threadIdx.x - 32 * W, nct = blockDim.x - 32 * W;
+      const real current = (R.n_src_er + R.n_src_et) > 0 ? (real)R.cur[istep] : real(0);
+      consume_ring(G, sg.y, sg.z, [&](unsigned char* st, int s, uint32_t ph) {
+        kf_consume<real, MAXDEG>(R, Ls, st, ct, nct, current, layout, group + s, ph, G, er_out, et_out, hr_out, ht_out);
+      });
+    }
+  }
+}
+
 }  // namespace pipe
 }  // namespace ifdtd

@@ -131,6 +131,7 @@ struct ifdtd_plan {
   bool fused_pipe = false;  // the fused step through the ring (pipe::kf_tma) rather than direct gathers
   int kf_stage = 0, kf_stages = 0, kf_grid = 0, kf_threads = 0, kf_producers = 0, kf_lanes = 0;
   size_t kf_smem = 0;
+  std::vector<float> kf_cost;  // staged bytes per fused patch (balances batched launches)
   FusedTables fused_tab{};
   size_t fused_smem = 0;
   void* d_rec_b = nullptr;
@@ -640,6 +641,8 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   int fpp_e = auto_e ? 16 : tune->e_faces_per_patch;
   const bool fused = tune && tune->fused_step != 0;
   if (tune && (tune->fused_step < 0 || tune->fused_step > 1)) return fail(IFDTD_ERR_ARGUMENT, "fused_step must be 0 or 1");
+  if (fused && (X->plasma_species > 0 || X->si_terms > 0))
+    return fail(IFDTD_ERR_UNSUPPORTED, "fused_step supports plans without plasma and without surface impedance");
   // the fused step replaces both phases; its plan keeps the direct kernels for
   // the single-phase entry points
   const int staging = fused ? 1 : (tune ? tune->staging : 0);
@@ -937,8 +940,6 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   // ---- fused step: E patches with their halo edge and face lists ----
   PipeTables tf_tab;  // the ring's descriptors and blobs (uploaded with the E-phase tables)
   if (fused) {
-    if (S > 0 || X->si_terms > 0)
-      return fail(IFDTD_ERR_UNSUPPORTED, "fused_step supports plans without plasma and without surface impedance");
     if (P->chunk % 2) return fail(IFDTD_ERR_ARGUMENT, "fused_step needs an even graph_chunk");
     std::vector<int> patch_of_edge(nE), stamp_e(nE), stamp_f(nF), loc_e(nE), loc_f(nF);
     std::vector<int> halo_e, own_f, halo_f;
@@ -1054,6 +1055,9 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
         const int wide = std::max((Pn / (int)(16 / sizeof(real)) + 7) & ~7, (Pm / (int)(16 / sizeof(real)) + 7) & ~7);
         P->kf_lanes = lane_layout == 2 && wide <= f_threads ? 1 : 0;
         P->pipe_copy = fused_staging == 3 ? 1 : 0;
+        P->kf_cost.assign(o.n, 0.f);
+        for (int q = 0; q < o.n; ++q)
+          for (int d = t.dptr[q]; d < t.dptr[q + 1]; ++d) P->kf_cost[q] += (float)t.desc[d].w;
         tf_tab = std::move(t);
         P->fused_pipe = true;
         done = true;
@@ -1718,10 +1722,14 @@ int grid_for(size_t n) {
 // are sampled by one launch per step.
 // ---------------------------------------------------------------------------
 struct BatchGroup {
-  int plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2, lanes = 0, e_threads = 0, e_producers = 2;
+  // fused: members on the fused step (pipe::kf_tma_batch; threads, producers
+  // and lanes are then the fused kernel's)
+  int fused = 0, plasma = 0, maxdeg = 6, copy = 0, threads = 0, producers = 2, lanes = 0, e_threads = 0, e_producers = 2;
   std::vector<int> members;
-  size_t kh_smem = 0, ke_smem = 0;
-  int kh_grid = 0, ke_grid = 0;
+  size_t kh_smem = 0, ke_smem = 0, kf_smem = 0;
+  int kh_grid = 0, ke_grid = 0, kf_grid = 0;
+  const int4* segs_f = nullptr;
+  const int* sptr_f = nullptr;
   const int4* segs_h = nullptr;
   const int* sptr_h = nullptr;
   const int4* segs_e = nullptr;
@@ -1736,6 +1744,12 @@ struct ifdtd_batch {
   DeviceArena arena;
   void* d_recs = nullptr;  // one record per member: bound fields, currents from d_cur
   std::vector<unsigned char> h_recs;
+  // fused-step members: their records pointed at the plans' second field
+  // copies (other members' records as in d_recs), and the ring table
+  bool any_fused = false;
+  void* d_recs_b = nullptr;
+  std::vector<unsigned char> h_recs_b;
+  const int2* d_ring_f = nullptr;
   size_t rec_bytes = 0;
   double* d_cur = nullptr;  // (n, chunk) step currents
   const int2* d_ring_h = nullptr;
@@ -1832,6 +1846,13 @@ auto batch_ke_kernel(const BatchGroup& g) {
               : g.copy ? ke_tma_batch<real, false, 12, 1, kMaxRegs> : ke_tma_batch<real, false, 12, 0, kMaxRegs>;
 }
 
+template <typename real>
+auto batch_kf_kernel(const BatchGroup& g) {
+  using namespace pipe;
+  if (g.maxdeg == 6) return g.copy ? kf_tma_batch<real, 6, 1> : kf_tma_batch<real, 6, 0>;
+  return g.copy ? kf_tma_batch<real, 12, 1> : kf_tma_batch<real, 12, 0>;
+}
+
 template <typename K>
 cudaError_t batch_grid(K kernel, int threads, size_t smem, int sm_count, int n_patches, int* grid) {
   cudaError_t e = allow_smem(kernel, smem);
@@ -1849,24 +1870,35 @@ int batch_build(ifdtd_batch* B) {
   B->rec_bytes = sizeof(Rec<real>);
   for (int i = 0; i < B->n; ++i) {
     ifdtd_plan* P = B->plans[i];
-    if (P->h_mode != 2 || P->e_mode != 2) {
+    BatchGroup key;
+    if (P->fused) {
+      if (!P->fused_pipe) return fail(IFDTD_ERR_UNSUPPORTED, "a fused-step plan on direct gathers cannot join a batch");
+      key.fused = 1;
+      key.maxdeg = P->maxdeg;
+      key.copy = P->pipe_copy;
+      key.threads = P->kf_threads;
+      key.producers = P->kf_producers;
+      key.lanes = P->kf_lanes;
+      key.e_threads = key.e_producers = 0;
+      B->any_fused = true;
+    } else if (P->h_mode != 2 || P->e_mode != 2) {
       B->solo.push_back(i);
       continue;
+    } else {
+      key.plasma = P->plasma ? 1 : 0;
+      key.maxdeg = P->maxdeg;
+      key.copy = P->pipe_copy;
+      key.threads = P->threads;
+      key.producers = P->producers;
+      key.lanes = P->lanes;
+      key.e_threads = P->e_threads;
+      key.e_producers = P->e_producers;
     }
-    BatchGroup key;
-    key.plasma = P->plasma ? 1 : 0;
-    key.maxdeg = P->maxdeg;
-    key.copy = P->pipe_copy;
-    key.threads = P->threads;
-    key.producers = P->producers;
-    key.lanes = P->lanes;
-    key.e_threads = P->e_threads;
-    key.e_producers = P->e_producers;
     BatchGroup* g = nullptr;
     for (auto& x : B->groups)
-      if (x.plasma == key.plasma && x.maxdeg == key.maxdeg && x.copy == key.copy && x.threads == key.threads &&
-          x.producers == key.producers && x.lanes == key.lanes && x.e_threads == key.e_threads &&
-          x.e_producers == key.e_producers)
+      if (x.fused == key.fused && x.plasma == key.plasma && x.maxdeg == key.maxdeg && x.copy == key.copy &&
+          x.threads == key.threads && x.producers == key.producers && x.lanes == key.lanes &&
+          x.e_threads == key.e_threads && x.e_producers == key.e_producers)
         g = &x;
     if (!g) {
       B->groups.push_back(key);
@@ -1874,17 +1906,37 @@ int batch_build(ifdtd_batch* B) {
     }
     g->members.push_back(i);
   }
-  std::vector<int2> ring_h(B->n, make_int2(0, 0)), ring_e(B->n, make_int2(0, 0));
+  std::vector<int2> ring_h(B->n, make_int2(0, 0)), ring_e(B->n, make_int2(0, 0)), ring_f(B->n, make_int2(0, 0));
   for (const auto& g : B->groups)
     for (const int i : g.members) {
       const ifdtd_plan* P = B->plans[i];
       ring_h[i] = make_int2(P->kh_stage, P->kh_stages);
       ring_e[i] = make_int2(P->ke_stage, P->ke_stages);
+      ring_f[i] = make_int2(P->kf_stage, P->kf_stages);
     }
-  if (B->arena.upload(ring_h, &B->d_ring_h) != cudaSuccess || B->arena.upload(ring_e, &B->d_ring_e) != cudaSuccess)
+  if (B->arena.upload(ring_h, &B->d_ring_h) != cudaSuccess || B->arena.upload(ring_e, &B->d_ring_e) != cudaSuccess ||
+      B->arena.upload(ring_f, &B->d_ring_f) != cudaSuccess)
     return fail(IFDTD_ERR_CUDA, "upload of batch ring table failed");
   const int sm_count = B->plans[0]->sm_count;
   for (auto& g : B->groups) {
+    if (g.fused) {
+      int nf = 0;
+      std::vector<const std::vector<float>*> cf;
+      for (const int i : g.members) {
+        const ifdtd_plan* P = B->plans[i];
+        g.kf_smem = std::max(g.kf_smem, P->kf_smem);
+        nf += P->n_patches_e;
+        cf.push_back(&P->kf_cost);
+      }
+      cudaError_t e = batch_grid(batch_kf_kernel<real>(g), g.threads + 32 * g.producers, g.kf_smem, sm_count, nf, &g.kf_grid);
+      if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batched launch shape: ") + cudaGetErrorString(e));
+      std::vector<int4> segs;
+      std::vector<int> sptr;
+      split_patches(g.members, cf, g.kf_grid, segs, sptr);
+      if (B->arena.upload(segs, &g.segs_f) != cudaSuccess || B->arena.upload(sptr, &g.sptr_f) != cudaSuccess)
+        return fail(IFDTD_ERR_CUDA, "upload of batch segments failed");
+      continue;
+    }
     int nh = 0, ne = 0;
     std::vector<const std::vector<float>*> ch, ce;
     for (const int i : g.members) {
@@ -1921,18 +1973,34 @@ int batch_build(ifdtd_batch* B) {
     std::memcpy(B->h_recs.data() + (size_t)i * B->rec_bytes, B->plans[i]->h_rec.data(), B->rec_bytes);
     reinterpret_cast<Rec<real>*>(B->h_recs.data() + (size_t)i * B->rec_bytes)->cur = B->d_cur + (size_t)i * B->chunk;
   }
+  if (B->any_fused && B->arena.alloc((size_t)B->n * B->rec_bytes, &B->d_recs_b) != cudaSuccess)
+    return fail(IFDTD_ERR_CUDA, "allocation of batch records failed");
   CUDA_TRY(cudaStreamCreateWithFlags(&B->capture_stream, cudaStreamNonBlocking));
   return IFDTD_OK;
 }
 
+// parity (fused-step members): 0 reads the caller's arrays and writes the
+// plans' second copies, 1 the reverse.
 template <typename real>
-cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row, cudaStream_t st) {
+cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row, cudaStream_t st, int parity = 0) {
   const Rec<real>* recs = (const Rec<real>*)B->d_recs;
+  const Rec<real>* recs_b = (const Rec<real>*)B->d_recs_b;
   cudaError_t e = cudaSuccess;
   // every launch is checked at once, so a failure reports its own error
   // rather than the invalidated capture it leaves behind
   for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
     const BatchGroup& g = B->groups[q];
+    if (!g.fused) continue;
+    auto k = batch_kf_kernel<real>(g);
+    k<<<g.kf_grid, g.threads + 32 * g.producers, g.kf_smem, st>>>(parity ? recs_b : recs, parity ? recs : recs_b,
+                                                                   g.segs_f, g.sptr_f, B->d_ring_f, g.producers, istep,
+                                                                   g.lanes);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) B->failed = "kf_tma_batch of group " + std::to_string(q);
+  }
+  for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
+    const BatchGroup& g = B->groups[q];
+    if (g.fused) continue;
     auto k = batch_kh_kernel<real>(g);
     k<<<g.kh_grid, g.threads + 32 * g.producers, g.kh_smem, st>>>(recs, g.segs_h, g.sptr_h, B->d_ring_h, g.producers,
                                                                    g.lanes);
@@ -1945,6 +2013,7 @@ cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row,
   }
   for (size_t q = 0; q < B->groups.size() && e == cudaSuccess; ++q) {
     const BatchGroup& g = B->groups[q];
+    if (g.fused) continue;
     auto k = batch_ke_kernel<real>(g);
     k<<<g.ke_grid, g.e_threads + 32 * g.e_producers, g.ke_smem, st>>>(recs, g.segs_e, g.sptr_e, B->d_ring_e, g.e_producers,
                                                                    istep, g.lanes);
@@ -1956,7 +2025,9 @@ cudaError_t batch_launch_step(ifdtd_batch* B, int istep, int rows, int step_row,
     if (e != cudaSuccess) B->failed = "E phase of member " + std::to_string(B->solo[q]);
   }
   if (rows > 0 && e == cudaSuccess) {
-    sample_batch_kernel<real><<<(rows * 32 + 255) / 256, 256, 0, st>>>(recs, (const ProbeRef*)B->d_refs,
+    // after a parity-0 step the fused members' state is in their second copies
+    const Rec<real>* now = B->any_fused && !parity ? recs_b : recs;
+    sample_batch_kernel<real><<<(rows * 32 + 255) / 256, 256, 0, st>>>(now, (const ProbeRef*)B->d_refs,
                                                                          (const int2*)B->d_rowmap, rows, step_row);
     e = cudaGetLastError();
     if (e != cudaSuccess) B->failed = "sample_batch_kernel";
@@ -1992,6 +2063,19 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
     }
     // pageable source: the runtime stages it before returning
     CUDA_TRY(cudaMemcpyAsync(B->d_recs, B->h_recs.data(), B->h_recs.size(), cudaMemcpyHostToDevice, stream));
+    if (B->any_fused) {
+      B->h_recs_b = B->h_recs;
+      for (int i = 0; i < B->n; ++i) {
+        const ifdtd_plan* P = B->plans[i];
+        if (!P->fused) continue;
+        Rec<real>* R = reinterpret_cast<Rec<real>*>(B->h_recs_b.data() + (size_t)i * B->rec_bytes);
+        R->er = (real*)P->fb[0];
+        R->et = (real*)P->fb[1];
+        R->hr = (real*)P->fb[2];
+        R->ht = (real*)P->fb[3];
+      }
+      CUDA_TRY(cudaMemcpyAsync(B->d_recs_b, B->h_recs_b.data(), B->h_recs_b.size(), cudaMemcpyHostToDevice, stream));
+    }
     B->last.assign(states, states + B->n);
     B->have_state = true;
   }
@@ -2037,6 +2121,7 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
     ~Range() { nvtxRangePop(); }
   } range("ifdtd_batch_step");
   const int cap = std::max(B->chunk, 1);
+  int parity = 0;  // fused-step members: 1 while their state is in the second copies
   for (int s0 = 0; s0 < n; s0 += cap) {
     const int c = std::min(cap, n - s0);
     if (currents) {
@@ -2057,7 +2142,9 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
         cudaGraph_t graph;
         CUDA_TRY(cudaStreamBeginCapture(B->capture_stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t le = cudaSuccess;
-        for (int i = 0; i < c && le == cudaSuccess; ++i) le = batch_launch_step<real>(B, i, rows, i, B->capture_stream);
+        // an even chunk (batches with fused-step members) starts and ends in the caller's arrays
+        for (int i = 0; i < c && le == cudaSuccess; ++i)
+          le = batch_launch_step<real>(B, i, rows, i, B->capture_stream, B->any_fused ? (i & 1) : 0);
         cudaError_t ce = cudaStreamEndCapture(B->capture_stream, &graph);
         if (le != cudaSuccess)
           return fail(IFDTD_ERR_CUDA, "batch graph capture: " + B->failed + ": " + cudaGetErrorString(le));
@@ -2071,8 +2158,9 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
       CUDA_TRY(cudaGraphLaunch(exec, stream));
     } else {
       for (int i = 0; i < c; ++i) {
-        cudaError_t e = batch_launch_step<real>(B, i, rows, i, stream);
+        cudaError_t e = batch_launch_step<real>(B, i, rows, i, stream, parity);
         if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, "batch step launch: " + B->failed + ": " + cudaGetErrorString(e));
+        if (B->any_fused) parity ^= 1;
       }
     }
     for (int i = 0; i < B->n; ++i) {
@@ -2081,6 +2169,16 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
       CUDA_TRY(cudaMemcpy2DAsync(out_rows[i] + (size_t)s0 * r, (size_t)r * sizeof(double), B->d_stage + offset[i],
                                  (size_t)rows * sizeof(double), (size_t)r * sizeof(double), c, cudaMemcpyDeviceToDevice,
                                  stream));
+    }
+  }
+  if (parity) {
+    // an odd number of steps left the fused members in their second copies
+    for (int i = 0; i < B->n; ++i) {
+      const ifdtd_plan* P = B->plans[i];
+      if (!P->fused) continue;
+      void* const dst[4] = {states[i].er, states[i].et, states[i].hr, states[i].ht};
+      for (int k = 0; k < 4; ++k)
+        CUDA_TRY(cudaMemcpyAsync(dst[k], P->fb[k], P->fb_bytes[k], cudaMemcpyDeviceToDevice, stream));
     }
   }
   return IFDTD_OK;
@@ -2373,7 +2471,6 @@ int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t 
       return fail(IFDTD_ERR_ARGUMENT, "batch members must share one device and one precision");
     for (int j = 0; j < i; ++j)
       if (plans[j] == plans[i]) return fail(IFDTD_ERR_ARGUMENT, "a plan appears twice in the batch");
-    if (plans[i]->fused) return fail(IFDTD_ERR_UNSUPPORTED, "a fused-step plan cannot join a batch");
   }
   DeviceGuard guard(plans[0]->device);
   ifdtd_batch* B = new ifdtd_batch();
@@ -2382,8 +2479,15 @@ int32_t ifdtd_batch_create(ifdtd_plan* const* plans, int32_t n_members, int32_t 
   B->n = n_members;
   B->plans.assign(plans, plans + n_members);
   B->chunk = chunk;
-  for (int i = 0; i < n_members; ++i)
+  bool fused = false;
+  for (int i = 0; i < n_members; ++i) {
     if (plans[i]->h_mode != 2 || plans[i]->e_mode != 2) B->chunk = std::min(B->chunk, std::max(plans[i]->chunk, 1));
+    fused |= plans[i]->fused;
+  }
+  if (fused && B->chunk % 2) {
+    delete B;
+    return fail(IFDTD_ERR_ARGUMENT, "a batch with fused-step members needs an even chunk");
+  }
   const int rc = B->dtype == 4 ? batch_build<float>(B) : batch_build<double>(B);
   if (rc) {
     delete B;

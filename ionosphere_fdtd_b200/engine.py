@@ -54,8 +54,8 @@ class Tuning:
     row gaps every E-phase copy bridges (0-8: fewer, longer bulk copies), and
     ``fused_step`` (1: one launch per leapfrog step in which every E patch
     recomputes the new H on its halo, for plans without plasma or surface
-    impedance; the plan then holds a second copy of the field arrays and
-    cannot join an ``Ensemble``).
+    impedance; the plan then holds a second copy of the field arrays, and in
+    an ``Ensemble`` it runs the batched fused kernel).
     Every choice computes the same bits."""
 
     faces_per_patch: int = 0

@@ -10,8 +10,9 @@ inside and across a captured graph chunk, direct launches (graph_chunk 0),
 the sampled step's receiver traces, several patch sizes, both kernels (the
 pipelined ring, whose stage holds the old rows and takes the new H in place,
 and direct gathers) and the 12-slot vertex tables of adaptive meshes.  Plans
-with plasma or surface impedance, odd graph chunks and batches of fused plans
-are refused.
+with plasma or surface impedance and odd graph chunks are refused; fused
+members of an ensemble run the batched fused kernel and must match their own
+runs bit for bit.
 """
 
 import numpy as np
@@ -101,7 +102,53 @@ def test_fused_step_refusals():
         build_product(CS.CASES["source_s1"], "float32", tuning=Tuning(fused_step=1, graph_chunk=3))
     with pytest.raises(ValueError, match="fused_step must be 0 or 1"):
         build_product(CS.CASES["source_s1"], "float32", tuning=Tuning(fused_step=2))
-    fused = build_product(CS.CASES["source_s1"], "float32", tuning=Tuning(fused_step=1))
+    direct = build_product(CS.CASES["source_s1"], "float32", tuning=Tuning(fused_step=1, staging=1))
     other = build_product(CS.CASES["source_s1"], "float32")
-    with pytest.raises(BackendUnavailableError, match="fused-step plan cannot join a batch"):
-        Ensemble([other, fused])
+    with pytest.raises(BackendUnavailableError, match="fused-step plan on direct gathers cannot join a batch"):
+        Ensemble([other, direct])
+
+
+def _state(sim) -> dict[str, np.ndarray]:
+    out = _fields(sim)
+    if sim._plasma_coupler is not None:
+        for i, j in enumerate(sim._plasma_coupler.ade.current_density):
+            out[f"plasma_current_{i}"] = sim.to_numpy(j)
+    if sim._surface_impedance_ade is not None:
+        out["si_memory"] = sim.to_numpy(sim._surface_impedance_ade.memory)
+    return out
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_fused_members_in_an_ensemble_match_their_own_runs(dtype):
+    """Fused-step members (two tunings, so two fused groups, and the 12-slot
+    adaptive mesh) batched with two-launch members: after odd and even step
+    counts and a sampled run across a graph chunk, every member holds the same
+    bits as the same member advanced on its own."""
+
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200.engine import Tuning
+
+    spec = [("source_s1", Tuning(fused_step=1)), ("config1_s2", Tuning(fused_step=1, lane_layout=2)),
+            ("adaptive_s1", Tuning(fused_step=1)), ("plasma_drude_s2", Tuning()), ("config1_s2", Tuning())]
+    together = [build_product(CS.CASES[n], dtype, tuning=t) for n, t in spec]
+    alone = [build_product(CS.CASES[n], dtype, tuning=t) for n, t in spec]
+    assert together[0]._engine.kernel_modes == ("fused", "pipeline")
+    rows = [CS.receiver_rows(m.mesh.n_vertices, m.altitudes_m, 3 + i, 4) for i, m in enumerate(together)]
+    with Ensemble(together) as ens:
+        assert ens.launch_layout()["groups"] >= 4 and ens.launch_layout()["solo"] == 0
+        for n in (3, 2):
+            ens.step(n)
+            for sim in alone:
+                sim.step(n)
+            for a, b in zip(together, alone):
+                ea, eb = _state(a), _state(b)
+                for key in ea:
+                    np.testing.assert_array_equal(ea[key], eb[key], err_msg=f"{key} after {n} steps")
+        traces = ens.record_er_observations(rows, 37)
+    for sim, (v, k, w), tr in zip(alone, rows, traces):
+        np.testing.assert_array_equal(tr, sim.record_er_observations(v, k, w, 37))
+    for a, b in zip(together, alone):
+        ea, eb = _state(a), _state(b)
+        for key in ea:
+            np.testing.assert_array_equal(ea[key], eb[key], err_msg=key)
+        assert a._engine.status_word() == 0
