@@ -15,7 +15,10 @@ the step currents resident in HBM; ``e2e`` is the same metric through the
 public API (``GeodesicFDTD.record_er_observations``) with host-computed source
 currents copied in and receiver traces copied out every bench step.
 ``--workload config2`` runs the s7 / 40-cell plasma workload (64 receivers,
-1000 leapfrog steps per bench step) the same way.
+1000 leapfrog steps per bench step) the same way.  After the s9 state is
+freed, the default run also measures the batched ensemble below on the same
+GPU and attaches its record as the line's ``ensemble`` object
+(``--no-ensemble`` skips it).
 
 ``--workload config3`` measures ensemble runs/s instead: 64 seeded members
 of uneven size (s5-s7, 24-60 radial cells, exponential ionospheres, 16
@@ -75,6 +78,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-drift", action="store_true", help="skip the float32-vs-float64 drift run")
+    p.add_argument("--no-ensemble", action="store_true",
+                   help="config4: skip the 64-member ensemble measurement attached to the line")
     p.add_argument("--subdivision", type=int, default=None, help="override the workload's subdivision (small profiling cases)")
     return p.parse_args()
 
@@ -425,9 +430,6 @@ def ensemble_cells(members: int) -> list[int]:
 def ensemble_main(args, world: int, rank: int, local: int) -> None:
     import torch
 
-    from ionosphere_fdtd_b200 import Ensemble
-    from ionosphere_fdtd_b200 import workloads as W
-
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -436,6 +438,23 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    line = ensemble_measure(args, world, rank, local, dist, cpu_baseline=not args.no_cpu_baseline)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ensemble_measure(args, world: int, rank: int, local: int, dist, cpu_baseline: bool) -> dict | None:
+    """Batched and sequential runs/s of the 64-member ensemble on this rank's GPU (max over
+    ranks); returns the config-3 JSON line on rank 0, None elsewhere."""
+
+    import torch
+
+    from ionosphere_fdtd_b200 import Ensemble
+    from ionosphere_fdtd_b200 import workloads as W
+
     device = f"cuda:{local}"
     t_setup = time.perf_counter()
     wls = W.config3_members(device=device, members=args.members)
@@ -538,7 +557,7 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
     }
     cells = [w.cells for w in wls]
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_baseline:
         steppers, sample_cells = oracle_ensemble_sampler()
         oracle_ensemble_time(steppers, sample_cells)
         r = oracle_ensemble_time(steppers, sample_cells, steps=60)
@@ -591,11 +610,25 @@ def ensemble_main(args, world: int, rank: int, local: int) -> None:
             "gpu_launches": args.steps * T * (2 * layout["groups"] + 2 * layout["solo"] + 1),
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
     ens.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def ensemble_summary(line: dict | None) -> dict | None:
+    """The config-3 line abridged for the config-4 line's ``ensemble`` object: batched and
+    sequential runs/s of the 64 members, their step times, roofline, e2e, launches and clocks."""
+
+    if line is None:
+        return None
+    keep = ("metric", "value", "unit", "ms_per_step", "sequential", "speedup_vs_sequential", "gcell_updates_per_s",
+            "e2e", "gpu_launches", "clocks")
+    out = {k: line[k] for k in keep}
+    cfg = line["config"]
+    out["config"] = {k: cfg[k] for k in ("workload", "members", "subdivisions", "radial_cells", "cells_total",
+                                         "receivers_per_member", "run_steps", "time_steps_per_step", "launch_layout",
+                                         "autotune")}
+    out["roofline"] = {k: line["roofline"][k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac")}
+    return out
 
 
 SURROGATE_METRIC = "surrogate traces/s"
@@ -945,10 +978,10 @@ def main() -> None:
                  "note": "timed region: both phase kernels and the receiver sampling of every leapfrog step"},
     }
     config = workload_config(args.workload, args.subdivision, world)
+    del wl, sim, eng
+    torch.cuda.empty_cache()
     drift = None
     if rank == 0 and world == 1 and not args.no_drift:
-        del wl, sim, eng
-        torch.cuda.empty_cache()
         drift = fp32_drift(args.workload, device, T, args.subdivision)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -961,6 +994,11 @@ def main() -> None:
             "sample": (f"{r['steps']} leapfrog steps of s{r['sub']}/L{r['L']} float32{r['note']} after 1 warm-up step "
                        f"({r['seconds']:.1f} s), the oracle's step on PyTorch CPU tensors over {r['cores']} threads"),
         }
+    ensemble = None
+    if args.workload == "config4" and args.subdivision is None and not args.no_ensemble:
+        # the batched-ensemble form (config 3) on the same GPU, after the s9 state is freed
+        torch.cuda.empty_cache()
+        ensemble = ensemble_summary(ensemble_measure(args, world, rank, local, dist, cpu_baseline=False))
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -988,6 +1026,7 @@ def main() -> None:
             "traces_finite": trace_finite,
             "gpu_launches": 3 * T * K,
             "clocks": clocks,
+            "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     if dist:

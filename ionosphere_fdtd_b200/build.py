@@ -19,6 +19,7 @@ SOURCES = [PACKAGE / "csrc" / "ifdtd.cu", PACKAGE / "csrc" / "surrogate.cu", PAC
 HEADERS = [
     PACKAGE / "csrc" / "step_kernels.cuh",
     PACKAGE / "csrc" / "pipe_kernels.cuh",
+    PACKAGE / "csrc" / "fused_kernels.cuh",
     PACKAGE / "csrc" / "errors.cuh",
     ROOT / "include" / "ifdtd.h",
     ROOT / "include" / "ifdtd_surrogate.h",

@@ -98,6 +98,27 @@ def test_ensemble_cells_follow_the_member_generator():
     assert all(55e3 <= d["h0"] <= 70e3 and 3e3 <= d["zeta"] <= 6e3 and 10.0 <= d["carrier"] <= 60.0 for d in draws)
 
 
+def test_ensemble_summary_keeps_the_runs_per_second_record():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.ensemble_summary(None) is None
+    config = {k: k for k in ("workload", "members", "subdivisions", "radial_cells", "cells_total",
+                             "receivers_per_member", "run_steps", "time_steps_per_step", "launch_layout",
+                             "autotune", "setup_s", "l2", "parallelism")}
+    roofline = {"bound": "hbm", "kernel": "k", "achieved": 1.0, "peak": 2.0, "unit": "GB/s", "frac": 0.5,
+                "traffic": None, "peak_source": "p", "algorithmic_bytes_per_step": 3}
+    line = {"metric": bench.ENSEMBLE_METRIC, "value": 2.8, "unit": "runs/s", "ms_per_step": 450.0,
+            "sequential": {"value": 2.4}, "speedup_vs_sequential": 2.8 / 2.4, "gcell_updates_per_s": 46.0,
+            "e2e": None, "gpu_launches": 10, "clocks": None, "config": config, "roofline": roofline,
+            "cpu_baseline": None, "n_gpus": 1}
+    out = bench.ensemble_summary(line)
+    assert out["metric"] == bench.ENSEMBLE_METRIC and out["value"] == 2.8 and out["sequential"] == {"value": 2.4}
+    assert "setup_s" not in out["config"] and out["config"]["members"] == "members"
+    assert out["roofline"] == {k: roofline[k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac")}
+    assert "cpu_baseline" not in out and "n_gpus" not in out
+
+
 def test_launch_geometry_record_lists_every_candidate(monkeypatch):
     """The bench's tuning record from an autotune result (the timing itself needs a GPU)."""
 
