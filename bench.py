@@ -81,6 +81,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-ensemble", action="store_true",
                    help="config4: skip the 64-member ensemble measurement attached to the line")
     p.add_argument("--subdivision", type=int, default=None, help="override the workload's subdivision (small profiling cases)")
+    p.add_argument("--plasma-frame", type=int, choices=(0, 1, 2), default=0,
+                   help="config2/config4: frame of the plasma current in the kernels (0 auto, 1 Cartesian, 2 face frames)")
     return p.parse_args()
 
 
@@ -124,28 +126,12 @@ def kernel_bytes(sim) -> dict[str, int]:
 
 
 def phase_times_ms(sim, reps: int, stream) -> dict[str, float]:
-    """Median device time of each phase kernel, CUDA events on the launching stream."""
+    """Median device time of each phase kernel: CUDA events around every launch on the
+    launching stream (``ifdtd_time_phases``, the plasma current turned into the plan's
+    frame once around all launches)."""
 
-    import torch
-
-    eng = sim._engine
-    state = sim._state()
-    marks = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(reps)]
-    for _ in range(3):
-        eng.update_magnetic(state)
-        eng.update_electric(state, 0.0)
-    torch.cuda.synchronize()
-    for m in marks:
-        m[0].record(stream)
-        eng.update_magnetic(state)
-        m[1].record(stream)
-        eng.update_electric(state, 0.0)
-        m[2].record(stream)
-    torch.cuda.synchronize()
-    return {
-        "h_phase": statistics.median(m[0].elapsed_time(m[1]) for m in marks),
-        "e_phase": statistics.median(m[1].elapsed_time(m[2]) for m in marks),
-    }
+    h, e = sim._engine.phase_times_ms(sim._state(), reps)
+    return {"h_phase": h, "e_phase": e}
 
 
 class ClockSampler:
@@ -212,10 +198,13 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
-def build(workload: str, device: str, dtype: str = "float32", subdivision: int | None = None):
+def build(workload: str, device: str, dtype: str = "float32", subdivision: int | None = None, plasma_frame: int = 0):
     from ionosphere_fdtd_b200 import workloads as W
+    from ionosphere_fdtd_b200.engine import Tuning
 
     extra = {} if subdivision is None else {"subdivision": subdivision}
+    if plasma_frame:
+        extra["tuning"] = Tuning(plasma_frame=plasma_frame)
     if workload == "config4":
         wl = W.config4(device=device, dtype=dtype, **extra)
     else:
@@ -224,7 +213,7 @@ def build(workload: str, device: str, dtype: str = "float32", subdivision: int |
     return wl
 
 
-def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None = None) -> dict:
+def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None = None, plasma_frame: int = 0) -> dict:
     """Relative L2 per (E, H) group between float32 and float64 runs of the
     engine from the same seeded state (the float64 run stands in for the
     float64 NumPy path, far too slow at these sizes) after ``steps`` steps."""
@@ -234,7 +223,7 @@ def fp32_drift(workload: str, device: str, steps: int, subdivision: int | None =
     out = {}
     sims = {}
     for dtype in ("float64", "float32"):
-        sim = build(workload, device, dtype, subdivision).simulation
+        sim = build(workload, device, dtype, subdivision, plasma_frame).simulation
         sim.step(steps)
         sims[dtype] = {f: getattr(sim, f).to(torch.float64) for f in ("er", "et", "hr", "ht")}
         del sim
@@ -863,7 +852,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=torch.device("cuda", local))
     device = f"cuda:{local}"
     t_setup = time.perf_counter()
-    wl = build(args.workload, device, subdivision=args.subdivision)
+    wl = build(args.workload, device, subdivision=args.subdivision, plasma_frame=args.plasma_frame)
     setup_s = time.perf_counter() - t_setup
     sim = wl.simulation
     tuning = None if args.no_autotune else tune_launch_geometry(sim)
@@ -982,7 +971,7 @@ def main() -> None:
     torch.cuda.empty_cache()
     drift = None
     if rank == 0 and world == 1 and not args.no_drift:
-        drift = fp32_drift(args.workload, device, T, args.subdivision)
+        drift = fp32_drift(args.workload, device, T, args.subdivision, args.plasma_frame)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = oracle_sample(args.workload, 3)
@@ -1019,6 +1008,7 @@ def main() -> None:
             "autotune": tuning,
             "hbm_gbs": achieved,
             "kernel_modes": list(modes),
+            "plasma_frame": {0: "auto: face frames (unmagnetised plasma)", 1: "cartesian", 2: "face frames"}[args.plasma_frame],
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -138,6 +138,15 @@ typedef struct ifdtd_tuning {
                                 staging 1: direct gathers with the halo's new H in shared memory.
                                 e_faces_per_patch sets the patch (0: the largest of 64 ... 8 faces whose stage
                                 fits twice, direct: of 128 ... 16 faces whose rows fit 110 KiB); 0: two launches */
+  int32_t plasma_frame;      /* frame the plasma current is held in while the step kernels run: 0 auto (face
+                                frames for an unmagnetised plasma, else Cartesian), 1 Cartesian, 2 face frames
+                                (unmagnetised plasma only).  In face frames component 0 lies along the face
+                                centre and 1, 2 in the face's tangent plane, so the E phase reads one current
+                                row per face at a vertex and two per face at an edge.  Every call that runs a
+                                plasma phase turns the caller's Cartesian currents into face frames first and
+                                back afterwards (two passes over the currents per call), so the state between
+                                calls is the reference's; the two frames round differently (float32: within a
+                                few ulp of the current per call) */
 } ifdtd_tuning;
 
 /* Mutable state of one simulation: device pointers owned by the caller. */
@@ -212,6 +221,16 @@ int32_t ifdtd_step_static_scratch(ifdtd_plan* plan, const ifdtd_state* state, co
  * with source current I (solver.py:923-989).  ifdtd_step is the pair. */
 int32_t ifdtd_update_magnetic(ifdtd_plan* plan, const ifdtd_state* state, void* stream);
 int32_t ifdtd_update_electric(ifdtd_plan* plan, const ifdtd_state* state, double current, void* stream);
+
+/* Measurement helper (no counterpart in the reference): device time of the
+ * H and E phase kernels, each launch bracketed by CUDA events on the stream;
+ * the medians of reps timed launches (after 3 untimed pairs) go to h_ms and
+ * e_ms.  Advances the state by 3 + reps leapfrog steps with a zero source
+ * current; the plasma current is turned into the plan's frame once around all
+ * of them, so the times are the phase kernels' alone.  Synchronises on the
+ * last event. */
+int32_t ifdtd_time_phases(ifdtd_plan* plan, const ifdtd_state* state, int32_t reps, float* h_ms, float* e_ms,
+                          void* stream);
 
 /* Weighted observation probe: out[r] = sum_k w[r,k] * field[index[r,k], layer[r,k]]
  * accumulated in float64.  field_kind: 0 er, 1 et, 2 hr, 3 ht.  Replaces the

@@ -93,7 +93,7 @@ class Tuning(C.Structure):
     _fields_ = [("faces_per_patch", _i32), ("threads", _i32), ("graph_chunk", _i32), ("e_faces_per_patch", _i32), ("staging", _i32),
                 ("producer_warps", _i32), ("lane_layout", _i32), ("e_threads", _i32), ("e_stages", _i32),
                 ("e_producer_warps", _i32), ("e_copy_gap", _i32),
-                ("fused_step", _i32)]
+                ("fused_step", _i32), ("plasma_frame", _i32)]
 
 
 class State(C.Structure):
@@ -125,6 +125,7 @@ _SIGNATURES = {
     "ifdtd_step_static_scratch": ([_vp, C.POINTER(State), _vp, _i32, _vp], _i32),
     "ifdtd_update_magnetic": ([_vp, C.POINTER(State), _vp], _i32),
     "ifdtd_update_electric": ([_vp, C.POINTER(State), C.c_double, _vp], _i32),
+    "ifdtd_time_phases": ([_vp, C.POINTER(State), _i32, C.POINTER(C.c_float), C.POINTER(C.c_float), _vp], _i32),
     "ifdtd_probe_create": ([_vp, _i32, _i32, _i32, _i64p, _i64p, _f64p, C.POINTER(_vp)], _i32),
     "ifdtd_probe_destroy": ([_vp], _i32),
     "ifdtd_sample": ([_vp, C.POINTER(State), _vp, _vp, _vp], _i32),

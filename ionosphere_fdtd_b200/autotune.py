@@ -8,8 +8,8 @@ for every candidate from the simulation's own mesh and physics, times
 graph-captured steps of each on the simulation's own state with CUDA events,
 restores that state, and installs the fastest plan.  Every candidate computes
 the same bits (patch size, lane layout, kernel family and the fused
-one-launch step do not change any result), so
-tuning changes speed only.  ``autotune_ensemble`` tunes the largest member
+one-launch step do not change any result; every candidate keeps the
+simulation's plasma frame, which does), so tuning changes speed only.  ``autotune_ensemble`` tunes the largest member
 of each class (by default: mesh level, radial cells, precision and physics)
 and gives the winner to the whole class.
 """
@@ -109,12 +109,14 @@ def autotune(sim, candidates: Sequence[Tuning] = DEFAULT_CANDIDATES, *, steps: i
     if not candidates:
         raise ValueError("at least one candidate tuning is required")
     chunk = sim._engine.tuning.graph_chunk
+    # the plasma frame changes rounding, not only speed: every candidate keeps the simulation's
+    frame = sim._engine.tuning.plasma_frame
     saved = _snapshot(sim)
     result = AutotuneResult(best=sim._engine.tuning, best_ms=float("inf"))
     best_engine = None
     try:
         for cand in candidates:
-            tuning = replace(cand, graph_chunk=chunk)
+            tuning = replace(cand, graph_chunk=chunk, plasma_frame=frame)
             try:
                 engine = _engine_for(sim, tuning)
             except (ValueError, RuntimeError, BackendUnavailableError) as err:

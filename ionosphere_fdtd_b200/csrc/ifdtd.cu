@@ -107,6 +107,8 @@ struct ifdtd_plan {
   size_t smem_bytes = 0, kh_smem = 0, ke_smem = 0;
   int* d_status = nullptr;
   bool plasma = false;
+  bool plasma_local = false;     // the plasma current runs in face frames (converted around every call)
+  const void* d_frame = nullptr;  // (F, 12) face-frame rows of those conversions
   DeviceArena arena;
   void* d_rec = nullptr;               // Rec<real> in device memory
   std::vector<unsigned char> h_rec;    // host image of the record
@@ -643,6 +645,15 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   if (tune && (tune->fused_step < 0 || tune->fused_step > 1)) return fail(IFDTD_ERR_ARGUMENT, "fused_step must be 0 or 1");
   if (fused && (X->plasma_species > 0 || X->si_terms > 0))
     return fail(IFDTD_ERR_UNSUPPORTED, "fused_step supports plans without plasma and without surface impedance");
+  const int plasma_frame = tune ? tune->plasma_frame : 0;
+  if (plasma_frame < 0 || plasma_frame > 2)
+    return fail(IFDTD_ERR_ARGUMENT, "plasma_frame must be 0 (auto), 1 (Cartesian) or 2 (face frames)");
+  if (plasma_frame == 2 && X->plasma_species > 0 && X->plasma_magnetized)
+    return fail(IFDTD_ERR_UNSUPPORTED, "plasma_frame 2 (face frames) supports an unmagnetised plasma only");
+  // face frames: the Drude update acts on each component alike, so it is the
+  // same in any orthonormal frame; a magnetised update would need B per face
+  const bool local = X->plasma_species > 0 && !X->plasma_magnetized && plasma_frame != 1;
+  P->plasma_local = local;
   // the fused step replaces both phases; its plan keeps the direct kernels for
   // the single-phase entry points
   const int staging = fused ? 1 : (tune ? tune->staging : 0);
@@ -693,6 +704,41 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   P->Pn = Pn;
   P->Pm = Pm;
   DeviceArena& A = P->arena;
+
+  // ---- face frames of the plasma current (float64): e0 along the face
+  // centre, e1 along the coordinate axis least aligned with it made
+  // orthogonal, e2 = e0 x e1; cnorm = |face centre| ----
+  std::vector<double> frame64, cnorm;
+  if (local) {
+    frame64.assign(9 * (size_t)nF, 0.0);
+    cnorm.assign(nF, 0.0);
+    for (int f = 0; f < nF; ++f) {
+      const double* c = X->face_centers + 3 * (size_t)f;
+      const double n = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      if (!(n > 0.0) || !std::isfinite(n)) return fail(IFDTD_ERR_ARGUMENT, "face centre of zero or non-finite length");
+      const double e0[3] = {c[0] / n, c[1] / n, c[2] / n};
+      int a = 0;
+      for (int i = 1; i < 3; ++i)
+        if (std::fabs(e0[i]) < std::fabs(e0[a])) a = i;
+      double e1[3] = {-e0[a] * e0[0], -e0[a] * e0[1], -e0[a] * e0[2]};
+      e1[a] += 1.0;
+      const double m = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+      for (int i = 0; i < 3; ++i) e1[i] /= m;
+      const double e2[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0]};
+      double* Q = frame64.data() + 9 * (size_t)f;
+      for (int i = 0; i < 3; ++i) {
+        Q[i] = e0[i];
+        Q[3 + i] = e1[i];
+        Q[6 + i] = e2[i];
+      }
+      cnorm[f] = n;
+    }
+  }
+  // row k of face f's frame applied to a Cartesian vector v
+  auto frame_dot = [&](int f, int k, const double* v) {
+    const double* Q = frame64.data() + 9 * (size_t)f + 3 * k;
+    return Q[0] * v[0] + Q[1] * v[1] + Q[2] * v[2];
+  };
 
   // ---- edges ----
   std::vector<int2> th(nE), lr(nE);
@@ -836,7 +882,10 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
           if (f < 0 || f >= nF || n >= MD) return false;
           if (first < 0) first = (int)f;
           out.face[(size_t)sl * SW + n] = (int)f;
-          for (int c = 0; c < 3; ++c) out.wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
+          if (local)  // face frames: the slots' weights packed first, w * |centre| (its e0 component)
+            out.wc[(size_t)sl * SW * 4 + n] = (real)(w * cnorm[f]);
+          else
+            for (int c = 0; c < 3; ++c) out.wc[((size_t)sl * SW + n) * 4 + c] = (real)(w * X->face_centers[3 * f + c]);
           ++n;
         }
         for (int q = n; q < SW; ++q) out.face[(size_t)sl * SW + q] = first < 0 ? 0 : first;
@@ -1260,17 +1309,43 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
     if (!(rows == 1 || rows == nF)) return fail(IFDTD_ERR_ARGUMENT, "plasma rows must be 1 or F");
     P->plasma = true;
     pl.assign(12 * (size_t)nF, real(0));
-    for (int f = 0; f < nF; ++f)
-      for (int i = 0; i < 3; ++i) {
-        for (int c = 0; c < 3; ++c) pl[12 * (size_t)f + 4 * i + c] = (real)X->plasma_reconstruction[9 * (size_t)f + 3 * i + c];
-        pl[12 * (size_t)f + 4 * i + 3] = (real)X->face_centers[3 * (size_t)f + i];
-      }
     tn.assign(8 * (size_t)nE, real(0));
-    for (int e = 0; e < nE; ++e)
-      for (int c = 0; c < 3; ++c) {
-        tn[8 * (size_t)e + c] = (real)X->plasma_tangent_left[3 * (size_t)e + c];
-        tn[8 * (size_t)e + 4 + c] = (real)X->plasma_tangent_right[3 * (size_t)e + c];
+    if (local) {
+      // reconstruction rows and centre in the face's frame (the centre is
+      // |centre| e0); edge tangents in their faces' frames, components 1 and 2
+      // (the tangents lie in the faces' tangent planes)
+      std::vector<real> fr(12 * (size_t)nF, real(0));
+      for (int f = 0; f < nF; ++f) {
+        for (int i = 0; i < 3; ++i) {
+          const double* row = X->plasma_reconstruction + 9 * (size_t)f + 3 * i;
+          for (int k = 0; k < 3; ++k) pl[12 * (size_t)f + 4 * i + k] = (real)frame_dot(f, k, row);
+          pl[12 * (size_t)f + 4 * i + 3] = (real)(i == 0 ? cnorm[f] : 0.0);
+          for (int c = 0; c < 3; ++c) fr[12 * (size_t)f + 4 * i + c] = (real)frame64[9 * (size_t)f + 3 * i + c];
+        }
       }
+      for (int e = 0; e < nE; ++e) {
+        const int fl = (int)M->edge_left_faces[e], fq = (int)M->edge_right_faces[e];
+        const double* tl = X->plasma_tangent_left + 3 * (size_t)e;
+        const double* tq = X->plasma_tangent_right + 3 * (size_t)e;
+        tn[8 * (size_t)e + 0] = (real)frame_dot(fl, 1, tl);
+        tn[8 * (size_t)e + 1] = (real)frame_dot(fl, 2, tl);
+        tn[8 * (size_t)e + 2] = (real)frame_dot(fq, 1, tq);
+        tn[8 * (size_t)e + 3] = (real)frame_dot(fq, 2, tq);
+      }
+      UP(fr, frame);
+      P->d_frame = R.frame;
+    } else {
+      for (int f = 0; f < nF; ++f)
+        for (int i = 0; i < 3; ++i) {
+          for (int c = 0; c < 3; ++c) pl[12 * (size_t)f + 4 * i + c] = (real)X->plasma_reconstruction[9 * (size_t)f + 3 * i + c];
+          pl[12 * (size_t)f + 4 * i + 3] = (real)X->face_centers[3 * (size_t)f + i];
+        }
+      for (int e = 0; e < nE; ++e)
+        for (int c = 0; c < 3; ++c) {
+          tn[8 * (size_t)e + c] = (real)X->plasma_tangent_left[3 * (size_t)e + c];
+          tn[8 * (size_t)e + 4 + c] = (real)X->plasma_tangent_right[3 * (size_t)e + c];
+        }
+    }
     auto pc = pad_rows(X->plasma_coef, S * 6 * rows, L, Pm);
     UP(pl, face_pl);
     UP(tn, tan);
@@ -1412,6 +1487,7 @@ int build_plan(ifdtd_plan* P, const ifdtd_mesh_desc* M, const ifdtd_grid_desc* G
   R.plasma_full = X->plasma_rows == nF && nF != 1 ? 1 : 0;
   R.magnetized = X->plasma_magnetized ? 1 : 0;
   R.coef_full = X->coef_rows_er != 1 ? 1 : 0;
+  R.plasma_local = local ? 1 : 0;
   R.n_src_er = X->n_src_er;
   R.n_src_et = X->n_src_et;
   R.maxdeg = MD;
@@ -1635,12 +1711,29 @@ cudaError_t launch_step(ifdtd_plan* P, int istep, const ifdtd_probe* probe, int 
   return cudaGetLastError();
 }
 
+// Face frames: the caller's Cartesian plasma currents turned into the plan's
+// face frames before a call's first phase kernel (to_local 1) and back after
+// its last (to_local 0), so the state between calls is Cartesian.  A call that
+// fails in between leaves the currents in face frames (its results are invalid
+// anyway).
+template <typename real>
+cudaError_t plasma_frames(const ifdtd_plan* P, const ifdtd_state* st, int to_local, cudaStream_t stream) {
+  if (!P->plasma_local) return cudaSuccess;
+  const size_t items = (size_t)P->nF * (size_t)(P->Pm / Lanes<real>::N);
+  const int grid = (int)std::min<size_t>(std::max<size_t>((items + 255) / 256, 1), (size_t)P->sm_count * 8);
+  for (int s = 0; s < P->S; ++s)
+    plasma_frame_kernel<real><<<grid, 256, 0, stream>>>(static_cast<real*>(st->plasma_current[s]),
+                                                        static_cast<const real*>(P->d_frame), P->nF, P->Pm, to_local);
+  return cudaGetLastError();
+}
+
 template <typename real>
 int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int n, const ifdtd_probe* probe,
               double* out_rows, cudaStream_t stream) {
   int rc = bind_state<real>(P, st, stream);
   if (rc) return rc;
   if (n <= 0) return IFDTD_OK;
+  CUDA_TRY(plasma_frames<real>(P, st, 1, stream));
   // NVTX range over the host-side enqueue of these steps (visible to profilers)
   struct Range {
     explicit Range(const char* name) { nvtxRangePushA(name); }
@@ -1691,6 +1784,7 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
     for (int i = 0; i < 4; ++i)
       CUDA_TRY(cudaMemcpyAsync(dst[i], P->fb[i], P->fb_bytes[i], cudaMemcpyDeviceToDevice, stream));
   }
+  CUDA_TRY(plasma_frames<real>(P, st, 0, stream));
   return IFDTD_OK;
 }
 
@@ -2096,6 +2190,7 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
       rows += p->rows;
     }
   if (n <= 0) return IFDTD_OK;
+  for (int i = 0; i < B->n; ++i) CUDA_TRY(plasma_frames<real>(B->plans[i], &states[i], 1, stream));
   if (rows > 0) {
     if ((int)refs.size() > B->cap_refs || rows > B->cap_rows) {
       CUDA_TRY(cudaStreamSynchronize(stream));
@@ -2181,6 +2276,7 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
         CUDA_TRY(cudaMemcpyAsync(dst[k], P->fb[k], P->fb_bytes[k], cudaMemcpyDeviceToDevice, stream));
     }
   }
+  for (int i = 0; i < B->n; ++i) CUDA_TRY(plasma_frames<real>(B->plans[i], &states[i], 0, stream));
   return IFDTD_OK;
 }
 
@@ -2302,7 +2398,9 @@ int32_t ifdtd_update_magnetic(ifdtd_plan* plan, const ifdtd_state* state, void* 
   cudaStream_t st = (cudaStream_t)stream;
   const int rc = plan->dtype == 4 ? bind_state<float>(plan, state, st) : bind_state<double>(plan, state, st);
   if (rc) return rc;
+  CUDA_TRY(plan->dtype == 4 ? plasma_frames<float>(plan, state, 1, st) : plasma_frames<double>(plan, state, 1, st));
   CUDA_TRY(plan->dtype == 4 ? launch_kh<float>(plan, st) : launch_kh<double>(plan, st));
+  CUDA_TRY(plan->dtype == 4 ? plasma_frames<float>(plan, state, 0, st) : plasma_frames<double>(plan, state, 0, st));
   CUDA_TRY(cudaGetLastError());
   return IFDTD_OK;
 }
@@ -2315,9 +2413,73 @@ int32_t ifdtd_update_electric(ifdtd_plan* plan, const ifdtd_state* state, double
   if (rc) return rc;
   // pageable source: staged by the runtime before the call returns
   CUDA_TRY(cudaMemcpyAsync(plan->d_cur, &current, sizeof(double), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(plan->dtype == 4 ? plasma_frames<float>(plan, state, 1, st) : plasma_frames<double>(plan, state, 1, st));
   CUDA_TRY(plan->dtype == 4 ? launch_ke<float>(plan, 0, st) : launch_ke<double>(plan, 0, st));
+  CUDA_TRY(plan->dtype == 4 ? plasma_frames<float>(plan, state, 0, st) : plasma_frames<double>(plan, state, 0, st));
   CUDA_TRY(cudaGetLastError());
   return IFDTD_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Device time of each phase kernel: the state is turned into the plan's plasma
+// frame once, the H and E phase kernels run 3 + reps times with a zero source
+// current (CUDA events around every launch on the caller's stream), and the
+// state is turned back.  Medians of the reps timed launches.
+template <typename real>
+int time_phases(ifdtd_plan* P, const ifdtd_state* s, int reps, float* h_ms, float* e_ms, cudaStream_t st) {
+  int rc = bind_state<real>(P, s, st);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemsetAsync(P->d_cur, 0, sizeof(double), st));
+  CUDA_TRY(plasma_frames<real>(P, s, 1, st));
+  for (int i = 0; i < 3; ++i) {
+    CUDA_TRY(launch_kh<real>(P, st));
+    CUDA_TRY(launch_ke<real>(P, 0, st));
+  }
+  std::vector<cudaEvent_t> ev(3 * (size_t)reps, nullptr);
+  struct Events {
+    std::vector<cudaEvent_t>& e;
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } hold{ev};
+  for (auto& x : ev) CUDA_TRY(cudaEventCreate(&x));
+  for (int i = 0; i < reps; ++i) {
+    CUDA_TRY(cudaEventRecord(ev[3 * i], st));
+    CUDA_TRY(launch_kh<real>(P, st));
+    CUDA_TRY(cudaEventRecord(ev[3 * i + 1], st));
+    CUDA_TRY(launch_ke<real>(P, 0, st));
+    CUDA_TRY(cudaEventRecord(ev[3 * i + 2], st));
+  }
+  CUDA_TRY(plasma_frames<real>(P, s, 0, st));
+  CUDA_TRY(cudaEventSynchronize(ev.back()));
+  std::vector<float> h(reps), e(reps);
+  for (int i = 0; i < reps; ++i) {
+    CUDA_TRY(cudaEventElapsedTime(&h[i], ev[3 * i], ev[3 * i + 1]));
+    CUDA_TRY(cudaEventElapsedTime(&e[i], ev[3 * i + 1], ev[3 * i + 2]));
+  }
+  std::sort(h.begin(), h.end());
+  std::sort(e.begin(), e.end());
+  *h_ms = reps % 2 ? h[reps / 2] : 0.5f * (h[reps / 2 - 1] + h[reps / 2]);
+  *e_ms = reps % 2 ? e[reps / 2] : 0.5f * (e[reps / 2 - 1] + e[reps / 2]);
+  return IFDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ifdtd_time_phases(ifdtd_plan* plan, const ifdtd_state* state, int32_t reps, float* h_ms, float* e_ms,
+                          void* stream) {
+  if (!plan || !h_ms || !e_ms) return fail(IFDTD_ERR_ARGUMENT, "null argument");
+  if (reps < 1) return fail(IFDTD_ERR_ARGUMENT, "reps must be positive");
+  DeviceGuard guard(plan->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  return plan->dtype == 4 ? time_phases<float>(plan, state, reps, h_ms, e_ms, st)
+                          : time_phases<double>(plan, state, reps, h_ms, e_ms, st);
 }
 
 int32_t ifdtd_probe_create(ifdtd_plan* plan, int32_t field_kind, int32_t rows, int32_t width, const int64_t* index,
@@ -2696,6 +2858,7 @@ int step_static(ifdtd_plan* P, const ifdtd_state* st, const double* currents, in
     A.uploaded = true;
   }
   const Rec<real>* drec = static_cast<const Rec<real>*>(A.record);
+  CUDA_TRY(plasma_frames<real>(P, st, 1, stream));
   for (int i = 0; i < n; ++i) {
     cudaError_t e = P->plasma ? launch_kh_t<real, true>(P, drec, stream) : launch_kh_t<real, false>(P, drec, stream);
     if (e == cudaSuccess) {
@@ -2709,6 +2872,7 @@ int step_static(ifdtd_plan* P, const ifdtd_state* st, const double* currents, in
     }
     if (e != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("static-scratch step launch: ") + cudaGetErrorString(e));
   }
+  CUDA_TRY(plasma_frames<real>(P, st, 0, stream));
   return IFDTD_OK;
 }
 

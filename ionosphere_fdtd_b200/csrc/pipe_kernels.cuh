@@ -395,6 +395,7 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
   const real* etan = reinterpret_cast<const real*>(st + hd[ke_o_etan]);
   const int Pn = R.Pn, Pm = R.Pm, SW = R.slot_width, cn = Pn / N, cm = Pm / N;
   const bool full = R.coef_full != 0;
+  const bool local = PLASMA && R.plasma_local != 0;
   auto slot_rows = [&](int vl, const real** hrows, const real** jrows) {
 #pragma unroll
     for (int q = 0; q < MAXDEG; q += 4) {
@@ -440,10 +441,17 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
         real rav[N + 1];
         if (PLASMA) {
           const real* wcs = vwc + vl * SW * 4;
-          const Run<real> own =
-              k0 < Pm ? vertex_radial_current<real, MAXDEG>(jrows, wcs, k0, Pm) : zero_run<real>();
+          Run<real> own = zero_run<real>();
+          if (local) {
+            if (k0 < Pm) own = vertex_radial_current_local<real, MAXDEG>(jrows, wcs, k0);
+          } else if (k0 < Pm) {
+            own = vertex_radial_current<real, MAXDEG>(jrows, wcs, k0, Pm);
+          }
           const real below = __shfl_up_sync(mask, own.x[N - 1], 1);
-          rav[0] = q == 0 ? real(0) : (lane > 0 ? below : vertex_radial_current_at<real, MAXDEG>(jrows, wcs, k0 - 1, Pm));
+          rav[0] = q == 0   ? real(0)
+                   : lane > 0 ? below
+                   : local    ? vertex_radial_current_local_at<real, MAXDEG>(jrows, wcs, k0 - 1)
+                              : vertex_radial_current_at<real, MAXDEG>(jrows, wcs, k0 - 1, Pm);
 #pragma unroll
           for (int r = 0; r < N; ++r) rav[r + 1] = own.x[r];
         }

@@ -45,6 +45,11 @@ struct Rec {
   int nV, nE, nF, L, Pn, Pm;
   int n_patches_h, fpp_h, n_patches_e, fpp_e;
   int full, si_terms, n_species, plasma_full, magnetized, coef_full;
+  // 1: the plasma current is held in face frames while the kernels run
+  // (component 0 along the face centre, 1 and 2 in the face's tangent plane);
+  // the reconstruction rows, vertex weights and edge tangents are then in the
+  // same frames and packed as the local runs read them
+  int plasma_local;
   int n_src_er, n_src_et;
   int maxdeg, slot_width, layer_reals;
   // state
@@ -64,6 +69,7 @@ struct Rec {
   const int4 *face_e, *face_v;
   const real* face_w;    // (F, 4): sign_i * theta_i / A_f, 0
   const real* face_pl;   // (F, 12): reconstruction row i then centre component i
+  const real* frame;     // (F, 12): face-frame rows e0, 0, e1, 0, e2, 0 (plasma_local only)
   // vertex slots in vlist order, slot_width entries per vertex
   const int* ps_edge;
   const real* ps_coef;   // sign * phi_e / A*_v, 0 in padding slots
@@ -352,6 +358,51 @@ __device__ __forceinline__ real vertex_radial_current_at(const real* const* jrow
     const real* jf = jrows[q];
     acc = rav_term(acc, jf[j], jf[Pm + j], jf[2 * Pm + j], wc[0], wc[1], wc[2]);
   }
+  return acc;
+}
+
+// Face-frame radial current of one vertex at midpoints j0..j0+N-1: sum over
+// its face slots of weight_q * J_r (component 0 of the face's current, the
+// component along the face centre), wq[q] = area weight * |face centre| of slot
+// q (zero in padding slots).  The terms the face frame makes zero (the
+// tangential components against a zero weight) are not formed.
+__device__ __forceinline__ float rav_local(float acc, float x, float w) { return __fadd_rn(acc, __fmul_rn(x, w)); }
+__device__ __forceinline__ double rav_local(double acc, double x, double w) { return __dadd_rn(acc, __dmul_rn(x, w)); }
+
+template <typename real, int MAXDEG>
+__device__ __forceinline__ void slot_weights(const real* wq, real (&w)[(MAXDEG + 3) / 4 * 4]) {
+#pragma unroll
+  for (int q = 0; q < MAXDEG; q += 4) {
+    real c4[4];
+    ld4(wq + q, c4);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) w[q + i] = c4[i];
+  }
+}
+
+template <typename real, int MAXDEG>
+__device__ __forceinline__ Run<real> vertex_radial_current_local(const real* const* jrows, const real* wq, int j0) {
+  constexpr int N = Lanes<real>::N;
+  real w[(MAXDEG + 3) / 4 * 4];
+  slot_weights<real, MAXDEG>(wq, w);
+  Run<real> acc = zero_run<real>();
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) {
+    const Run<real> jr = ld16(jrows[q] + j0);
+#pragma unroll
+    for (int r = 0; r < N; ++r) acc.x[r] = rav_local(acc.x[r], jr.x[r], w[q]);
+  }
+  return acc;
+}
+
+// The same sum at the single midpoint j (same sequence, same bits).
+template <typename real, int MAXDEG>
+__device__ __forceinline__ real vertex_radial_current_local_at(const real* const* jrows, const real* wq, int j) {
+  real w[(MAXDEG + 3) / 4 * 4];
+  slot_weights<real, MAXDEG>(wq, w);
+  real acc = real(0);
+#pragma unroll
+  for (int q = 0; q < MAXDEG; ++q) acc = rav_local(acc, jrows[q][j], w[q]);
   return acc;
 }
 
@@ -735,6 +786,17 @@ __device__ __forceinline__ void e_vertex_run(const Rec<real>& R, const VertexLay
     if (rav_in) {
 #pragma unroll
       for (int r = 0; r <= N; ++r) rav[r] = rav_in[r];
+    } else if (R.plasma_local) {
+      real w[(MAXDEG + 3) / 4 * 4];
+      slot_weights<real, MAXDEG>(wcs, w);
+#pragma unroll
+      for (int q = 0; q < MAXDEG; ++q) {
+        const real* jf = jrows[q];
+        const Run<real> jr = in ? ld16(jf + k0) : zero_run<real>();
+        if (below) rav[0] = rav_local(rav[0], jf[k0 - 1], w[q]);
+#pragma unroll
+        for (int r = 0; r < N; ++r) rav[r + 1] = rav_local(rav[r + 1], jr.x[r], w[q]);
+      }
     } else {
 #pragma unroll
       for (int q = 0; q < MAXDEG; ++q) {
@@ -785,7 +847,21 @@ __device__ __forceinline__ void e_edge_run(const Rec<real>& R, const EdgeLayer<r
       for (int s = 0; s < R.n_src_et; ++s)
         if (R.src_et_e[s] == e && R.src_et_j[s] == j0 + r) out.x[r] -= R.src_et_c[s] * current;
   }
-  if (PLASMA) {
+  if (PLASMA && R.plasma_local) {
+    // face frames: the edge tangents lie in the faces' tangent planes, so
+    // only components 1 and 2 of each face's current enter; tp = left
+    // tangent (1, 2), right tangent (1, 2)
+    real t4[4];
+    ld4(tp, t4);
+    const Run<real> ly = ld16(jl + Pm + j0), lz = ld16(jl + 2 * Pm + j0);
+    const Run<real> qy = ld16(jq + Pm + j0), qz = ld16(jq + 2 * Pm + j0);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      const real left = ly.x[r] * t4[0] + lz.x[r] * t4[1];
+      const real right = qy.x[r] * t4[2] + qz.x[r] * t4[3];
+      out.x[r] -= cb.x[r] * (real(0.5) * (left + right));
+    }
+  } else if (PLASMA) {
     real tl[4], tq[4];
     ld4(tp, tl);
     ld4(tp + 4, tq);
@@ -889,6 +965,43 @@ __global__ void __launch_bounds__(256) ke_kernel(const Rec<real>* __restrict__ r
                              R.ht + (size_t)e * Pn, PLASMA ? Jsum + (size_t)lr.x * 3 * Pm : nullptr,
                              PLASMA ? Jsum + (size_t)lr.y * 3 * Pm : nullptr, R.et + (size_t)e * Pm,
                              R.et + (size_t)e * Pm, current, __ldg(R.inv_phi + e), PLASMA ? R.tan + 8 * (size_t)e : nullptr);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plasma current between the Cartesian frame of the caller's state and the
+// face frames the step kernels read when Rec::plasma_local is set: rows of Q
+// (F, 12) are e0 (along the face centre), e1, e2, each padded to four reals.
+// to_local: J <- Q J; else J <- Q^T J, midpoint quad by midpoint quad of one
+// species' (F, 3, Pm) buffer.  Zero padding midpoints stay zero.
+// ---------------------------------------------------------------------------
+template <typename real>
+__global__ void __launch_bounds__(256) plasma_frame_kernel(real* __restrict__ J, const real* __restrict__ Q, int nF,
+                                                           int Pm, int to_local) {
+  constexpr int N = Lanes<real>::N;
+  const int cm = Pm / N;
+  const long long n = (long long)nF * cm;
+  for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < n;
+       it += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(it / cm);
+    const int j0 = (int)(it - (long long)f * cm) * N;
+    real q[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) q[i][c] = __ldg(Q + 12 * (size_t)f + 4 * i + c);
+    real* base = J + (size_t)f * 3 * Pm + j0;
+    const Run<real> a = ld16(base), b = ld16(base + Pm), c = ld16(base + 2 * Pm);
+    Run<real> o[3];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        o[i].x[r] = to_local ? q[i][0] * a.x[r] + q[i][1] * b.x[r] + q[i][2] * c.x[r]
+                             : q[0][i] * a.x[r] + q[1][i] * b.x[r] + q[2][i] * c.x[r];
+    st16(base, o[0]);
+    st16(base + Pm, o[1]);
+    st16(base + 2 * Pm, o[2]);
   }
 }
 

@@ -56,7 +56,10 @@ class Tuning:
     recomputes the new H on its halo, for plans without plasma or surface
     impedance; the plan then holds a second copy of the field arrays, and in
     an ``Ensemble`` it runs the batched fused kernel).
-    Every choice computes the same bits."""
+    Every choice above computes the same bits.  ``plasma_frame`` (0 auto:
+    face frames for an unmagnetised plasma, 1 Cartesian, 2 face frames) picks
+    the frame the plasma current is held in while the kernels run; the state
+    is Cartesian between calls, and the two frames round differently."""
 
     faces_per_patch: int = 0
     threads: int = 0
@@ -70,6 +73,7 @@ class Tuning:
     e_producer_warps: int = 0
     e_copy_gap: int = 0
     fused_step: int = 0
+    plasma_frame: int = 0
 
 
 def _dedupe_last(index_a, index_b, coef):
@@ -181,7 +185,7 @@ class Engine:
         t = self.tuning
         td = N.Tuning(t.faces_per_patch, t.threads, t.graph_chunk, t.e_faces_per_patch, t.staging, t.producer_warps, t.lane_layout,
                       t.e_threads, t.e_stages, t.e_producer_warps, t.e_copy_gap,
-                      t.fused_step)
+                      t.fused_step, t.plasma_frame)
         handle = C.c_void_p()
         with backend.torch.cuda.device(backend.torch_device):
             N.check(
@@ -327,6 +331,15 @@ class Engine:
             N.load().ifdtd_update_electric(self.plan, C.byref(state), float(current), self.backend.stream_handle()),
             "ifdtd_update_electric",
         )
+
+    def phase_times_ms(self, state: N.State, reps: int) -> tuple[float, float]:
+        """Median device time (ms) of the H and E phase kernels over ``reps`` launches
+        each (``ifdtd_time_phases``; advances the state by 3 + reps steps)."""
+
+        h, e = C.c_float(), C.c_float()
+        N.check(N.load().ifdtd_time_phases(self.plan, C.byref(state), int(reps), C.byref(h), C.byref(e),
+                                           self.backend.stream_handle()), "ifdtd_time_phases")
+        return float(h.value), float(e.value)
 
     def probe(self, kind: str, index, layer, weight) -> Probe:
         return Probe(self, {"er": 0, "et": 1, "hr": 2, "ht": 3}[kind], index, layer, weight)
