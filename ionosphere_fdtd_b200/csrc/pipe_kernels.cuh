@@ -425,8 +425,13 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
     if (lm.on) {
       const int q = lm.q, k0 = q * N, per = lm.per;
       const int lane = threadIdx.x & 31, wbase = ct - lane;
-      // the vertex layer factors are re-read per run here: hoisting them too
-      // would push this kernel past its register budget into local memory
+      // the vertex layer factors of this thread's quad: loaded once per patch
+      // in the float kernels of vertex degree 6 when they are altitude rows;
+      // elsewhere (float64, 12-slot tables) holding them would push the kernel
+      // past its register budget into local memory, so they are re-read per run
+      constexpr bool kHoist = sizeof(real) == 4 && MAXDEG == 6;
+      VertexLayer<real> fixed_v{};
+      if (kHoist && !full) fixed_v = vertex_layer(R, Ls, 0, k0);
       for (int k = 0;; ++k) {
         const int vl = ct / lm.G + k * per;
         if (vl >= nv) break;
@@ -455,7 +460,7 @@ __device__ __forceinline__ void ke_consume(const Rec<real>& R, const Layers<real
 #pragma unroll
           for (int r = 0; r < N; ++r) rav[r + 1] = own.x[r];
         }
-        e_vertex_run<real, PLASMA, MAXDEG>(R, vertex_layer(R, Ls, v, k0), (src & 1) != 0, v, k0, hrows,
+        e_vertex_run<real, PLASMA, MAXDEG>(R, kHoist && !full ? fixed_v : vertex_layer(R, Ls, v, k0), (src & 1) != 0, v, k0, hrows,
                                            jrows, vcoef + vl * SW, PLASMA ? vwc + vl * SW * 4 : nullptr,
                                            s_er + vl * Pn, R.er + (size_t)v * Pn, current, PLASMA ? rav : nullptr);
       }
