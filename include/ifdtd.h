@@ -145,8 +145,9 @@ typedef struct ifdtd_tuning {
                                 row per face at a vertex and two per face at an edge.  Every call that runs a
                                 plasma phase turns the caller's Cartesian currents into face frames first and
                                 back afterwards (two passes over the currents per call), so the state between
-                                calls is the reference's; the two frames round differently (float32: within a
-                                few ulp of the current per call) */
+                                calls is the reference's (a call that fails part-way may leave the currents in
+                                face frames, like its other results invalid); the two frames round differently
+                                (float32: within a few ulp of the current per call) */
 } ifdtd_tuning;
 
 /* Mutable state of one simulation: device pointers owned by the caller. */
