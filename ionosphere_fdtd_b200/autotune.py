@@ -102,7 +102,8 @@ def autotune(sim, candidates: Sequence[Tuning] = DEFAULT_CANDIDATES, *, steps: i
     simulation's fields, plasma currents and surface-impedance memory are
     restored afterwards, and its step count and time do not move.  A
     candidate the plan builder rejects (for example a pipelined staging whose
-    stage does not fit twice in shared memory) is recorded with its error."""
+    stage does not fit twice in shared memory), or whose launches the device
+    refuses, is recorded with its error."""
 
     if steps < 1 or repeats < 1:
         raise ValueError("steps and repeats must be positive")
@@ -124,6 +125,13 @@ def autotune(sim, candidates: Sequence[Tuning] = DEFAULT_CANDIDATES, *, steps: i
                 continue
             try:
                 ms = _time_engine(sim, engine, steps, repeats)
+            except RuntimeError as err:
+                # a launch the device refuses (for example a launch shape with no
+                # resident CTA) is recorded like a plan the builder rejects
+                engine.close()
+                _restore(sim, saved)
+                result.timings.append((tuning, None, str(err)))
+                continue
             except BaseException:
                 engine.close()
                 raise

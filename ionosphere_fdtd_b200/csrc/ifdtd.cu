@@ -1759,7 +1759,10 @@ int run_steps(ifdtd_plan* P, const ifdtd_state* st, const double* currents, int 
         for (int i = 0; i < c && le == cudaSuccess; ++i)
           le = launch_step<real>(P, i, probe, i, P->capture_stream, P->fused ? (i & 1) : 0);
         cudaError_t ce = cudaStreamEndCapture(P->capture_stream, &graph);
-        if (le != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le));
+        if (le != cudaSuccess) {
+          if (ce == cudaSuccess) cudaGraphDestroy(graph);  // the partial capture is not kept
+          return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(le));
+        }
         if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
         cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
@@ -2241,8 +2244,10 @@ int run_batch(ifdtd_batch* B, const ifdtd_state* states, const double* currents,
         for (int i = 0; i < c && le == cudaSuccess; ++i)
           le = batch_launch_step<real>(B, i, rows, i, B->capture_stream, B->any_fused ? (i & 1) : 0);
         cudaError_t ce = cudaStreamEndCapture(B->capture_stream, &graph);
-        if (le != cudaSuccess)
+        if (le != cudaSuccess) {
+          if (ce == cudaSuccess) cudaGraphDestroy(graph);  // the partial capture is not kept
           return fail(IFDTD_ERR_CUDA, "batch graph capture: " + B->failed + ": " + cudaGetErrorString(le));
+        }
         if (ce != cudaSuccess) return fail(IFDTD_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
         cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
