@@ -119,3 +119,27 @@ def test_array_level_ade_update_equals_the_oracle():
         np.testing.assert_allclose(j, want, rtol=1e-13, atol=1e-15)
         want_total += want
     np.testing.assert_allclose(total, want_total, rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize("level", [0, 2, 4])
+def test_edge_tangents_and_reconstruction_lie_in_the_face_tangent_planes(level):
+    """The face frames of the step kernels (component 0 along the face centre, 1 and 2
+    in the face's tangent plane) drop the centre component of every edge tangent and
+    carry the face centre as (|c|, 0, 0): both rest on the reference's tangents being
+    normal to their face's centre (plasma.py:548-559, cross(normal, centre)) and on
+    |centre| = 1.  Here the dropped parts are round-off, and the reconstruction rows
+    (the pseudo-inverse of the tangents) lie in the tangent planes too."""
+
+    mesh = P.build_geodesic_mesh(level)
+    recon, tangents = PL.face_reconstruction(mesh)
+    centres = np.asarray(mesh.face_centers)
+    np.testing.assert_allclose(np.linalg.norm(centres, axis=1), 1.0, rtol=0, atol=1e-15)
+    left = PL.edge_face_slots(mesh, mesh.edge_left_faces)
+    right = PL.edge_face_slots(mesh, mesh.edge_right_faces)
+    for faces, slots in ((mesh.edge_left_faces, left), (mesh.edge_right_faces, right)):
+        t = tangents[faces, slots]
+        np.testing.assert_allclose(np.linalg.norm(t, axis=1), 1.0, rtol=0, atol=1e-15)
+        assert np.max(np.abs(np.einsum("ec,ec->e", t, centres[faces]))) < 1e-15
+    # reconstruction rows: no component along the centre beyond round-off of their own size
+    along = np.einsum("fic,fc->fi", recon, centres)
+    assert np.max(np.abs(along)) < 1e-14 * np.max(np.abs(recon))
