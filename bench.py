@@ -125,7 +125,7 @@ def kernel_bytes(sim) -> dict[str, int]:
     return {"h_phase": item * (e + 2 * (h + j + si)), "e_phase": item * (h + j + 2 * e)}
 
 
-def phase_times_ms(sim, reps: int, stream) -> dict[str, float]:
+def phase_times_ms(sim, reps: int) -> dict[str, float]:
     """Median device time of each phase kernel: CUDA events around every launch on the
     launching stream (``ifdtd_time_phases``, the plasma current turned into the plan's
     frame once around all launches)."""
@@ -935,7 +935,7 @@ def main() -> None:
     step_ms = statistics.median(per_step_ms) / T
     achieved = wl.bytes_per_step / (step_ms / 1e3) / 1e9
     # per-kernel roofline: each phase kernel timed alone after the timed region
-    phase_ms = phase_times_ms(sim, 50, stream)
+    phase_ms = phase_times_ms(sim, 50)
     nbytes = kernel_bytes(sim)
     modes = eng.kernel_modes
     names = {"h_phase": "kh_tma" if modes[0] == "pipeline" else "kh_kernel", "e_phase": "ke_tma" if modes[1] == "pipeline" else "ke_kernel"}
