@@ -967,6 +967,7 @@ def main() -> None:
                  "note": "timed region: both phase kernels and the receiver sampling of every leapfrog step"},
     }
     config = workload_config(args.workload, args.subdivision, world)
+    n_species, face_frames = eng.species, eng.face_frames
     del wl, sim, eng
     torch.cuda.empty_cache()
     drift = None
@@ -1014,7 +1015,9 @@ def main() -> None:
             "e2e": e2e,
             "fp32_drift": drift,
             "traces_finite": trace_finite,
-            "gpu_launches": 3 * T * K,
+            # per bench step: H phase, E phase and sampling per leapfrog step, and with the plasma
+            # current in face frames one conversion per species each way around the call
+            "gpu_launches": (3 * T + (2 * n_species if face_frames else 0)) * K,
             "clocks": clocks,
             "ensemble": ensemble,
         }

@@ -165,9 +165,13 @@ class Engine:
             pd.si_scale, pd.si_decay, pd.si_drive, pd.si_history = f64(si["scale"]), f64(si["decay"]), f64(si["drive"]), f64(si["history"])
             pd.si_metric = float(si["metric"])
         self.species = 0
+        # the plan holds the plasma current in face frames while its kernels run
+        # (automatic for an unmagnetised plasma unless the Cartesian frame is asked for)
+        self.face_frames = False
         if physics.plasma is not None:
             p = physics.plasma
             self.species = int(p["coef"].shape[0])
+            self.face_frames = not p["magnetized"] and self.tuning.plasma_frame != 1
             if self.species > N.MAX_SPECIES:
                 raise ValueError(f"at most {N.MAX_SPECIES} plasma species are supported")
             pd.plasma_species = self.species
